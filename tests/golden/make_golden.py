@@ -1,0 +1,262 @@
+"""Generate golden fixtures by running the reference gridfoam on CPU.
+
+Run in a container where the reference source tree is available::
+
+    GRIDFOAM_REF=/root/reference/src python tests/golden/make_golden.py
+
+It imports the unmodified reference package (with the import stubs in
+``tests/golden/refshim`` for its absent optional dependencies), builds each
+case of ``tests/golden/cases.py`` on the synthetic fluxel-compatible mesh,
+runs a few algorithm steps in float64 and dumps the per-step fields and
+solver statistics plus operator-level outputs to ``tests/golden/<case>.npz``.
+The fixtures are committed; nothing on the GPU side reads the reference.
+"""
+
+from __future__ import annotations
+
+import os
+import pathlib
+import sys
+
+HERE = pathlib.Path(__file__).resolve().parent
+REPO = HERE.parents[1]
+REF_SRC = os.environ.get("GRIDFOAM_REF", "/root/reference/src")
+os.environ.setdefault("GRIDFOAM_RUNTIME_TYPE_CHECKS", "0")
+sys.path[:0] = [str(HERE / "refshim"), REF_SRC, str(REPO)]
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+torch.set_num_threads(max(1, os.cpu_count() or 1))
+
+from gridfoam.algorithms.factory import create_algorithm  # noqa: E402
+from gridfoam.boundaries import factory as bc_factory  # noqa: E402
+from gridfoam.boundaries.basic.dirichlet import DirichletBC  # noqa: E402
+from gridfoam.algorithms.utils.reference_value import (  # noqa: E402
+    needs_reference_value,
+    set_reference_value,
+)
+from gridfoam.core import field as ref_field  # noqa: E402
+from gridfoam.core.equation import equation  # noqa: E402
+from gridfoam.core.fvmatrix import FvMatrix  # noqa: E402
+from gridfoam.core.grid.axis_projected import AxisProjectedGrid  # noqa: E402
+from gridfoam.fv import fvc, fvm  # noqa: E402
+from gridfoam.meta.config import SimulatorConfig, SolverConfig  # noqa: E402
+from gridfoam.meta.enums import DomainBoundaryPatch  # noqa: E402
+from gridfoam.solvers.bicgstab import BiCGSTABSolver  # noqa: E402
+from gridfoam.solvers.cg import CGSolver  # noqa: E402
+
+from tests.golden.cases import ALL_CASES, build_mesh  # noqa: E402
+
+DIV_SCHEMES = [
+    "upwind",
+    "linear",
+    "vanleer",
+    "minmod",
+    "superbee",
+    "monotonized_central",
+    "limitedlinear",
+    "koren",
+]
+
+
+class ParabolicInletBC(DirichletBC):
+    """Per-face Dirichlet velocity: a parabolic profile on a domain patch."""
+
+    def __init__(self, profile: dict):
+        super().__init__(torch.zeros(3, dtype=torch.float64))
+        self.profile = profile
+
+    def evaluate(self, field, patch_name, side=None):
+        grid = field.grid
+        mask = grid.get_domain_bnd_mask(patch_name)
+        cells = grid.domain_bnd_owner[mask]
+        c = grid.cell_centers[cells]
+        cx, cy = self.profile["center"]
+        r2 = (c[:, 0] - cx) ** 2 + (c[:, 1] - cy) ** 2
+        uz = self.profile["umax"] * torch.clamp(
+            1.0 - r2 / self.profile["radius"] ** 2, min=0.0
+        )
+        ref_v = torch.zeros((cells.shape[0], 3), dtype=grid.dtype)
+        ref_v[:, 2] = uz
+        fraction = torch.ones(cells.shape[0], dtype=grid.dtype)
+        return fraction, ref_v, torch.zeros_like(ref_v)
+
+
+def make_grid(case: dict) -> AxisProjectedGrid:
+    sim = SimulatorConfig.model_validate(case["simulator"])
+    mesh = build_mesh(case["mesh"])
+    return AxisProjectedGrid(sim, mesh), mesh
+
+
+def packed(face_field) -> np.ndarray:
+    return face_field.pack().detach().numpy().copy()
+
+
+def stats_array(stats) -> np.ndarray:
+    return np.array(
+        [
+            [s.initial_residual, s.final_residual, s.iterations, float(s.converged)]
+            for s in stats
+        ]
+    )
+
+
+def run_case(name: str, n_steps: int) -> dict:
+    case = ALL_CASES[name]()
+    out: dict[str, np.ndarray] = {}
+    profile = case["inlet_profile"]
+    original = bc_factory.create_boundary_condition
+
+    def patched(bc_config, dtype, device):
+        if profile is not None and [str(p) for p in bc_config.patches] == [
+            profile["patch"]
+        ] and bc_config.type == "dirichlet" and bc_config.value is not None and len(
+            np.atleast_1d(bc_config.value)
+        ) == 3:
+            return ParabolicInletBC(profile)
+        return original(bc_config, dtype, device)
+
+    ref_field.boundary_factory.create_boundary_condition = patched
+    try:
+        grid, mesh = make_grid(case)
+        algo = create_algorithm(grid)
+    finally:
+        ref_field.boundary_factory.create_boundary_condition = original
+
+    captured: list[dict] = []
+    orig_finalize = algo._finalize_diagnostics
+
+    def capture(phi, solve_stats):
+        captured.append(dict(solve_stats))
+        return orig_finalize(phi, solve_stats)
+
+    algo._finalize_diagnostics = capture
+
+    out["init_U"] = algo.U.data.numpy().copy()
+    out["init_p"] = algo.p.data.numpy().copy()
+    out["init_phi"] = packed(algo.phi)
+    for step in range(n_steps):
+        with torch.no_grad():
+            algo.step()
+        out[f"step{step}_U"] = algo.U.data.numpy().copy()
+        out[f"step{step}_p"] = algo.p.data.numpy().copy()
+        out[f"step{step}_phi"] = packed(algo.phi)
+        if step == 0:
+            out["step0_HbyA"] = algo.HbyA.data.numpy().copy()
+            out["step0_rAtU"] = algo.rAtU.data.numpy().copy()
+            out["step0_phiHbyA"] = packed(algo.phi_hbya)
+        stats = captured[-1]
+        out[f"step{step}_stats_U"] = stats_array(stats["U"])
+        out[f"step{step}_stats_p"] = stats_array(stats["p"])
+    if hasattr(algo, "_current_residuals"):
+        for key, val in getattr(algo, "_current_residuals").items():
+            out[f"residual_{key}"] = np.array(val)
+
+    out.update(operator_dumps(grid, algo))
+    out["mesh_n_cells"] = np.array(mesh.n_cells)
+    out["mesh_checksum"] = np.array(
+        [
+            float(mesh.internal_faces_owner.sum()),
+            float(mesh.cell_centers.sum()),
+            float(mesh.ap.dist_owner_to_bnd.sum()),
+            float(mesh.ap.is_immersed_face.sum()),
+        ]
+    )
+    return out
+
+
+def matrix_dict(prefix: str, mat: FvMatrix) -> dict:
+    d = {
+        f"{prefix}_diag": mat.diag.detach().numpy().copy(),
+        f"{prefix}_upper": mat.upper.detach().numpy().copy(),
+        f"{prefix}_lower": mat.lower.detach().numpy().copy(),
+        f"{prefix}_source": mat.source.detach().numpy().copy(),
+    }
+    if mat.face_flux_correction is not None:
+        d[f"{prefix}_ffc"] = mat.face_flux_correction.detach().numpy().copy()
+    return d
+
+
+def operator_dumps(grid: AxisProjectedGrid, algo) -> dict:
+    """Operator outputs evaluated on the final algorithm state."""
+    out: dict[str, np.ndarray] = {}
+    U, p, phi = algo.U, algo.p, algo.phi
+    nu_eff = algo.turbulence.nu_eff()
+    with torch.no_grad():
+        out.update(matrix_dict("op_lap_U", fvm.laplacian(nu_eff, U)))
+        base_cfg = grid.sim_config
+        for scheme in DIV_SCHEMES:
+            schemes = base_cfg.fvSchemes.model_copy(
+                update={"divSchemes": {"default": scheme}}
+            )
+            grid.sim_config = base_cfg.model_copy(update={"fvSchemes": schemes})
+            out.update(matrix_dict(f"op_div_{scheme}", fvm.div(phi, U)))
+        grid.sim_config = base_cfg
+        out["op_grad_p"] = fvc.grad(p).data.numpy().copy()
+        out["op_grad_U"] = fvc.grad(U).data.numpy().copy()
+        out["op_interp_U"] = packed(fvc.interpolate(U))
+        out["op_div_phi"] = fvc.div(phi).data.numpy().copy()
+        out["op_sngrad_p"] = packed(fvc.sn_grad(p))
+
+        # Pressure-type system with a positive cell coefficient field.
+        rng = np.random.default_rng(0)
+        gamma = torch.from_numpy(0.5 + rng.random(grid.num_cells))
+        out["op_gamma"] = gamma.numpy().copy()
+        pmat = -fvm.laplacian(gamma, p)
+        pmat.source = pmat.source - torch.from_numpy(
+            rng.standard_normal(grid.num_cells)
+        ) * grid.cell_volumes
+        if needs_reference_value(p):
+            set_reference_value(pmat, 0, 0.0)
+        out.update(matrix_dict("op_pmat", pmat))
+        peq = equation(p, pmat)
+        out.update(matrix_dict("op_pmat_solve", peq.fv_matrix))
+        cg = CGSolver(
+            SolverConfig.model_validate(
+                {"method": "cg", "preconditioner": "jacobi", "tolerance": 1e-9, "rel_tolerance": 0.0}
+            )
+        )
+        res = cg._solve_primal(peq)
+        out["op_cg_x"] = res.solution.numpy().copy()
+        out["op_cg_stats"] = stats_array(res.stats)
+        out["op_cg_x0"] = p.data.numpy().copy()
+
+        # Momentum-type system: convection + diffusion + ddt-like diagonal.
+        umat = fvm.div(phi, U) - fvm.laplacian(nu_eff, U)
+        umat.diag = umat.diag + grid.cell_volumes / 0.01
+        umat.source = umat.source + torch.from_numpy(
+            rng.standard_normal((grid.num_cells, 3))
+        ) * grid.cell_volumes[:, None]
+        ueq = equation(U, umat)
+        out.update(matrix_dict("op_umat_solve", ueq.fv_matrix))
+        bi = BiCGSTABSolver(
+            SolverConfig.model_validate(
+                {"method": "bicgstab", "preconditioner": "jacobi", "tolerance": 1e-10, "rel_tolerance": 0.0}
+            )
+        )
+        res = bi._solve_primal(ueq)
+        out["op_bicg_x"] = res.solution.numpy().copy()
+        out["op_bicg_stats"] = stats_array(res.stats)
+        out["op_bicg_x0"] = U.data.numpy().copy()
+        out["op_spmv_U"] = umat.multiply(U.data).numpy().copy()
+        out["op_H_U"] = umat.H(U.data).numpy().copy()
+        out["op_H1_U"] = umat.H1().numpy().copy()
+        out["op_flux_p"] = (-pmat).flux(p.data).numpy().copy()
+    return out
+
+
+STEPS = {"cavity8": 4, "pipe10x20": 3, "channel": 3, "channel_ffp": 3, "ibplane": 3}
+
+
+def main() -> None:
+    names = sys.argv[1:] or list(STEPS)
+    for name in names:
+        data = run_case(name, STEPS[name])
+        path = HERE / f"{name}.npz"
+        np.savez_compressed(path, **data)
+        print(f"{name}: {len(data)} arrays -> {path} ({path.stat().st_size} B)")
+
+
+if __name__ == "__main__":
+    main()
