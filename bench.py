@@ -1,0 +1,344 @@
+"""Benchmark: cell-iterations/s of the immersed-boundary Hagen-Poiseuille
+pipe (box 1x1x4 on 64x64x256 cells, cylindrical IB r = 0.4 along z,
+parabolic inlet with mean velocity 1, nu = 0.02, PISO dt = 1e-3, two
+correctors, upwind convection), float64 on one B200.
+
+One step is one PISO time step (momentum BiCGStab + 2 pressure CG solves to
+tolerance).  ``value`` is device-timed with inputs resident in HBM; ``e2e``
+times the public API with the step's state copied host->device from pinned
+memory and the result read back every step.  ``--impl reference`` times the
+CPU oracle (the reference algorithm restated in numpy) on a bounded sample.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+REPO = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+METRIC = "cell-iters/s"
+WORKLOAD = "ib_pipe_64x64x256_piso"
+
+
+def pipe_config(n: int = 64, nz: int = 256, length: float = 4.0) -> dict:
+    from tests.golden.cases import pipe_case
+
+    return pipe_case(n, nz, length)
+
+
+def peaks() -> tuple[float, str]:
+    path = REPO / "MEASURED_PEAKS.json"
+    try:
+        data = json.loads(path.read_text())
+        return float(data["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    QUERY = (
+        "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+        "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+        "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+    )
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = tempfile.NamedTemporaryFile(prefix="gf_clocks_", suffix=".csv", delete=False).name
+
+    def start(self) -> None:
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"],
+                stdout=self.fh, stderr=subprocess.DEVNULL,
+            )
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in pathlib.Path(self.path).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {
+            "sm_mhz": statistics.median(sm) if sm else None,
+            "sm_max_mhz": max(smax) if smax else None,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+def pcg_bytes_per_iter(C: int, F: int) -> float:
+    """Algorithmic bytes of one fused Jacobi-PCG iteration (fp64, int32 indices):
+    14 C s + F (s + 8), s = 8."""
+    return 14 * C * 8 + F * (8 + 8)
+
+
+def pcg_bytes_setup(C: int, F: int) -> float:
+    """Initial residual pass: x, b, diag read; r, p written; matrix once."""
+    return 5 * C * 8 + F * (8 + 8)
+
+
+def cpu_baseline(seconds: float = 15.0) -> dict:
+    """The CPU oracle on a bounded sample: a 16x16x64 downscale of the pipe."""
+    import numpy as np  # noqa: F401
+
+    from tests.golden.oracle_harness import oracle_case
+
+    case = pipe_config(16, 64, 4.0)
+    _, mesh, _, algo = oracle_case("pipe_cpu", case_def=case)
+    algo.step()
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        algo.step()
+        steps += 1
+        el = time.perf_counter() - t0
+        if el > seconds or steps >= 200:
+            break
+    return {
+        "value": mesh.n_cells * steps / el,
+        "unit": METRIC,
+        "cores": 1,
+        "kind": "port",
+        "sample": f"numpy oracle, pipe 16x16x64 ({mesh.n_cells} cells) PISO, {steps} steps in {el:.1f} s",
+    }
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import numpy as np  # noqa: F401
+
+    from tests.golden.oracle_harness import oracle_case
+
+    case = pipe_config(32, 128, 4.0)
+    _, mesh, _, algo = oracle_case("pipe_ref", case_def=case)
+    for _ in range(args.warmup):
+        algo.step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        algo.step()
+    el = time.perf_counter() - t0
+    value = mesh.n_cells * args.steps / el
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": METRIC,
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample": "pipe 32x32x128 per step (bounded sample)"},
+        "cpu_baseline": {
+            "value": value,
+            "unit": METRIC,
+            "cores": 1,
+            "kind": "port",
+            "sample": f"numpy oracle (reference algorithm restated), pipe 32x32x128 "
+                      f"({mesh.n_cells} cells) PISO, {args.steps} steps",
+        },
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def run_gpu(args) -> None:
+    import torch
+
+    import gridfoam_b200._lib as gl
+    from tests.golden.device_harness import device_case
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    case = pipe_config()
+    _, mesh, grid, algo = device_case(case_def=case, device=f"cuda:{local}")
+    C, F = grid.num_cells, grid.num_internal_faces
+    for _ in range(args.warmup):
+        algo.step()
+    torch.cuda.synchronize()
+
+    # Per-launch events around every pressure solve (the dominant kernel).
+    psolvers = [s for name, s in algo.solvers.items() if name.startswith("p")]
+    events: list = []
+    for s in psolvers:
+        s.profile_events = events
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.4)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    gl.LAUNCHES.clear()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stats = []
+    start.record()
+    for _ in range(args.steps):
+        algo.step()
+        stats.append(algo.last_stats)
+    stop.record()
+    torch.cuda.synchronize()
+    launches = sum(gl.LAUNCHES.values())
+    ms = start.elapsed_time(stop)
+    for s in psolvers:
+        s.profile_events = None
+    clocks = sampler.stop()
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+
+    # Roofline of the pressure PCG launches.
+    durations, iters = [], []
+    for ev0, ev1, st in events:
+        durations.append(ev0.elapsed_time(ev1) * 1e-3)
+        iters.append(st[0].iterations)
+    total_bytes = sum(pcg_bytes_setup(C, F) + it * pcg_bytes_per_iter(C, F) for it in iters)
+    total_time = sum(durations)
+    peak, peak_kind = peaks()
+    achieved = total_bytes / total_time / 1e9 if total_time > 0 else 0.0
+
+    # End-to-end through the public API: state in from pinned host memory,
+    # one step, result read back, every step.
+    U_h = algo.U.data.detach().cpu().pin_memory()
+    p_h = algo.p.data.detach().cpu().pin_memory()
+    U_out = torch.empty_like(U_h).pin_memory()
+    p_out = torch.empty_like(p_h).pin_memory()
+    e2e_steps = max(1, args.steps // 2)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(e2e_steps):
+        algo.U.data = U_h.to(algo.U.store.device, non_blocking=True)
+        algo.p.data = p_h.to(algo.p.store.device, non_blocking=True)
+        algo.step()
+        U_out.copy_(algo.U.data, non_blocking=True)
+        p_out.copy_(algo.p.data, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    h2d = U_h.numel() * 8 + p_h.numel() * 8
+
+    value = C * world * args.steps / (ms * 1e-3)
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": METRIC,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {
+            "workload": WORKLOAD,
+            "cells": C,
+            "internal_faces": F,
+            "immersed_faces": grid.num_immersed_faces,
+            "algorithm": "piso nCorrectors=2, dt=1e-3, upwind, p cg+jacobi tol 1e-7 rel 0.01 (pFinal rel 0), "
+                         "U bicgstab+jacobi tol 1e-8 rel 0.1",
+            "l2": "working set larger than L2 (126 MB), no flush",
+            "parallelism": f"replicas x{world}",
+            "p_iterations_per_solve": (sum(iters) / len(iters)) if iters else None,
+        },
+        "roofline": {
+            "kernel": "k_pcg (persistent Jacobi-PCG, fp64)",
+            "bound": "hbm",
+            "achieved": achieved,
+            "peak": peak,
+            "peak_source": peak_kind,
+            "unit": "GB/s",
+            "frac": achieved / peak if peak else None,
+            "traffic": None,
+            "launches": len(durations),
+            "avg_launch_ms": 1e3 * total_time / max(1, len(durations)),
+        },
+        "clocks": clocks,
+        "gpu_launches": launches,
+        "e2e": {
+            "value": C * world / (e2e_ms * 1e-3),
+            "unit": METRIC,
+            "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": h2d,
+        },
+    }
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gridfoam_b200")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

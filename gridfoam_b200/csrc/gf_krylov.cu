@@ -1,0 +1,737 @@
+// Persistent cooperative Krylov solvers (sm_100a).
+//
+// One launch runs a whole solve (all iterations, up to three right-hand
+// sides sharing the matrix).  Blocks synchronise through a grid barrier that
+// also finishes every dot product: each block writes its partial sums, the
+// last block to arrive reduces them in a fixed order and releases the
+// others, so each reduction costs one barrier and is bitwise reproducible.
+// Every wait is bounded; on expiry the kernel raises an error flag and
+// returns instead of hanging.  The launch is cooperative, so all blocks are
+// co-resident and the barrier is always reachable.
+#include "gf_common.cuh"
+
+namespace gf {
+
+constexpr int kKThreads = 512;
+constexpr int kMaxBlocks = 1024;
+constexpr int kMaxNV = 16;
+constexpr int kCtlDoubles = 32;
+constexpr long long kSpinLimit = 10000000LL;  // x ~100 ns sleeps: about a second
+
+struct KCtl {
+    unsigned int count;
+    unsigned int gen;
+    int error;
+    int pad;
+    double results[kMaxNV];
+};
+
+__device__ __forceinline__ unsigned vload(const unsigned* p) { return *(const volatile unsigned*)p; }
+__device__ __forceinline__ int vload(const int* p) { return *(const volatile int*)p; }
+
+__device__ __forceinline__ double nmax(double a, double b) {
+    if (a != a || b != b) return __longlong_as_double(0x7ff8000000000000LL);
+    return fmax(a, b);
+}
+
+__device__ __forceinline__ double inv_diag(const double* __restrict__ diag, int64_t c, bool jac) {
+    if (!jac) return 1.0;
+    const double d = __ldg(diag + c);
+    return fabs(d) < 2.220446049250313e-16 ? 1.0 : 1.0 / d;
+}
+
+// Grid-wide reduction of NV values per thread (sum, or max where maxmask
+// has the bit set), fused with the grid barrier.  Returns false when the
+// barrier wait expired.
+template <int NV>
+__device__ bool grid_reduce(KCtl* ctl, double* partials, double (&v)[NV], unsigned maxmask) {
+    __shared__ double sm[kMaxNV * 32];
+    __shared__ int s_last;
+    __shared__ unsigned s_gen;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        const bool mx = (maxmask >> j) & 1u;
+        double x = v[j];
+        for (int o = 16; o > 0; o >>= 1) {
+            const double y = __shfl_xor_sync(0xffffffffu, x, o);
+            x = mx ? nmax(x, y) : x + y;
+        }
+        if (lane == 0) sm[j * 32 + warp] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < NV) {
+        const int j = threadIdx.x;
+        const bool mx = (maxmask >> j) & 1u;
+        double x = sm[j * 32];
+        for (int w = 1; w < nw; ++w) x = mx ? nmax(x, sm[j * 32 + w]) : x + sm[j * 32 + w];
+        __stcg(partials + (int64_t)blockIdx.x * NV + j, x);
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned gen = vload(&ctl->gen);
+        const unsigned prev = atomicAdd(&ctl->count, 1u);
+        s_gen = gen;
+        s_last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (s_last) {
+        for (int j = warp; j < NV; j += nw) {
+            const bool mx = (maxmask >> j) & 1u;
+            double x = 0.0;
+            for (int b = lane; b < (int)gridDim.x; b += 32) {
+                const double y = __ldcg(partials + (int64_t)b * NV + j);
+                x = mx ? nmax(x, y) : x + y;
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const double y = __shfl_xor_sync(0xffffffffu, x, o);
+                x = mx ? nmax(x, y) : x + y;
+            }
+            if (lane == 0) __stcg(&ctl->results[j], x);
+        }
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            atomicExch(&ctl->count, 0u);
+            __threadfence();
+            atomicAdd(&ctl->gen, 1u);
+        }
+    } else if (threadIdx.x == 0) {
+        long long it = 0;
+        while (vload(&ctl->gen) == s_gen) {
+            __nanosleep(100);
+            if (++it > kSpinLimit) {
+                atomicExch(&ctl->error, 1);
+                break;
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < NV; ++j) v[j] = __ldcg(&ctl->results[j]);
+    return vload(&ctl->error) == 0;
+}
+
+// y_k(c) = diag(c) * g(k, c) + sum_s val(s, c) * g(k, nbr(s, c))
+template <int NC, class G>
+__device__ __forceinline__ void row_apply(const gf_krylov_t& K, int64_t c, const G& g, double (&out)[NC]) {
+    const int64_t n = K.n;
+    const double d = __ldg(K.diag + c);
+#pragma unroll
+    for (int k = 0; k < NC; ++k) out[k] = d * g(k, c);
+    for (int s = 0; s < K.width; ++s) {
+        const double a = __ldg(K.val + s * n + c);
+        const int nb = __ldg(K.nbr + s * n + c);
+#pragma unroll
+        for (int k = 0; k < NC; ++k) out[k] += a * g(k, nb);
+    }
+}
+
+__device__ __forceinline__ double norm_acc(double acc, double r, bool linf) {
+    return linf ? nmax(acc, fabs(r)) : acc + r * r;
+}
+
+__device__ __forceinline__ double norm_fin(double acc, bool linf) { return linf ? acc : sqrt(acc); }
+
+struct CgState {
+    double thresh, r0, final, rz_old, alpha, beta;
+    int done, its, converged, status;
+};
+
+template <int NC>
+__global__ void __launch_bounds__(kKThreads) k_pcg(gf_krylov_t K) {
+    __shared__ CgState st[NC];
+    __shared__ int s_all_done;
+    KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
+    double* partials = K.work + kCtlDoubles;
+    double* vec = partials + kMaxBlocks * kMaxNV;
+    const int64_t n = K.n;
+    double* r = vec;
+    double* p = vec + NC * n;
+    double* q = vec + 2 * NC * n;
+    double* x = K.x;
+    const bool jac = K.jacobi != 0, linf = K.norm_inf != 0;
+    const unsigned nmask = linf ? ((1u << NC) - 1u) : 0u;
+    const int64_t t0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    bool ok = true;
+
+    {  // r = b - A x, z = M r, p = z; reduce |r| and r.z
+        double loc[2 * NC];
+#pragma unroll
+        for (int j = 0; j < 2 * NC; ++j) loc[j] = 0.0;
+        auto gx = [&](int k, int64_t i) { return __ldcg(x + k * n + i); };
+        for (int64_t c = t0; c < n; c += stride) {
+            double ax[NC];
+            row_apply<NC>(K, c, gx, ax);
+            const double ic = inv_diag(K.diag, c, jac);
+#pragma unroll
+            for (int k = 0; k < NC; ++k) {
+                const double rk = __ldg(K.rhs + k * n + c) - ax[k];
+                const double zk = ic * rk;
+                __stcg(r + k * n + c, rk);
+                __stcg(p + k * n + c, zk);
+                loc[k] = norm_acc(loc[k], rk, linf);
+                loc[NC + k] += rk * zk;
+            }
+        }
+        ok = grid_reduce<2 * NC>(ctl, partials, loc, nmask);
+        if (threadIdx.x == 0) {
+            for (int k = 0; k < NC; ++k) {
+                const double r0 = norm_fin(loc[k], linf);
+                st[k].r0 = r0;
+                st[k].final = r0;
+                st[k].thresh = fmax(K.atol, K.rtol * r0);
+                st[k].rz_old = loc[NC + k];
+                st[k].its = 0;
+                st[k].converged = 0;
+                st[k].status = GF_MAX_ITER;
+                st[k].done = 0;
+                if (r0 < st[k].thresh) {
+                    st[k].done = 1;
+                    st[k].converged = 1;
+                    st[k].status = GF_OK;
+                } else if (!isfinite(r0)) {
+                    st[k].done = 1;
+                    st[k].status = GF_NONFINITE;
+                }
+            }
+        }
+        __syncthreads();
+    }
+
+    for (int it = 1; ok && it <= K.max_iter; ++it) {
+        if (threadIdx.x == 0) {
+            int all = 1;
+            for (int k = 0; k < NC; ++k) all &= st[k].done;
+            s_all_done = all;
+        }
+        __syncthreads();
+        if (s_all_done) break;
+
+        {  // q = A p, p.q
+            double loc[NC];
+#pragma unroll
+            for (int k = 0; k < NC; ++k) loc[k] = 0.0;
+            auto gp = [&](int k, int64_t i) { return __ldcg(p + k * n + i); };
+            for (int64_t c = t0; c < n; c += stride) {
+                double ap[NC];
+                row_apply<NC>(K, c, gp, ap);
+#pragma unroll
+                for (int k = 0; k < NC; ++k) {
+                    if (st[k].done) continue;
+                    __stcg(q + k * n + c, ap[k]);
+                    loc[k] += __ldcg(p + k * n + c) * ap[k];
+                }
+            }
+            ok = grid_reduce<NC>(ctl, partials, loc, 0u);
+            if (!ok) break;
+            if (threadIdx.x == 0)
+                for (int k = 0; k < NC; ++k)
+                    if (!st[k].done) st[k].alpha = st[k].rz_old / loc[k];
+            __syncthreads();
+        }
+        {  // x += alpha p, r -= alpha q, |r|, r.z
+            double loc[2 * NC];
+#pragma unroll
+            for (int j = 0; j < 2 * NC; ++j) loc[j] = 0.0;
+            for (int64_t c = t0; c < n; c += stride) {
+                const double ic = inv_diag(K.diag, c, jac);
+#pragma unroll
+                for (int k = 0; k < NC; ++k) {
+                    if (st[k].done) continue;
+                    const double a = st[k].alpha;
+                    const double pk = __ldcg(p + k * n + c);
+                    __stcg(x + k * n + c, __ldcg(x + k * n + c) + a * pk);
+                    const double rk = __ldcg(r + k * n + c) - a * __ldcg(q + k * n + c);
+                    __stcg(r + k * n + c, rk);
+                    loc[k] = norm_acc(loc[k], rk, linf);
+                    loc[NC + k] += rk * (ic * rk);
+                }
+            }
+            ok = grid_reduce<2 * NC>(ctl, partials, loc, nmask);
+            if (!ok) break;
+            if (threadIdx.x == 0) {
+                int all = 1;
+                for (int k = 0; k < NC; ++k) {
+                    if (st[k].done) continue;
+                    const double fin = norm_fin(loc[k], linf);
+                    st[k].final = fin;
+                    if (fin < st[k].thresh) {
+                        st[k].done = 1;
+                        st[k].converged = 1;
+                        st[k].its = it;
+                        st[k].status = GF_OK;
+                    } else if (!isfinite(fin)) {
+                        st[k].done = 1;
+                        st[k].its = it;
+                        st[k].status = GF_NONFINITE;
+                    } else {
+                        st[k].beta = loc[NC + k] / st[k].rz_old;
+                        st[k].rz_old = loc[NC + k];
+                    }
+                    all &= st[k].done;
+                }
+                for (int k = 0; k < NC; ++k) all &= st[k].done;
+                s_all_done = all;
+            }
+            __syncthreads();
+            if (s_all_done) break;
+        }
+        {  // p = z + p beta
+            double dummy[1] = {0.0};
+            for (int64_t c = t0; c < n; c += stride) {
+                const double ic = inv_diag(K.diag, c, jac);
+#pragma unroll
+                for (int k = 0; k < NC; ++k) {
+                    if (st[k].done) continue;
+                    const double rk = __ldcg(r + k * n + c);
+                    __stcg(p + k * n + c, ic * rk + __ldcg(p + k * n + c) * st[k].beta);
+                }
+            }
+            ok = grid_reduce<1>(ctl, partials, dummy, 0u);
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        for (int k = 0; k < NC; ++k) {
+            double* s = K.stats + 5 * k;
+            s[0] = st[k].r0;
+            s[1] = st[k].final;
+            s[2] = st[k].done ? st[k].its : K.max_iter;
+            s[3] = st[k].converged;
+            s[4] = ok ? st[k].status : GF_ERR_TIMEOUT;
+        }
+    }
+}
+
+// BiCGStab per-component modes.
+enum { kDone = 0, kRun = 1, kRestart = 2, kIdle = 3, kConvS = 4 };
+
+struct BiState {
+    double thresh, r0, final, rho_old, alpha, omega, beta;
+    int mode, restarts, its, converged, status;
+};
+
+__device__ __forceinline__ void breakdown(BiState& s, int it, int max_restart) {
+    if (s.restarts >= max_restart) {
+        s.mode = kDone;
+        s.its = it;
+        s.status = GF_BREAKDOWN;
+    } else {
+        s.restarts += 1;
+        s.mode = kRestart;
+    }
+}
+
+template <int NC>
+__global__ void __launch_bounds__(kKThreads) k_bicgstab(gf_krylov_t K) {
+    __shared__ BiState st[NC];
+    __shared__ int s_any;
+    KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
+    double* partials = K.work + kCtlDoubles;
+    double* vec = partials + kMaxBlocks * kMaxNV;
+    const int64_t n = K.n;
+    double* r = vec;
+    double* rh = vec + NC * n;
+    double* p = vec + 2 * NC * n;
+    double* v = vec + 3 * NC * n;
+    double* s = vec + 4 * NC * n;
+    double* t = vec + 5 * NC * n;
+    double* x = K.x;
+    const bool jac = K.jacobi != 0, linf = K.norm_inf != 0;
+    const int64_t t0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    bool ok = true;
+
+    {  // r = b - A x; r_hat = p = r; |r|, r.r
+        double loc[2 * NC];
+#pragma unroll
+        for (int j = 0; j < 2 * NC; ++j) loc[j] = 0.0;
+        auto gx = [&](int k, int64_t i) { return __ldcg(x + k * n + i); };
+        for (int64_t c = t0; c < n; c += stride) {
+            double ax[NC];
+            row_apply<NC>(K, c, gx, ax);
+#pragma unroll
+            for (int k = 0; k < NC; ++k) {
+                const double rk = __ldg(K.rhs + k * n + c) - ax[k];
+                __stcg(r + k * n + c, rk);
+                __stcg(rh + k * n + c, rk);
+                __stcg(p + k * n + c, rk);
+                loc[k] = norm_acc(loc[k], rk, linf);
+                loc[NC + k] += rk * rk;
+            }
+        }
+        ok = grid_reduce<2 * NC>(ctl, partials, loc, linf ? ((1u << NC) - 1u) : 0u);
+        if (threadIdx.x == 0) {
+            for (int k = 0; k < NC; ++k) {
+                BiState& b = st[k];
+                const double r0 = norm_fin(loc[k], linf);
+                b.r0 = r0;
+                b.final = r0;
+                b.thresh = fmax(K.atol, K.rtol * r0);
+                b.rho_old = loc[NC + k];
+                b.restarts = 0;
+                b.its = 0;
+                b.converged = 0;
+                b.status = GF_MAX_ITER;
+                b.mode = kRun;
+                if (r0 < b.thresh) {
+                    b.mode = kDone;
+                    b.converged = 1;
+                    b.status = GF_OK;
+                } else if (!isfinite(r0)) {
+                    b.mode = kDone;
+                    b.status = GF_NONFINITE;
+                }
+            }
+        }
+        __syncthreads();
+    }
+
+    for (int it = 1; ok && it <= K.max_iter; ++it) {
+        if (threadIdx.x == 0) {
+            int any = 0;
+            for (int k = 0; k < NC; ++k) {
+                if (st[k].mode == kIdle) st[k].mode = kRun;
+                any |= (st[k].mode == kRun);
+            }
+            s_any = any;
+        }
+        __syncthreads();
+        if (!s_any) break;
+
+        // P1: y = M p, v = A y; r_hat.v, |r_hat|^2, |v|^2
+        {
+            double loc[3 * NC];
+#pragma unroll
+            for (int j = 0; j < 3 * NC; ++j) loc[j] = 0.0;
+            auto gy = [&](int k, int64_t i) { return inv_diag(K.diag, i, jac) * __ldcg(p + k * n + i); };
+            for (int64_t c = t0; c < n; c += stride) {
+                double av[NC];
+                row_apply<NC>(K, c, gy, av);
+#pragma unroll
+                for (int k = 0; k < NC; ++k) {
+                    if (st[k].mode != kRun) continue;
+                    __stcg(v + k * n + c, av[k]);
+                    const double h = __ldcg(rh + k * n + c);
+                    loc[k] += h * av[k];
+                    loc[NC + k] += h * h;
+                    loc[2 * NC + k] += av[k] * av[k];
+                }
+            }
+            ok = grid_reduce<3 * NC>(ctl, partials, loc, 0u);
+            if (!ok) break;
+            if (threadIdx.x == 0) {
+                for (int k = 0; k < NC; ++k) {
+                    BiState& b = st[k];
+                    if (b.mode != kRun) continue;
+                    const double da = loc[k];
+                    if (fabs(da) <= 1e-6 * sqrt(loc[NC + k]) * sqrt(loc[2 * NC + k]))
+                        breakdown(b, it, K.max_restart);
+                    else
+                        b.alpha = b.rho_old / da;
+                }
+            }
+            __syncthreads();
+        }
+        // P2: s = r - alpha v, |s|; restarting systems copy r and reduce r.r
+        {
+            double loc[2 * NC];
+#pragma unroll
+            for (int j = 0; j < 2 * NC; ++j) loc[j] = 0.0;
+            for (int64_t c = t0; c < n; c += stride) {
+#pragma unroll
+                for (int k = 0; k < NC; ++k) {
+                    const int md = st[k].mode;
+                    if (md == kRun) {
+                        const double sk = __ldcg(r + k * n + c) - st[k].alpha * __ldcg(v + k * n + c);
+                        __stcg(s + k * n + c, sk);
+                        loc[k] = norm_acc(loc[k], sk, linf);
+                    } else if (md == kRestart) {
+                        const double rk = __ldcg(r + k * n + c);
+                        __stcg(rh + k * n + c, rk);
+                        __stcg(p + k * n + c, rk);
+                        loc[NC + k] += rk * rk;
+                    }
+                }
+            }
+            ok = grid_reduce<2 * NC>(ctl, partials, loc, linf ? ((1u << NC) - 1u) : 0u);
+            if (!ok) break;
+            if (threadIdx.x == 0) {
+                for (int k = 0; k < NC; ++k) {
+                    BiState& b = st[k];
+                    if (b.mode == kRestart) {
+                        b.rho_old = loc[NC + k];
+                        b.mode = kIdle;
+                    } else if (b.mode == kRun) {
+                        const double fin = norm_fin(loc[k], linf);
+                        b.final = fin;
+                        if (fin < b.thresh) {
+                            b.mode = kConvS;
+                            b.converged = 1;
+                            b.its = it;
+                            b.status = GF_OK;
+                        } else if (!isfinite(fin)) {
+                            b.mode = kDone;
+                            b.its = it;
+                            b.status = GF_NONFINITE;
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        // P3: converged-on-s systems take x += alpha y; others z = M s, t = A z
+        {
+            double loc[2 * NC];
+#pragma unroll
+            for (int j = 0; j < 2 * NC; ++j) loc[j] = 0.0;
+            auto gz = [&](int k, int64_t i) { return inv_diag(K.diag, i, jac) * __ldcg(s + k * n + i); };
+            for (int64_t c = t0; c < n; c += stride) {
+                double at[NC];
+                row_apply<NC>(K, c, gz, at);
+                const double ic = inv_diag(K.diag, c, jac);
+#pragma unroll
+                for (int k = 0; k < NC; ++k) {
+                    const int md = st[k].mode;
+                    if (md == kConvS) {
+                        const double y = ic * __ldcg(p + k * n + c);
+                        __stcg(x + k * n + c, __ldcg(x + k * n + c) + st[k].alpha * y);
+                    } else if (md == kRun) {
+                        __stcg(t + k * n + c, at[k]);
+                        loc[k] += at[k] * at[k];
+                        loc[NC + k] += at[k] * __ldcg(s + k * n + c);
+                    }
+                }
+            }
+            ok = grid_reduce<2 * NC>(ctl, partials, loc, 0u);
+            if (!ok) break;
+            if (threadIdx.x == 0) {
+                for (int k = 0; k < NC; ++k) {
+                    BiState& b = st[k];
+                    if (b.mode == kConvS) {
+                        b.mode = kDone;
+                        continue;
+                    }
+                    if (b.mode != kRun) continue;
+                    const double dd = loc[k];
+                    const double tn = sqrt(loc[k]);
+                    if (fabs(dd) <= 1e-6 * tn * tn) {
+                        breakdown(b, it, K.max_restart);
+                        continue;
+                    }
+                    b.omega = loc[NC + k] / dd;
+                    if (fabs(b.omega) <= 1e-6) breakdown(b, it, K.max_restart);
+                }
+            }
+            __syncthreads();
+        }
+        // P4: x += alpha y + omega z, r = s - omega t; |r|, r_hat.r, |r_hat|^2, |r|^2
+        {
+            double loc[4 * NC];
+#pragma unroll
+            for (int j = 0; j < 4 * NC; ++j) loc[j] = 0.0;
+            for (int64_t c = t0; c < n; c += stride) {
+                const double ic = inv_diag(K.diag, c, jac);
+#pragma unroll
+                for (int k = 0; k < NC; ++k) {
+                    const int md = st[k].mode;
+                    if (md == kRun) {
+                        const double sk = __ldcg(s + k * n + c);
+                        const double y = ic * __ldcg(p + k * n + c);
+                        const double z = ic * sk;
+                        __stcg(x + k * n + c, __ldcg(x + k * n + c) + st[k].alpha * y + st[k].omega * z);
+                        const double rk = sk - st[k].omega * __ldcg(t + k * n + c);
+                        __stcg(r + k * n + c, rk);
+                        const double h = __ldcg(rh + k * n + c);
+                        loc[k] = norm_acc(loc[k], rk, linf);
+                        loc[NC + k] += h * rk;
+                        loc[2 * NC + k] += h * h;
+                        loc[3 * NC + k] += rk * rk;
+                    } else if (md == kRestart) {
+                        const double rk = __ldcg(r + k * n + c);
+                        __stcg(rh + k * n + c, rk);
+                        __stcg(p + k * n + c, rk);
+                        loc[3 * NC + k] += rk * rk;
+                    }
+                }
+            }
+            ok = grid_reduce<4 * NC>(ctl, partials, loc, linf ? ((1u << NC) - 1u) : 0u);
+            if (!ok) break;
+            if (threadIdx.x == 0) {
+                for (int k = 0; k < NC; ++k) {
+                    BiState& b = st[k];
+                    if (b.mode == kRestart) {
+                        b.rho_old = loc[3 * NC + k];
+                        b.mode = kIdle;
+                        continue;
+                    }
+                    if (b.mode != kRun) continue;
+                    const double fin = norm_fin(loc[k], linf);
+                    b.final = fin;
+                    if (fin < b.thresh) {
+                        b.mode = kDone;
+                        b.converged = 1;
+                        b.its = it;
+                        b.status = GF_OK;
+                        continue;
+                    }
+                    if (!isfinite(fin)) {
+                        b.mode = kDone;
+                        b.its = it;
+                        b.status = GF_NONFINITE;
+                        continue;
+                    }
+                    const double rho_new = loc[NC + k];
+                    if (fabs(rho_new) <= 1e-6 * sqrt(loc[2 * NC + k]) * sqrt(loc[3 * NC + k])) {
+                        breakdown(b, it, K.max_restart);
+                        continue;
+                    }
+                    b.beta = (rho_new / b.rho_old) * (b.alpha / b.omega);
+                    b.rho_old = rho_new;
+                }
+            }
+            __syncthreads();
+        }
+        // P5: p = r + beta (p - omega v); restarting systems copy r
+        {
+            double loc[NC];
+#pragma unroll
+            for (int k = 0; k < NC; ++k) loc[k] = 0.0;
+            for (int64_t c = t0; c < n; c += stride) {
+#pragma unroll
+                for (int k = 0; k < NC; ++k) {
+                    const int md = st[k].mode;
+                    if (md == kRun) {
+                        const double pk = __ldcg(p + k * n + c);
+                        __stcg(p + k * n + c,
+                               __ldcg(r + k * n + c) + st[k].beta * (pk - st[k].omega * __ldcg(v + k * n + c)));
+                    } else if (md == kRestart) {
+                        const double rk = __ldcg(r + k * n + c);
+                        __stcg(rh + k * n + c, rk);
+                        __stcg(p + k * n + c, rk);
+                        loc[k] += rk * rk;
+                    }
+                }
+            }
+            ok = grid_reduce<NC>(ctl, partials, loc, 0u);
+            if (!ok) break;
+            if (threadIdx.x == 0) {
+                for (int k = 0; k < NC; ++k) {
+                    if (st[k].mode == kRestart) {
+                        st[k].rho_old = loc[k];
+                        st[k].mode = kIdle;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        for (int k = 0; k < NC; ++k) {
+            double* o = K.stats + 5 * k;
+            const bool fin = st[k].mode == kDone;
+            o[0] = st[k].r0;
+            o[1] = st[k].final;
+            o[2] = fin ? st[k].its : K.max_iter;
+            o[3] = st[k].converged;
+            o[4] = ok ? (fin ? st[k].status : GF_MAX_ITER) : GF_ERR_TIMEOUT;
+        }
+    }
+}
+
+template <class Kern>
+static int launch_persistent(Kern kern, const gf_krylov_t* k, void* stream, const char* what) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int sms = 0, coop = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    if (!coop) {
+        set_error("%s: device does not support cooperative launch", what);
+        return GF_ERR_CUDA;
+    }
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kKThreads, 0);
+    if (e != cudaSuccess || per_sm < 1) {
+        set_error("%s: occupancy query failed: %s", what, cudaGetErrorString(e));
+        return GF_ERR_CUDA;
+    }
+    int64_t want = (k->n + kKThreads - 1) / kKThreads;
+    int64_t cap = (int64_t)per_sm * sms;
+    if (cap > kMaxBlocks) cap = kMaxBlocks;
+    int grid = (int)(want < cap ? want : cap);
+    if (grid < 1) grid = 1;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    e = cudaMemsetAsync(k->work, 0, sizeof(KCtl), s);
+    if (e != cudaSuccess) {
+        set_error("%s: %s", what, cudaGetErrorString(e));
+        return GF_ERR_CUDA;
+    }
+    gf_krylov_t arg = *k;
+    void* args[] = {&arg};
+    e = cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(kKThreads), args, 0, s);
+    if (e != cudaSuccess) {
+        set_error("%s: cooperative launch failed: %s", what, cudaGetErrorString(e));
+        return GF_ERR_CUDA;
+    }
+    return GF_OK;
+}
+
+static bool valid_krylov(const gf_krylov_t* k, int nvec, const char* what) {
+    if (k == nullptr || k->n <= 0 || k->width <= 0 || k->ncomp < 1 || k->ncomp > 3 || k->nbr == nullptr ||
+        k->diag == nullptr || k->val == nullptr || k->rhs == nullptr || k->x == nullptr || k->work == nullptr ||
+        k->stats == nullptr || k->max_iter < 0) {
+        set_error("%s: invalid arguments", what);
+        return false;
+    }
+    const int64_t need = kCtlDoubles + (int64_t)kMaxBlocks * kMaxNV + (int64_t)nvec * k->ncomp * k->n;
+    if (k->work_len < need) {
+        set_error("%s: workspace holds %lld doubles, %lld needed", what, (long long)k->work_len, (long long)need);
+        return false;
+    }
+    if (k->n * (int64_t)k->width > 2147483647LL) {
+        set_error("%s: system too large", what);
+        return false;
+    }
+    return true;
+}
+
+}  // namespace gf
+
+using namespace gf;
+
+extern "C" {
+
+int64_t gf_krylov_workspace_size(int64_t n, int32_t ncomp, int32_t bicgstab) {
+    const int nvec = bicgstab ? 6 : 3;
+    return kCtlDoubles + (int64_t)kMaxBlocks * kMaxNV + (int64_t)nvec * ncomp * n;
+}
+
+int gf_pcg_solve(const gf_krylov_t* k, void* stream) {
+    if (!valid_krylov(k, 3, "gf_pcg_solve")) return GF_ERR_INVALID;
+    switch (k->ncomp) {
+        case 1:
+            return launch_persistent(k_pcg<1>, k, stream, "gf_pcg_solve");
+        case 2:
+            return launch_persistent(k_pcg<2>, k, stream, "gf_pcg_solve");
+        default:
+            return launch_persistent(k_pcg<3>, k, stream, "gf_pcg_solve");
+    }
+}
+
+int gf_bicgstab_solve(const gf_krylov_t* k, void* stream) {
+    if (!valid_krylov(k, 6, "gf_bicgstab_solve")) return GF_ERR_INVALID;
+    switch (k->ncomp) {
+        case 1:
+            return launch_persistent(k_bicgstab<1>, k, stream, "gf_bicgstab_solve");
+        case 2:
+            return launch_persistent(k_bicgstab<2>, k, stream, "gf_bicgstab_solve");
+        default:
+            return launch_persistent(k_bicgstab<3>, k, stream, "gf_bicgstab_solve");
+    }
+}
+
+}  // extern "C"

@@ -1,0 +1,82 @@
+"""Explicit operators (gridfoam ``fv/fvc``): ``grad``, ``div``,
+``interpolate``, ``sn_grad``.  Each wraps one library kernel."""
+
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from gridfoam_b200._lib import GfBcAux, call, ptr, stream_ptr
+from gridfoam_b200.core.field import (
+    CellField,
+    FaceField,
+    get_or_create_cellfield,
+    get_or_create_facefield,
+)
+from gridfoam_b200.fv import schemes
+from gridfoam_b200.meta.config import GradScheme
+
+
+def _eval_state(field: CellField) -> None:
+    aux = GfBcAux()
+    phi = field.grid.get_facefield("phi")
+    if phi is not None:
+        aux.phi_bnd = ptr(phi.boundary_store)
+    field.evaluate_bc(aux)
+
+
+def grad(field: CellField) -> CellField:
+    """fv/fvc/grad.py:8-34 (least-squares, fv/kernels/least_squares.py:29-101)."""
+    grid = field.grid
+    if schemes.grad_scheme(grid.sim_config, field.name) != GradScheme.LEASTSQUARE:
+        raise NotImplementedError("the device path implements the leastsquare gradient scheme")
+    _eval_state(field)
+    out = get_or_create_cellfield(grid, f"grad({field.name})", field.role, field.component_shape + (3,))
+    t = field.table
+    call("gf_lsq_grad", ctypes.byref(grid.cmesh), field.num_components, ptr(field.store), ptr(t.kind),
+         ptr(t.psib), ptr(out.store), stream_ptr())
+    return out
+
+
+def div(phi: FaceField) -> CellField:
+    """fv/fvc/div.py:15-64."""
+    grid = phi.grid
+    nc = phi.store.shape[0]
+    out = get_or_create_cellfield(grid, f"div({phi.name})", "local", phi.component_shape)
+    call("gf_fvc_div", ctypes.byref(grid.cmesh), nc, ptr(phi.store), ptr(out.store), stream_ptr())
+    return out
+
+
+def interpolate(field: CellField) -> FaceField:
+    """fv/fvc/interpolate.py:7-26 (hierarchy-aware linear + boundary fill)."""
+    grid = field.grid
+    _eval_state(field)
+    out = get_or_create_facefield(grid, f"{field.name}_f", "local", field.component_shape)
+    t = field.table
+    call("gf_interpolate", ctypes.byref(grid.cmesh), field.num_components, ptr(field.store), ptr(t.kind),
+         ptr(t.psib), ptr(out.store), stream_ptr())
+    return out
+
+
+def sn_grad(field: CellField) -> FaceField:
+    """fv/fvc/sn_grad.py:16-55."""
+    grid = field.grid
+    _eval_state(field)
+    out = get_or_create_facefield(grid, f"snGrad({field.name})", "local", field.component_shape)
+    t = field.table
+    call("gf_sn_grad", ctypes.byref(grid.cmesh), field.num_components, ptr(field.store), ptr(t.kind),
+         ptr(t.frac), ptr(t.refv), ptr(t.refg), ptr(out.store), stream_ptr())
+    return out
+
+
+def face_flux(phi: FaceField, U: CellField) -> None:
+    """fv/flux.py:132-162 ``correct_flux(phi, U, update_internal=True)``."""
+    _eval_state(U)
+    t = U.table
+    call("gf_face_flux", ctypes.byref(U.grid.cmesh), 0, ptr(U.store), ptr(t.kind), ptr(t.psib), None,
+         ptr(phi.store), stream_ptr())
+
+
+def spmv_check(mat, x: torch.Tensor) -> torch.Tensor:
+    return mat.multiply(x)

@@ -1,0 +1,111 @@
+"""Implicit operators returning ``FvMatrix`` (gridfoam ``fv/fvm``).
+
+``ddt(field)``, ``div(phi, field)`` and ``laplacian(gamma, field)`` keep the
+reference signatures (``fv/fvm/ddt.py:7-40``, ``div.py:15-73``,
+``laplacian.py:101-201``).  Each is one ``gf_assemble`` launch; the
+algorithms fuse all three terms into a single launch instead.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from gridfoam_b200 import _lib
+from gridfoam_b200._lib import GfAssembly, GfBcAux, call, ptr, stream_ptr
+from gridfoam_b200.core.field import CellField, FaceField
+from gridfoam_b200.core.fvmatrix import FvMatrix
+from gridfoam_b200.fv import schemes
+from gridfoam_b200.meta.config import GradScheme
+
+
+def _eval_state(field: CellField) -> None:
+    aux = GfBcAux()
+    phi = field.grid.get_facefield("phi")
+    if phi is not None:
+        aux.phi_bnd = ptr(phi.boundary_store)
+    field.evaluate_bc(aux)
+
+
+def _base(field: CellField, mat: FvMatrix) -> GfAssembly:
+    t = field.table
+    a = GfAssembly()
+    a.ncomp = field.num_components
+    a.psi = ptr(field.store)
+    a.bc_kind = ptr(t.kind)
+    a.frac = ptr(t.frac)
+    a.refv = ptr(t.refv)
+    a.refg = ptr(t.refg)
+    a.diag = ptr(mat.diag_store)
+    a.val = ptr(mat.val)
+    a.source = ptr(mat.source_store)
+    return a
+
+
+def _run(field: CellField, a: GfAssembly) -> None:
+    call("gf_assemble", ctypes.byref(field.grid.cmesh), ctypes.byref(a), stream_ptr())
+
+
+def ddt(field: CellField) -> FvMatrix:
+    """fv/fvm/ddt.py:7-40."""
+    mat = FvMatrix(field)
+    _eval_state(field)
+    a = _base(field, mat)
+    ca, cb, cc = schemes.ddt_coefficients(field)
+    a.use_ddt = 1
+    a.ddt_a, a.ddt_b, a.ddt_c, a.dt = ca, cb, cc, field.grid.dt
+    a.psi_old = ptr(field.old_store)
+    a.psi_older = ptr(field.older_store) if cc != 0.0 else None
+    _run(field, a)
+    return mat
+
+
+def div(phi: FaceField, field: CellField) -> FvMatrix:
+    """fv/fvm/div.py:15-73 with the configured scheme."""
+    if phi.component_shape != ():
+        raise ValueError("convection requires scalar face flux")
+    mat = FvMatrix(field)
+    _eval_state(field)
+    scheme = schemes.div_scheme(field.grid.sim_config, phi.name, field.name)
+    code = _lib.DIV_CODES[scheme.value]
+    grad = None
+    if code >= _lib.DIV_CODES["vanleer"]:
+        if schemes.grad_scheme(field.grid.sim_config, field.name) != GradScheme.LEASTSQUARE:
+            raise NotImplementedError("the device path implements the leastsquare gradient scheme")
+        grad = torch.empty((field.num_components * 3, field.grid.num_cells), dtype=torch.float64,
+                           device=field.grid.device)
+        t = field.table
+        call("gf_lsq_grad", ctypes.byref(field.grid.cmesh), field.num_components, ptr(field.store),
+             ptr(t.kind), ptr(t.psib), ptr(grad), stream_ptr())
+    a = _base(field, mat)
+    a.div_scheme = code
+    a.div_sign = 1.0
+    a.phi = ptr(phi.store)
+    a.grad_psi = ptr(grad)
+    _run(field, a)
+    return mat
+
+
+def laplacian(gamma, field: CellField) -> FvMatrix:
+    """fv/fvm/laplacian.py:101-201 (uniform or per-cell diffusivity)."""
+    grid = field.grid
+    mat = FvMatrix(field)
+    _eval_state(field)
+    scheme = schemes.laplacian_scheme(grid.sim_config, field.name)
+    a = _base(field, mat)
+    a.lap_sign = 1.0
+    a.lap_harmonic = int(scheme in schemes.HARMONIC)
+    g_t = None
+    if isinstance(gamma, torch.Tensor) and gamma.dim() == 1:
+        if gamma.shape[0] != grid.num_cells:
+            raise ValueError("diffusivity must have one value per cell")
+        g_t = gamma.to(device=grid.device, dtype=torch.float64).contiguous()
+        if a.lap_harmonic and not bool(torch.all(torch.isfinite(g_t) & (g_t >= 0))):
+            raise ValueError("Harmonic diffusivity must be finite and nonnegative")
+        a.gamma = ptr(g_t)
+    else:
+        a.gamma_scalar = float(gamma)
+    _run(field, a)
+    mat._keep = g_t
+    return mat

@@ -1,0 +1,120 @@
+"""Device CG and BiCGStab solvers (solvers/cg.py, bicgstab.py, krylov.py).
+
+All components of a field are solved by one persistent cooperative launch
+(``gf_pcg_solve`` / ``gf_bicgstab_solve``) that shares the matrix reads
+between components; the reference loops over components serially
+(``solvers/krylov.py:75-79``).  Convergence is decided on the device with the
+reference's rule ``|r| < max(atol, rtol |r0|)``; the BiCGStab breakdown
+restarts follow ``solvers/bicgstab.py:123-272``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from gridfoam_b200._lib import GfKrylov, call, load, ptr, stream_ptr
+from gridfoam_b200.meta.config import NormType, PreconditionerType, SolverConfig
+from gridfoam_b200.solvers.base import LinearSolver, SolveResult, SolveStats, _StatsBuffer
+
+_WORKSPACES: dict[tuple, torch.Tensor] = {}
+
+
+def workspace(device: torch.device, n: int, ncomp: int, bicgstab: bool) -> torch.Tensor:
+    """Cached per-shape workspace (allocated once, reused by every solve)."""
+    key = (str(device), n, ncomp, bicgstab)
+    ws = _WORKSPACES.get(key)
+    if ws is None:
+        size = load().gf_krylov_workspace_size(n, ncomp, int(bicgstab))
+        ws = torch.empty(size, dtype=torch.float64, device=device)
+        _WORKSPACES[key] = ws
+    return ws
+
+
+class DeviceKrylov(LinearSolver):
+    method: str = ""
+    bicgstab: bool = False
+
+    def __init__(self, config: SolverConfig):
+        self.config = config
+        self.solver_name = config.method.value
+        self.precon_type = config.preconditioner
+        self.atol = float(config.tolerance)
+        self.rtol = float(config.rel_tolerance)
+        self.max_iter = int(config.max_iter)
+        self.max_restart = int(config.max_restart)
+        self.norm_inf = config.norm_type == NormType.L_inf
+        self.log_interval = config.log_interval
+        self._stats_dev: dict[tuple, torch.Tensor] = {}
+        # Optional list receiving (start event, end event, stats) per solve.
+        self.profile_events: list | None = None
+
+    def solve_arrays(self, grid, diag: torch.Tensor, val: torch.Tensor, rhs: torch.Tensor,
+                     x: torch.Tensor) -> tuple[SolveStats, ...]:
+        """Solve in place: ``x [ncomp, C]`` holds the guess and gets the solution."""
+        nc, n = rhs.shape
+        key = (str(grid.device), nc)
+        stats = self._stats_dev.get(key)
+        if stats is None:
+            stats = torch.zeros((nc, 5), dtype=torch.float64, device=grid.device)
+            self._stats_dev[key] = stats
+        ws = workspace(grid.device, n, nc, self.bicgstab)
+        k = GfKrylov()
+        k.n = n
+        k.width = grid.ell_width
+        k.ncomp = nc
+        k.max_iter = self.max_iter
+        k.max_restart = self.max_restart
+        k.norm_inf = int(self.norm_inf)
+        k.jacobi = int(self.precon_type == PreconditionerType.JACOBI)
+        k.atol = self.atol
+        k.rtol = self.rtol
+        k.nbr = ptr(grid.dev["ell_nbr"])
+        k.diag = ptr(diag)
+        k.val = ptr(val)
+        k.rhs = ptr(rhs)
+        k.x = ptr(x)
+        k.work = ptr(ws)
+        k.work_len = ws.numel()
+        k.stats = ptr(stats)
+        ev = None
+        if self.profile_events is not None:
+            ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            ev[0].record()
+        call("gf_bicgstab_solve" if self.bicgstab else "gf_pcg_solve", ctypes.byref(k), stream_ptr())
+        if ev is not None:
+            ev[1].record()
+        buf = _StatsBuffer(stats)
+        out = tuple(SolveStats(self.solver_name, buf, i) for i in range(nc))
+        if ev is not None:
+            self.profile_events.append((ev[0], ev[1], out))
+        return out
+
+    def _solve_matrix(self, A, rhs_store: torch.Tensor, x0_store: torch.Tensor) -> SolveResult:
+        x = x0_store.clone()
+        stats = self.solve_arrays(A.grid, A.diag_store, A.val, rhs_store.contiguous(), x)
+        sol = x[0] if A.field.component_shape == () else x.t()
+        return SolveResult(solution=sol, stats=stats)
+
+    def _solve_primal(self, eq) -> SolveResult:
+        A = eq.fv_matrix
+        return self._solve_matrix(A, A.source_store, eq.target.store)
+
+    def solve_transpose(self, A_T, rhs: torch.Tensor) -> torch.Tensor:
+        nc = A_T.num_components
+        r = rhs.reshape(1, -1) if nc == 1 else rhs.t()
+        res = self._solve_matrix(A_T, r.contiguous(), torch.zeros_like(r))
+        return res.solution
+
+
+class CGSolver(DeviceKrylov):
+    """Jacobi-preconditioned CG (solvers/cg.py:23-174)."""
+
+    bicgstab = False
+
+
+class BiCGSTABSolver(DeviceKrylov):
+    """Right-preconditioned BiCGStab with restarts (solvers/bicgstab.py:23-272)."""
+
+    bicgstab = True
