@@ -183,6 +183,48 @@ def run_reference(args) -> None:
     print(json.dumps(line))
 
 
+def mixed_variant(args, local: int, ref_algo, torch) -> dict:
+    """Same workload with the pressure CG in FP32 inside FP64 refinement.
+
+    Both runs start from the same initial state and take the same number of
+    steps; the reported errors are relative L2 norms against the FP64 run.
+    """
+    from tests.golden.device_harness import device_case
+
+    case = pipe_config()
+    for key in ("p", "pFinal"):
+        case["simulator"]["fvSolution"]["solvers"][key]["inner_precision"] = "float32"
+    _, _, grid, algo = device_case(case_def=case, device=f"cuda:{local}")
+    _, _, _, ref = device_case(case_def=pipe_config(), device=f"cuda:{local}")
+    n_steps = args.warmup + args.steps
+    for _ in range(args.warmup):
+        algo.step()
+        ref.step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        algo.step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    for _ in range(args.steps):
+        ref.step()
+    torch.cuda.synchronize()
+    du = torch.linalg.vector_norm(algo.U.data - ref.U.data) / torch.linalg.vector_norm(ref.U.data)
+    dp = torch.linalg.vector_norm(algo.p.data - ref.p.data) / torch.linalg.vector_norm(ref.p.data)
+    its = [s.iterations for s in algo.last_stats["p"]]
+    return {
+        "value": grid.num_cells * args.steps / (ms * 1e-3),
+        "unit": METRIC,
+        "ms_per_step": ms / args.steps,
+        "steps_compared": n_steps,
+        "rel_l2_U_vs_fp64": float(du),
+        "rel_l2_p_vs_fp64": float(dp),
+        "last_p_iterations": its,
+    }
+
+
 def run_gpu(args) -> None:
     import torch
 
@@ -316,6 +358,8 @@ def run_gpu(args) -> None:
             "d2h_bytes_per_step": h2d,
         },
     }
+    if not args.no_variants:
+        line["variants"] = {"mixed_fp32_inner": mixed_variant(args, local, algo, torch)}
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
     if rank == 0:
@@ -333,6 +377,7 @@ def main() -> None:
     ap.add_argument("--impl", default="gridfoam_b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-variants", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -141,6 +141,9 @@ class GfKrylov(ctypes.Structure):
         ("work", P),
         ("work_len", I64),
         ("stats", P),
+        ("mixed", I32),
+        ("max_outer", I32),
+        ("inner_eta", F64),
     ]
 
 

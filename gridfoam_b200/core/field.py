@@ -170,8 +170,8 @@ class CellField:
         self._name = name
         self._role = FieldRole(role)
         self._component_shape = tuple(component_shape)
-        if self.num_components not in (1, 3):
-            raise ValueError("device fields support scalar and 3-vector components")
+        if self.num_components not in (1, 3, 9):
+            raise ValueError("device fields support scalar, vector and 3x3 tensor components")
         self._store = torch.zeros(
             (self.num_components, grid.num_cells), dtype=torch.float64, device=grid.device
         )
@@ -245,7 +245,9 @@ class CellField:
     def _view(self, store: torch.Tensor) -> torch.Tensor:
         if self._component_shape == ():
             return store[0]
-        return store.t()
+        if len(self._component_shape) == 1:
+            return store.t()
+        return store.t().reshape(store.shape[1], *self._component_shape)
 
     @property
     def data(self) -> torch.Tensor:
@@ -260,7 +262,7 @@ class CellField:
         if self._component_shape == ():
             self._store[0].copy_(value)
         else:
-            self._store.copy_(value.t())
+            self._store.copy_(value.reshape(value.shape[0], -1).t())
 
     def reset_data(self, init_value) -> None:
         v = torch.as_tensor(init_value, dtype=torch.float64)

@@ -16,7 +16,7 @@ constexpr int kKThreads = 512;
 constexpr int kMaxBlocks = 1024;
 constexpr int kMaxNV = 16;
 constexpr int kCtlDoubles = 32;
-constexpr long long kSpinLimit = 10000000LL;  // x ~100 ns sleeps: about a second
+constexpr long long kSpinLimit = 20000000LL;  // x ~50 ns polls: about a second
 
 struct KCtl {
     unsigned int count;
@@ -100,7 +100,7 @@ __device__ bool grid_reduce(KCtl* ctl, double* partials, double (&v)[NV], unsign
     } else if (threadIdx.x == 0) {
         long long it = 0;
         while (vload(&ctl->gen) == s_gen) {
-            __nanosleep(100);
+            __nanosleep(32);
             if (++it > kSpinLimit) {
                 atomicExch(&ctl->error, 1);
                 break;
@@ -303,6 +303,344 @@ __global__ void __launch_bounds__(kKThreads) k_pcg(gf_krylov_t K) {
             s[3] = st[k].converged;
             s[4] = ok ? st[k].status : GF_ERR_TIMEOUT;
         }
+    }
+}
+
+// Single-system Jacobi-PCG with the direction update fused into the SpMV
+// pass: p_new = z + beta p_old is stored for the own cell and recomputed
+// (bitwise identically) at the neighbours, so an iteration needs two grid
+// reductions (p.Ap, then |r| and r.z) instead of three.  WIDTH > 0 fixes
+// the ELL width at compile time so the slot loop unrolls.
+constexpr int kCgThreads = 256;
+
+template <int WIDTH>
+__global__ void __launch_bounds__(kCgThreads, 4) k_pcg1(gf_krylov_t K) {
+    __shared__ CgState st;
+    KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
+    double* partials = K.work + kCtlDoubles;
+    double* vec = partials + kMaxBlocks * kMaxNV;
+    const int64_t n = K.n;
+    double* r = vec;
+    double* z = vec + n;
+    double* pa = vec + 2 * n;
+    double* pb = vec + 3 * n;
+    double* q = vec + 4 * n;
+    double* x = K.x;
+    const int W = WIDTH > 0 ? WIDTH : K.width;
+    const bool jac = K.jacobi != 0, linf = K.norm_inf != 0;
+    const int64_t t0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    bool ok = true;
+    {
+        double loc[2] = {0.0, 0.0};
+        for (int64_t c = t0; c < n; c += stride) {
+            double ax = __ldg(K.diag + c) * __ldcg(x + c);
+#pragma unroll
+            for (int s = 0; s < (WIDTH > 0 ? WIDTH : 1); ++s) {
+                if (WIDTH > 0) {
+                    const int nb = __ldg(K.nbr + s * n + c);
+                    ax += __ldg(K.val + s * n + c) * __ldcg(x + nb);
+                }
+            }
+            if (WIDTH == 0) {
+                for (int s = 0; s < W; ++s) {
+                    const int nb = __ldg(K.nbr + s * n + c);
+                    ax += __ldg(K.val + s * n + c) * __ldcg(x + nb);
+                }
+            }
+            const double rk = __ldg(K.rhs + c) - ax;
+            const double zk = inv_diag(K.diag, c, jac) * rk;
+            __stcg(r + c, rk);
+            __stcg(z + c, zk);
+            __stcg(pa + c, 0.0);
+            loc[0] = norm_acc(loc[0], rk, linf);
+            loc[1] += rk * zk;
+        }
+        ok = grid_reduce<2>(ctl, partials, loc, linf ? 1u : 0u);
+        if (threadIdx.x == 0) {
+            const double r0 = norm_fin(loc[0], linf);
+            st.r0 = r0;
+            st.final = r0;
+            st.thresh = fmax(K.atol, K.rtol * r0);
+            st.rz_old = loc[1];
+            st.beta = 0.0;
+            st.its = 0;
+            st.converged = 0;
+            st.status = GF_MAX_ITER;
+            st.done = 0;
+            if (r0 < st.thresh) {
+                st.done = 1;
+                st.converged = 1;
+                st.status = GF_OK;
+            } else if (!isfinite(r0)) {
+                st.done = 1;
+                st.status = GF_NONFINITE;
+            }
+        }
+        __syncthreads();
+    }
+    double* p_old = pa;
+    double* p_new = pb;
+    for (int it = 1; ok && !st.done && it <= K.max_iter; ++it) {
+        const double beta = st.beta;
+        {  // p_new = z + p_old beta; q = A p_new; p_new . q
+            double loc[1] = {0.0};
+            for (int64_t c = t0; c < n; c += stride) {
+                const double pc = __ldcg(z + c) + __ldcg(p_old + c) * beta;
+                __stcg(p_new + c, pc);
+                double ap = __ldg(K.diag + c) * pc;
+                if (WIDTH > 0) {
+                    int nb[WIDTH > 0 ? WIDTH : 1];
+                    double a[WIDTH > 0 ? WIDTH : 1];
+#pragma unroll
+                    for (int s = 0; s < (WIDTH > 0 ? WIDTH : 1); ++s) {
+                        nb[s] = __ldg(K.nbr + s * n + c);
+                        a[s] = __ldg(K.val + s * n + c);
+                    }
+#pragma unroll
+                    for (int s = 0; s < (WIDTH > 0 ? WIDTH : 1); ++s)
+                        ap += a[s] * (__ldcg(z + nb[s]) + __ldcg(p_old + nb[s]) * beta);
+                } else {
+                    for (int s = 0; s < W; ++s) {
+                        const int nb = __ldg(K.nbr + s * n + c);
+                        ap += __ldg(K.val + s * n + c) * (__ldcg(z + nb) + __ldcg(p_old + nb) * beta);
+                    }
+                }
+                __stcg(q + c, ap);
+                loc[0] += pc * ap;
+            }
+            ok = grid_reduce<1>(ctl, partials, loc, 0u);
+            if (!ok) break;
+            if (threadIdx.x == 0) st.alpha = st.rz_old / loc[0];
+            __syncthreads();
+        }
+        {  // x += alpha p; r -= alpha q; z = M r; |r|, r.z
+            const double alpha = st.alpha;
+            double loc[2] = {0.0, 0.0};
+            for (int64_t c = t0; c < n; c += stride) {
+                const double pc = __ldcg(p_new + c);
+                __stcg(x + c, __ldcg(x + c) + alpha * pc);
+                const double rk = __ldcg(r + c) - alpha * __ldcg(q + c);
+                const double zk = inv_diag(K.diag, c, jac) * rk;
+                __stcg(r + c, rk);
+                __stcg(z + c, zk);
+                loc[0] = norm_acc(loc[0], rk, linf);
+                loc[1] += rk * zk;
+            }
+            ok = grid_reduce<2>(ctl, partials, loc, linf ? 1u : 0u);
+            if (!ok) break;
+            if (threadIdx.x == 0) {
+                const double fin = norm_fin(loc[0], linf);
+                st.final = fin;
+                if (fin < st.thresh) {
+                    st.done = 1;
+                    st.converged = 1;
+                    st.its = it;
+                    st.status = GF_OK;
+                } else if (!isfinite(fin)) {
+                    st.done = 1;
+                    st.its = it;
+                    st.status = GF_NONFINITE;
+                } else {
+                    st.beta = loc[1] / st.rz_old;
+                    st.rz_old = loc[1];
+                }
+            }
+            __syncthreads();
+        }
+        double* tmp = p_old;
+        p_old = p_new;
+        p_new = tmp;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        double* o = K.stats;
+        o[0] = st.r0;
+        o[1] = st.final;
+        o[2] = st.done ? st.its : K.max_iter;
+        o[3] = st.converged;
+        o[4] = ok ? st.status : GF_ERR_TIMEOUT;
+    }
+}
+
+// Mixed precision: FP32 inner Jacobi-PCG cycles inside FP64 iterative
+// refinement.  Each cycle starts from the true FP64 residual r = b - A x
+// (also the stopping test, |r| < max(atol, rtol |r0|) as in FP64), runs
+// FP32 CG on A d = r with FP64-accumulated dot products until the recurrence
+// residual falls below max(eta |r|, thresh / 2), then folds x += d in FP64.
+// The FP32 copy of the matrix is made once per solve.  WIDTH as in k_pcg1.
+constexpr int kMaxEll = 32;
+
+template <int WIDTH>
+__global__ void __launch_bounds__(kCgThreads, 4) k_pcg1_mixed(gf_krylov_t K) {
+    __shared__ CgState st;
+    __shared__ double s_rtrue, s_target;
+    __shared__ int s_cycle_done;
+    KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
+    double* partials = K.work + kCtlDoubles;
+    double* base = partials + kMaxBlocks * kMaxNV;
+    const int64_t n = K.n;
+    const int W = WIDTH > 0 ? WIDTH : K.width;
+    float* f = reinterpret_cast<float*>(base + n);
+    float* val32 = f;
+    float* inv32 = f + (int64_t)W * n;
+    float* r = inv32 + n;
+    float* z = r + n;
+    float* pa = z + n;
+    float* pb = pa + n;
+    float* q = pb + n;
+    float* d = q + n;
+    double* x = K.x;
+    const bool jac = K.jacobi != 0, linf = K.norm_inf != 0;
+    const int64_t t0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    bool ok = true;
+    int its = 0;
+
+    for (int64_t c = t0; c < n; c += stride) {
+        for (int s = 0; s < W; ++s) val32[s * n + c] = (float)__ldg(K.val + s * n + c);
+        inv32[c] = (float)inv_diag(K.diag, c, jac);
+    }
+    if (threadIdx.x == 0) {
+        st.its = 0;
+        st.converged = 0;
+        st.status = GF_MAX_ITER;
+        st.done = 0;
+    }
+    bool pending = false;
+    // max_outer inner cycles, each preceded by a true-residual evaluation,
+    // plus a final evaluation that verifies the last correction.
+    for (int cycle = 0; ok && cycle <= K.max_outer; ++cycle) {
+        {  // fold the pending correction, then the true residual in FP64
+            double loc[3] = {0.0, 0.0, 0.0};
+            if (pending) {
+                for (int64_t c = t0; c < n; c += stride) __stcg(x + c, __ldcg(x + c) + (double)__ldcg(d + c));
+                double dummy[1] = {0.0};
+                ok = grid_reduce<1>(ctl, partials, dummy, 0u);
+                if (!ok) break;
+                pending = false;
+            }
+            for (int64_t c = t0; c < n; c += stride) {
+                double ax = __ldg(K.diag + c) * __ldcg(x + c);
+                for (int s = 0; s < W; ++s) {
+                    const int nb = __ldg(K.nbr + s * n + c);
+                    ax += __ldg(K.val + s * n + c) * __ldcg(x + nb);
+                }
+                const double rk = __ldg(K.rhs + c) - ax;
+                const float r32 = (float)rk;
+                const float z32 = __ldcg(inv32 + c) * r32;
+                __stcg(r + c, r32);
+                __stcg(z + c, z32);
+                __stcg(pa + c, 0.0f);
+                __stcg(d + c, 0.0f);
+                loc[0] = norm_acc(loc[0], rk, linf);
+                loc[1] += (double)r32 * (double)z32;
+                loc[2] += rk * rk;
+            }
+            ok = grid_reduce<3>(ctl, partials, loc, linf ? 1u : 0u);
+            if (!ok) break;
+            if (threadIdx.x == 0) {
+                const double nr = norm_fin(loc[0], linf);
+                if (cycle == 0) {
+                    st.r0 = nr;
+                    st.thresh = fmax(K.atol, K.rtol * nr);
+                }
+                st.final = nr;
+                if (nr < st.thresh) {
+                    st.done = 1;
+                    st.converged = 1;
+                    st.status = GF_OK;
+                } else if (!isfinite(nr)) {
+                    st.done = 1;
+                    st.status = GF_NONFINITE;
+                }
+                st.rz_old = loc[1];
+                st.beta = 0.0;
+                s_rtrue = nr;
+                s_target = fmax(K.inner_eta * nr, 0.5 * st.thresh);
+                s_cycle_done = 0;
+            }
+            __syncthreads();
+            if (st.done || cycle == K.max_outer || its >= K.max_iter) break;
+        }
+        pending = true;
+        float* p_old = pa;
+        float* p_new = pb;
+        while (ok && !s_cycle_done && its < K.max_iter) {
+            ++its;
+            const float beta = (float)st.beta;
+            {
+                double loc[1] = {0.0};
+                for (int64_t c = t0; c < n; c += stride) {
+                    const float pc = __ldcg(z + c) + __ldcg(p_old + c) * beta;
+                    __stcg(p_new + c, pc);
+                    float ap = (float)__ldg(K.diag + c) * pc;
+                    if (WIDTH > 0) {
+                        int nb[WIDTH > 0 ? WIDTH : 1];
+                        float a[WIDTH > 0 ? WIDTH : 1];
+#pragma unroll
+                        for (int s = 0; s < (WIDTH > 0 ? WIDTH : 1); ++s) {
+                            nb[s] = __ldg(K.nbr + s * n + c);
+                            a[s] = __ldcg(val32 + s * n + c);
+                        }
+#pragma unroll
+                        for (int s = 0; s < (WIDTH > 0 ? WIDTH : 1); ++s)
+                            ap += a[s] * (__ldcg(z + nb[s]) + __ldcg(p_old + nb[s]) * beta);
+                    } else {
+                        for (int s = 0; s < W; ++s) {
+                            const int nb = __ldg(K.nbr + s * n + c);
+                            ap += __ldcg(val32 + s * n + c) * (__ldcg(z + nb) + __ldcg(p_old + nb) * beta);
+                        }
+                    }
+                    __stcg(q + c, ap);
+                    loc[0] += (double)pc * (double)ap;
+                }
+                ok = grid_reduce<1>(ctl, partials, loc, 0u);
+                if (!ok) break;
+                if (threadIdx.x == 0) st.alpha = st.rz_old / loc[0];
+                __syncthreads();
+            }
+            {
+                const float alpha = (float)st.alpha;
+                double loc[2] = {0.0, 0.0};
+                for (int64_t c = t0; c < n; c += stride) {
+                    const float pc = __ldcg(p_new + c);
+                    __stcg(d + c, __ldcg(d + c) + alpha * pc);
+                    const float rk = __ldcg(r + c) - alpha * __ldcg(q + c);
+                    const float zk = __ldcg(inv32 + c) * rk;
+                    __stcg(r + c, rk);
+                    __stcg(z + c, zk);
+                    loc[0] = norm_acc(loc[0], (double)rk, linf);
+                    loc[1] += (double)rk * (double)zk;
+                }
+                ok = grid_reduce<2>(ctl, partials, loc, linf ? 1u : 0u);
+                if (!ok) break;
+                if (threadIdx.x == 0) {
+                    const double nr = norm_fin(loc[0], linf);
+                    if (!(nr >= s_target) || !isfinite(nr)) {
+                        s_cycle_done = 1;
+                    } else {
+                        st.beta = loc[1] / st.rz_old;
+                        st.rz_old = loc[1];
+                    }
+                }
+                __syncthreads();
+            }
+            float* tmp = p_old;
+            p_old = p_new;
+            p_new = tmp;
+        }
+    }
+    if (ok && pending) {
+        // iteration budget spent inside a cycle: keep its correction
+        for (int64_t c = t0; c < n; c += stride) __stcg(x + c, __ldcg(x + c) + (double)__ldcg(d + c));
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        double* o = K.stats;
+        o[0] = st.r0;
+        o[1] = st.final;
+        o[2] = its;
+        o[3] = st.converged;
+        o[4] = ok ? st.status : GF_ERR_TIMEOUT;
     }
 }
 
@@ -643,7 +981,8 @@ __global__ void __launch_bounds__(kKThreads) k_bicgstab(gf_krylov_t K) {
 }
 
 template <class Kern>
-static int launch_persistent(Kern kern, const gf_krylov_t* k, void* stream, const char* what) {
+static int launch_persistent(Kern kern, const gf_krylov_t* k, void* stream, const char* what,
+                             int threads = kKThreads) {
     int dev = 0;
     cudaGetDevice(&dev);
     int sms = 0, coop = 0;
@@ -654,12 +993,12 @@ static int launch_persistent(Kern kern, const gf_krylov_t* k, void* stream, cons
         return GF_ERR_CUDA;
     }
     int per_sm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kKThreads, 0);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, 0);
     if (e != cudaSuccess || per_sm < 1) {
         set_error("%s: occupancy query failed: %s", what, cudaGetErrorString(e));
         return GF_ERR_CUDA;
     }
-    int64_t want = (k->n + kKThreads - 1) / kKThreads;
+    int64_t want = (k->n + threads - 1) / threads;
     int64_t cap = (int64_t)per_sm * sms;
     if (cap > kMaxBlocks) cap = kMaxBlocks;
     int grid = (int)(want < cap ? want : cap);
@@ -672,7 +1011,7 @@ static int launch_persistent(Kern kern, const gf_krylov_t* k, void* stream, cons
     }
     gf_krylov_t arg = *k;
     void* args[] = {&arg};
-    e = cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(kKThreads), args, 0, s);
+    e = cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(threads), args, 0, s);
     if (e != cudaSuccess) {
         set_error("%s: cooperative launch failed: %s", what, cudaGetErrorString(e));
         return GF_ERR_CUDA;
@@ -705,16 +1044,42 @@ using namespace gf;
 
 extern "C" {
 
-int64_t gf_krylov_workspace_size(int64_t n, int32_t ncomp, int32_t bicgstab) {
-    const int nvec = bicgstab ? 6 : 3;
+int64_t gf_krylov_workspace_size(int64_t n, int32_t ncomp, int32_t kind) {
+    // kind 2 + 100 * width: mixed-precision CG for an ELL of that width.
+    if (kind >= 2) {
+        const int64_t width = (kind - 2) / 100 > 0 ? (kind - 2) / 100 : kMaxEll;
+        const int64_t floats = (width + 7) * n;
+        return kCtlDoubles + (int64_t)kMaxBlocks * kMaxNV + n + (floats + 1) / 2 + 1;
+    }
+    const int bicgstab = kind == 1;
+    const int nvec = bicgstab ? 6 : (ncomp == 1 ? 5 : 3);
     return kCtlDoubles + (int64_t)kMaxBlocks * kMaxNV + (int64_t)nvec * ncomp * n;
 }
 
 int gf_pcg_solve(const gf_krylov_t* k, void* stream) {
-    if (!valid_krylov(k, 3, "gf_pcg_solve")) return GF_ERR_INVALID;
+    if (k != nullptr && k->mixed) {
+        if (k->ncomp != 1 || k->max_outer < 1 || k->width > kMaxEll) {
+            set_error("gf_pcg_solve: mixed precision needs one system, max_outer >= 1, width <= %d", kMaxEll);
+            return GF_ERR_INVALID;
+        }
+        if (!valid_krylov(k, 0, "gf_pcg_solve")) return GF_ERR_INVALID;
+        const int64_t need = gf_krylov_workspace_size(k->n, 1, 2 + 100 * k->width);
+        if (k->work_len < need) {
+            set_error("gf_pcg_solve: mixed workspace holds %lld doubles, %lld needed", (long long)k->work_len,
+                      (long long)need);
+            return GF_ERR_INVALID;
+        }
+        if (k->width == 6) return launch_persistent(k_pcg1_mixed<6>, k, stream, "gf_pcg_solve", kCgThreads);
+        return launch_persistent(k_pcg1_mixed<0>, k, stream, "gf_pcg_solve", kCgThreads);
+    }
+    if (k == nullptr || !valid_krylov(k, k->ncomp == 1 ? 5 : 3, "gf_pcg_solve")) {
+        if (k == nullptr) set_error("gf_pcg_solve: invalid arguments (null descriptor)");
+        return GF_ERR_INVALID;
+    }
     switch (k->ncomp) {
         case 1:
-            return launch_persistent(k_pcg<1>, k, stream, "gf_pcg_solve");
+            if (k->width == 6) return launch_persistent(k_pcg1<6>, k, stream, "gf_pcg_solve", kCgThreads);
+            return launch_persistent(k_pcg1<0>, k, stream, "gf_pcg_solve", kCgThreads);
         case 2:
             return launch_persistent(k_pcg<2>, k, stream, "gf_pcg_solve");
         default:

@@ -206,6 +206,14 @@ class SolverConfig(BaseModel, frozen=True):
     norm_type: NormType = NormType.L_2
     max_restart: int = 5
     log_interval: int = 25
+    # Extension (not in the reference schema; defaults keep its behaviour):
+    # ``inner_precision: float32`` runs CG's inner iterations in FP32 inside
+    # FP64 iterative refinement; the stopping test stays the FP64 true
+    # residual.  ``max_outer`` bounds the refinement cycles and
+    # ``inner_eta`` is the relative reduction of one FP32 cycle.
+    inner_precision: PrecisionType = PrecisionType.FLOAT64
+    max_outer: int = Field(default=10, ge=1)
+    inner_eta: float = Field(default=1e-4, gt=0.0, lt=1.0)
 
 
 class PotentialFlowConfig(BaseModel, frozen=True):

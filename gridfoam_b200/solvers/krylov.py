@@ -15,18 +15,21 @@ import ctypes
 import torch
 
 from gridfoam_b200._lib import GfKrylov, call, load, ptr, stream_ptr
-from gridfoam_b200.meta.config import NormType, PreconditionerType, SolverConfig
+from gridfoam_b200.meta.config import NormType, PrecisionType, PreconditionerType, SolverConfig
 from gridfoam_b200.solvers.base import LinearSolver, SolveResult, SolveStats, _StatsBuffer
 
 _WORKSPACES: dict[tuple, torch.Tensor] = {}
 
 
-def workspace(device: torch.device, n: int, ncomp: int, bicgstab: bool) -> torch.Tensor:
-    """Cached per-shape workspace (allocated once, reused by every solve)."""
-    key = (str(device), n, ncomp, bicgstab)
+def workspace(device: torch.device, n: int, ncomp: int, kind: int) -> torch.Tensor:
+    """Cached per-shape workspace (allocated once, reused by every solve).
+
+    ``kind``: 0 CG, 1 BiCGStab, ``2 + 100 * width`` mixed-precision CG.
+    """
+    key = (str(device), n, ncomp, kind)
     ws = _WORKSPACES.get(key)
     if ws is None:
-        size = load().gf_krylov_workspace_size(n, ncomp, int(bicgstab))
+        size = load().gf_krylov_workspace_size(n, ncomp, kind)
         ws = torch.empty(size, dtype=torch.float64, device=device)
         _WORKSPACES[key] = ws
     return ws
@@ -46,6 +49,9 @@ class DeviceKrylov(LinearSolver):
         self.max_restart = int(config.max_restart)
         self.norm_inf = config.norm_type == NormType.L_inf
         self.log_interval = config.log_interval
+        self.mixed = config.inner_precision == PrecisionType.FLOAT32
+        self.max_outer = int(config.max_outer)
+        self.inner_eta = float(config.inner_eta)
         self._stats_dev: dict[tuple, torch.Tensor] = {}
         # Optional list receiving (start event, end event, stats) per solve.
         self.profile_events: list | None = None
@@ -59,7 +65,9 @@ class DeviceKrylov(LinearSolver):
         if stats is None:
             stats = torch.zeros((nc, 5), dtype=torch.float64, device=grid.device)
             self._stats_dev[key] = stats
-        ws = workspace(grid.device, n, nc, self.bicgstab)
+        mixed = self.mixed and nc == 1 and not self.bicgstab
+        kind = (2 + 100 * grid.ell_width) if mixed else int(self.bicgstab)
+        ws = workspace(grid.device, n, nc, kind)
         k = GfKrylov()
         k.n = n
         k.width = grid.ell_width
@@ -78,6 +86,9 @@ class DeviceKrylov(LinearSolver):
         k.work = ptr(ws)
         k.work_len = ws.numel()
         k.stats = ptr(stats)
+        k.mixed = int(mixed)
+        k.max_outer = self.max_outer
+        k.inner_eta = self.inner_eta
         ev = None
         if self.profile_events is not None:
             ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))

@@ -388,3 +388,17 @@ ALL_CASES = {
     "channel_ffp": ffp_case,
     "ibplane": ibplane_case,
 }
+
+
+# Steps stored per golden case and the convection schemes dumped per case.
+STEPS = {"cavity8": 4, "pipe10x20": 3, "channel": 3, "channel_ffp": 3, "ibplane": 3}
+DIV_SCHEMES = [
+    "upwind",
+    "linear",
+    "vanleer",
+    "minmod",
+    "superbee",
+    "monotonized_central",
+    "limitedlinear",
+    "koren",
+]

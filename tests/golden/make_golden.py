@@ -46,18 +46,8 @@ from gridfoam.meta.enums import DomainBoundaryPatch  # noqa: E402
 from gridfoam.solvers.bicgstab import BiCGSTABSolver  # noqa: E402
 from gridfoam.solvers.cg import CGSolver  # noqa: E402
 
-from tests.golden.cases import ALL_CASES, build_mesh  # noqa: E402
+from tests.golden.cases import ALL_CASES, DIV_SCHEMES, STEPS, build_mesh  # noqa: E402
 
-DIV_SCHEMES = [
-    "upwind",
-    "linear",
-    "vanleer",
-    "minmod",
-    "superbee",
-    "monotonized_central",
-    "limitedlinear",
-    "koren",
-]
 
 
 class ParabolicInletBC(DirichletBC):
@@ -246,7 +236,6 @@ def operator_dumps(grid: AxisProjectedGrid, algo) -> dict:
     return out
 
 
-STEPS = {"cavity8": 4, "pipe10x20": 3, "channel": 3, "channel_ffp": 3, "ibplane": 3}
 
 
 def main() -> None:

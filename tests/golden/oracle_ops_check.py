@@ -11,7 +11,7 @@ import numpy as np
 
 from oracle import ops, solvers
 from oracle.algorithms import needs_reference_value, set_reference_value
-from tests.golden.make_golden import DIV_SCHEMES, STEPS
+from tests.golden.cases import DIV_SCHEMES, STEPS
 from tests.golden.oracle_harness import load_golden, oracle_case
 
 

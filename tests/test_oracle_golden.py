@@ -15,7 +15,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from tests.golden.make_golden import STEPS
+from tests.golden.cases import STEPS
 from tests.golden.oracle_harness import load_golden, oracle_case
 from tests.golden.oracle_ops_check import oracle_operator_outputs
 
