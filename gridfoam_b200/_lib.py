@@ -144,6 +144,10 @@ class GfKrylov(ctypes.Structure):
         ("mixed", I32),
         ("max_outer", I32),
         ("inner_eta", F64),
+        ("stride_y", I64),
+        ("stride_z", I64),
+        ("symmetric", I32),
+        ("reserved2", I32),
     ]
 
 

@@ -357,7 +357,7 @@ class _PressureVelocity:
             solver = self._solvers[self.p.name]
             if final_solver is not None and corr == self.n_non_orthogonal_correctors:
                 solver = final_solver
-            stats = solver.solve_arrays(g, d, v, src, self.p.store)
+            stats = solver.solve_arrays(g, d, v, src, self.p.store, symmetric=True)
         return stats, first_res, last_res
 
     def _correct_phi(self) -> None:

@@ -85,9 +85,11 @@ class AxisProjectedGrid:
         self._device = torch.device(device)
         self._cellfields: dict = {}
         self._facefields: dict = {}
+        self._mesh_ref = fluxel_mesh
         self.host = self._build_host(fluxel_mesh)
         self._build_ell()
         self._upload()
+        self._mesh_ref = None
 
     # ------------------------------------------------------------------
     # host set-up
@@ -254,9 +256,40 @@ class AxisProjectedGrid:
         pos_owner[face_of[side_of == 0]] = p_int[side_of == 0]
         pos_neigh[face_of[side_of == 1]] = p_int[side_of == 1]
         self._ell_width = W
+        self.box_strides = self._detect_box(ell_code, ell_nbr, W)
         h.extra.update(
             ell_code=ell_code, ell_nbr=ell_nbr, face_pos_owner=pos_owner, face_pos_neigh=pos_neigh
         )
+
+    def _detect_box(self, ell_code: np.ndarray, ell_nbr: np.ndarray, W: int) -> tuple[int, int] | None:
+        """``(stride_y, stride_z)`` when the ELL is a uniform lexicographic box.
+
+        Slot ``2a + side`` of cell ``c`` then couples ``c -/+ stride_a``
+        (``stride_x = 1``) or is a boundary slot; the Krylov kernels use the
+        implicit neighbours and skip the index table.
+        """
+        res = getattr(self._mesh_ref, "resolution", None)
+        if res is None or W != 6:
+            return None
+        nx, ny, nz = (int(v) for v in res)
+        C = self._num_cells
+        if nx * ny * nz != C:
+            return None
+        cells = np.arange(C, dtype=np.int64)
+        strides = (1, nx, nx * ny)
+        F = self._num_internal_faces
+        for a, st in enumerate(strides):
+            for side, sign in ((0, -1), (1, 1)):
+                slot = 2 * a + side
+                code = ell_code[slot * C : (slot + 1) * C]
+                nbr = ell_nbr[slot * C : (slot + 1) * C]
+                internal = (code >= 0) & (code < 2 * F)
+                if np.any(code < 0):
+                    return None
+                want = np.where(internal, cells + sign * st, cells)
+                if not np.array_equal(nbr, want):
+                    return None
+        return (nx, nx * ny)
 
     def _upload(self) -> None:
         h = self.host

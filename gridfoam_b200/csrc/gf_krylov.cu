@@ -306,15 +306,88 @@ __global__ void __launch_bounds__(kKThreads) k_pcg(gf_krylov_t K) {
     }
 }
 
+// Row products A_c . g for the single-system CG kernels.  EllRows gathers
+// through the neighbour table; BoxRows uses implicit neighbours of a
+// uniform lexicographic box (slot order -x,+x,-y,+y,-z,+z; the coefficient
+// of a boundary slot is zero, so clamped neighbour indices are harmless).
+// With SYM the "-" coefficient of cell c is the "+" coefficient of
+// c - stride, so only three coefficient arrays are read.  T is the storage
+// type of the coefficients; COMPACT means the array holds only the needed
+// slots (3 for SYM) instead of the 6-slot ELL layout.
+// Coefficient loads: FP64 coefficients are kernel inputs (read-only path);
+// the FP32 copies are written inside the kernel, so they bypass L1.
+__device__ __forceinline__ double ld_coef(const double* p) { return __ldg(p); }
+__device__ __forceinline__ float ld_coef(const float* p) { return __ldcg(p); }
+
+template <typename T, int WIDTH>
+struct EllRows {
+    const T* val;
+    const int32_t* nbr;
+    int64_t n;
+    int w;
+    template <typename A, class G>
+    __device__ __forceinline__ A apply(int64_t c, A dc, const G& g) const {
+        A acc = dc * g(c);
+        if (WIDTH > 0) {
+            int nb[WIDTH > 0 ? WIDTH : 1];
+            A a[WIDTH > 0 ? WIDTH : 1];
+#pragma unroll
+            for (int s = 0; s < (WIDTH > 0 ? WIDTH : 1); ++s) {
+                nb[s] = __ldg(nbr + s * n + c);
+                a[s] = (A)ld_coef(val + s * n + c);
+            }
+#pragma unroll
+            for (int s = 0; s < (WIDTH > 0 ? WIDTH : 1); ++s) acc += a[s] * g(nb[s]);
+        } else {
+            for (int s = 0; s < w; ++s) acc += (A)ld_coef(val + s * n + c) * g(__ldg(nbr + s * n + c));
+        }
+        return acc;
+    }
+};
+
+template <typename T, bool SYM, bool COMPACT>
+struct BoxRows {
+    const T* val;
+    int64_t n, sy, sz;
+    __device__ __forceinline__ int64_t plus_slot(int a) const { return COMPACT ? a : 2 * a + 1; }
+    template <typename A, class G>
+    __device__ __forceinline__ A apply(int64_t c, A dc, const G& g) const {
+        const int64_t st[3] = {1, sy, sz};
+        A ap[3], am[3];
+        int64_t ip[3], im[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const int64_t s = st[a];
+            const T* pv = val + plus_slot(a) * n;
+            ap[a] = (A)ld_coef(pv + c);
+            if (SYM) {
+                am[a] = c >= s ? (A)ld_coef(pv + c - s) : (A)0;
+            } else {
+                am[a] = (A)ld_coef(val + (2 * a) * n + c);
+            }
+            im[a] = c >= s ? c - s : c;
+            ip[a] = c + s < n ? c + s : c;
+        }
+        // Same accumulation order as the ELL slots (-x, +x, -y, +y, -z, +z),
+        // so both layouts give bitwise identical products.
+        A acc = dc * g(c);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            acc += am[a] * g(im[a]);
+            acc += ap[a] * g(ip[a]);
+        }
+        return acc;
+    }
+};
+
 // Single-system Jacobi-PCG with the direction update fused into the SpMV
-// pass: p_new = z + beta p_old is stored for the own cell and recomputed
+// pass: p_new = z + p_old beta is stored for the own cell and recomputed
 // (bitwise identically) at the neighbours, so an iteration needs two grid
-// reductions (p.Ap, then |r| and r.z) instead of three.  WIDTH > 0 fixes
-// the ELL width at compile time so the slot loop unrolls.
+// reductions (p.Ap, then |r| and r.z) instead of three.
 constexpr int kCgThreads = 256;
 
-template <int WIDTH>
-__global__ void __launch_bounds__(kCgThreads, 4) k_pcg1(gf_krylov_t K) {
+template <class Rows>
+__device__ void pcg1_body(const gf_krylov_t& K, const Rows& rows) {
     __shared__ CgState st;
     KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
     double* partials = K.work + kCtlDoubles;
@@ -326,28 +399,15 @@ __global__ void __launch_bounds__(kCgThreads, 4) k_pcg1(gf_krylov_t K) {
     double* pb = vec + 3 * n;
     double* q = vec + 4 * n;
     double* x = K.x;
-    const int W = WIDTH > 0 ? WIDTH : K.width;
     const bool jac = K.jacobi != 0, linf = K.norm_inf != 0;
     const int64_t t0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     bool ok = true;
     {
         double loc[2] = {0.0, 0.0};
+        auto gx = [&](int64_t i) { return __ldcg(x + i); };
         for (int64_t c = t0; c < n; c += stride) {
-            double ax = __ldg(K.diag + c) * __ldcg(x + c);
-#pragma unroll
-            for (int s = 0; s < (WIDTH > 0 ? WIDTH : 1); ++s) {
-                if (WIDTH > 0) {
-                    const int nb = __ldg(K.nbr + s * n + c);
-                    ax += __ldg(K.val + s * n + c) * __ldcg(x + nb);
-                }
-            }
-            if (WIDTH == 0) {
-                for (int s = 0; s < W; ++s) {
-                    const int nb = __ldg(K.nbr + s * n + c);
-                    ax += __ldg(K.val + s * n + c) * __ldcg(x + nb);
-                }
-            }
+            const double ax = rows.apply(c, __ldg(K.diag + c), gx);
             const double rk = __ldg(K.rhs + c) - ax;
             const double zk = inv_diag(K.diag, c, jac) * rk;
             __stcg(r + c, rk);
@@ -385,27 +445,11 @@ __global__ void __launch_bounds__(kCgThreads, 4) k_pcg1(gf_krylov_t K) {
         const double beta = st.beta;
         {  // p_new = z + p_old beta; q = A p_new; p_new . q
             double loc[1] = {0.0};
+            auto gp = [&](int64_t i) { return __ldcg(z + i) + __ldcg(p_old + i) * beta; };
             for (int64_t c = t0; c < n; c += stride) {
-                const double pc = __ldcg(z + c) + __ldcg(p_old + c) * beta;
+                const double pc = gp(c);
                 __stcg(p_new + c, pc);
-                double ap = __ldg(K.diag + c) * pc;
-                if (WIDTH > 0) {
-                    int nb[WIDTH > 0 ? WIDTH : 1];
-                    double a[WIDTH > 0 ? WIDTH : 1];
-#pragma unroll
-                    for (int s = 0; s < (WIDTH > 0 ? WIDTH : 1); ++s) {
-                        nb[s] = __ldg(K.nbr + s * n + c);
-                        a[s] = __ldg(K.val + s * n + c);
-                    }
-#pragma unroll
-                    for (int s = 0; s < (WIDTH > 0 ? WIDTH : 1); ++s)
-                        ap += a[s] * (__ldcg(z + nb[s]) + __ldcg(p_old + nb[s]) * beta);
-                } else {
-                    for (int s = 0; s < W; ++s) {
-                        const int nb = __ldg(K.nbr + s * n + c);
-                        ap += __ldg(K.val + s * n + c) * (__ldcg(z + nb) + __ldcg(p_old + nb) * beta);
-                    }
-                }
+                const double ap = rows.apply(c, __ldg(K.diag + c), gp);
                 __stcg(q + c, ap);
                 loc[0] += pc * ap;
             }
@@ -462,27 +506,40 @@ __global__ void __launch_bounds__(kCgThreads, 4) k_pcg1(gf_krylov_t K) {
     }
 }
 
+template <int WIDTH>
+__global__ void __launch_bounds__(kCgThreads, 4) k_pcg1(gf_krylov_t K) {
+    EllRows<double, WIDTH> rows{K.val, K.nbr, K.n, K.width};
+    pcg1_body(K, rows);
+}
+
+template <bool SYM>
+__global__ void __launch_bounds__(kCgThreads, 4) k_pcg1_box(gf_krylov_t K) {
+    BoxRows<double, SYM, false> rows{K.val, K.n, K.stride_y, K.stride_z};
+    pcg1_body(K, rows);
+}
+
 // Mixed precision: FP32 inner Jacobi-PCG cycles inside FP64 iterative
 // refinement.  Each cycle starts from the true FP64 residual r = b - A x
 // (also the stopping test, |r| < max(atol, rtol |r0|) as in FP64), runs
 // FP32 CG on A d = r with FP64-accumulated dot products until the recurrence
 // residual falls below max(eta |r|, thresh / 2), then folds x += d in FP64.
-// The FP32 copy of the matrix is made once per solve.  WIDTH as in k_pcg1.
+// The FP32 copy of the matrix coefficients (all ELL slots, or the three "+"
+// slots of a symmetric box) is made once per solve.
 constexpr int kMaxEll = 32;
 
-template <int WIDTH>
-__global__ void __launch_bounds__(kCgThreads, 4) k_pcg1_mixed(gf_krylov_t K) {
+template <class Rows64, class Rows32>
+__device__ void pcg1_mixed_body(const gf_krylov_t& K, const Rows64& rows64, Rows32 rows32, int ncoef) {
     __shared__ CgState st;
-    __shared__ double s_rtrue, s_target;
+    __shared__ double s_target;
     __shared__ int s_cycle_done;
     KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
     double* partials = K.work + kCtlDoubles;
     double* base = partials + kMaxBlocks * kMaxNV;
     const int64_t n = K.n;
-    const int W = WIDTH > 0 ? WIDTH : K.width;
     float* f = reinterpret_cast<float*>(base + n);
     float* val32 = f;
-    float* inv32 = f + (int64_t)W * n;
+    float* diag32 = f + (int64_t)ncoef * n;
+    float* inv32 = diag32 + n;
     float* r = inv32 + n;
     float* z = r + n;
     float* pa = z + n;
@@ -493,12 +550,18 @@ __global__ void __launch_bounds__(kCgThreads, 4) k_pcg1_mixed(gf_krylov_t K) {
     const bool jac = K.jacobi != 0, linf = K.norm_inf != 0;
     const int64_t t0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const bool sym_box = K.stride_y > 0 && K.symmetric;
     bool ok = true;
     int its = 0;
+    rows32.val = val32;
 
     for (int64_t c = t0; c < n; c += stride) {
-        for (int s = 0; s < W; ++s) val32[s * n + c] = (float)__ldg(K.val + s * n + c);
-        inv32[c] = (float)inv_diag(K.diag, c, jac);
+        for (int s = 0; s < ncoef; ++s) {
+            const int64_t src = sym_box ? (2 * s + 1) : s;
+            __stcg(val32 + s * n + c, (float)__ldg(K.val + src * n + c));
+        }
+        __stcg(diag32 + c, (float)__ldg(K.diag + c));
+        __stcg(inv32 + c, (float)inv_diag(K.diag, c, jac));
     }
     if (threadIdx.x == 0) {
         st.its = 0;
@@ -511,20 +574,18 @@ __global__ void __launch_bounds__(kCgThreads, 4) k_pcg1_mixed(gf_krylov_t K) {
     // plus a final evaluation that verifies the last correction.
     for (int cycle = 0; ok && cycle <= K.max_outer; ++cycle) {
         {  // fold the pending correction, then the true residual in FP64
-            double loc[3] = {0.0, 0.0, 0.0};
+            double loc[2] = {0.0, 0.0};
             if (pending) {
                 for (int64_t c = t0; c < n; c += stride) __stcg(x + c, __ldcg(x + c) + (double)__ldcg(d + c));
-                double dummy[1] = {0.0};
-                ok = grid_reduce<1>(ctl, partials, dummy, 0u);
-                if (!ok) break;
                 pending = false;
             }
+            // The barrier also publishes the FP32 coefficients (cycle 0).
+            double dummy[1] = {0.0};
+            ok = grid_reduce<1>(ctl, partials, dummy, 0u);
+            if (!ok) break;
+            auto gx = [&](int64_t i) { return __ldcg(x + i); };
             for (int64_t c = t0; c < n; c += stride) {
-                double ax = __ldg(K.diag + c) * __ldcg(x + c);
-                for (int s = 0; s < W; ++s) {
-                    const int nb = __ldg(K.nbr + s * n + c);
-                    ax += __ldg(K.val + s * n + c) * __ldcg(x + nb);
-                }
+                const double ax = rows64.apply(c, __ldg(K.diag + c), gx);
                 const double rk = __ldg(K.rhs + c) - ax;
                 const float r32 = (float)rk;
                 const float z32 = __ldcg(inv32 + c) * r32;
@@ -534,9 +595,8 @@ __global__ void __launch_bounds__(kCgThreads, 4) k_pcg1_mixed(gf_krylov_t K) {
                 __stcg(d + c, 0.0f);
                 loc[0] = norm_acc(loc[0], rk, linf);
                 loc[1] += (double)r32 * (double)z32;
-                loc[2] += rk * rk;
             }
-            ok = grid_reduce<3>(ctl, partials, loc, linf ? 1u : 0u);
+            ok = grid_reduce<2>(ctl, partials, loc, linf ? 1u : 0u);
             if (!ok) break;
             if (threadIdx.x == 0) {
                 const double nr = norm_fin(loc[0], linf);
@@ -555,7 +615,6 @@ __global__ void __launch_bounds__(kCgThreads, 4) k_pcg1_mixed(gf_krylov_t K) {
                 }
                 st.rz_old = loc[1];
                 st.beta = 0.0;
-                s_rtrue = nr;
                 s_target = fmax(K.inner_eta * nr, 0.5 * st.thresh);
                 s_cycle_done = 0;
             }
@@ -570,27 +629,11 @@ __global__ void __launch_bounds__(kCgThreads, 4) k_pcg1_mixed(gf_krylov_t K) {
             const float beta = (float)st.beta;
             {
                 double loc[1] = {0.0};
+                auto gp = [&](int64_t i) { return __ldcg(z + i) + __ldcg(p_old + i) * beta; };
                 for (int64_t c = t0; c < n; c += stride) {
-                    const float pc = __ldcg(z + c) + __ldcg(p_old + c) * beta;
+                    const float pc = gp(c);
                     __stcg(p_new + c, pc);
-                    float ap = (float)__ldg(K.diag + c) * pc;
-                    if (WIDTH > 0) {
-                        int nb[WIDTH > 0 ? WIDTH : 1];
-                        float a[WIDTH > 0 ? WIDTH : 1];
-#pragma unroll
-                        for (int s = 0; s < (WIDTH > 0 ? WIDTH : 1); ++s) {
-                            nb[s] = __ldg(K.nbr + s * n + c);
-                            a[s] = __ldcg(val32 + s * n + c);
-                        }
-#pragma unroll
-                        for (int s = 0; s < (WIDTH > 0 ? WIDTH : 1); ++s)
-                            ap += a[s] * (__ldcg(z + nb[s]) + __ldcg(p_old + nb[s]) * beta);
-                    } else {
-                        for (int s = 0; s < W; ++s) {
-                            const int nb = __ldg(K.nbr + s * n + c);
-                            ap += __ldcg(val32 + s * n + c) * (__ldcg(z + nb) + __ldcg(p_old + nb) * beta);
-                        }
-                    }
+                    const float ap = rows32.apply(c, __ldcg(diag32 + c), gp);
                     __stcg(q + c, ap);
                     loc[0] += (double)pc * (double)ap;
                 }
@@ -642,6 +685,20 @@ __global__ void __launch_bounds__(kCgThreads, 4) k_pcg1_mixed(gf_krylov_t K) {
         o[3] = st.converged;
         o[4] = ok ? st.status : GF_ERR_TIMEOUT;
     }
+}
+
+template <int WIDTH>
+__global__ void __launch_bounds__(kCgThreads, 4) k_pcg1_mixed(gf_krylov_t K) {
+    EllRows<double, WIDTH> rows64{K.val, K.nbr, K.n, K.width};
+    EllRows<float, WIDTH> rows32{nullptr, K.nbr, K.n, K.width};
+    pcg1_mixed_body(K, rows64, rows32, K.width);
+}
+
+template <bool SYM>
+__global__ void __launch_bounds__(kCgThreads, 4) k_pcg1_mixed_box(gf_krylov_t K) {
+    BoxRows<double, SYM, false> rows64{K.val, K.n, K.stride_y, K.stride_z};
+    BoxRows<float, SYM, true> rows32{nullptr, K.n, K.stride_y, K.stride_z};
+    pcg1_mixed_body(K, rows64, rows32, SYM ? 3 : 6);
 }
 
 // BiCGStab per-component modes.
@@ -1048,7 +1105,7 @@ int64_t gf_krylov_workspace_size(int64_t n, int32_t ncomp, int32_t kind) {
     // kind 2 + 100 * width: mixed-precision CG for an ELL of that width.
     if (kind >= 2) {
         const int64_t width = (kind - 2) / 100 > 0 ? (kind - 2) / 100 : kMaxEll;
-        const int64_t floats = (width + 7) * n;
+        const int64_t floats = (width + 8) * n;
         return kCtlDoubles + (int64_t)kMaxBlocks * kMaxNV + n + (floats + 1) / 2 + 1;
     }
     const int bicgstab = kind == 1;
@@ -1057,7 +1114,16 @@ int64_t gf_krylov_workspace_size(int64_t n, int32_t ncomp, int32_t kind) {
 }
 
 int gf_pcg_solve(const gf_krylov_t* k, void* stream) {
-    if (k != nullptr && k->mixed) {
+    if (k == nullptr) {
+        set_error("gf_pcg_solve: invalid arguments (null descriptor)");
+        return GF_ERR_INVALID;
+    }
+    const bool box = k->stride_y > 0;
+    if (box && (k->width != 6 || k->stride_z < k->stride_y || k->stride_y < 1)) {
+        set_error("gf_pcg_solve: a box layout needs width 6 and strides 1 <= stride_y <= stride_z");
+        return GF_ERR_INVALID;
+    }
+    if (k->mixed) {
         if (k->ncomp != 1 || k->max_outer < 1 || k->width > kMaxEll) {
             set_error("gf_pcg_solve: mixed precision needs one system, max_outer >= 1, width <= %d", kMaxEll);
             return GF_ERR_INVALID;
@@ -1069,15 +1135,17 @@ int gf_pcg_solve(const gf_krylov_t* k, void* stream) {
                       (long long)need);
             return GF_ERR_INVALID;
         }
+        if (box && k->symmetric)
+            return launch_persistent(k_pcg1_mixed_box<true>, k, stream, "gf_pcg_solve", kCgThreads);
+        if (box) return launch_persistent(k_pcg1_mixed_box<false>, k, stream, "gf_pcg_solve", kCgThreads);
         if (k->width == 6) return launch_persistent(k_pcg1_mixed<6>, k, stream, "gf_pcg_solve", kCgThreads);
         return launch_persistent(k_pcg1_mixed<0>, k, stream, "gf_pcg_solve", kCgThreads);
     }
-    if (k == nullptr || !valid_krylov(k, k->ncomp == 1 ? 5 : 3, "gf_pcg_solve")) {
-        if (k == nullptr) set_error("gf_pcg_solve: invalid arguments (null descriptor)");
-        return GF_ERR_INVALID;
-    }
+    if (!valid_krylov(k, k->ncomp == 1 ? 5 : 3, "gf_pcg_solve")) return GF_ERR_INVALID;
     switch (k->ncomp) {
         case 1:
+            if (box && k->symmetric) return launch_persistent(k_pcg1_box<true>, k, stream, "gf_pcg_solve", kCgThreads);
+            if (box) return launch_persistent(k_pcg1_box<false>, k, stream, "gf_pcg_solve", kCgThreads);
             if (k->width == 6) return launch_persistent(k_pcg1<6>, k, stream, "gf_pcg_solve", kCgThreads);
             return launch_persistent(k_pcg1<0>, k, stream, "gf_pcg_solve", kCgThreads);
         case 2:

@@ -57,8 +57,12 @@ class DeviceKrylov(LinearSolver):
         self.profile_events: list | None = None
 
     def solve_arrays(self, grid, diag: torch.Tensor, val: torch.Tensor, rhs: torch.Tensor,
-                     x: torch.Tensor) -> tuple[SolveStats, ...]:
-        """Solve in place: ``x [ncomp, C]`` holds the guess and gets the solution."""
+                     x: torch.Tensor, *, symmetric: bool = False) -> tuple[SolveStats, ...]:
+        """Solve in place: ``x [ncomp, C]`` holds the guess and gets the solution.
+
+        ``symmetric`` declares that ``A`` is symmetric (the pressure system),
+        which lets CG on a uniform box read only three coefficient arrays.
+        """
         nc, n = rhs.shape
         key = (str(grid.device), nc)
         stats = self._stats_dev.get(key)
@@ -89,6 +93,10 @@ class DeviceKrylov(LinearSolver):
         k.mixed = int(mixed)
         k.max_outer = self.max_outer
         k.inner_eta = self.inner_eta
+        box = getattr(grid, "box_strides", None)
+        if box is not None and not self.bicgstab and nc == 1:
+            k.stride_y, k.stride_z = box
+            k.symmetric = int(symmetric)
         ev = None
         if self.profile_events is not None:
             ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))

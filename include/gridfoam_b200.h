@@ -181,6 +181,12 @@ typedef struct gf_krylov {
                              refinement (CG, one system); 0: FP64 throughout */
     int32_t max_outer;    /* refinement cycles allowed when mixed (>= 1) */
     double inner_eta;     /* inner FP32 cycle stops at eta * |r_true| */
+    int64_t stride_y;     /* > 0: the ELL is a uniform lexicographic box with
+                             slots -x,+x,-y,+y,-z,+z, so neighbours are
+                             c -+ 1, c -+ stride_y, c -+ stride_z (nbr unread) */
+    int64_t stride_z;
+    int32_t symmetric;    /* 1 (box only): A is symmetric, only + slots read */
+    int32_t reserved2;
 } gf_krylov_t;
 
 const char* gf_last_error(void);

@@ -230,3 +230,34 @@ def test_mixed_precision_pcg_meets_fp64_criterion():
         thresh = max(tol, rel_tol * s64[0].initial_residual)
         assert float(torch.linalg.vector_norm(r)) < thresh
         assert abs(s32[0].initial_residual - s64[0].initial_residual) <= 1e-12 * s64[0].initial_residual
+
+
+def test_box_layout_matches_ell_layout():
+    """On a uniform box, CG with implicit neighbours (symmetric three-array
+    coefficient reads) gives the same solve as the generic ELL path."""
+    from gridfoam_b200.fv import fvm
+    from gridfoam_b200.meta.config import SolverConfig
+    from gridfoam_b200.solvers.krylov import CGSolver
+
+    from tests.golden.cases import pipe_case
+
+    _, _, grid, algo = device_case(case_def=pipe_case(16, 32))
+    assert grid.box_strides == (16, 256)
+    gamma = torch.linspace(0.2, 0.4, grid.num_cells, dtype=torch.float64, device="cuda")
+    A = -fvm.laplacian(gamma, algo.p)
+    gen = torch.Generator(device="cpu").manual_seed(2)
+    rhs = torch.randn((1, grid.num_cells), generator=gen, dtype=torch.float64).cuda()
+    for precision in ("float64", "float32"):
+        cfg = SolverConfig(method="cg", preconditioner="jacobi", tolerance=1e-10, rel_tolerance=0.0,
+                           max_iter=4000, inner_precision=precision)
+        x_box = torch.zeros_like(rhs)
+        s_box = CGSolver(cfg).solve_arrays(grid, A.diag_store, A.val, rhs, x_box, symmetric=True)
+        strides, grid.box_strides = grid.box_strides, None
+        try:
+            x_ell = torch.zeros_like(rhs)
+            s_ell = CGSolver(cfg).solve_arrays(grid, A.diag_store, A.val, rhs, x_ell)
+        finally:
+            grid.box_strides = strides
+        assert s_box[0].converged and s_ell[0].converged
+        assert s_box[0].iterations == s_ell[0].iterations
+        torch.testing.assert_close(x_box, x_ell, rtol=0, atol=0)
