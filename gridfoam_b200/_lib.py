@@ -147,7 +147,7 @@ class GfKrylov(ctypes.Structure):
         ("stride_y", I64),
         ("stride_z", I64),
         ("symmetric", I32),
-        ("reserved2", I32),
+        ("block_cap", I32),
     ]
 
 

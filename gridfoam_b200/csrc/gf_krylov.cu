@@ -349,7 +349,8 @@ template <typename T, bool SYM, bool COMPACT>
 struct BoxRows {
     const T* val;
     int64_t n, sy, sz;
-    __device__ __forceinline__ int64_t plus_slot(int a) const { return COMPACT ? a : 2 * a + 1; }
+    // COMPACT arrays hold only the three '+' slots, which only SYM uses.
+    __device__ __forceinline__ int64_t plus_slot(int a) const { return (COMPACT && SYM) ? a : 2 * a + 1; }
     template <typename A, class G>
     __device__ __forceinline__ A apply(int64_t c, A dc, const G& g) const {
         const int64_t st[3] = {1, sy, sz};
@@ -697,7 +698,7 @@ __global__ void __launch_bounds__(kCgThreads, 4) k_pcg1_mixed(gf_krylov_t K) {
 template <bool SYM>
 __global__ void __launch_bounds__(kCgThreads, 4) k_pcg1_mixed_box(gf_krylov_t K) {
     BoxRows<double, SYM, false> rows64{K.val, K.n, K.stride_y, K.stride_z};
-    BoxRows<float, SYM, true> rows32{nullptr, K.n, K.stride_y, K.stride_z};
+    BoxRows<float, SYM, SYM> rows32{nullptr, K.n, K.stride_y, K.stride_z};
     pcg1_mixed_body(K, rows64, rows32, SYM ? 3 : 6);
 }
 
@@ -1058,6 +1059,7 @@ static int launch_persistent(Kern kern, const gf_krylov_t* k, void* stream, cons
     int64_t want = (k->n + threads - 1) / threads;
     int64_t cap = (int64_t)per_sm * sms;
     if (cap > kMaxBlocks) cap = kMaxBlocks;
+    if (k->block_cap > 0 && k->block_cap < cap) cap = k->block_cap;
     int grid = (int)(want < cap ? want : cap);
     if (grid < 1) grid = 1;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);

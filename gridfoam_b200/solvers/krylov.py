@@ -55,6 +55,8 @@ class DeviceKrylov(LinearSolver):
         self._stats_dev: dict[tuple, torch.Tensor] = {}
         # Optional list receiving (start event, end event, stats) per solve.
         self.profile_events: list | None = None
+        # Upper bound on persistent blocks (0: one wave at full occupancy).
+        self.block_cap = 0
 
     def solve_arrays(self, grid, diag: torch.Tensor, val: torch.Tensor, rhs: torch.Tensor,
                      x: torch.Tensor, *, symmetric: bool = False) -> tuple[SolveStats, ...]:
@@ -93,6 +95,7 @@ class DeviceKrylov(LinearSolver):
         k.mixed = int(mixed)
         k.max_outer = self.max_outer
         k.inner_eta = self.inner_eta
+        k.block_cap = int(self.block_cap)
         box = getattr(grid, "box_strides", None)
         if box is not None and not self.bicgstab and nc == 1:
             k.stride_y, k.stride_z = box

@@ -186,7 +186,7 @@ typedef struct gf_krylov {
                              c -+ 1, c -+ stride_y, c -+ stride_z (nbr unread) */
     int64_t stride_z;
     int32_t symmetric;    /* 1 (box only): A is symmetric, only + slots read */
-    int32_t reserved2;
+    int32_t block_cap;    /* > 0: at most this many persistent blocks (tuning) */
 } gf_krylov_t;
 
 const char* gf_last_error(void);
