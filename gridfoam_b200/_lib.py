@@ -148,6 +148,8 @@ class GfKrylov(ctypes.Structure):
         ("stride_z", I64),
         ("symmetric", I32),
         ("block_cap", I32),
+        ("variant", I32),
+        ("reserved3", I32),
     ]
 
 

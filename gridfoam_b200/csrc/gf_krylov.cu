@@ -13,10 +13,11 @@
 namespace gf {
 
 constexpr int kKThreads = 512;
+constexpr int kCgThreads = 256;
 constexpr int kMaxBlocks = 1024;
 constexpr int kMaxNV = 16;
 constexpr int kCtlDoubles = 32;
-constexpr long long kSpinLimit = 20000000LL;  // x ~50 ns polls: about a second
+constexpr long long kSpinLimit = 30000000LL;  // x ~40 ns polls: about a second
 
 struct KCtl {
     unsigned int count;
@@ -43,10 +44,11 @@ __device__ __forceinline__ double inv_diag(const double* __restrict__ diag, int6
 // Grid-wide reduction of NV values per thread (sum, or max where maxmask
 // has the bit set), fused with the grid barrier.  Returns false when the
 // barrier wait expired.
-template <int NV>
+template <int NV, int THREADS = kKThreads>
 __device__ bool grid_reduce(KCtl* ctl, double* partials, double (&v)[NV], unsigned maxmask) {
     __shared__ double sm[kMaxNV * 32];
-    __shared__ int s_last;
+    __shared__ double s_res[kMaxNV];
+    __shared__ int s_last, s_err;
     __shared__ unsigned s_gen;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
@@ -67,51 +69,85 @@ __device__ bool grid_reduce(KCtl* ctl, double* partials, double (&v)[NV], unsign
         for (int w = 1; w < nw; ++w) x = mx ? nmax(x, sm[j * 32 + w]) : x + sm[j * 32 + w];
         __stcg(partials + (int64_t)blockIdx.x * NV + j, x);
     }
-    __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) {
+        // Release: the CTA barrier orders every thread's writes of this phase
+        // before this fence, which orders them before the arrival.
+        __threadfence();
         const unsigned gen = vload(&ctl->gen);
         const unsigned prev = atomicAdd(&ctl->count, 1u);
         s_gen = gen;
         s_last = (prev == gridDim.x - 1);
+        s_err = 0;
     }
     __syncthreads();
     if (s_last) {
-        for (int j = warp; j < NV; j += nw) {
-            const bool mx = (maxmask >> j) & 1u;
-            double x = 0.0;
-            for (int b = lane; b < (int)gridDim.x; b += 32) {
-                const double y = __ldcg(partials + (int64_t)b * NV + j);
-                x = mx ? nmax(x, y) : x + y;
-            }
-            for (int o = 16; o > 0; o >>= 1) {
-                const double y = __shfl_xor_sync(0xffffffffu, x, o);
-                x = mx ? nmax(x, y) : x + y;
-            }
-            if (lane == 0) __stcg(&ctl->results[j], x);
+        // Every thread loads its (at most kMaxBlocks / blockDim) partials of
+        // each value at once, then a fixed-order block reduction: one L2
+        // round trip instead of a chain of dependent loads.
+        double acc[NV];
+#pragma unroll
+        for (int j = 0; j < NV; ++j) acc[j] = 0.0;
+        constexpr int kPer = (kMaxBlocks + THREADS - 1) / THREADS;
+        double y[kPer][NV];
+#pragma unroll
+        for (int i = 0; i < kPer; ++i) {
+            const int b = threadIdx.x + i * blockDim.x;
+#pragma unroll
+            for (int j = 0; j < NV; ++j) y[i][j] = b < (int)gridDim.x ? __ldcg(partials + (int64_t)b * NV + j) : 0.0;
         }
-        __threadfence();
+#pragma unroll
+        for (int i = 0; i < kPer; ++i) {
+#pragma unroll
+            for (int j = 0; j < NV; ++j) {
+                const bool mx = (maxmask >> j) & 1u;
+                acc[j] = mx ? nmax(acc[j], y[i][j]) : acc[j] + y[i][j];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
+            const bool mx = (maxmask >> j) & 1u;
+            double x = acc[j];
+            for (int o = 16; o > 0; o >>= 1) {
+                const double t = __shfl_xor_sync(0xffffffffu, x, o);
+                x = mx ? nmax(x, t) : x + t;
+            }
+            if (lane == 0) sm[j * 32 + warp] = x;
+        }
+        __syncthreads();
+        if (threadIdx.x < NV) {
+            const int j = threadIdx.x;
+            const bool mx = (maxmask >> j) & 1u;
+            double x = sm[j * 32];
+            for (int w = 1; w < nw; ++w) x = mx ? nmax(x, sm[j * 32 + w]) : x + sm[j * 32 + w];
+            __stcg(&ctl->results[j], x);
+            s_res[j] = x;
+        }
         __syncthreads();
         if (threadIdx.x == 0) {
             atomicExch(&ctl->count, 0u);
             __threadfence();
             atomicAdd(&ctl->gen, 1u);
+            s_err = vload(&ctl->error);
         }
     } else if (threadIdx.x == 0) {
         long long it = 0;
         while (vload(&ctl->gen) == s_gen) {
-            __nanosleep(32);
+            __nanosleep(20);
             if (++it > kSpinLimit) {
                 atomicExch(&ctl->error, 1);
                 break;
             }
         }
-        __threadfence();
+        __threadfence();  // acquire side of the release above
+#pragma unroll
+        for (int j = 0; j < NV; ++j) s_res[j] = __ldcg(&ctl->results[j]);
+        s_err = vload(&ctl->error);
     }
     __syncthreads();
 #pragma unroll
-    for (int j = 0; j < NV; ++j) v[j] = __ldcg(&ctl->results[j]);
-    return vload(&ctl->error) == 0;
+    for (int j = 0; j < NV; ++j) v[j] = s_res[j];
+    return s_err == 0;
 }
 
 // y_k(c) = diag(c) * g(k, c) + sum_s val(s, c) * g(k, nbr(s, c))
@@ -385,9 +421,8 @@ struct BoxRows {
 // pass: p_new = z + p_old beta is stored for the own cell and recomputed
 // (bitwise identically) at the neighbours, so an iteration needs two grid
 // reductions (p.Ap, then |r| and r.z) instead of three.
-constexpr int kCgThreads = 256;
 
-template <class Rows>
+template <int U, class Rows>
 __device__ void pcg1_body(const gf_krylov_t& K, const Rows& rows) {
     __shared__ CgState st;
     KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
@@ -417,7 +452,7 @@ __device__ void pcg1_body(const gf_krylov_t& K, const Rows& rows) {
             loc[0] = norm_acc(loc[0], rk, linf);
             loc[1] += rk * zk;
         }
-        ok = grid_reduce<2>(ctl, partials, loc, linf ? 1u : 0u);
+        ok = grid_reduce<2, kCgThreads>(ctl, partials, loc, linf ? 1u : 0u);
         if (threadIdx.x == 0) {
             const double r0 = norm_fin(loc[0], linf);
             st.r0 = r0;
@@ -447,14 +482,31 @@ __device__ void pcg1_body(const gf_krylov_t& K, const Rows& rows) {
         {  // p_new = z + p_old beta; q = A p_new; p_new . q
             double loc[1] = {0.0};
             auto gp = [&](int64_t i) { return __ldcg(z + i) + __ldcg(p_old + i) * beta; };
-            for (int64_t c = t0; c < n; c += stride) {
-                const double pc = gp(c);
-                __stcg(p_new + c, pc);
-                const double ap = rows.apply(c, __ldg(K.diag + c), gp);
-                __stcg(q + c, ap);
-                loc[0] += pc * ap;
+            // U cells per thread per pass: all loads of the U rows are issued
+            // before any store, and loc accumulates in the U = 1 order.
+            for (int64_t c0 = t0; c0 < n; c0 += U * stride) {
+                double pc[U], ap[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int64_t c = c0 + u * stride;
+                    if (c < n) pc[u] = gp(c);
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int64_t c = c0 + u * stride;
+                    if (c < n) ap[u] = rows.apply(c, __ldg(K.diag + c), gp);
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int64_t c = c0 + u * stride;
+                    if (c < n) {
+                        __stcg(p_new + c, pc[u]);
+                        __stcg(q + c, ap[u]);
+                        loc[0] += pc[u] * ap[u];
+                    }
+                }
             }
-            ok = grid_reduce<1>(ctl, partials, loc, 0u);
+            ok = grid_reduce<1, kCgThreads>(ctl, partials, loc, 0u);
             if (!ok) break;
             if (threadIdx.x == 0) st.alpha = st.rz_old / loc[0];
             __syncthreads();
@@ -462,17 +514,34 @@ __device__ void pcg1_body(const gf_krylov_t& K, const Rows& rows) {
         {  // x += alpha p; r -= alpha q; z = M r; |r|, r.z
             const double alpha = st.alpha;
             double loc[2] = {0.0, 0.0};
-            for (int64_t c = t0; c < n; c += stride) {
-                const double pc = __ldcg(p_new + c);
-                __stcg(x + c, __ldcg(x + c) + alpha * pc);
-                const double rk = __ldcg(r + c) - alpha * __ldcg(q + c);
-                const double zk = inv_diag(K.diag, c, jac) * rk;
-                __stcg(r + c, rk);
-                __stcg(z + c, zk);
-                loc[0] = norm_acc(loc[0], rk, linf);
-                loc[1] += rk * zk;
+            for (int64_t c0 = t0; c0 < n; c0 += U * stride) {
+                double pc[U], xo[U], ro[U], qo[U], dg[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int64_t c = c0 + u * stride;
+                    if (c < n) {
+                        pc[u] = __ldcg(p_new + c);
+                        xo[u] = __ldcg(x + c);
+                        ro[u] = __ldcg(r + c);
+                        qo[u] = __ldcg(q + c);
+                        dg[u] = inv_diag(K.diag, c, jac);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int64_t c = c0 + u * stride;
+                    if (c < n) {
+                        __stcg(x + c, xo[u] + alpha * pc[u]);
+                        const double rk = ro[u] - alpha * qo[u];
+                        const double zk = dg[u] * rk;
+                        __stcg(r + c, rk);
+                        __stcg(z + c, zk);
+                        loc[0] = norm_acc(loc[0], rk, linf);
+                        loc[1] += rk * zk;
+                    }
+                }
             }
-            ok = grid_reduce<2>(ctl, partials, loc, linf ? 1u : 0u);
+            ok = grid_reduce<2, kCgThreads>(ctl, partials, loc, linf ? 1u : 0u);
             if (!ok) break;
             if (threadIdx.x == 0) {
                 const double fin = norm_fin(loc[0], linf);
@@ -510,13 +579,15 @@ __device__ void pcg1_body(const gf_krylov_t& K, const Rows& rows) {
 template <int WIDTH>
 __global__ void __launch_bounds__(kCgThreads, 4) k_pcg1(gf_krylov_t K) {
     EllRows<double, WIDTH> rows{K.val, K.nbr, K.n, K.width};
-    pcg1_body(K, rows);
+    pcg1_body<1>(K, rows);
 }
 
-template <bool SYM>
-__global__ void __launch_bounds__(kCgThreads, 4) k_pcg1_box(gf_krylov_t K) {
+// Box kernels come in tuning variants: MINB resident blocks per SM (the
+// register budget follows from it) and U cells per thread per pass.
+template <bool SYM, int MINB, int U>
+__global__ void __launch_bounds__(kCgThreads, MINB) k_pcg1_box(gf_krylov_t K) {
     BoxRows<double, SYM, false> rows{K.val, K.n, K.stride_y, K.stride_z};
-    pcg1_body(K, rows);
+    pcg1_body<U>(K, rows);
 }
 
 // Mixed precision: FP32 inner Jacobi-PCG cycles inside FP64 iterative
@@ -528,7 +599,7 @@ __global__ void __launch_bounds__(kCgThreads, 4) k_pcg1_box(gf_krylov_t K) {
 // slots of a symmetric box) is made once per solve.
 constexpr int kMaxEll = 32;
 
-template <class Rows64, class Rows32>
+template <int U, class Rows64, class Rows32>
 __device__ void pcg1_mixed_body(const gf_krylov_t& K, const Rows64& rows64, Rows32 rows32, int ncoef) {
     __shared__ CgState st;
     __shared__ double s_target;
@@ -582,7 +653,7 @@ __device__ void pcg1_mixed_body(const gf_krylov_t& K, const Rows64& rows64, Rows
             }
             // The barrier also publishes the FP32 coefficients (cycle 0).
             double dummy[1] = {0.0};
-            ok = grid_reduce<1>(ctl, partials, dummy, 0u);
+            ok = grid_reduce<1, kCgThreads>(ctl, partials, dummy, 0u);
             if (!ok) break;
             auto gx = [&](int64_t i) { return __ldcg(x + i); };
             for (int64_t c = t0; c < n; c += stride) {
@@ -597,7 +668,7 @@ __device__ void pcg1_mixed_body(const gf_krylov_t& K, const Rows64& rows64, Rows
                 loc[0] = norm_acc(loc[0], rk, linf);
                 loc[1] += (double)r32 * (double)z32;
             }
-            ok = grid_reduce<2>(ctl, partials, loc, linf ? 1u : 0u);
+            ok = grid_reduce<2, kCgThreads>(ctl, partials, loc, linf ? 1u : 0u);
             if (!ok) break;
             if (threadIdx.x == 0) {
                 const double nr = norm_fin(loc[0], linf);
@@ -631,14 +702,29 @@ __device__ void pcg1_mixed_body(const gf_krylov_t& K, const Rows64& rows64, Rows
             {
                 double loc[1] = {0.0};
                 auto gp = [&](int64_t i) { return __ldcg(z + i) + __ldcg(p_old + i) * beta; };
-                for (int64_t c = t0; c < n; c += stride) {
-                    const float pc = gp(c);
-                    __stcg(p_new + c, pc);
-                    const float ap = rows32.apply(c, __ldcg(diag32 + c), gp);
-                    __stcg(q + c, ap);
-                    loc[0] += (double)pc * (double)ap;
+                for (int64_t c0 = t0; c0 < n; c0 += U * stride) {
+                    float pc[U], ap[U];
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const int64_t c = c0 + u * stride;
+                        if (c < n) pc[u] = gp(c);
+                    }
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const int64_t c = c0 + u * stride;
+                        if (c < n) ap[u] = rows32.apply(c, __ldcg(diag32 + c), gp);
+                    }
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const int64_t c = c0 + u * stride;
+                        if (c < n) {
+                            __stcg(p_new + c, pc[u]);
+                            __stcg(q + c, ap[u]);
+                            loc[0] += (double)pc[u] * (double)ap[u];
+                        }
+                    }
                 }
-                ok = grid_reduce<1>(ctl, partials, loc, 0u);
+                ok = grid_reduce<1, kCgThreads>(ctl, partials, loc, 0u);
                 if (!ok) break;
                 if (threadIdx.x == 0) st.alpha = st.rz_old / loc[0];
                 __syncthreads();
@@ -646,17 +732,34 @@ __device__ void pcg1_mixed_body(const gf_krylov_t& K, const Rows64& rows64, Rows
             {
                 const float alpha = (float)st.alpha;
                 double loc[2] = {0.0, 0.0};
-                for (int64_t c = t0; c < n; c += stride) {
-                    const float pc = __ldcg(p_new + c);
-                    __stcg(d + c, __ldcg(d + c) + alpha * pc);
-                    const float rk = __ldcg(r + c) - alpha * __ldcg(q + c);
-                    const float zk = __ldcg(inv32 + c) * rk;
-                    __stcg(r + c, rk);
-                    __stcg(z + c, zk);
-                    loc[0] = norm_acc(loc[0], (double)rk, linf);
-                    loc[1] += (double)rk * (double)zk;
+                for (int64_t c0 = t0; c0 < n; c0 += U * stride) {
+                    float pc[U], dd[U], ro[U], qo[U], iv[U];
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const int64_t c = c0 + u * stride;
+                        if (c < n) {
+                            pc[u] = __ldcg(p_new + c);
+                            dd[u] = __ldcg(d + c);
+                            ro[u] = __ldcg(r + c);
+                            qo[u] = __ldcg(q + c);
+                            iv[u] = __ldcg(inv32 + c);
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const int64_t c = c0 + u * stride;
+                        if (c < n) {
+                            __stcg(d + c, dd[u] + alpha * pc[u]);
+                            const float rk = ro[u] - alpha * qo[u];
+                            const float zk = iv[u] * rk;
+                            __stcg(r + c, rk);
+                            __stcg(z + c, zk);
+                            loc[0] = norm_acc(loc[0], (double)rk, linf);
+                            loc[1] += (double)rk * (double)zk;
+                        }
+                    }
                 }
-                ok = grid_reduce<2>(ctl, partials, loc, linf ? 1u : 0u);
+                ok = grid_reduce<2, kCgThreads>(ctl, partials, loc, linf ? 1u : 0u);
                 if (!ok) break;
                 if (threadIdx.x == 0) {
                     const double nr = norm_fin(loc[0], linf);
@@ -692,14 +795,33 @@ template <int WIDTH>
 __global__ void __launch_bounds__(kCgThreads, 4) k_pcg1_mixed(gf_krylov_t K) {
     EllRows<double, WIDTH> rows64{K.val, K.nbr, K.n, K.width};
     EllRows<float, WIDTH> rows32{nullptr, K.nbr, K.n, K.width};
-    pcg1_mixed_body(K, rows64, rows32, K.width);
+    pcg1_mixed_body<1>(K, rows64, rows32, K.width);
 }
 
-template <bool SYM>
-__global__ void __launch_bounds__(kCgThreads, 4) k_pcg1_mixed_box(gf_krylov_t K) {
+template <bool SYM, int MINB, int U>
+__global__ void __launch_bounds__(kCgThreads, MINB) k_pcg1_mixed_box(gf_krylov_t K) {
     BoxRows<double, SYM, false> rows64{K.val, K.n, K.stride_y, K.stride_z};
     BoxRows<float, SYM, SYM> rows32{nullptr, K.n, K.stride_y, K.stride_z};
-    pcg1_mixed_body(K, rows64, rows32, SYM ? 3 : 6);
+    pcg1_mixed_body<U>(K, rows64, rows32, SYM ? 3 : 6);
+}
+
+// Tuning variants of the box kernels: {MINB, U}.
+constexpr int kBoxVariants = 5;
+
+template <bool MIXED, bool SYM>
+static void* box_kernel(int variant) {
+    switch (variant) {
+        case 1:
+            return MIXED ? (void*)k_pcg1_mixed_box<SYM, 4, 2> : (void*)k_pcg1_box<SYM, 4, 2>;
+        case 2:
+            return MIXED ? (void*)k_pcg1_mixed_box<SYM, 6, 1> : (void*)k_pcg1_box<SYM, 6, 1>;
+        case 3:
+            return MIXED ? (void*)k_pcg1_mixed_box<SYM, 8, 1> : (void*)k_pcg1_box<SYM, 8, 1>;
+        case 4:
+            return MIXED ? (void*)k_pcg1_mixed_box<SYM, 6, 2> : (void*)k_pcg1_box<SYM, 6, 2>;
+        default:
+            return MIXED ? (void*)k_pcg1_mixed_box<SYM, 4, 1> : (void*)k_pcg1_box<SYM, 4, 1>;
+    }
 }
 
 // BiCGStab per-component modes.
@@ -1040,7 +1162,7 @@ __global__ void __launch_bounds__(kKThreads) k_bicgstab(gf_krylov_t K) {
 
 template <class Kern>
 static int launch_persistent(Kern kern, const gf_krylov_t* k, void* stream, const char* what,
-                             int threads = kKThreads) {
+                             int threads = kKThreads, int unroll = 1) {
     int dev = 0;
     cudaGetDevice(&dev);
     int sms = 0, coop = 0;
@@ -1051,12 +1173,13 @@ static int launch_persistent(Kern kern, const gf_krylov_t* k, void* stream, cons
         return GF_ERR_CUDA;
     }
     int per_sm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, 0);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)kern, threads, 0);
     if (e != cudaSuccess || per_sm < 1) {
         set_error("%s: occupancy query failed: %s", what, cudaGetErrorString(e));
         return GF_ERR_CUDA;
     }
     int64_t want = (k->n + threads - 1) / threads;
+    if (unroll > 1) want = (want + unroll - 1) / unroll;
     int64_t cap = (int64_t)per_sm * sms;
     if (cap > kMaxBlocks) cap = kMaxBlocks;
     if (k->block_cap > 0 && k->block_cap < cap) cap = k->block_cap;
@@ -1137,17 +1260,22 @@ int gf_pcg_solve(const gf_krylov_t* k, void* stream) {
                       (long long)need);
             return GF_ERR_INVALID;
         }
-        if (box && k->symmetric)
-            return launch_persistent(k_pcg1_mixed_box<true>, k, stream, "gf_pcg_solve", kCgThreads);
-        if (box) return launch_persistent(k_pcg1_mixed_box<false>, k, stream, "gf_pcg_solve", kCgThreads);
+        if (box) {
+            const int v = (k->variant >= 0 && k->variant < kBoxVariants) ? k->variant : 0;
+            void* kern = k->symmetric ? box_kernel<true, true>(v) : box_kernel<true, false>(v);
+            return launch_persistent(kern, k, stream, "gf_pcg_solve", kCgThreads, (v == 1 || v == 4) ? 2 : 1);
+        }
         if (k->width == 6) return launch_persistent(k_pcg1_mixed<6>, k, stream, "gf_pcg_solve", kCgThreads);
         return launch_persistent(k_pcg1_mixed<0>, k, stream, "gf_pcg_solve", kCgThreads);
     }
     if (!valid_krylov(k, k->ncomp == 1 ? 5 : 3, "gf_pcg_solve")) return GF_ERR_INVALID;
     switch (k->ncomp) {
         case 1:
-            if (box && k->symmetric) return launch_persistent(k_pcg1_box<true>, k, stream, "gf_pcg_solve", kCgThreads);
-            if (box) return launch_persistent(k_pcg1_box<false>, k, stream, "gf_pcg_solve", kCgThreads);
+            if (box) {
+                const int v = (k->variant >= 0 && k->variant < kBoxVariants) ? k->variant : 0;
+                void* kern = k->symmetric ? box_kernel<false, true>(v) : box_kernel<false, false>(v);
+                return launch_persistent(kern, k, stream, "gf_pcg_solve", kCgThreads, (v == 1 || v == 4) ? 2 : 1);
+            }
             if (k->width == 6) return launch_persistent(k_pcg1<6>, k, stream, "gf_pcg_solve", kCgThreads);
             return launch_persistent(k_pcg1<0>, k, stream, "gf_pcg_solve", kCgThreads);
         case 2:

@@ -57,6 +57,8 @@ class DeviceKrylov(LinearSolver):
         self.profile_events: list | None = None
         # Upper bound on persistent blocks (0: one wave at full occupancy).
         self.block_cap = 0
+        # Box-layout CG kernel variant (see gf_krylov.cu); None: autotuned.
+        self.variant: int | None = None
 
     def solve_arrays(self, grid, diag: torch.Tensor, val: torch.Tensor, rhs: torch.Tensor,
                      x: torch.Tensor, *, symmetric: bool = False) -> tuple[SolveStats, ...]:
@@ -96,6 +98,7 @@ class DeviceKrylov(LinearSolver):
         k.max_outer = self.max_outer
         k.inner_eta = self.inner_eta
         k.block_cap = int(self.block_cap)
+        k.variant = int(self.variant or 0)
         box = getattr(grid, "box_strides", None)
         if box is not None and not self.bicgstab and nc == 1:
             k.stride_y, k.stride_z = box

@@ -187,6 +187,8 @@ typedef struct gf_krylov {
     int64_t stride_z;
     int32_t symmetric;    /* 1 (box only): A is symmetric, only + slots read */
     int32_t block_cap;    /* > 0: at most this many persistent blocks (tuning) */
+    int32_t variant;      /* box CG kernel variant (0..4, see gf_krylov.cu) */
+    int32_t reserved3;
 } gf_krylov_t;
 
 const char* gf_last_error(void);
