@@ -178,6 +178,8 @@ _SIGNATURES = {
     "gf_fixed_values": ([P, I32, P, P, P, I64, P, P, P, P, P, P, P, P], ctypes.c_int),
     "gf_spmv": ([P, I32, P, P, P, P, P], ctypes.c_int),
     "gf_pcg_solve": ([P, P], ctypes.c_int),
+    "gf_pcg_solve_static": ([P, P], ctypes.c_int),
+    "gf_pcg_static_scratch_doubles": ([], I64),
     "gf_bicgstab_solve": ([P, P], ctypes.c_int),
     "gf_rau_hbya": ([P, I32, P, P, P, P, P, P, P, P], ctypes.c_int),
     "gf_simplec_rAtU": ([P, P, P, P, P], ctypes.c_int),

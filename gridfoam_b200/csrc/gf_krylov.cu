@@ -10,6 +10,8 @@
 // co-resident and the barrier is always reachable.
 #include "gf_common.cuh"
 
+#include <mutex>
+
 namespace gf {
 
 constexpr int kKThreads = 512;
@@ -1295,6 +1297,92 @@ int gf_bicgstab_solve(const gf_krylov_t* k, void* stream) {
         default:
             return launch_persistent(k_bicgstab<3>, k, stream, "gf_bicgstab_solve");
     }
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free CG entry point.
+//
+// Some callers cannot allocate device memory at solve time: a host
+// framework that has already reserved the device pool for its own caching
+// allocator (so a raw cudaMalloc would fail or fragment it), or a serving
+// loop that must not allocate after start-up to keep its latency and memory
+// footprint fixed.  gf_pcg_solve_static runs the same persistent CG as
+// gf_pcg_solve, but its scratch (barrier control block, block partials and
+// Krylov vectors) lives in the file-scope device array below instead of a
+// caller workspace.  Every GPU that loads this library holds that array
+// until the process exits.
+// ---------------------------------------------------------------------------
+namespace gf {
+
+// One FP64 system of up to 262,144 cells (10.1 MiB).
+constexpr int64_t kStaticScratchCells = 262144;
+constexpr int64_t kStaticScratchDoubles =
+    kCtlDoubles + (int64_t)kMaxBlocks * kMaxNV + 5 * kStaticScratchCells;
+
+static __device__ __align__(256) double g_static_scratch[kStaticScratchDoubles];
+
+constexpr int kMaxDevices = 128;
+static std::mutex g_static_mutex;
+static double* g_static_addr[kMaxDevices] = {};
+
+// Device address of g_static_scratch on the current device.  In host code
+// the array's name is only a host-side stand-in, so the address is looked
+// up once per device (with that device current) and cached.
+static int static_scratch(double** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        set_error("gf_pcg_solve_static: cudaGetDevice failed: %s", cudaGetErrorString(e));
+        return GF_ERR_CUDA;
+    }
+    if (dev < 0 || dev >= kMaxDevices) {
+        set_error("gf_pcg_solve_static: device ordinal %d out of range", dev);
+        return GF_ERR_INVALID;
+    }
+    std::lock_guard<std::mutex> lock(g_static_mutex);
+    if (g_static_addr[dev] == nullptr) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (e != cudaSuccess || p == nullptr) {
+            set_error("gf_pcg_solve_static: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+            return GF_ERR_CUDA;
+        }
+        g_static_addr[dev] = static_cast<double*>(p);
+    }
+    *out = g_static_addr[dev];
+    return GF_OK;
+}
+
+}  // namespace gf
+
+extern "C" {
+
+int64_t gf_pcg_static_scratch_doubles(void) { return kStaticScratchDoubles; }
+
+int gf_pcg_solve_static(const gf_krylov_t* k, void* stream) {
+    if (k == nullptr) {
+        set_error("gf_pcg_solve_static: invalid arguments (null descriptor)");
+        return GF_ERR_INVALID;
+    }
+    const int32_t kind = k->mixed ? 2 + 100 * k->width : 0;
+    const int64_t need = gf_krylov_workspace_size(k->n, k->ncomp, kind);
+    if (k->n <= 0 || need > kStaticScratchDoubles) {
+        set_error("gf_pcg_solve_static: the system needs %lld scratch doubles but the static scratch holds "
+                  "%lld (at most %lld cells for one FP64 system); use gf_pcg_solve with a caller workspace",
+                  (long long)need, (long long)kStaticScratchDoubles, (long long)kStaticScratchCells);
+        return GF_ERR_INVALID;
+    }
+    double* scratch = nullptr;
+    const int st = static_scratch(&scratch);
+    if (st != GF_OK) return st;
+    gf_krylov_t local = *k;
+    local.work = scratch;
+    local.work_len = kStaticScratchDoubles;
+    // gf_pcg_solve clears the barrier control block before its launch; the
+    // partials and vectors are written before they are read.
+    return gf_pcg_solve(&local, stream);
 }
 
 }  // extern "C"

@@ -244,6 +244,22 @@ int gf_spmv(const gf_mesh_t* m, int32_t ncomp, const double* diag,
  * cooperative launch for the whole solve, ncomp systems at once. */
 int gf_pcg_solve(const gf_krylov_t* k, void* stream);
 
+/* No counterpart in the reference.  Allocation-free variant of
+ * gf_pcg_solve for callers that cannot allocate device memory at solve
+ * time (a host framework that owns the device pool through its own caching
+ * allocator, or a serving loop that must not allocate after start-up).
+ * k->work and k->work_len are ignored: the scratch is a file-scope device
+ * array of gf_pcg_static_scratch_doubles() doubles (10.1 MiB; one FP64
+ * system of up to 262,144 cells) that every GPU loading this library holds
+ * until exit.  Larger systems are rejected with GF_ERR_INVALID.  The first
+ * call on a device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the one array, so calls that overlap on the GPU (other
+ * streams, other host threads) race; serialise them.  Results are those of
+ * gf_pcg_solve. */
+int gf_pcg_solve_static(const gf_krylov_t* k, void* stream);
+int64_t gf_pcg_static_scratch_doubles(void);
+
 /* solvers/bicgstab.py:76-272: right-preconditioned BiCGStab with breakdown
  * restarts, one persistent cooperative launch, ncomp systems at once. */
 int gf_bicgstab_solve(const gf_krylov_t* k, void* stream);
