@@ -149,7 +149,7 @@ class GfKrylov(ctypes.Structure):
         ("symmetric", I32),
         ("block_cap", I32),
         ("variant", I32),
-        ("reserved3", I32),
+        ("single_reduction", I32),
     ]
 
 

@@ -2,11 +2,12 @@
 //
 // One launch runs a whole solve (all iterations, up to three right-hand
 // sides sharing the matrix).  Blocks synchronise through a grid barrier that
-// also finishes every dot product: each block writes its partial sums, the
-// last block to arrive reduces them in a fixed order and releases the
-// others, so each reduction costs one barrier and is bitwise reproducible.
-// Every wait is bounded; on expiry the kernel raises an error flag and
-// returns instead of hanging.  The launch is cooperative, so all blocks are
+// also finishes every dot product: each block writes its partial sums,
+// arrives on a monotonic counter, and once every block has arrived each
+// block reduces all partials itself in one fixed order, so every block gets
+// the same bitwise-reproducible value without a second publish step.  Every
+// wait is bounded; on expiry the kernel raises an error flag and returns
+// instead of hanging.  The launch is cooperative, so all blocks are
 // co-resident and the barrier is always reachable.
 #include "gf_common.cuh"
 
@@ -21,16 +22,39 @@ constexpr int kMaxNV = 16;
 constexpr int kCtlDoubles = 32;
 constexpr long long kSpinLimit = 30000000LL;  // x ~40 ns polls: about a second
 
+// Partial sums are double-buffered by barrier parity: a block may write the
+// next barrier's partials while a slower block still reads this one's, but
+// not the one after (that needs the slow block's arrival).
+constexpr int64_t kPartials = 2LL * kMaxBlocks * kMaxNV;
+constexpr int64_t kHeader = kCtlDoubles + kPartials;
+
 struct KCtl {
-    unsigned int count;
-    unsigned int gen;
+    unsigned long long count;  // barrier arrivals since launch (zeroed per launch)
     int error;
     int pad;
-    double results[kMaxNV];
 };
 
-__device__ __forceinline__ unsigned vload(const unsigned* p) { return *(const volatile unsigned*)p; }
+// Barriers this block has passed since the kernel started; barrier_init()
+// must run at the top of every kernel that calls grid_reduce.
+__shared__ unsigned g_epoch;
+
+__device__ __forceinline__ void barrier_init() {
+    if (threadIdx.x == 0) g_epoch = 0;
+}
+
 __device__ __forceinline__ int vload(const int* p) { return *(const volatile int*)p; }
+
+// Release-add / acquire-load pair of the grid barrier (the CTA barrier
+// before the add makes it cumulative over the whole block's writes).
+__device__ __forceinline__ void arrive_release(unsigned long long* p) {
+    asm volatile("fence.acq_rel.gpu;\n\tred.relaxed.gpu.global.add.u64 [%0], 1;" ::"l"(p) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long load_acquire(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
 
 __device__ __forceinline__ double nmax(double a, double b) {
     if (a != a || b != b) return __longlong_as_double(0x7ff8000000000000LL);
@@ -45,13 +69,12 @@ __device__ __forceinline__ double inv_diag(const double* __restrict__ diag, int6
 
 // Grid-wide reduction of NV values per thread (sum, or max where maxmask
 // has the bit set), fused with the grid barrier.  Returns false when the
-// barrier wait expired.
+// barrier wait expired or another block reported an error.
 template <int NV, int THREADS = kKThreads>
 __device__ bool grid_reduce(KCtl* ctl, double* partials, double (&v)[NV], unsigned maxmask) {
-    __shared__ double sm[kMaxNV * 32];
-    __shared__ double s_res[kMaxNV];
-    __shared__ int s_last, s_err;
-    __shared__ unsigned s_gen;
+    __shared__ double sm1[NV * 32];
+    __shared__ double sm2[NV * 32];
+    __shared__ int s_err;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
     for (int j = 0; j < NV; ++j) {
@@ -61,95 +84,82 @@ __device__ bool grid_reduce(KCtl* ctl, double* partials, double (&v)[NV], unsign
             const double y = __shfl_xor_sync(0xffffffffu, x, o);
             x = mx ? nmax(x, y) : x + y;
         }
-        if (lane == 0) sm[j * 32 + warp] = x;
+        if (lane == 0) sm1[j * 32 + warp] = x;
     }
     __syncthreads();
+    const unsigned ep = g_epoch;
+    double* part = partials + (ep & 1u) * (kPartials / 2);
     if (threadIdx.x < NV) {
         const int j = threadIdx.x;
         const bool mx = (maxmask >> j) & 1u;
-        double x = sm[j * 32];
-        for (int w = 1; w < nw; ++w) x = mx ? nmax(x, sm[j * 32 + w]) : x + sm[j * 32 + w];
-        __stcg(partials + (int64_t)blockIdx.x * NV + j, x);
+        double x = sm1[j * 32];
+        for (int w = 1; w < nw; ++w) x = mx ? nmax(x, sm1[j * 32 + w]) : x + sm1[j * 32 + w];
+        __stcg(part + (int64_t)blockIdx.x * NV + j, x);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        // Release: the CTA barrier orders every thread's writes of this phase
-        // before this fence, which orders them before the arrival.
-        __threadfence();
-        const unsigned gen = vload(&ctl->gen);
-        const unsigned prev = atomicAdd(&ctl->count, 1u);
-        s_gen = gen;
-        s_last = (prev == gridDim.x - 1);
-        s_err = 0;
-    }
-    __syncthreads();
-    if (s_last) {
-        // Every thread loads its (at most kMaxBlocks / blockDim) partials of
-        // each value at once, then a fixed-order block reduction: one L2
-        // round trip instead of a chain of dependent loads.
-        double acc[NV];
-#pragma unroll
-        for (int j = 0; j < NV; ++j) acc[j] = 0.0;
-        constexpr int kPer = (kMaxBlocks + THREADS - 1) / THREADS;
-        double y[kPer][NV];
-#pragma unroll
-        for (int i = 0; i < kPer; ++i) {
-            const int b = threadIdx.x + i * blockDim.x;
-#pragma unroll
-            for (int j = 0; j < NV; ++j) y[i][j] = b < (int)gridDim.x ? __ldcg(partials + (int64_t)b * NV + j) : 0.0;
-        }
-#pragma unroll
-        for (int i = 0; i < kPer; ++i) {
-#pragma unroll
-            for (int j = 0; j < NV; ++j) {
-                const bool mx = (maxmask >> j) & 1u;
-                acc[j] = mx ? nmax(acc[j], y[i][j]) : acc[j] + y[i][j];
-            }
-        }
-#pragma unroll
-        for (int j = 0; j < NV; ++j) {
-            const bool mx = (maxmask >> j) & 1u;
-            double x = acc[j];
-            for (int o = 16; o > 0; o >>= 1) {
-                const double t = __shfl_xor_sync(0xffffffffu, x, o);
-                x = mx ? nmax(x, t) : x + t;
-            }
-            if (lane == 0) sm[j * 32 + warp] = x;
-        }
-        __syncthreads();
-        if (threadIdx.x < NV) {
-            const int j = threadIdx.x;
-            const bool mx = (maxmask >> j) & 1u;
-            double x = sm[j * 32];
-            for (int w = 1; w < nw; ++w) x = mx ? nmax(x, sm[j * 32 + w]) : x + sm[j * 32 + w];
-            __stcg(&ctl->results[j], x);
-            s_res[j] = x;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            atomicExch(&ctl->count, 0u);
-            __threadfence();
-            atomicAdd(&ctl->gen, 1u);
-            s_err = vload(&ctl->error);
-        }
-    } else if (threadIdx.x == 0) {
+        arrive_release(&ctl->count);
+        const unsigned long long target = (unsigned long long)(ep + 1u) * gridDim.x;
+        int err = 0;
         long long it = 0;
-        while (vload(&ctl->gen) == s_gen) {
+        while (load_acquire(&ctl->count) < target) {
             __nanosleep(20);
-            if (++it > kSpinLimit) {
+            ++it;
+            if ((it & 255) == 0 && vload(&ctl->error) != 0) {
+                err = 1;
+                break;
+            }
+            if (it > kSpinLimit) {
                 atomicExch(&ctl->error, 1);
+                err = 1;
                 break;
             }
         }
-        __threadfence();  // acquire side of the release above
-#pragma unroll
-        for (int j = 0; j < NV; ++j) s_res[j] = __ldcg(&ctl->results[j]);
-        s_err = vload(&ctl->error);
+        // A block that gave up raised the flag; the others see it at their
+        // next wait (checked every 256 polls) and leave as well.
+        s_err = err;
+        g_epoch = ep + 1u;
     }
     __syncthreads();
+    if (s_err) return false;
+    // Every thread loads its (at most kMaxBlocks / THREADS) partials of each
+    // value at once, then a fixed-order block reduction: one L2 round trip,
+    // and every block computes the same bits.
+    double acc[NV];
 #pragma unroll
-    for (int j = 0; j < NV; ++j) v[j] = s_res[j];
-    return s_err == 0;
+    for (int j = 0; j < NV; ++j) acc[j] = 0.0;
+    constexpr int kPer = (kMaxBlocks + THREADS - 1) / THREADS;
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+        const int b = threadIdx.x + i * blockDim.x;
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
+            const bool mx = (maxmask >> j) & 1u;
+            const double y = b < (int)gridDim.x ? __ldcg(part + (int64_t)b * NV + j) : 0.0;
+            acc[j] = mx ? nmax(acc[j], y) : acc[j] + y;
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        const bool mx = (maxmask >> j) & 1u;
+        double x = acc[j];
+        for (int o = 16; o > 0; o >>= 1) {
+            const double t = __shfl_xor_sync(0xffffffffu, x, o);
+            x = mx ? nmax(x, t) : x + t;
+        }
+        if (lane == 0) sm2[j * 32 + warp] = x;
+    }
+    __syncthreads();
+    // sm2 is next written after the first CTA barrier of the next call, and
+    // sm1 is next read after the second: no trailing barrier is needed.
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        const bool mx = (maxmask >> j) & 1u;
+        double x = sm2[j * 32];
+        for (int w = 1; w < nw; ++w) x = mx ? nmax(x, sm2[j * 32 + w]) : x + sm2[j * 32 + w];
+        v[j] = x;
+    }
+    return true;
 }
 
 // y_k(c) = diag(c) * g(k, c) + sum_s val(s, c) * g(k, nbr(s, c))
@@ -183,8 +193,9 @@ __global__ void __launch_bounds__(kKThreads) k_pcg(gf_krylov_t K) {
     __shared__ CgState st[NC];
     __shared__ int s_all_done;
     KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
+    barrier_init();
     double* partials = K.work + kCtlDoubles;
-    double* vec = partials + kMaxBlocks * kMaxNV;
+    double* vec = partials + kPartials;
     const int64_t n = K.n;
     double* r = vec;
     double* p = vec + NC * n;
@@ -424,12 +435,13 @@ struct BoxRows {
 // (bitwise identically) at the neighbours, so an iteration needs two grid
 // reductions (p.Ap, then |r| and r.z) instead of three.
 
-template <int U, class Rows>
+template <int THREADS, int U, class Rows>
 __device__ void pcg1_body(const gf_krylov_t& K, const Rows& rows) {
     __shared__ CgState st;
     KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
+    barrier_init();
     double* partials = K.work + kCtlDoubles;
-    double* vec = partials + kMaxBlocks * kMaxNV;
+    double* vec = partials + kPartials;
     const int64_t n = K.n;
     double* r = vec;
     double* z = vec + n;
@@ -454,7 +466,7 @@ __device__ void pcg1_body(const gf_krylov_t& K, const Rows& rows) {
             loc[0] = norm_acc(loc[0], rk, linf);
             loc[1] += rk * zk;
         }
-        ok = grid_reduce<2, kCgThreads>(ctl, partials, loc, linf ? 1u : 0u);
+        ok = grid_reduce<2, THREADS>(ctl, partials, loc, linf ? 1u : 0u);
         if (threadIdx.x == 0) {
             const double r0 = norm_fin(loc[0], linf);
             st.r0 = r0;
@@ -508,7 +520,7 @@ __device__ void pcg1_body(const gf_krylov_t& K, const Rows& rows) {
                     }
                 }
             }
-            ok = grid_reduce<1, kCgThreads>(ctl, partials, loc, 0u);
+            ok = grid_reduce<1, THREADS>(ctl, partials, loc, 0u);
             if (!ok) break;
             if (threadIdx.x == 0) st.alpha = st.rz_old / loc[0];
             __syncthreads();
@@ -543,7 +555,7 @@ __device__ void pcg1_body(const gf_krylov_t& K, const Rows& rows) {
                     }
                 }
             }
-            ok = grid_reduce<2, kCgThreads>(ctl, partials, loc, linf ? 1u : 0u);
+            ok = grid_reduce<2, THREADS>(ctl, partials, loc, linf ? 1u : 0u);
             if (!ok) break;
             if (threadIdx.x == 0) {
                 const double fin = norm_fin(loc[0], linf);
@@ -581,15 +593,170 @@ __device__ void pcg1_body(const gf_krylov_t& K, const Rows& rows) {
 template <int WIDTH>
 __global__ void __launch_bounds__(kCgThreads, 4) k_pcg1(gf_krylov_t K) {
     EllRows<double, WIDTH> rows{K.val, K.nbr, K.n, K.width};
-    pcg1_body<1>(K, rows);
+    pcg1_body<kCgThreads, 1>(K, rows);
+}
+
+// Single-reduction Jacobi-PCG (A. T. Chronopoulos and C. W. Gear, "s-step
+// iterative methods for symmetric linear systems", J. Comput. Appl. Math.
+// 25 (1989)).  With u = M r and w = A u the recurrences
+//   gamma = r.u, delta = w.u, beta = gamma / gamma_old,
+//   alpha = gamma / (delta - beta gamma / alpha_old),
+//   p = u + beta p, s = w + beta s, x += alpha p, r -= alpha s
+// are those of PCG (s = A p, delta - beta gamma / alpha_old = p.Ap), and
+// both inner products of an iteration come from one grid reduction.  One
+// pass per iteration: the new u is recomputed at the neighbours from the
+// previous pass's r, w and s (double-buffered, since other blocks overwrite
+// them in the same pass), so w = A u needs no second barrier.  Stopping
+// test, iteration count and statistics are those of pcg1_body.
+template <int THREADS, class Rows>
+__device__ void pcg1_sr_body(const gf_krylov_t& K, const Rows& rows) {
+    __shared__ CgState st;
+    KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
+    barrier_init();
+    double* partials = K.work + kCtlDoubles;
+    double* vec = partials + kPartials;
+    const int64_t n = K.n;
+    double* rb[2] = {vec, vec + n};
+    double* wb[2] = {vec + 2 * n, vec + 3 * n};
+    double* sb[2] = {vec + 4 * n, vec + 5 * n};
+    double* p = vec + 6 * n;
+    double* x = K.x;
+    const bool jac = K.jacobi != 0, linf = K.norm_inf != 0;
+    const int64_t t0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    bool ok = true;
+    {  // r = b - A x, p = s = 0; |r|, gamma = r.u
+        double loc[2] = {0.0, 0.0};
+        auto gx = [&](int64_t i) { return __ldcg(x + i); };
+        for (int64_t c = t0; c < n; c += stride) {
+            const double ax = rows.apply(c, __ldg(K.diag + c), gx);
+            const double rk = __ldg(K.rhs + c) - ax;
+            const double uk = inv_diag(K.diag, c, jac) * rk;
+            __stcg(rb[0] + c, rk);
+            __stcg(sb[0] + c, 0.0);
+            __stcg(p + c, 0.0);
+            loc[0] = norm_acc(loc[0], rk, linf);
+            loc[1] += rk * uk;
+        }
+        ok = grid_reduce<2, THREADS>(ctl, partials, loc, linf ? 1u : 0u);
+        if (threadIdx.x == 0) {
+            const double r0 = norm_fin(loc[0], linf);
+            st.r0 = r0;
+            st.final = r0;
+            st.thresh = fmax(K.atol, K.rtol * r0);
+            st.rz_old = loc[1];
+            st.beta = 0.0;
+            st.its = 0;
+            st.converged = 0;
+            st.status = GF_MAX_ITER;
+            st.done = 0;
+            if (r0 < st.thresh) {
+                st.done = 1;
+                st.converged = 1;
+                st.status = GF_OK;
+            } else if (!isfinite(r0)) {
+                st.done = 1;
+                st.status = GF_NONFINITE;
+            }
+        }
+        __syncthreads();
+    }
+    if (ok && !st.done) {  // w = A u; alpha = gamma / (w.u)
+        double loc[1] = {0.0};
+        const double* r0v = rb[0];
+        auto gu = [&](int64_t i) { return inv_diag(K.diag, i, jac) * __ldcg(r0v + i); };
+        for (int64_t c = t0; c < n; c += stride) {
+            const double wk = rows.apply(c, __ldg(K.diag + c), gu);
+            __stcg(wb[0] + c, wk);
+            loc[0] += wk * gu(c);
+        }
+        ok = grid_reduce<1, THREADS>(ctl, partials, loc, 0u);
+        if (threadIdx.x == 0) st.alpha = st.rz_old / loc[0];
+        __syncthreads();
+    }
+    int a = 0;
+    for (int it = 1; ok && !st.done && it <= K.max_iter; ++it) {
+        const double alpha = st.alpha, beta = st.beta;
+        const double* ra = rb[a];
+        const double* wa = wb[a];
+        const double* sa = sb[a];
+        double* rn = rb[a ^ 1];
+        double* wn = wb[a ^ 1];
+        double* sn = sb[a ^ 1];
+        // s and the new u of any cell from the previous pass's vectors; the
+        // own cell and its neighbours evaluate the same expressions.
+        auto gs = [&](int64_t i) { return __ldcg(wa + i) + beta * __ldcg(sa + i); };
+        auto gr = [&](int64_t i) { return __ldcg(ra + i) - alpha * gs(i); };
+        auto gu = [&](int64_t i) { return inv_diag(K.diag, i, jac) * gr(i); };
+        double loc[3] = {0.0, 0.0, 0.0};
+        for (int64_t c = t0; c < n; c += stride) {
+            const double dinv = inv_diag(K.diag, c, jac);
+            const double si = gs(c);
+            const double pi = dinv * __ldcg(ra + c) + beta * __ldcg(p + c);
+            const double rk = gr(c);
+            const double uk = dinv * rk;
+            const double wk = rows.apply(c, __ldg(K.diag + c), gu);
+            __stcg(x + c, __ldcg(x + c) + alpha * pi);
+            __stcg(p + c, pi);
+            __stcg(sn + c, si);
+            __stcg(rn + c, rk);
+            __stcg(wn + c, wk);
+            loc[0] = norm_acc(loc[0], rk, linf);
+            loc[1] += rk * uk;
+            loc[2] += wk * uk;
+        }
+        ok = grid_reduce<3, THREADS>(ctl, partials, loc, linf ? 1u : 0u);
+        if (!ok) break;
+        if (threadIdx.x == 0) {
+            const double fin = norm_fin(loc[0], linf);
+            st.final = fin;
+            if (fin < st.thresh) {
+                st.done = 1;
+                st.converged = 1;
+                st.its = it;
+                st.status = GF_OK;
+            } else if (!isfinite(fin)) {
+                st.done = 1;
+                st.its = it;
+                st.status = GF_NONFINITE;
+            } else {
+                const double b = loc[1] / st.rz_old;
+                st.alpha = loc[1] / (loc[2] - b * loc[1] / st.alpha);
+                st.beta = b;
+                st.rz_old = loc[1];
+            }
+        }
+        __syncthreads();
+        a ^= 1;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        double* o = K.stats;
+        o[0] = st.r0;
+        o[1] = st.final;
+        o[2] = st.done ? st.its : K.max_iter;
+        o[3] = st.converged;
+        o[4] = ok ? st.status : GF_ERR_TIMEOUT;
+    }
+}
+
+template <int WIDTH>
+__global__ void __launch_bounds__(kCgThreads, 4) k_pcg1_sr(gf_krylov_t K) {
+    EllRows<double, WIDTH> rows{K.val, K.nbr, K.n, K.width};
+    pcg1_sr_body<kCgThreads>(K, rows);
+}
+
+template <bool SYM, int THREADS>
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_pcg1_sr_box(gf_krylov_t K) {
+    BoxRows<double, SYM, false> rows{K.val, K.n, K.stride_y, K.stride_z};
+    pcg1_sr_body<THREADS>(K, rows);
 }
 
 // Box kernels come in tuning variants: MINB resident blocks per SM (the
 // register budget follows from it) and U cells per thread per pass.
-template <bool SYM, int MINB, int U>
-__global__ void __launch_bounds__(kCgThreads, MINB) k_pcg1_box(gf_krylov_t K) {
+template <bool SYM, int THREADS, int U>
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_pcg1_box(gf_krylov_t K) {
     BoxRows<double, SYM, false> rows{K.val, K.n, K.stride_y, K.stride_z};
-    pcg1_body<U>(K, rows);
+    pcg1_body<THREADS, U>(K, rows);
 }
 
 // Mixed precision: FP32 inner Jacobi-PCG cycles inside FP64 iterative
@@ -601,14 +768,15 @@ __global__ void __launch_bounds__(kCgThreads, MINB) k_pcg1_box(gf_krylov_t K) {
 // slots of a symmetric box) is made once per solve.
 constexpr int kMaxEll = 32;
 
-template <int U, class Rows64, class Rows32>
+template <int THREADS, int U, class Rows64, class Rows32>
 __device__ void pcg1_mixed_body(const gf_krylov_t& K, const Rows64& rows64, Rows32 rows32, int ncoef) {
     __shared__ CgState st;
     __shared__ double s_target;
     __shared__ int s_cycle_done;
     KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
+    barrier_init();
     double* partials = K.work + kCtlDoubles;
-    double* base = partials + kMaxBlocks * kMaxNV;
+    double* base = partials + kPartials;
     const int64_t n = K.n;
     float* f = reinterpret_cast<float*>(base + n);
     float* val32 = f;
@@ -655,7 +823,7 @@ __device__ void pcg1_mixed_body(const gf_krylov_t& K, const Rows64& rows64, Rows
             }
             // The barrier also publishes the FP32 coefficients (cycle 0).
             double dummy[1] = {0.0};
-            ok = grid_reduce<1, kCgThreads>(ctl, partials, dummy, 0u);
+            ok = grid_reduce<1, THREADS>(ctl, partials, dummy, 0u);
             if (!ok) break;
             auto gx = [&](int64_t i) { return __ldcg(x + i); };
             for (int64_t c = t0; c < n; c += stride) {
@@ -670,7 +838,7 @@ __device__ void pcg1_mixed_body(const gf_krylov_t& K, const Rows64& rows64, Rows
                 loc[0] = norm_acc(loc[0], rk, linf);
                 loc[1] += (double)r32 * (double)z32;
             }
-            ok = grid_reduce<2, kCgThreads>(ctl, partials, loc, linf ? 1u : 0u);
+            ok = grid_reduce<2, THREADS>(ctl, partials, loc, linf ? 1u : 0u);
             if (!ok) break;
             if (threadIdx.x == 0) {
                 const double nr = norm_fin(loc[0], linf);
@@ -726,7 +894,7 @@ __device__ void pcg1_mixed_body(const gf_krylov_t& K, const Rows64& rows64, Rows
                         }
                     }
                 }
-                ok = grid_reduce<1, kCgThreads>(ctl, partials, loc, 0u);
+                ok = grid_reduce<1, THREADS>(ctl, partials, loc, 0u);
                 if (!ok) break;
                 if (threadIdx.x == 0) st.alpha = st.rz_old / loc[0];
                 __syncthreads();
@@ -761,7 +929,7 @@ __device__ void pcg1_mixed_body(const gf_krylov_t& K, const Rows64& rows64, Rows
                         }
                     }
                 }
-                ok = grid_reduce<2, kCgThreads>(ctl, partials, loc, linf ? 1u : 0u);
+                ok = grid_reduce<2, THREADS>(ctl, partials, loc, linf ? 1u : 0u);
                 if (!ok) break;
                 if (threadIdx.x == 0) {
                     const double nr = norm_fin(loc[0], linf);
@@ -797,32 +965,457 @@ template <int WIDTH>
 __global__ void __launch_bounds__(kCgThreads, 4) k_pcg1_mixed(gf_krylov_t K) {
     EllRows<double, WIDTH> rows64{K.val, K.nbr, K.n, K.width};
     EllRows<float, WIDTH> rows32{nullptr, K.nbr, K.n, K.width};
-    pcg1_mixed_body<1>(K, rows64, rows32, K.width);
+    pcg1_mixed_body<kCgThreads, 1>(K, rows64, rows32, K.width);
 }
 
-template <bool SYM, int MINB, int U>
-__global__ void __launch_bounds__(kCgThreads, MINB) k_pcg1_mixed_box(gf_krylov_t K) {
+template <bool SYM, int THREADS, int U>
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_pcg1_mixed_box(gf_krylov_t K) {
     BoxRows<double, SYM, false> rows64{K.val, K.n, K.stride_y, K.stride_z};
     BoxRows<float, SYM, SYM> rows32{nullptr, K.n, K.stride_y, K.stride_z};
-    pcg1_mixed_body<U>(K, rows64, rows32, SYM ? 3 : 6);
+    pcg1_mixed_body<THREADS, U>(K, rows64, rows32, SYM ? 3 : 6);
 }
 
-// Tuning variants of the box kernels: {MINB, U}.
+// Tuning variants of the box kernels: threads per block and U cells per
+// thread per pass.  Every variant keeps 1024 resident threads per SM (64
+// registers a thread); fewer, larger blocks mean fewer barrier arrivals.
+struct BoxVariant {
+    void* kern;
+    int threads, unroll;
+};
 constexpr int kBoxVariants = 5;
+// FP64 symmetric box CG with shared-memory tiles (k_pcg1_box_staged); falls
+// back to variant 0 when the system does not qualify.
+constexpr int kStagedVariant = 5;
+
+template <bool MIXED, bool SYM, int THREADS, int U>
+static BoxVariant box_variant() {
+    void* k = MIXED ? (void*)k_pcg1_mixed_box<SYM, THREADS, U> : (void*)k_pcg1_box<SYM, THREADS, U>;
+    return {k, THREADS, U};
+}
 
 template <bool MIXED, bool SYM>
-static void* box_kernel(int variant) {
+static BoxVariant box_kernel(int variant) {
     switch (variant) {
         case 1:
-            return MIXED ? (void*)k_pcg1_mixed_box<SYM, 4, 2> : (void*)k_pcg1_box<SYM, 4, 2>;
+            return box_variant<MIXED, SYM, 256, 2>();
         case 2:
-            return MIXED ? (void*)k_pcg1_mixed_box<SYM, 6, 1> : (void*)k_pcg1_box<SYM, 6, 1>;
+            return box_variant<MIXED, SYM, 512, 1>();
         case 3:
-            return MIXED ? (void*)k_pcg1_mixed_box<SYM, 8, 1> : (void*)k_pcg1_box<SYM, 8, 1>;
+            return box_variant<MIXED, SYM, 1024, 1>();
         case 4:
-            return MIXED ? (void*)k_pcg1_mixed_box<SYM, 6, 2> : (void*)k_pcg1_box<SYM, 6, 2>;
+            return box_variant<MIXED, SYM, 1024, 2>();
         default:
-            return MIXED ? (void*)k_pcg1_mixed_box<SYM, 4, 1> : (void*)k_pcg1_box<SYM, 4, 1>;
+            return box_variant<MIXED, SYM, 256, 1>();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Box CG with shared-memory tiles filled by bulk asynchronous copies.
+//
+// The register-resident kernels keep only a few loads per thread in flight,
+// which at a million cells leaves them bound by memory latency rather than
+// bandwidth.  Here each block walks tiles of T consecutive cells; one thread
+// issues 1-D bulk copies (cp.async.bulk, completion counted on an mbarrier)
+// of every window a tile reads into one of two shared-memory stages, so the
+// next tile (~90 KB) is in flight while the current one is computed.
+//   SpMV pass, cells [c0, c1): z and p_old over [c0-sz, c1-sz),
+//   [c0-sy, c1+sy) and [c0+sz, c1+sz); the '+' coefficient slots over
+//   [c0-1, c1), [c0-sy, c1), [c0-sz, c1-sz) and [c0, c1); diag over [c0, c1).
+//   Update pass: p, q, x, r and diag over [c0, c1).
+// Per cell the arithmetic and its order are those of BoxRows, so matrix
+// products are bitwise those of k_pcg1_box.  Requires a symmetric box, even
+// n and 16-byte aligned arrays (the host checks; other systems use
+// k_pcg1_box).  No copy uses cluster multicast.
+constexpr int kStThreads = 512;
+constexpr int kStMaxSmem = 220 * 1024;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* b) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(b)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect(uint64_t* b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_test(uint64_t* b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for the phase with this parity; false when it expired.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity) {
+    long long it = 0;
+    while (!mbar_test(b, parity)) {
+        if (++it > 1024) __nanosleep(20);
+        if (it > kSpinLimit) return false;
+    }
+    return true;
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* b) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(b))
+        : "memory");
+}
+
+// Shared-memory slots of one stage (in doubles, all even so every slot
+// starts 16-byte aligned): eight short ones (T + 4) and three long ones
+// (T + 2 sy + 4) for the windows that carry the y halo.
+struct StLayout {
+    int a, b;  // slot lengths
+    __host__ __device__ StLayout(int T, int64_t sy) : a(T + 4), b(T + 2 * (int)sy + 4) {}
+    __host__ __device__ int stage() const { return 8 * a + 3 * b; }
+    // SpMV pass
+    __host__ __device__ int zm() const { return 0; }
+    __host__ __device__ int zo() const { return a; }
+    __host__ __device__ int zp() const { return a + b; }
+    __host__ __device__ int pm() const { return 2 * a + b; }
+    __host__ __device__ int po() const { return 3 * a + b; }
+    __host__ __device__ int pp() const { return 3 * a + 2 * b; }
+    __host__ __device__ int cx() const { return 4 * a + 2 * b; }
+    __host__ __device__ int cy() const { return 5 * a + 2 * b; }
+    __host__ __device__ int czm() const { return 5 * a + 3 * b; }
+    __host__ __device__ int czo() const { return 6 * a + 3 * b; }
+    __host__ __device__ int dg() const { return 7 * a + 3 * b; }
+};
+
+// Window [lo, hi) of an array, clamped to [0, n) and widened to even ends
+// (n is even, arrays 16-byte aligned): its first index, and its bytes.
+struct Window {
+    int64_t base;
+    uint32_t bytes;
+};
+
+__device__ __forceinline__ Window window(int64_t lo, int64_t hi, int64_t n) {
+    lo = lo < 0 ? 0 : lo;
+    hi = hi > n ? n : hi;
+    if (hi <= lo) return {lo & ~1LL, 0u};
+    const int64_t a = lo & ~1LL, e = (hi + 1) & ~1LL;
+    return {a, (uint32_t)((e - a) * 8)};
+}
+
+struct StGeom {  // window first indices of one SpMV tile
+    int64_t c0, c1, bm, bo, bp, bx, by;
+};
+
+__device__ __forceinline__ StGeom st_geom(int64_t t, int T, int64_t n, int64_t sy, int64_t sz) {
+    StGeom g;
+    g.c0 = t * T;
+    g.c1 = g.c0 + T < n ? g.c0 + T : n;
+    g.bm = window(g.c0 - sz, g.c1 - sz, n).base;
+    g.bo = window(g.c0 - sy, g.c1 + sy, n).base;
+    g.bp = window(g.c0 + sz, g.c1 + sz, n).base;
+    g.bx = window(g.c0 - 1, g.c1, n).base;
+    g.by = window(g.c0 - sy, g.c1, n).base;
+    return g;
+}
+
+// Thread 0: expect the tile's bytes on the stage barrier, then issue every
+// window copy of the list (array, window, slot offset).
+struct StCopy {
+    const double* src;
+    Window w;
+    int off;
+};
+
+template <int N>
+__device__ __forceinline__ void st_issue(const StCopy (&cp)[N], double* stage, uint64_t* bar) {
+    uint32_t total = 0;
+#pragma unroll
+    for (int i = 0; i < N; ++i) total += cp[i].w.bytes;
+    mbar_expect(bar, total);
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+        if (cp[i].w.bytes) bulk_g2s(stage + cp[i].off, cp[i].src + cp[i].w.base, cp[i].w.bytes, bar);
+}
+
+__device__ __forceinline__ void st_issue_spmv(int64_t t, int T, const gf_krylov_t& K, const double* z,
+                                              const double* pold, const StLayout& L, double* stage,
+                                              uint64_t* bar) {
+    const int64_t n = K.n, sy = K.stride_y, sz = K.stride_z;
+    const int64_t c0 = t * T, c1 = c0 + T < n ? c0 + T : n;
+    const Window wm = window(c0 - sz, c1 - sz, n), wo = window(c0 - sy, c1 + sy, n),
+                 wp = window(c0 + sz, c1 + sz, n);
+    const double* vx = K.val + 1 * n;  // '+' slots of the box ELL: 1, 3, 5
+    const double* vy = K.val + 3 * n;
+    const double* vz = K.val + 5 * n;
+    const StCopy cp[11] = {
+        {z, wm, L.zm()},    {z, wo, L.zo()},    {z, wp, L.zp()},
+        {pold, wm, L.pm()}, {pold, wo, L.po()}, {pold, wp, L.pp()},
+        {vx, window(c0 - 1, c1, n), L.cx()},     {vy, window(c0 - sy, c1, n), L.cy()},
+        {vz, wm, L.czm()},  {vz, window(c0, c1, n), L.czo()},
+        {K.diag, window(c0, c1, n), L.dg()},
+    };
+    st_issue(cp, stage, bar);
+}
+
+__device__ __forceinline__ void st_issue_update(int64_t t, int T, const gf_krylov_t& K, const double* p,
+                                                const double* q, const double* r, const StLayout& L,
+                                                double* stage, uint64_t* bar) {
+    const int64_t n = K.n;
+    const int64_t c0 = t * T, c1 = c0 + T < n ? c0 + T : n;
+    const Window w = window(c0, c1, n);
+    const StCopy cp[5] = {{p, w, 0 * L.a}, {q, w, 1 * L.a}, {K.x, w, 2 * L.a}, {r, w, 3 * L.a}, {K.diag, w, 4 * L.a}};
+    st_issue(cp, stage, bar);
+}
+
+// One pass over this block's tiles (t = blockIdx.x, + gridDim.x, ...) with a
+// two-stage pipeline.  issue(t, stage, bar) runs on thread 0; compute(t,
+// stage) on all threads.  Returns false when a stage wait expired (after a
+// second bounded wait so no copy is left landing in shared memory).
+template <class Issue, class Compute>
+__device__ bool st_pass(int64_t ntiles, double* st0, double* st1, uint64_t* bars, uint32_t& phase,
+                        const Issue& issue, const Compute& compute) {
+    const int64_t g = gridDim.x;
+    const int64_t t0 = blockIdx.x;
+    if (threadIdx.x == 0) {
+        // Generic-proxy writes (this pass's inputs) before async-proxy reads.
+        asm volatile("fence.proxy.async.global;" ::: "memory");
+        if (t0 < ntiles) issue(t0, st0, &bars[0]);
+        if (t0 + g < ntiles) issue(t0 + g, st1, &bars[1]);
+    }
+    int s = 0;
+    for (int64_t t = t0; t < ntiles; t += g, s ^= 1) {
+        const uint32_t par = (phase >> s) & 1u;
+        // The vote keeps the block's control flow uniform if a wait expired.
+        if (__syncthreads_or(!mbar_wait(&bars[s], par))) {
+            // Drain both stages (bounded) before leaving.
+            mbar_wait(&bars[s], par);
+            if (t + g < ntiles) mbar_wait(&bars[s ^ 1], (phase >> (s ^ 1)) & 1u);
+            return false;
+        }
+        phase ^= 1u << s;
+        compute(t, s ? st1 : st0);
+        __syncthreads();  // the stage is free again
+        if (threadIdx.x == 0 && t + 2 * g < ntiles) issue(t + 2 * g, s ? st1 : st0, &bars[s]);
+    }
+    return true;
+}
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, 1) k_pcg1_box_staged(gf_krylov_t K, int T) {
+    __shared__ CgState st;
+    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ int s_stage_err;
+    extern __shared__ __align__(16) double smem[];
+    KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
+    barrier_init();
+    double* partials = K.work + kCtlDoubles;
+    double* vec = partials + kPartials;
+    const int64_t n = K.n, sy = K.stride_y, sz = K.stride_z;
+    double* r = vec;
+    double* z = vec + n;
+    double* pa = vec + 2 * n;
+    double* pb = vec + 3 * n;
+    double* q = vec + 4 * n;
+    double* x = K.x;
+    const bool jac = K.jacobi != 0, linf = K.norm_inf != 0;
+    const StLayout L(T, sy);
+    double* st0 = smem;
+    double* st1 = smem + L.stage();
+    const int64_t ntiles = (n + T - 1) / T;
+    uint32_t phase = 0;
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0]);
+        mbar_init(&bars[1]);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_stage_err = 0;
+    }
+    __syncthreads();
+    const BoxRows<double, true, false> rows{K.val, n, sy, sz};
+    const int64_t gt0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t gstride = (int64_t)gridDim.x * blockDim.x;
+    bool ok = true;
+    {  // r = b - A x, z = M r, p = 0; |r| and r.z (register path, once)
+        double loc[2] = {0.0, 0.0};
+        auto gx = [&](int64_t i) { return __ldcg(x + i); };
+        for (int64_t c = gt0; c < n; c += gstride) {
+            const double ax = rows.apply(c, __ldg(K.diag + c), gx);
+            const double rk = __ldg(K.rhs + c) - ax;
+            const double zk = inv_diag(K.diag, c, jac) * rk;
+            __stcg(r + c, rk);
+            __stcg(z + c, zk);
+            __stcg(pa + c, 0.0);
+            loc[0] = norm_acc(loc[0], rk, linf);
+            loc[1] += rk * zk;
+        }
+        ok = grid_reduce<2, THREADS>(ctl, partials, loc, linf ? 1u : 0u);
+        if (threadIdx.x == 0) {
+            const double r0 = norm_fin(loc[0], linf);
+            st.r0 = r0;
+            st.final = r0;
+            st.thresh = fmax(K.atol, K.rtol * r0);
+            st.rz_old = loc[1];
+            st.beta = 0.0;
+            st.its = 0;
+            st.converged = 0;
+            st.status = GF_MAX_ITER;
+            st.done = 0;
+            if (r0 < st.thresh) {
+                st.done = 1;
+                st.converged = 1;
+                st.status = GF_OK;
+            } else if (!isfinite(r0)) {
+                st.done = 1;
+                st.status = GF_NONFINITE;
+            }
+        }
+        __syncthreads();
+    }
+    double* p_old = pa;
+    double* p_new = pb;
+    for (int it = 1; ok && !st.done && it <= K.max_iter; ++it) {
+        const double beta = st.beta;
+        {  // p_new = z + p_old beta; q = A p_new; p_new . q
+            double loc[1] = {0.0};
+            auto issue = [&](int64_t t, double* stage, uint64_t* bar) {
+                st_issue_spmv(t, T, K, z, p_old, L, stage, bar);
+            };
+            auto compute = [&](int64_t t, const double* S) {
+                const StGeom g = st_geom(t, T, n, sy, sz);
+                for (int64_t c = g.c0 + threadIdx.x; c < g.c1; c += THREADS) {
+                    auto po = [&](int64_t i) { return S[L.zo() + (i - g.bo)] + S[L.po() + (i - g.bo)] * beta; };
+                    const double dc = S[L.dg() + (c - g.c0 + (g.c0 & 1))];
+                    const double pc = po(c);
+                    double acc = dc * pc;
+                    {
+                        const double am = c >= 1 ? S[L.cx() + (c - 1 - g.bx)] : 0.0;
+                        const double ap = S[L.cx() + (c - g.bx)];
+                        acc += am * po(c >= 1 ? c - 1 : c);
+                        acc += ap * po(c + 1 < n ? c + 1 : c);
+                    }
+                    {
+                        const double am = c >= sy ? S[L.cy() + (c - sy - g.by)] : 0.0;
+                        const double ap = S[L.cy() + (c - g.by)];
+                        acc += am * po(c >= sy ? c - sy : c);
+                        acc += ap * po(c + sy < n ? c + sy : c);
+                    }
+                    {
+                        const double am = c >= sz ? S[L.czm() + (c - sz - g.bm)] : 0.0;
+                        const double ap = S[L.czo() + (c - g.c0 + (g.c0 & 1))];
+                        const double gm =
+                            c >= sz ? S[L.zm() + (c - sz - g.bm)] + S[L.pm() + (c - sz - g.bm)] * beta : pc;
+                        const double gp =
+                            c + sz < n ? S[L.zp() + (c + sz - g.bp)] + S[L.pp() + (c + sz - g.bp)] * beta : pc;
+                        acc += am * gm;
+                        acc += ap * gp;
+                    }
+                    __stcg(p_new + c, pc);
+                    __stcg(q + c, acc);
+                    loc[0] += pc * acc;
+                }
+            };
+            ok = st_pass(ntiles, st0, st1, bars, phase, issue, compute);
+            if (!ok) {
+                if (threadIdx.x == 0) atomicExch(&ctl->error, 1);
+                break;
+            }
+            ok = grid_reduce<1, THREADS>(ctl, partials, loc, 0u);
+            if (!ok) break;
+            if (threadIdx.x == 0) st.alpha = st.rz_old / loc[0];
+            __syncthreads();
+        }
+        {  // x += alpha p; r -= alpha q; z = M r; |r|, r.z
+            const double alpha = st.alpha;
+            double loc[2] = {0.0, 0.0};
+            auto issue = [&](int64_t t, double* stage, uint64_t* bar) {
+                st_issue_update(t, T, K, p_new, q, r, L, stage, bar);
+            };
+            auto compute = [&](int64_t t, const double* S) {
+                const int64_t c0 = t * T, c1 = c0 + T < n ? c0 + T : n;
+                const int64_t b = c0 & ~1LL;
+                for (int64_t c = c0 + threadIdx.x; c < c1; c += THREADS) {
+                    const int i = (int)(c - b);
+                    const double pc = S[0 * L.a + i], qo = S[1 * L.a + i], xo = S[2 * L.a + i],
+                                 ro = S[3 * L.a + i], d = S[4 * L.a + i];
+                    const double dg = jac ? (fabs(d) < 2.220446049250313e-16 ? 1.0 : 1.0 / d) : 1.0;
+                    __stcg(x + c, xo + alpha * pc);
+                    const double rk = ro - alpha * qo;
+                    const double zk = dg * rk;
+                    __stcg(r + c, rk);
+                    __stcg(z + c, zk);
+                    loc[0] = norm_acc(loc[0], rk, linf);
+                    loc[1] += rk * zk;
+                }
+            };
+            ok = st_pass(ntiles, st0, st1, bars, phase, issue, compute);
+            if (!ok) {
+                if (threadIdx.x == 0) atomicExch(&ctl->error, 1);
+                break;
+            }
+            ok = grid_reduce<2, THREADS>(ctl, partials, loc, linf ? 1u : 0u);
+            if (!ok) break;
+            if (threadIdx.x == 0) {
+                const double fin = norm_fin(loc[0], linf);
+                st.final = fin;
+                if (fin < st.thresh) {
+                    st.done = 1;
+                    st.converged = 1;
+                    st.its = it;
+                    st.status = GF_OK;
+                } else if (!isfinite(fin)) {
+                    st.done = 1;
+                    st.its = it;
+                    st.status = GF_NONFINITE;
+                } else {
+                    st.beta = loc[1] / st.rz_old;
+                    st.rz_old = loc[1];
+                }
+            }
+            __syncthreads();
+        }
+        double* tmp = p_old;
+        p_old = p_new;
+        p_new = tmp;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        double* o = K.stats;
+        o[0] = st.r0;
+        o[1] = st.final;
+        o[2] = st.done ? st.its : K.max_iter;
+        o[3] = st.converged;
+        o[4] = ok ? st.status : GF_ERR_TIMEOUT;
+    }
+}
+
+// Tile length for the staged kernel (0: the system does not qualify).
+static int staged_tile(const gf_krylov_t* k) {
+    if (!k->symmetric || k->stride_y < 1 || (k->n & 1)) return 0;
+    const void* ptrs[] = {k->diag, k->val, k->x, k->work, k->rhs};
+    for (const void* p : ptrs)
+        if (reinterpret_cast<uintptr_t>(p) & 15u) return 0;
+    for (int T = 1024; T >= 128; T /= 2) {
+        const StLayout L(T, k->stride_y);
+        if ((size_t)2 * L.stage() * sizeof(double) <= (size_t)kStMaxSmem) return T;
+    }
+    return 0;
+}
+
+// Single-reduction CG on a box: the variant picks the block size only.
+template <bool SYM>
+static BoxVariant sr_box_kernel(int variant) {
+    switch (variant) {
+        case 2:
+            return {(void*)k_pcg1_sr_box<SYM, 512>, 512, 1};
+        case 3:
+        case 4:
+            return {(void*)k_pcg1_sr_box<SYM, 1024>, 1024, 1};
+        default:
+            return {(void*)k_pcg1_sr_box<SYM, 256>, 256, 1};
     }
 }
 
@@ -850,8 +1443,9 @@ __global__ void __launch_bounds__(kKThreads) k_bicgstab(gf_krylov_t K) {
     __shared__ BiState st[NC];
     __shared__ int s_any;
     KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
+    barrier_init();
     double* partials = K.work + kCtlDoubles;
-    double* vec = partials + kMaxBlocks * kMaxNV;
+    double* vec = partials + kPartials;
     const int64_t n = K.n;
     double* r = vec;
     double* rh = vec + NC * n;
@@ -1203,6 +1797,43 @@ static int launch_persistent(Kern kern, const gf_krylov_t* k, void* stream, cons
     return GF_OK;
 }
 
+// Cooperative launch of the staged box CG: one block per SM, two stages of
+// dynamic shared memory.
+static int launch_staged(const gf_krylov_t* k, int T, void* stream) {
+    const char* what = "gf_pcg_solve";
+    const void* kern = (const void*)k_pcg1_box_staged<kStThreads>;
+    const size_t smem = (size_t)2 * StLayout(T, k->stride_y).stage() * sizeof(double);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int dev = 0, sms = 0, per_sm = 0;
+    if (e == cudaSuccess) e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kStThreads, smem);
+    if (e != cudaSuccess || per_sm < 1) {
+        set_error("%s: staged kernel set-up failed: %s", what, cudaGetErrorString(e));
+        return GF_ERR_CUDA;
+    }
+    const int64_t ntiles = (k->n + T - 1) / T;
+    int64_t cap = (int64_t)per_sm * sms;
+    if (cap > kMaxBlocks) cap = kMaxBlocks;
+    if (k->block_cap > 0 && k->block_cap < cap) cap = k->block_cap;
+    const int grid = (int)(ntiles < cap ? ntiles : cap);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    e = cudaMemsetAsync(k->work, 0, sizeof(KCtl), s);
+    if (e != cudaSuccess) {
+        set_error("%s: %s", what, cudaGetErrorString(e));
+        return GF_ERR_CUDA;
+    }
+    gf_krylov_t arg = *k;
+    int targ = T;
+    void* args[] = {&arg, &targ};
+    e = cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kStThreads), args, smem, s);
+    if (e != cudaSuccess) {
+        set_error("%s: cooperative launch failed: %s", what, cudaGetErrorString(e));
+        return GF_ERR_CUDA;
+    }
+    return GF_OK;
+}
+
 static bool valid_krylov(const gf_krylov_t* k, int nvec, const char* what) {
     if (k == nullptr || k->n <= 0 || k->width <= 0 || k->ncomp < 1 || k->ncomp > 3 || k->nbr == nullptr ||
         k->diag == nullptr || k->val == nullptr || k->rhs == nullptr || k->x == nullptr || k->work == nullptr ||
@@ -1210,7 +1841,7 @@ static bool valid_krylov(const gf_krylov_t* k, int nvec, const char* what) {
         set_error("%s: invalid arguments", what);
         return false;
     }
-    const int64_t need = kCtlDoubles + (int64_t)kMaxBlocks * kMaxNV + (int64_t)nvec * k->ncomp * k->n;
+    const int64_t need = kHeader + (int64_t)nvec * k->ncomp * k->n;
     if (k->work_len < need) {
         set_error("%s: workspace holds %lld doubles, %lld needed", what, (long long)k->work_len, (long long)need);
         return false;
@@ -1233,11 +1864,11 @@ int64_t gf_krylov_workspace_size(int64_t n, int32_t ncomp, int32_t kind) {
     if (kind >= 2) {
         const int64_t width = (kind - 2) / 100 > 0 ? (kind - 2) / 100 : kMaxEll;
         const int64_t floats = (width + 8) * n;
-        return kCtlDoubles + (int64_t)kMaxBlocks * kMaxNV + n + (floats + 1) / 2 + 1;
+        return kHeader + n + (floats + 1) / 2 + 1;
     }
     const int bicgstab = kind == 1;
-    const int nvec = bicgstab ? 6 : (ncomp == 1 ? 5 : 3);
-    return kCtlDoubles + (int64_t)kMaxBlocks * kMaxNV + (int64_t)nvec * ncomp * n;
+    const int nvec = bicgstab ? 6 : (ncomp == 1 ? 7 : 3);
+    return kHeader + (int64_t)nvec * ncomp * n;
 }
 
 int gf_pcg_solve(const gf_krylov_t* k, void* stream) {
@@ -1264,19 +1895,32 @@ int gf_pcg_solve(const gf_krylov_t* k, void* stream) {
         }
         if (box) {
             const int v = (k->variant >= 0 && k->variant < kBoxVariants) ? k->variant : 0;
-            void* kern = k->symmetric ? box_kernel<true, true>(v) : box_kernel<true, false>(v);
-            return launch_persistent(kern, k, stream, "gf_pcg_solve", kCgThreads, (v == 1 || v == 4) ? 2 : 1);
+            const BoxVariant bv = k->symmetric ? box_kernel<true, true>(v) : box_kernel<true, false>(v);
+            return launch_persistent(bv.kern, k, stream, "gf_pcg_solve", bv.threads, bv.unroll);
         }
         if (k->width == 6) return launch_persistent(k_pcg1_mixed<6>, k, stream, "gf_pcg_solve", kCgThreads);
         return launch_persistent(k_pcg1_mixed<0>, k, stream, "gf_pcg_solve", kCgThreads);
     }
-    if (!valid_krylov(k, k->ncomp == 1 ? 5 : 3, "gf_pcg_solve")) return GF_ERR_INVALID;
+    if (!valid_krylov(k, k->ncomp == 1 ? (k->single_reduction ? 7 : 5) : 3, "gf_pcg_solve")) return GF_ERR_INVALID;
     switch (k->ncomp) {
         case 1:
+            if (k->single_reduction) {
+                if (box) {
+                    const int v = (k->variant >= 0 && k->variant < kBoxVariants) ? k->variant : 0;
+                    const BoxVariant bv = k->symmetric ? sr_box_kernel<true>(v) : sr_box_kernel<false>(v);
+                    return launch_persistent(bv.kern, k, stream, "gf_pcg_solve", bv.threads, 1);
+                }
+                if (k->width == 6) return launch_persistent(k_pcg1_sr<6>, k, stream, "gf_pcg_solve", kCgThreads);
+                return launch_persistent(k_pcg1_sr<0>, k, stream, "gf_pcg_solve", kCgThreads);
+            }
+            if (box && k->variant == kStagedVariant) {
+                const int T = staged_tile(k);
+                if (T > 0) return launch_staged(k, T, stream);
+            }
             if (box) {
                 const int v = (k->variant >= 0 && k->variant < kBoxVariants) ? k->variant : 0;
-                void* kern = k->symmetric ? box_kernel<false, true>(v) : box_kernel<false, false>(v);
-                return launch_persistent(kern, k, stream, "gf_pcg_solve", kCgThreads, (v == 1 || v == 4) ? 2 : 1);
+                const BoxVariant bv = k->symmetric ? box_kernel<false, true>(v) : box_kernel<false, false>(v);
+                return launch_persistent(bv.kern, k, stream, "gf_pcg_solve", bv.threads, bv.unroll);
             }
             if (k->width == 6) return launch_persistent(k_pcg1<6>, k, stream, "gf_pcg_solve", kCgThreads);
             return launch_persistent(k_pcg1<0>, k, stream, "gf_pcg_solve", kCgThreads);
@@ -1316,10 +1960,9 @@ int gf_bicgstab_solve(const gf_krylov_t* k, void* stream) {
 // ---------------------------------------------------------------------------
 namespace gf {
 
-// One FP64 system of up to 262,144 cells (10.1 MiB).
+// One FP64 system of up to 262,144 cells (14.3 MiB).
 constexpr int64_t kStaticScratchCells = 262144;
-constexpr int64_t kStaticScratchDoubles =
-    kCtlDoubles + (int64_t)kMaxBlocks * kMaxNV + 5 * kStaticScratchCells;
+constexpr int64_t kStaticScratchDoubles = kHeader + 7 * kStaticScratchCells;
 
 static __device__ __align__(256) double g_static_scratch[kStaticScratchDoubles];
 

@@ -1,0 +1,175 @@
+"""Launch-shape autotuner and fixed-iteration timing of the CG kernels.
+
+The box-layout CG kernels (uniform lexicographic grids, implicit
+neighbours) come in variants that differ in threads per block and cells per
+thread per pass (``gf_krylov.cu``: ``box_kernel``).  Which one is fastest
+depends on the system size: small systems are bound by the two grid
+barriers of each iteration, where fewer and larger blocks arrive faster,
+and large ones by memory latency.  ``best_variant`` times a fixed number of
+iterations of every variant on the caller's own matrix and caches the
+winner per (device, cells, strides, symmetric, precision).  That cache is
+the package's only global state and a lock guards it.
+
+Run as a module it times one synthetic box system, for profiling a single
+fixed-length kernel launch::
+
+    python -m gridfoam_b200.solvers.autotune --box 64 64 256 --iters 200
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import threading
+from dataclasses import dataclass, field
+
+import torch
+
+from gridfoam_b200.meta.config import PrecisionType, PreconditionerType, SolverConfig, SolverType
+
+N_VARIANTS = 6
+VARIANTS = {
+    0: "256 threads x 1 cell/pass",
+    1: "256 threads x 2 cells/pass",
+    2: "512 threads x 1 cell/pass",
+    3: "1024 threads x 1 cell/pass",
+    4: "1024 threads x 2 cells/pass",
+    5: "512 threads, shared-memory tiles by bulk async copy (symmetric FP64 only)",
+}
+
+_LOCK = threading.Lock()
+_CACHE: dict[tuple, int] = {}
+
+
+@dataclass
+class BoxSystem:
+    """A symmetric 7-point system on an ``nx x ny x nz`` lexicographic box.
+
+    It carries what ``DeviceKrylov.solve_arrays`` reads from a grid
+    (``device``, ``ell_width``, ``dev["ell_nbr"]``, ``box_strides``) plus the
+    matrix: unit couplings between face neighbours, Dirichlet ends in z, so
+    ``-A`` is an M-matrix (the sign of gridfoam's pressure Laplacian).
+    """
+
+    nx: int
+    ny: int
+    nz: int
+    device: torch.device
+    ell_width: int = 6
+    dev: dict = field(default_factory=dict)
+    box_strides: tuple[int, int] = (0, 0)
+
+    def __post_init__(self):
+        nx, ny, nz = self.nx, self.ny, self.nz
+        n = nx * ny * nz
+        c = torch.arange(n, device=self.device, dtype=torch.int64)
+        i, j, k = c % nx, (c // nx) % ny, c // (nx * ny)
+        sy, sz = nx, nx * ny
+        self.box_strides = (sy, sz)
+        nbr = torch.empty((6, n), dtype=torch.int64, device=self.device)
+        val = torch.zeros((6, n), dtype=torch.float64, device=self.device)
+        for s, (has, off) in enumerate(((i > 0, -1), (i < nx - 1, 1), (j > 0, -sy), (j < ny - 1, sy),
+                                        (k > 0, -sz), (k < nz - 1, sz))):
+            nbr[s] = torch.where(has, c + off, c)
+            val[s] = has.to(torch.float64)
+        self.dev["ell_nbr"] = nbr.to(torch.int32).contiguous()
+        ends = (k == 0).to(torch.float64) + (k == nz - 1).to(torch.float64)
+        self.diag = -(val.sum(0) + 2.0 * ends)
+        self.val = val.contiguous()
+        g = torch.Generator(device="cpu").manual_seed(0)
+        self.rhs = torch.randn((1, n), generator=g, dtype=torch.float64).to(self.device)
+
+    @property
+    def num_cells(self) -> int:
+        return self.nx * self.ny * self.nz
+
+
+def _solver(iters: int, mixed: bool, variant: int, single_reduction: bool = False):
+    from gridfoam_b200.solvers.krylov import CGSolver
+
+    cfg = SolverConfig(
+        method=SolverType.CG,
+        preconditioner=PreconditionerType.JACOBI,
+        tolerance=0.0,
+        rel_tolerance=0.0,
+        max_iter=iters,
+        inner_precision=PrecisionType.FLOAT32 if mixed else PrecisionType.FLOAT64,
+    )
+    s = CGSolver(cfg)
+    s.variant = variant
+    s.single_reduction = single_reduction
+    return s
+
+
+def time_variant(grid, diag, val, rhs, *, symmetric: bool, mixed: bool, variant: int,
+                 iters: int = 100, repeats: int = 3, single_reduction: bool = False) -> tuple[float, int]:
+    """Microseconds per CG iteration of one variant (best of ``repeats``).
+
+    Tolerances are zero, so FP64 runs exactly ``iters`` iterations; the
+    mixed solver is normalised by the iterations its statistics report.
+    ``x`` is a scratch zero vector; the caller's data are only read.
+    """
+    s = _solver(iters, mixed, variant, single_reduction)
+    x = torch.zeros_like(rhs)
+    s.solve_arrays(grid, diag, val, rhs, x, symmetric=symmetric)  # warm-up
+    best, its = float("inf"), 0
+    for _ in range(repeats):
+        x.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        st = s.solve_arrays(grid, diag, val, rhs, x, symmetric=symmetric)
+        e1.record()
+        e1.synchronize()
+        its = max(1, st[0].iterations)
+        best = min(best, 1e3 * e0.elapsed_time(e1) / its)
+    return best, its
+
+
+def best_variant(grid, diag, val, rhs, *, symmetric: bool, mixed: bool, iters: int = 60) -> int:
+    """Fastest box CG variant for this system shape (timed once, then cached)."""
+    key = (str(grid.device), torch.cuda.get_device_name(grid.device), grid.num_cells,
+           tuple(grid.box_strides), bool(symmetric), bool(mixed))
+    with _LOCK:
+        hit = _CACHE.get(key)
+        if hit is not None:
+            return hit
+        times = [time_variant(grid, diag, val, rhs, symmetric=symmetric, mixed=mixed, variant=v,
+                              iters=iters, repeats=2)[0] for v in range(N_VARIANTS)]
+        best = min(range(N_VARIANTS), key=lambda v: times[v])
+        _CACHE[key] = best
+        return best
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--box", type=int, nargs=3, default=[64, 64, 256], metavar=("NX", "NY", "NZ"))
+    ap.add_argument("--iters", type=int, default=200)
+    ap.add_argument("--repeats", type=int, default=3)
+    ap.add_argument("--variant", type=int, default=-1, help="one variant; -1 times all of them")
+    ap.add_argument("--precision", choices=["float64", "float32"], default="float64",
+                    help="float32: FP32 inner CG inside FP64 refinement")
+    ap.add_argument("--single-reduction", action="store_true",
+                    help="FP64 Chronopoulos-Gear CG (one grid reduction per iteration)")
+    args = ap.parse_args()
+    dev = torch.device("cuda")
+    sysm = BoxSystem(*args.box, device=dev)
+    mixed = args.precision == "float32"
+    variants = range(N_VARIANTS) if args.variant < 0 else [args.variant]
+    n = sysm.num_cells
+    for v in variants:
+        us, its = time_variant(sysm, sysm.diag, sysm.val, sysm.rhs, symmetric=True, mixed=mixed, variant=v,
+                               iters=args.iters, repeats=args.repeats, single_reduction=args.single_reduction)
+        # Algorithmic bytes of one fused symmetric PCG-Jacobi iteration:
+        # 14 C s + F (s + 8), F the internal faces of the box.
+        s = 4 if mixed else 8
+        nx, ny, nz = args.box
+        f = (nx - 1) * ny * nz + nx * (ny - 1) * nz + nx * ny * (nz - 1)
+        gbs = (14 * n * s + f * (s + 8)) / (us * 1e-6) / 1e9
+        print(json.dumps({"box": args.box, "cells": n, "precision": args.precision,
+                          "single_reduction": args.single_reduction, "variant": v,
+                          "shape": VARIANTS[v], "iterations": its, "us_per_iter": round(us, 3),
+                          "algorithmic_GBps": round(gbs, 1)}))
+
+
+if __name__ == "__main__":
+    main()

@@ -35,6 +35,19 @@ def workspace(device: torch.device, n: int, ncomp: int, kind: int) -> torch.Tens
     return ws
 
 
+def default_variant(n: int, mixed: bool, symmetric: bool) -> int:
+    """Box CG launch shape by system size, from fixed-iteration timings on
+    B200 (``python -m gridfoam_b200.solvers.autotune``): 256-thread blocks
+    below ~128K cells, where the grid barrier dominates; 512-thread blocks
+    up to ~1.5M; above that the shared-memory tiled kernel (FP64 symmetric
+    systems) or 512-thread blocks."""
+    if n < 131072:
+        return 0
+    if n < 1536000 or mixed or not symmetric:
+        return 2
+    return 5
+
+
 class DeviceKrylov(LinearSolver):
     method: str = ""
     bicgstab: bool = False
@@ -57,8 +70,11 @@ class DeviceKrylov(LinearSolver):
         self.profile_events: list | None = None
         # Upper bound on persistent blocks (0: one wave at full occupancy).
         self.block_cap = 0
-        # Box-layout CG kernel variant (see gf_krylov.cu); None: autotuned.
+        # Box-layout CG kernel variant (launch shape, see gf_krylov.cu and
+        # solvers/autotune.py); None: chosen by system size.
         self.variant: int | None = None
+        # FP64 CG with one grid reduction per iteration (Chronopoulos-Gear).
+        self.single_reduction = False
 
     def solve_arrays(self, grid, diag: torch.Tensor, val: torch.Tensor, rhs: torch.Tensor,
                      x: torch.Tensor, *, symmetric: bool = False) -> tuple[SolveStats, ...]:
@@ -98,8 +114,9 @@ class DeviceKrylov(LinearSolver):
         k.max_outer = self.max_outer
         k.inner_eta = self.inner_eta
         k.block_cap = int(self.block_cap)
-        k.variant = int(self.variant or 0)
         box = getattr(grid, "box_strides", None)
+        k.variant = int(self.variant) if self.variant is not None else default_variant(n, mixed, symmetric)
+        k.single_reduction = int(self.single_reduction and not mixed and not self.bicgstab and nc == 1)
         if box is not None and not self.bicgstab and nc == 1:
             k.stride_y, k.stride_z = box
             k.symmetric = int(symmetric)

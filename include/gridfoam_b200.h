@@ -188,7 +188,9 @@ typedef struct gf_krylov {
     int32_t symmetric;    /* 1 (box only): A is symmetric, only + slots read */
     int32_t block_cap;    /* > 0: at most this many persistent blocks (tuning) */
     int32_t variant;      /* box CG kernel variant (0..4, see gf_krylov.cu) */
-    int32_t reserved3;
+    int32_t single_reduction; /* 1 (FP64 CG, one system): Chronopoulos-Gear
+                             CG, one grid reduction per iteration; needs the
+                             kind-0 workspace (7 vectors) */
 } gf_krylov_t;
 
 const char* gf_last_error(void);
@@ -249,7 +251,7 @@ int gf_pcg_solve(const gf_krylov_t* k, void* stream);
  * time (a host framework that owns the device pool through its own caching
  * allocator, or a serving loop that must not allocate after start-up).
  * k->work and k->work_len are ignored: the scratch is a file-scope device
- * array of gf_pcg_static_scratch_doubles() doubles (10.1 MiB; one FP64
+ * array of gf_pcg_static_scratch_doubles() doubles (14.3 MiB; one FP64
  * system of up to 262,144 cells) that every GPU loading this library holds
  * until exit.  Larger systems are rejected with GF_ERR_INVALID.  The first
  * call on a device looks up the array's device address

@@ -36,10 +36,16 @@ def _cuda():
         pytest.skip("needs a CUDA device")
 
 
+@pytest.mark.parametrize("algorithm", ["pcg", "sr", "staged"])
 @pytest.mark.parametrize("name", CASES)
-def test_steps_match_reference(name):
+def test_steps_match_reference(name, algorithm):
+    """pcg: two-reduction fused PCG; sr: single-reduction CG; staged: the
+    shared-memory tiled box kernel (box grids; ELL grids fall back)."""
     golden = load_golden(name)
     _, _, _, algo = device_case(name)
+    for s in algo.solvers.values():
+        s.single_reduction = algorithm == "sr"
+        s.variant = 5 if algorithm == "staged" else 0
     np.testing.assert_allclose(to_np(algo.phi.pack()), golden["init_phi"], rtol=0, atol=1e-13)
     tol = STEP_TOL[name]
     slack = 1 if name.startswith("pipe") else 0
@@ -261,3 +267,73 @@ def test_box_layout_matches_ell_layout():
         assert s_box[0].converged and s_ell[0].converged
         assert s_box[0].iterations == s_ell[0].iterations
         torch.testing.assert_close(x_box, x_ell, rtol=0, atol=0)
+
+
+@pytest.mark.parametrize("layout", ["box", "ell"])
+def test_single_reduction_cg_matches_pcg(layout):
+    """Chronopoulos-Gear CG (one reduction per iteration) against the
+    two-reduction PCG on a symmetric 7-point system: same iteration count
+    within one, solutions within the stopping tolerance, and the true
+    residual of both below the threshold."""
+    from gridfoam_b200.solvers.autotune import BoxSystem, _solver
+
+    sysm = BoxSystem(24, 20, 28, device=torch.device("cuda"))
+    if layout == "ell":
+        sysm.box_strides = None
+    out = {}
+    for sr in (False, True):
+        s = _solver(2000, False, 0, sr)
+        s.atol, s.rtol = 0.0, 1e-10
+        x = torch.zeros_like(sysm.rhs)
+        st = s.solve_arrays(sysm, sysm.diag, sysm.val, sysm.rhs, x, symmetric=True)
+        out[sr] = (x.clone(), st[0])
+    (x0, s0), (x1, s1) = out[False], out[True]
+    assert s0.converged and s1.converged
+    assert abs(s0.iterations - s1.iterations) <= 1, (s0.iterations, s1.iterations)
+    assert s0.initial_residual == pytest.approx(s1.initial_residual, rel=1e-14)
+    assert rel(to_np(x1), to_np(x0)) < 1e-8
+    # true residual of the single-reduction solution
+    nb = sysm.dev["ell_nbr"].long()
+    ax = sysm.diag * x1[0] + (sysm.val * x1[0][nb]).sum(0)
+    r = torch.linalg.vector_norm(sysm.rhs[0] - ax).item()
+    assert r < 1e-9 * s1.initial_residual
+
+
+@pytest.mark.parametrize("shape", [(24, 20, 28), (64, 64, 40), (7, 5, 6), (130, 3, 4)])
+def test_staged_box_cg_matches_register_kernel(shape):
+    """The shared-memory tiled box kernel (variant 5) against the register
+    kernel (variant 0): same iteration count within one and the same
+    solution to the stopping tolerance, on shapes with partial last tiles,
+    odd strides and a y halo larger than a tile's x extent."""
+    from gridfoam_b200.solvers.autotune import BoxSystem, _solver
+
+    sysm = BoxSystem(*shape, device=torch.device("cuda"))
+    out = {}
+    for v in (0, 5):
+        s = _solver(3000, False, v)
+        s.atol, s.rtol = 0.0, 1e-10
+        x = torch.zeros_like(sysm.rhs)
+        st = s.solve_arrays(sysm, sysm.diag, sysm.val, sysm.rhs, x, symmetric=True)
+        out[v] = (x.clone(), st[0])
+    (x0, s0), (x1, s1) = out[0], out[5]
+    assert s0.converged and s1.converged, (s0.status, s1.status)
+    assert abs(s0.iterations - s1.iterations) <= 1, (s0.iterations, s1.iterations)
+    assert s0.initial_residual == pytest.approx(s1.initial_residual, rel=1e-13)
+    assert rel(to_np(x1), to_np(x0)) < 1e-8
+
+
+def test_staged_box_cg_fixed_iterations_match_register_kernel():
+    """With tolerances 0 both kernels run exactly max_iter iterations; the
+    SpMV products are bitwise those of BoxRows, so the two iterates differ
+    only through the order of the dot-product partial sums."""
+    from gridfoam_b200.solvers.autotune import BoxSystem, _solver
+
+    sysm = BoxSystem(32, 16, 48, device=torch.device("cuda"))
+    xs = []
+    for v in (0, 5):
+        s = _solver(50, False, v)
+        x = torch.zeros_like(sysm.rhs)
+        st = s.solve_arrays(sysm, sysm.diag, sysm.val, sysm.rhs, x, symmetric=True)
+        assert st[0].iterations == 50 and st[0].status == "max_iter"
+        xs.append(to_np(x))
+    assert rel(xs[1], xs[0]) < 1e-11
