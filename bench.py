@@ -225,6 +225,58 @@ def mixed_variant(args, local: int, ref_algo, torch) -> dict:
     }
 
 
+def serving_bench(args, local: int) -> dict:
+    """Solve-server stream (cavity SIMPLE solves of uneven sizes arriving as
+    a Poisson process): the continuous-batching engine (FP64, and FP32-inner
+    pressure CG) against one-at-a-time FP64 solves through the plain API,
+    on the same requests."""
+    import numpy as np
+    import torch
+
+    from gridfoam_b200.serving import SIZES, ServingEngine, poisson_stream, serve_sequential, summarize
+
+    reqs = poisson_stream(args.serve_requests, rate=50.0, sizes=SIZES, seed=local)
+    common = dict(max_outer=args.serve_end_time, p_tol=1e-6, p_solver_tol=1e-6, keep_fields=True)
+    out = {
+        "workload": "cavity SIMPLE stream: sizes uniform over 16^3..96^3, Re log-uniform [10,1000], "
+                    "lid U uniform [0.5,2], Poisson arrivals 50/s, p cg tol 1e-6, residualControl p 1e-6",
+        "requests": len(reqs),
+        "end_time": args.serve_end_time,
+        "sample": f"{len(reqs)} of the 1024-request stream, endTime capped at {args.serve_end_time} iterations",
+    }
+    runs = {}
+    for name, kw in (("engine_fp64", {}), ("engine_mixed", {"inner_precision": "float32"})):
+        eng = ServingEngine(device=f"cuda:{local}", max_slots=args.serve_slots, gpu_share=args.serve_share,
+                            **common, **kw)
+        t0 = time.perf_counter()
+        eng.prepare(SIZES)
+        prep = time.perf_counter() - t0
+        res = eng.run(reqs)
+        runs[name] = {r.id: r for r in res}
+        if name == "engine_fp64":
+            fp_variants = dict(eng.variants)
+        out[name] = {**summarize(res), "prepare_s": prep, "slots": args.serve_slots, "gpu_share": args.serve_share,
+                     "autotuned_variants": {str(k): v for k, v in eng.variants.items()}}
+        del eng
+        torch.cuda.empty_cache()
+    seq = serve_sequential(reqs, device=f"cuda:{local}", variants=fp_variants, **common)
+    runs["sequential_fp64"] = {r.id: r for r in seq}
+    out["sequential_fp64"] = summarize(seq)
+    fp = runs["engine_fp64"]
+    same = all(np.array_equal(fp[i].U, runs["sequential_fp64"][i].U) or
+               np.allclose(fp[i].U, runs["sequential_fp64"][i].U, rtol=0, atol=1e-12) for i in fp)
+    errs = []
+    for i, r in runs["engine_mixed"].items():
+        ref = fp[i].U
+        errs.append(float(np.linalg.norm(r.U - ref) / max(np.linalg.norm(ref), 1e-300)))
+    out["engine_fp64"]["matches_sequential"] = bool(same)
+    out["engine_mixed"]["max_rel_l2_U_vs_fp64"] = max(errs) if errs else None
+    for k in ("engine_fp64", "engine_mixed"):
+        out[k]["speedup_solves_per_s_vs_sequential"] = (
+            out[k]["solves_per_s"] / out["sequential_fp64"]["solves_per_s"])
+    return out
+
+
 def run_gpu(args) -> None:
     import torch
 
@@ -360,6 +412,8 @@ def run_gpu(args) -> None:
     }
     if not args.no_variants:
         line["variants"] = {"mixed_fp32_inner": mixed_variant(args, local, algo, torch)}
+    if not args.no_serving and world == 1:
+        line["serving"] = serving_bench(args, local)
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
     if rank == 0:
@@ -378,6 +432,11 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-variants", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=64)
+    ap.add_argument("--serve-end-time", type=int, default=100)
+    ap.add_argument("--serve-slots", type=int, default=16)
+    ap.add_argument("--serve-share", type=float, default=0.25)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -81,6 +81,10 @@ class _PressureVelocity:
         self.nu_t = get_or_create_cellfield(g, "nu_t", FieldRole.LOCAL, ())
         sim = g.sim_config
         self._solvers = {name: create_solver(cfg) for name, cfg in sim.fvSolution.solvers.items()}
+        # False: a step makes no pinned host copies (solver statistics,
+        # residual scalars), so it can be captured into a CUDA graph; the
+        # residuals stay in ``res_buf`` on the device.
+        self.host_readback = True
         self.nu = float(sim.properties.transport.nu)
         alg = sim.fvSolution.algorithm
         self._alg = alg
@@ -122,6 +126,17 @@ class _PressureVelocity:
     @property
     def solvers(self) -> dict:
         return self._solvers
+
+    def set_host_readback(self, enabled: bool) -> None:
+        """Switch the per-step pinned host copies on or off (see ``host_readback``)."""
+        self.host_readback = bool(enabled)
+        for s in self._solvers.values():
+            s.host_stats = bool(enabled)
+
+    @property
+    def p_residual(self) -> torch.Tensor:
+        """Device scalar: the last recorded pressure-equation residual."""
+        return self.res_buf[0:1]
 
     def set_grad_mode(self, grad_mode: str) -> None:
         for solver in self._solvers.values():
@@ -351,7 +366,7 @@ class _PressureVelocity:
             if record:
                 call("gf_field_residual", byref(g.cmesh), 1, ptr(d), ptr(v), ptr(src), ptr(self.p.store),
                      ptr(self.scratch), ptr(self.res_buf), s)
-                last_res = _LazyScalar(self.res_buf[0])
+                last_res = _LazyScalar(self.res_buf[0]) if self.host_readback else None
                 if first_res is None:
                     first_res = last_res
             solver = self._solvers[self.p.name]
@@ -389,7 +404,7 @@ class _PressureVelocity:
         g = self._grid
         call("gf_field_residual", byref(g.cmesh), field.num_components, ptr(d), ptr(v), ptr(src),
              ptr(field.store), ptr(self.scratch), ptr(self.res_buf[1:]), stream_ptr())
-        self._pending_residual = (key, _LazyScalar(self.res_buf[1]))
+        self._pending_residual = (key, _LazyScalar(self.res_buf[1]) if self.host_readback else None)
 
     def continuity_residual(self) -> float:
         """residual.py:39-53: |div(phi)|_2."""

@@ -91,6 +91,17 @@ class AxisProjectedGrid:
         self._upload()
         self._mesh_ref = None
 
+    def with_config(self, simulator_config: SimulatorConfig) -> "AxisProjectedGrid":
+        """A grid sharing this one's topology, geometry and device arrays
+        (all read-only after set-up) with its own configuration and field
+        registry: many cases on one mesh pay the host set-up once."""
+        g = object.__new__(AxisProjectedGrid)
+        g.__dict__.update(self.__dict__)
+        g._sim_config = simulator_config
+        g._cellfields = {}
+        g._facefields = {}
+        return g
+
     # ------------------------------------------------------------------
     # host set-up
     # ------------------------------------------------------------------

@@ -18,20 +18,20 @@ from gridfoam_b200._lib import GfKrylov, call, load, ptr, stream_ptr
 from gridfoam_b200.meta.config import NormType, PrecisionType, PreconditionerType, SolverConfig
 from gridfoam_b200.solvers.base import LinearSolver, SolveResult, SolveStats, _StatsBuffer
 
-_WORKSPACES: dict[tuple, torch.Tensor] = {}
+def workspace(cache: dict, device: torch.device, n: int, ncomp: int, kind: int) -> torch.Tensor:
+    """Per-shape workspace held in ``cache`` (allocated once, reused by
+    every solve of its owner).
 
-
-def workspace(device: torch.device, n: int, ncomp: int, kind: int) -> torch.Tensor:
-    """Cached per-shape workspace (allocated once, reused by every solve).
-
-    ``kind``: 0 CG, 1 BiCGStab, ``2 + 100 * width`` mixed-precision CG.
+    Each solver owns its cache: solves on different streams (concurrent
+    cases) must never share scratch.  ``kind``: 0 CG, 1 BiCGStab,
+    ``2 + 100 * width`` mixed-precision CG.
     """
     key = (str(device), n, ncomp, kind)
-    ws = _WORKSPACES.get(key)
+    ws = cache.get(key)
     if ws is None:
         size = load().gf_krylov_workspace_size(n, ncomp, kind)
         ws = torch.empty(size, dtype=torch.float64, device=device)
-        _WORKSPACES[key] = ws
+        cache[key] = ws
     return ws
 
 
@@ -66,6 +66,7 @@ class DeviceKrylov(LinearSolver):
         self.max_outer = int(config.max_outer)
         self.inner_eta = float(config.inner_eta)
         self._stats_dev: dict[tuple, torch.Tensor] = {}
+        self._workspaces: dict[tuple, torch.Tensor] = {}
         # Optional list receiving (start event, end event, stats) per solve.
         self.profile_events: list | None = None
         # Upper bound on persistent blocks (0: one wave at full occupancy).
@@ -75,6 +76,9 @@ class DeviceKrylov(LinearSolver):
         self.variant: int | None = None
         # FP64 CG with one grid reduction per iteration (Chronopoulos-Gear).
         self.single_reduction = False
+        # False: no pinned statistics copy per solve (stream capture into a
+        # CUDA graph); the statistics stay in the device buffer.
+        self.host_stats = True
 
     def solve_arrays(self, grid, diag: torch.Tensor, val: torch.Tensor, rhs: torch.Tensor,
                      x: torch.Tensor, *, symmetric: bool = False) -> tuple[SolveStats, ...]:
@@ -91,7 +95,7 @@ class DeviceKrylov(LinearSolver):
             self._stats_dev[key] = stats
         mixed = self.mixed and nc == 1 and not self.bicgstab
         kind = (2 + 100 * grid.ell_width) if mixed else int(self.bicgstab)
-        ws = workspace(grid.device, n, nc, kind)
+        ws = workspace(self._workspaces, grid.device, n, nc, kind)
         k = GfKrylov()
         k.n = n
         k.width = grid.ell_width
@@ -127,6 +131,8 @@ class DeviceKrylov(LinearSolver):
         call("gf_bicgstab_solve" if self.bicgstab else "gf_pcg_solve", ctypes.byref(k), stream_ptr())
         if ev is not None:
             ev[1].record()
+        if not self.host_stats:
+            return ()
         buf = _StatsBuffer(stats)
         out = tuple(SolveStats(self.solver_name, buf, i) for i in range(nc))
         if ev is not None:
