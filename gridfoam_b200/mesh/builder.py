@@ -253,3 +253,204 @@ def _axis_projected_payload(
         neighbour_near_boundary=(d_nei / dx_nei) <= (dx_nei / extent),
     )
     return ap, patches
+
+
+# ----------------------------------------------------------------------
+# Octree meshes (2:1 balanced, hanging faces)
+# ----------------------------------------------------------------------
+@dataclass
+class BoxRegion:
+    """Refine every leaf that holds a finest-level cell centre inside the
+    box ``[lo, hi]`` to at least ``level``."""
+
+    lo: tuple[float, float, float]
+    hi: tuple[float, float, float]
+    level: int
+
+
+@dataclass
+class SdfRegion:
+    """Refine to ``level`` where the body's signed distance is below
+    ``distance`` (a band around and inside the body)."""
+
+    sdf: SdfFn
+    distance: float
+    level: int
+
+
+def _block_max(a: np.ndarray, s: int) -> np.ndarray:
+    """Max over aligned ``s^3`` blocks of a 3-D array (sizes divisible by s)."""
+    X, Y, Z = a.shape
+    return a.reshape(X // s, s, Y // s, s, Z // s, s).max(axis=(1, 3, 5))
+
+
+def _morton(i: np.ndarray, j: np.ndarray, k: np.ndarray, bits: int) -> np.ndarray:
+    code = np.zeros(i.shape, dtype=np.int64)
+    for b in range(bits):
+        code |= ((i >> b) & 1) << (3 * b)
+        code |= ((j >> b) & 1) << (3 * b + 1)
+        code |= ((k >> b) & 1) << (3 * b + 2)
+    return code
+
+
+def build_octree_mesh(
+    lower: tuple[float, float, float],
+    upper: tuple[float, float, float],
+    root_resolution: tuple[int, int, int],
+    regions: list | None = None,
+    *,
+    bodies: list[Body] | None = None,
+) -> FluxelMesh:
+    """Octree refinement of a root Cartesian grid, 2:1 balanced across faces.
+
+    Leaves are refined to the highest level any region asks for, then leaves
+    with a face neighbour more than one level finer are refined until the
+    2:1 rule holds.  The result follows the fluxel mesh contract:
+
+    * one internal face per fine sub-face at a coarse-fine interface, owner
+      the lower-coordinate cell (the reference derives the face centre as
+      the centre of the two cells' overlap and the area from the finer cell,
+      ``core/grid/axis_projected.py:715-767``);
+    * one domain-boundary face per leaf face on the domain boundary;
+    * cells sorted by refinement level, then Morton order of their
+      finest-level lower corner; internal faces sorted by (axis, owner,
+      neighbour), domain faces by (direction, owner).
+
+    Immersed bodies must lie inside uniformly refined regions: an immersed
+    face between cells of different levels raises ``ValueError``.
+    """
+    regions = list(regions or [])
+    rx, ry, rz = (int(v) for v in root_resolution)
+    lo = np.asarray(lower, dtype=np.float64)
+    hi = np.asarray(upper, dtype=np.float64)
+    L = max([r.level for r in regions], default=0)
+    f = 1 << L
+    FX, FY, FZ = rx * f, ry * f, rz * f
+    hf = (hi - lo) / np.array([FX, FY, FZ], dtype=np.float64)
+
+    # Required level per finest cell (max over regions).
+    req = np.zeros((FX, FY, FZ), dtype=np.int8)
+    if regions:
+        xs = lo[0] + (np.arange(FX) + 0.5) * hf[0]
+        ys = lo[1] + (np.arange(FY) + 0.5) * hf[1]
+        zs = lo[2] + (np.arange(FZ) + 0.5) * hf[2]
+        for r in regions:
+            if isinstance(r, BoxRegion):
+                mx = (xs >= r.lo[0]) & (xs <= r.hi[0])
+                my = (ys >= r.lo[1]) & (ys <= r.hi[1])
+                mz = (zs >= r.lo[2]) & (zs <= r.hi[2])
+                m = mx[:, None, None] & my[None, :, None] & mz[None, None, :]
+            elif isinstance(r, SdfRegion):
+                P = np.stack(np.meshgrid(xs, ys, zs, indexing="ij"), axis=-1)
+                m = r.sdf(P) <= r.distance
+            else:
+                raise TypeError(f"unknown refinement region {r!r}")
+            req = np.maximum(req, np.where(m, np.int8(r.level), np.int8(0)))
+
+    # Level of the leaf covering each finest cell; refine level by level.
+    lev = np.zeros((FX, FY, FZ), dtype=np.int8)
+    for _ in range(64):
+        changed = False
+        # 2:1 balance: highest level among each finest cell's face neighbours.
+        nb = lev.copy()
+        for ax in range(3):
+            sl_a = [slice(None)] * 3
+            sl_b = [slice(None)] * 3
+            sl_a[ax], sl_b[ax] = slice(1, None), slice(None, -1)
+            np.maximum(nb[tuple(sl_b)], lev[tuple(sl_a)], out=nb[tuple(sl_b)])
+            np.maximum(nb[tuple(sl_a)], lev[tuple(sl_b)], out=nb[tuple(sl_a)])
+        for level in range(L):
+            s = 1 << (L - level)
+            at = _block_max(lev, s) == level  # leaves of this level (uniform blocks)
+            at &= -_block_max(-lev, s) == level
+            want = (_block_max(req, s) > level) | (_block_max(nb, s) > level + 1)
+            grow = at & want
+            if np.any(grow):
+                changed = True
+                g = np.repeat(np.repeat(np.repeat(grow, s, 0), s, 1), s, 2)
+                lev[g] = level + 1
+        if not changed:
+            break
+    else:
+        raise RuntimeError("octree refinement did not settle")
+
+    # Leaves: one per aligned block of its level.
+    li, lj, lk, ll = [], [], [], []
+    for level in range(L + 1):
+        s = 1 << (L - level)
+        blk = (_block_max(lev, s) == level) & (-_block_max(-lev, s) == level)
+        I, J, K = np.nonzero(blk)
+        li.append(I * s)
+        lj.append(J * s)
+        lk.append(K * s)
+        ll.append(np.full(I.shape, level, dtype=np.int64))
+    li, lj, lk, ll = (np.concatenate(a).astype(np.int64) for a in (li, lj, lk, ll))
+    bits = int(np.ceil(np.log2(max(FX, FY, FZ, 2))))
+    order = np.lexsort((_morton(li, lj, lk, bits), ll))
+    li, lj, lk, ll = li[order], lj[order], lk[order], ll[order]
+    n_cells = li.shape[0]
+    size_f = (1 << (L - ll)).astype(np.int64)  # leaf edge in finest cells
+
+    ids = np.empty((FX, FY, FZ), dtype=np.int64)
+    for level in range(L + 1):
+        s = 1 << (L - level)
+        sel = np.nonzero(ll == level)[0]
+        if sel.size == 0:
+            continue
+        blk = np.full((FX // s, FY // s, FZ // s), -1, dtype=np.int64)
+        blk[li[sel] // s, lj[sel] // s, lk[sel] // s] = sel
+        full = np.repeat(np.repeat(np.repeat(blk, s, 0), s, 1), s, 2)
+        m = full >= 0
+        ids[m] = full[m]
+
+    centers = np.stack(
+        [lo[0] + (li + 0.5 * size_f) * hf[0], lo[1] + (lj + 0.5 * size_f) * hf[1],
+         lo[2] + (lk + 0.5 * size_f) * hf[2]], axis=1)
+    sizes = size_f[:, None] * hf[None, :]
+
+    owners, neighbours, axes = [], [], []
+    for ax in range(3):
+        sl_a = [slice(None)] * 3
+        sl_b = [slice(None)] * 3
+        sl_a[ax], sl_b[ax] = slice(None, -1), slice(1, None)
+        a = ids[tuple(sl_a)].ravel()
+        b = ids[tuple(sl_b)].ravel()
+        d = a != b
+        pairs = np.unique(np.stack([a[d], b[d]], axis=1), axis=0)
+        owners.append(pairs[:, 0])
+        neighbours.append(pairs[:, 1])
+        axes.append(np.full(pairs.shape[0], ax, dtype=np.int64))
+    owner = np.concatenate(owners)
+    neighbour = np.concatenate(neighbours)
+    axis_arr = np.concatenate(axes)
+
+    bnd_owner, bnd_dir = [], []
+    for direction in range(6):
+        ax, side_max = direction // 2, direction % 2 == 1
+        sl = [slice(None)] * 3
+        sl[ax] = -1 if side_max else 0
+        cells = np.unique(ids[tuple(sl)].ravel())
+        bnd_owner.append(cells)
+        bnd_dir.append(np.full(cells.shape, direction, dtype=np.int64))
+    domain_owner = np.concatenate(bnd_owner)
+    domain_dir = np.concatenate(bnd_dir)
+
+    extent = float(np.max(hi - lo))
+    ap, patches = _axis_projected_payload(centers, sizes, owner, neighbour, axis_arr, bodies or [], extent)
+    imm = np.nonzero(ap.is_immersed_face)[0]
+    if imm.size and np.any(ll[owner[imm]] != ll[neighbour[imm]]):
+        raise ValueError("an immersed face lies on a coarse-fine interface; refine around the body")
+    return FluxelMesh(
+        n_cells=n_cells,
+        internal_faces_owner=owner,
+        internal_faces_neighbour=neighbour,
+        internal_faces_axis=axis_arr,
+        domain_bnd_faces_owner=domain_owner,
+        domain_bnd_faces_dir=domain_dir,
+        patch_name_to_id=patches,
+        cell_centers=centers,
+        cell_sizes=sizes,
+        ap=ap,
+        resolution=None if L > 0 else (rx, ry, rz),
+        meta={"lower": tuple(lo), "upper": tuple(hi), "levels": ll, "root_resolution": (rx, ry, rz)},
+    )

@@ -14,6 +14,9 @@ import numpy as np
 
 from gridfoam_b200.mesh.builder import (
     Body,
+    BoxRegion,
+    SdfRegion,
+    build_octree_mesh,
     build_uniform_mesh,
     cylinder_sdf,
     plane_sdf,
@@ -350,17 +353,27 @@ def ibplane_case() -> dict:
     }
 
 
+def _sdf(b: dict):
+    if b["kind"] == "cylinder":
+        return cylinder_sdf(tuple(b["center"]), b["radius"], b["axis"])
+    if b["kind"] == "plane":
+        return plane_sdf(b["point"], b["axis"])
+    raise ValueError(b["kind"])
+
+
 def build_mesh(spec: dict):
     """Build the mesh described by a case's ``mesh`` entry."""
-    bodies = []
-    for b in spec.get("bodies", []):
-        if b["kind"] == "cylinder":
-            sdf = cylinder_sdf(tuple(b["center"]), b["radius"], b["axis"])
-        elif b["kind"] == "plane":
-            sdf = plane_sdf(b["point"], b["axis"])
-        else:
-            raise ValueError(b["kind"])
-        bodies.append(Body(sdf=sdf, patch=b["patch"]))
+    bodies = [Body(sdf=_sdf(b), patch=b["patch"]) for b in spec.get("bodies", [])]
+    if spec["kind"] == "octree":
+        regions = []
+        for r in spec.get("regions", []):
+            if r["kind"] == "box":
+                regions.append(BoxRegion(tuple(r["lo"]), tuple(r["hi"]), r["level"]))
+            else:
+                regions.append(SdfRegion(_sdf(r["body"]), r["distance"], r["level"]))
+        return build_octree_mesh(
+            tuple(spec["lower"]), tuple(spec["upper"]), tuple(spec["res"]), regions, bodies=bodies
+        )
     return build_uniform_mesh(
         tuple(spec["lower"]), tuple(spec["upper"]), tuple(spec["res"]), bodies=bodies
     )
@@ -381,17 +394,141 @@ def inlet_profile_values(mesh, profile: dict) -> np.ndarray:
     return out
 
 
+def cavity_oct_case() -> dict:
+    """Cavity on a two-level octree: refined under the lid and again near
+    its centre, so hanging faces meet the lid, the walls and each other.
+    SIMPLE, linear convection, corrected Laplacian."""
+    case = cavity_case(6)
+    case["name"] = "cavity_oct"
+    case["mesh"] = {
+        "kind": "octree", "lower": [0, 0, 0], "upper": [1, 1, 1], "res": [6, 6, 6],
+        "regions": [
+            {"kind": "box", "lo": [0.2, 0.55, 0.2], "hi": [0.8, 1.0, 0.8], "level": 1},
+            {"kind": "box", "lo": [0.4, 0.8, 0.4], "hi": [0.6, 1.0, 0.6], "level": 2},
+        ],
+    }
+    return case
+
+
+def duct_oct_case() -> dict:
+    """Duct flow on an octree refined in the middle: PISO, vanLeer TVD
+    convection (the hanging-face offset correction of the linear value),
+    inletOutlet outlet."""
+    sim = {
+        "control": _control(0.01, 1.0),
+        "fvSchemes": {"divSchemes": {"default": "vanleer"}},
+        "fvSolution": {
+            "adjustPhi": True,
+            "algorithm": {"type": "piso", "nCorrectors": 2, "pRefCell": 0, "pRefValue": 0.0},
+            "solvers": {
+                "U": {"method": "bicgstab", "preconditioner": "jacobi", "tolerance": 1e-10, "rel_tolerance": 0.0},
+                "p": {"method": "cg", "preconditioner": "jacobi", "tolerance": 1e-9, "rel_tolerance": 0.0},
+            },
+        },
+        "conditions": {
+            "U": {
+                "internal": [0.2, 0.0, 0.0],
+                "boundary": {
+                    "inlet": {"type": "dirichlet", "patches": ["x_minus"], "value": [1.0, 0.0, 0.0]},
+                    "outlet": {"type": "inlet_outlet", "patches": ["x_plus"], "value": WALL0},
+                    "walls": {"type": "dirichlet", "patches": ["y_minus", "y_plus", "z_minus", "z_plus"],
+                              "value": WALL0},
+                },
+            },
+            "p": {
+                "internal": 0.0,
+                "boundary": {
+                    "inlet": {"type": "neumann", "patches": ["x_minus"], "value": 0.0},
+                    "outlet": {"type": "dirichlet", "patches": ["x_plus"], "value": 0.0},
+                    "walls": {"type": "neumann", "patches": ["y_minus", "y_plus", "z_minus", "z_plus"],
+                              "value": 0.0},
+                },
+            },
+        },
+        "properties": _props(0.02),
+        "device": "cpu",
+    }
+    return {
+        "name": "duct_oct",
+        "mesh": {
+            "kind": "octree", "lower": [0, 0, 0], "upper": [2.0, 1.0, 1.0], "res": [8, 4, 4],
+            "regions": [{"kind": "box", "lo": [0.6, 0.2, 0.2], "hi": [1.4, 0.8, 0.8], "level": 1}],
+        },
+        "simulator": sim,
+        "inlet_profile": None,
+    }
+
+
+def ibcyl_oct_case() -> dict:
+    """Immersed cylinder inside a refined band (octree), PISO, upwind: IB
+    faces on the fine level, hanging faces around the band."""
+    cyl = {"kind": "cylinder", "center": [0.5, 0.5], "radius": 0.2, "axis": 2, "patch": "cylinder"}
+    sim = {
+        "control": _control(5e-3, 1.0),
+        "fvSchemes": {"divSchemes": {"default": "upwind"}},
+        "fvSolution": {
+            "adjustPhi": True,
+            "algorithm": {"type": "piso", "nCorrectors": 2, "pRefCell": 0, "pRefValue": 0.0},
+            "solvers": {
+                "U": {"method": "bicgstab", "preconditioner": "jacobi", "tolerance": 1e-10, "rel_tolerance": 0.0},
+                "p": {"method": "cg", "preconditioner": "jacobi", "tolerance": 1e-9, "rel_tolerance": 0.0},
+            },
+        },
+        "conditions": {
+            "U": {
+                "internal": [0.5, 0.0, 0.0],
+                "boundary": {
+                    "inlet": {"type": "dirichlet", "patches": ["x_minus"], "value": [1.0, 0.0, 0.0]},
+                    "outlet": {"type": "neumann", "patches": ["x_plus"], "value": WALL0},
+                    "side": {"type": "slip", "patches": ["y_minus", "y_plus"]},
+                    "ends": {"type": "neumann", "patches": ["z_minus", "z_plus"], "value": WALL0},
+                    "cyl": {"type": "dirichlet", "patches": ["cylinder"], "value": WALL0},
+                },
+            },
+            "p": {
+                "internal": 0.0,
+                "boundary": {
+                    "outlet": {"type": "dirichlet", "patches": ["x_plus"], "value": 0.0},
+                    # Dirichlet on the body also pins the (disconnected) interior.
+                    "cyl": {"type": "dirichlet", "patches": ["cylinder"], "value": 0.0},
+                    "rest": {"type": "neumann",
+                             "patches": ["x_minus", "y_minus", "y_plus", "z_minus", "z_plus"],
+                             "value": 0.0},
+                },
+            },
+        },
+        "properties": _props(0.05),
+        "device": "cpu",
+    }
+    return {
+        "name": "ibcyl_oct",
+        "mesh": {
+            "kind": "octree", "lower": [0, 0, 0], "upper": [1.0, 1.0, 0.5], "res": [8, 8, 4],
+            "regions": [{"kind": "sdf", "body": cyl, "distance": 0.12, "level": 1}],
+            "bodies": [cyl],
+        },
+        "simulator": sim,
+        "inlet_profile": None,
+    }
+
+
 ALL_CASES = {
     "cavity8": lambda: cavity_case(8),
     "pipe10x20": lambda: pipe_case(10, 20),
     "channel": channel_case,
     "channel_ffp": ffp_case,
     "ibplane": ibplane_case,
+    "cavity_oct": cavity_oct_case,
+    "duct_oct": duct_oct_case,
+    "ibcyl_oct": ibcyl_oct_case,
 }
+# Cases on octree meshes (hanging faces).
+OCTREE_CASES = ("cavity_oct", "duct_oct", "ibcyl_oct")
 
 
 # Steps stored per golden case and the convection schemes dumped per case.
-STEPS = {"cavity8": 4, "pipe10x20": 3, "channel": 3, "channel_ffp": 3, "ibplane": 3}
+STEPS = {"cavity8": 4, "pipe10x20": 3, "channel": 3, "channel_ffp": 3, "ibplane": 3,
+         "cavity_oct": 4, "duct_oct": 3, "ibcyl_oct": 3}
 DIV_SCHEMES = [
     "upwind",
     "linear",

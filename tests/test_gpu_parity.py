@@ -16,12 +16,12 @@ import pytest
 torch = pytest.importorskip("torch")
 
 from tests.golden.device_harness import device_case, to_np  # noqa: E402
-from tests.golden.cases import DIV_SCHEMES, STEPS  # noqa: E402
+from tests.golden.cases import DIV_SCHEMES, OCTREE_CASES, STEPS  # noqa: E402
 from tests.golden.oracle_harness import load_golden  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
-CASES = list(STEPS)
+CASES = [c for c in STEPS if c not in OCTREE_CASES]
 # Relative L2 tolerance of whole-step fields against the reference run.
 STEP_TOL = {"cavity8": 1e-10, "channel": 1e-9, "channel_ffp": 1e-9, "ibplane": 1e-10, "pipe10x20": 1e-4}
 

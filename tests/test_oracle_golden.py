@@ -21,7 +21,8 @@ from tests.golden.oracle_ops_check import oracle_operator_outputs
 
 CASES = list(STEPS)
 # Relative L2 tolerance of whole-step fields against the reference.
-STEP_TOL = {"cavity8": 1e-12, "channel": 1e-11, "channel_ffp": 1e-11, "ibplane": 1e-12, "pipe10x20": 1e-4}
+STEP_TOL = {"cavity8": 1e-12, "channel": 1e-11, "channel_ffp": 1e-11, "ibplane": 1e-12, "pipe10x20": 1e-4,
+            "cavity_oct": 1e-11, "duct_oct": 1e-9, "ibcyl_oct": 1e-9}
 
 
 def rel(a: np.ndarray, b: np.ndarray) -> float:
@@ -53,7 +54,10 @@ def test_oracle_steps_match_reference(name):
     for step in range(STEPS[name]):
         algo.step()
         assert rel(algo.U.data, golden[f"step{step}_U"]) < tol
-        assert rel(algo.p.data, golden[f"step{step}_p"]) < max(tol, 10 * tol if name.startswith("pipe") else tol)
+        # p carries the Krylov stopping band (absolute tolerance 1e-9 on the
+        # octree cases) more directly than U.
+        ptol = 10 * tol if name.startswith("pipe") or name.endswith("_oct") else tol
+        assert rel(algo.p.data, golden[f"step{step}_p"]) < ptol
         assert rel(algo.phi.pack(), golden[f"step{step}_phi"]) < tol
         its_u = [s.iterations for s in algo.last_stats["U"]]
         its_p = [s.iterations for s in algo.last_stats["p"]]
@@ -62,7 +66,7 @@ def test_oracle_steps_match_reference(name):
         assert np.all(np.abs(np.array(its_p) - golden[f"step{step}_stats_p"][:, 2]) <= slack)
 
 
-@pytest.mark.parametrize("name", ["cavity8", "pipe10x20", "channel", "channel_ffp", "ibplane"])
+@pytest.mark.parametrize("name", CASES)
 def test_oracle_operators_match_reference(name):
     out, golden = oracle_operator_outputs(name)
     flux_scale = np.abs(golden[f"step{STEPS[name]-1}_phi"]).max()
