@@ -72,6 +72,12 @@ class GfMesh(ctypes.Structure):
         ("bnd_near", P),
         ("face_pos_owner", P),
         ("face_pos_neigh", P),
+        ("n_hang", I64),
+        ("hang_face", P),
+        ("face_hang", P),
+        ("hang_offset", P),
+        ("hang_move_o", P),
+        ("hang_move_n", P),
     ]
 
 
@@ -119,6 +125,10 @@ class GfAssembly(ctypes.Structure):
         ("diag", P),
         ("val", P),
         ("source", P),
+        ("lap_corrected", I32),
+        ("reserved", I32),
+        ("grad_lsq", P),
+        ("ffc", P),
     ]
 
 
@@ -183,11 +193,11 @@ _SIGNATURES = {
     "gf_bicgstab_solve": ([P, P], ctypes.c_int),
     "gf_rau_hbya": ([P, I32, P, P, P, P, P, P, P, P], ctypes.c_int),
     "gf_simplec_rAtU": ([P, P, P, P, P], ctypes.c_int),
-    "gf_face_flux": ([P, I32, P, P, P, P, P, P], ctypes.c_int),
+    "gf_face_flux": ([P, I32, P, P, P, P, P, P, P], ctypes.c_int),
     "gf_fvc_div": ([P, I32, P, P, P], ctypes.c_int),
-    "gf_interpolate": ([P, I32, P, P, P, P, P], ctypes.c_int),
-    "gf_sn_grad": ([P, I32, P, P, P, P, P, P, P], ctypes.c_int),
-    "gf_correct_phi": ([P, P, P, P, P, P, P, P, F64, I32, P, P], ctypes.c_int),
+    "gf_interpolate": ([P, I32, P, P, P, P, P, P], ctypes.c_int),
+    "gf_sn_grad": ([P, I32, P, P, P, P, P, P, P, P], ctypes.c_int),
+    "gf_correct_phi": ([P, P, P, P, P, P, P, P, F64, I32, P, P, P, P], ctypes.c_int),
     "gf_close_fixed_flux": ([P, I64, P, P, P, P, P], ctypes.c_int),
     "gf_correct_velocity": ([P, P, P, P, P, P], ctypes.c_int),
     "gf_set_cell_values": ([I64, I32, I64, P, P, I64, P, P], ctypes.c_int),
@@ -198,7 +208,7 @@ _SIGNATURES = {
     "gf_ell_to_ldu": ([P, P, P, P, P], ctypes.c_int),
     "gf_ldu_to_ell": ([P, P, P, P, P], ctypes.c_int),
     "gf_field_residual": ([P, I32, P, P, P, P, P, P, P], ctypes.c_int),
-    "gf_matrix_flux": ([P, I32, P, P, P, P], ctypes.c_int),
+    "gf_matrix_flux": ([P, I32, P, P, P, P, P], ctypes.c_int),
 }
 
 EXPORTED = tuple(_SIGNATURES)

@@ -102,6 +102,11 @@ class _PressureVelocity:
             self.p_ref_value = float(alg.pRefValue)
         self._u_harmonic = int(schemes.laplacian_scheme(sim, self.U.name) in schemes.HARMONIC)
         self._p_harmonic = int(schemes.laplacian_scheme(sim, self.p.name) in schemes.HARMONIC)
+        self._u_corrected = int(schemes.laplacian_scheme(sim, self.U.name) in schemes.CORRECTED)
+        self._p_corrected = int(schemes.laplacian_scheme(sim, self.p.name) in schemes.CORRECTED)
+        # Octree meshes: explicit hanging-face corrections need least-squares
+        # gradients of U, p and HbyA (fv/kernels/face_interpolation.py).
+        self._hanging = g.num_hanging > 0
         self._div_code = _lib.DIV_CODES[schemes.div_scheme(sim, self.phi.name, self.U.name).value]
         for fld in (self.U, self.p):
             if schemes.grad_scheme(sim, fld.name) != GradScheme.LEASTSQUARE:
@@ -112,8 +117,11 @@ class _PressureVelocity:
         self.last_stats: dict = {}
         # flux.py:132-162 correct_flux(phi, U, update_internal=True)
         self._eval_U()
+        if self._hanging:
+            self._grad(self.U, self.grad_U)
         call("gf_face_flux", byref(g.cmesh), 0, ptr(self.U.store), ptr(self.U.table.kind),
-             ptr(self.U.table.psib), None, ptr(self.phi.store), stream_ptr())
+             ptr(self.U.table.psib), None, ptr(self.grad_U) if self._hanging else None, ptr(self.phi.store),
+             stream_ptr())
         if self.transient:
             self.U.update_history(reset=True)
             self.phi.update_history(reset=True)
@@ -157,6 +165,10 @@ class _PressureVelocity:
         self.pred_source = torch.zeros((3, C), **f64)
         self.grad_p = torch.zeros((3, C), **f64)
         self.grad_U = torch.zeros((9, C), **f64)
+        # Hanging faces: HbyA gradient and the pressure Laplacian's face flux
+        # correction (zero off hanging faces).
+        self.grad_H = torch.zeros((9, C) if self._hanging else (9, 1), **f64)
+        self.p_ffc = torch.zeros(max(1, g.num_internal_faces) if self._hanging else 1, **f64)
         self.div_buf = torch.zeros(C, **f64)
         self.p_old = torch.zeros(C, **f64)
         self.h1 = torch.zeros(C, **f64)
@@ -216,7 +228,7 @@ class _PressureVelocity:
     def _assemble_momentum(self, relax: float) -> None:
         g = self._grid
         self._eval_U()
-        if self._div_code >= _lib.DIV_CODES["vanleer"]:
+        if self._div_code >= _lib.DIV_CODES["vanleer"] or self._hanging:
             self._grad(self.U, self.grad_U)
         a = GfAssembly()
         a.ncomp = 3
@@ -243,6 +255,9 @@ class _PressureVelocity:
         a.diag = ptr(self.UEqn.diag_store)
         a.val = ptr(self.UEqn.val)
         a.source = ptr(self.UEqn.source_store)
+        if self._hanging:
+            a.grad_lsq = ptr(self.grad_U)
+            a.lap_corrected = self._u_corrected
         s = stream_ptr()
         call("gf_assemble", byref(g.cmesh), byref(a), s)
         if relax > 0.0:
@@ -316,8 +331,16 @@ class _PressureVelocity:
             d.phi_old = ptr(self.phi.old_store)
             d.phi_older = ptr(self.phi.older_store) if cc != 0.0 else None
             d.b, d.c, d.dt = cb, cc, g.dt
+        grad_h = None
+        if self._hanging:
+            # fvc.interpolate(HbyA): HbyA carries no boundary conditions, so
+            # its least-squares gradient has internal equations only.
+            t = self.HbyA.table
+            call("gf_lsq_grad", byref(g.cmesh), 3, ptr(self.HbyA.store), ptr(t.kind), ptr(t.psib),
+                 ptr(self.grad_H), s)
+            grad_h = ptr(self.grad_H)
         call("gf_face_flux", byref(g.cmesh), 1, ptr(self.HbyA.store), ptr(self.U.table.kind),
-             ptr(self.U.table.psib), None if d is None else byref(d), ptr(self.phi_hbya.store), s)
+             ptr(self.U.table.psib), None if d is None else byref(d), grad_h, ptr(self.phi_hbya.store), s)
         if self.adjust_phi_enabled and self.p_needs_ref:
             call("gf_adjust_phi", byref(g.cmesh), ptr(self._adjust_classes), ptr(self.phi_hbya.store), s)
         if consistent:
@@ -326,9 +349,10 @@ class _PressureVelocity:
             call("gf_axpby", g.num_cells, 1.0, ptr(self.rAtU.store), -1.0, ptr(self.rAU.store), ptr(self.d_r), s)
             self._eval_p()
             t = self.p.table
-            call("gf_correct_phi", byref(g.cmesh), ptr(self.phi_hbya.store), ptr(self.d_r), ptr(self.p.store),
-                 ptr(t.kind), ptr(t.frac), ptr(t.refv), ptr(t.refg), 1.0, 1, ptr(self.phi_hbya.store), s)
             self._grad(self.p, self.grad_p)
+            call("gf_correct_phi", byref(g.cmesh), ptr(self.phi_hbya.store), ptr(self.d_r), ptr(self.p.store),
+                 ptr(t.kind), ptr(t.frac), ptr(t.refv), ptr(t.refg), 1.0, 1,
+                 ptr(self.grad_p) if self._hanging else None, None, ptr(self.phi_hbya.store), s)
             call("gf_axpby", g.num_cells, 1.0, ptr(self.rAU.store), -1.0, ptr(self.rAtU.store), ptr(self.d_r), s)
             call("gf_correct_velocity", byref(g.cmesh), ptr(self.HbyA.store), ptr(self.d_r), ptr(self.grad_p),
                  ptr(self.HbyA.store), s)
@@ -357,6 +381,11 @@ class _PressureVelocity:
             a.diag = ptr(self.pEqn.diag_store)
             a.val = ptr(self.pEqn.val)
             a.source = ptr(self.pEqn.source_store)
+            if self._hanging:
+                self._grad(self.p, self.grad_p)
+                a.grad_lsq = ptr(self.grad_p)
+                a.lap_corrected = self._p_corrected
+                a.ffc = ptr(self.p_ffc)
             call("gf_assemble", byref(g.cmesh), byref(a), s)
             call("gf_pressure_finalize", byref(g.cmesh), ptr(self.phi_hbya.store), ptr(self.pEqn.diag_store),
                  ptr(self.pEqn.source_store), ptr(self.div_buf), self.p_ref_cell, self.p_ref_value, s)
@@ -382,7 +411,8 @@ class _PressureVelocity:
         self._eval_p()
         t = self.p.table
         call("gf_correct_phi", byref(g.cmesh), ptr(self.phi_hbya.store), ptr(self.rAtU.store), ptr(self.p.store),
-             ptr(t.kind), ptr(t.frac), ptr(t.refv), ptr(t.refg), -1.0, 0, ptr(self.phi.store), s)
+             ptr(t.kind), ptr(t.frac), ptr(t.refv), ptr(t.refg), -1.0, 0, None,
+             ptr(self.p_ffc) if self._hanging else None, ptr(self.phi.store), s)
         n = int(self.p_fixed_faces.numel())
         if n:
             call("gf_close_fixed_flux", byref(g.cmesh), n, ptr(self.p_fixed_faces), ptr(self.p_fixed_frac),

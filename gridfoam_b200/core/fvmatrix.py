@@ -29,7 +29,9 @@ class FvMatrix:
             self.diag_store = torch.zeros(g.num_cells, dtype=torch.float64, device=g.device)
             self.val = torch.zeros(g.ell_width * g.num_cells, dtype=torch.float64, device=g.device)
             self.source_store = torch.zeros((nc, g.num_cells), dtype=torch.float64, device=g.device)
-        self._face_flux_correction = None
+        # Explicit face-flux correction [nc][F] on internal faces (zero off
+        # hanging faces), or None: FvMatrix.face_flux_correction.
+        self._ffc: torch.Tensor | None = None
 
     # ------------------------------------------------------------------
     @property
@@ -98,7 +100,23 @@ class FvMatrix:
 
     @property
     def face_flux_correction(self):
-        return self._face_flux_correction
+        """core/fvmatrix.py:137-164: ``[F_single, *comp]`` or None."""
+        if self._ffc is None:
+            return None
+        g = self._grid
+        out = self._ffc if g.single_is_identity else self._ffc.index_select(1, g.single_idx)
+        return out[0] if self.num_components == 1 else out.t()
+
+    @staticmethod
+    def _combine_ffc(x, y, a: float, b: float):
+        """``a x + b y`` of two optional corrections (fvmatrix.py:167-180)."""
+        if x is None and y is None:
+            return None
+        if y is None:
+            return a * x
+        if x is None:
+            return b * y
+        return a * x + b * y
 
     # ------------------------------------------------------------------
     def _combine(self, other: "FvMatrix", a: float, b: float) -> "FvMatrix":
@@ -110,6 +128,7 @@ class FvMatrix:
             (self.source_store, other.source_store, res.source_store),
         ):
             call("gf_axpby", x.numel(), a, ptr(x), b, ptr(y), ptr(out), s)
+        res._ffc = self._combine_ffc(self._ffc, other._ffc, a, b)
         return res
 
     def __add__(self, other: "FvMatrix") -> "FvMatrix":
@@ -177,7 +196,8 @@ class FvMatrix:
         ps = torch.as_tensor(psi, dtype=torch.float64, device=g.device)
         ps = ps.reshape(1, -1).contiguous() if nc == 1 else ps.t().contiguous()
         out = torch.empty((nc, g.num_internal_faces), dtype=torch.float64, device=g.device)
-        call("gf_matrix_flux", ctypes_ref(g.cmesh), nc, ptr(self.val), ptr(ps), ptr(out), stream_ptr())
+        call("gf_matrix_flux", ctypes_ref(g.cmesh), nc, ptr(self.val), ptr(ps), ptr(self._ffc), ptr(out),
+             stream_ptr())
         if not g.single_is_identity:
             out = out.index_select(1, g.single_idx)
         return out[0] if nc == 1 else out.t()
@@ -205,6 +225,7 @@ class FvMatrix:
             n, None, ptr(prescribed), ptr(mask), ptr(res.diag_store), ptr(res.val), ptr(res.source_store),
             ptr(scratch), s,
         )
+        res._ffc = self._ffc
         return res
 
     def as_transpose(self) -> "FvMatrix":
@@ -214,4 +235,5 @@ class FvMatrix:
         res.diag_store.copy_(self.diag_store)
         res.source_store.copy_(self.source_store)
         res._set_ldu(lower, upper)
+        res._ffc = self._ffc
         return res

@@ -15,8 +15,9 @@ uploads an SoA layout that the kernels read coalesced:
 
 Face geometry (``fv/kernels/face_geometry.py:107-262``) is computed here:
 linear weights, ``|Sf|``, delta coefficients and the least-squares normal
-matrix inverse.  Hanging (2:1) faces are detected; meshes that contain them
-are rejected until the hanging-face kernels exist.
+matrix inverse.  Hanging (2:1) faces carry their offset and tangential-move
+vectors for the explicit corrections of interpolation, normal gradient,
+convection and Laplacian.
 """
 
 from __future__ import annotations
@@ -156,17 +157,20 @@ class AxisProjectedGrid:
         d_own = np.asarray(ap.dist_owner_to_bnd, dtype=np.float64).reshape(-1)
         d_nei = np.asarray(ap.dist_neighbour_to_bnd, dtype=np.float64).reshape(-1)
 
-        # Hanging faces (face_geometry.py:141-149)
+        # Hanging faces (face_geometry.py:141-162): face centre off the
+        # owner-neighbour segment; offset from the linear-weight point, and
+        # the tangential moves from each cell centre to the face centre.
         s_idx = np.nonzero(~immersed)[0]
         centroid = w[s_idx, None] * c_o[s_idx] + (1.0 - w[s_idx])[:, None] * c_n[s_idx]
         offset = face_centers[s_idx] - centroid
         tol = 1.0e-8 * float(sizes.min())
-        n_hang = int(np.count_nonzero(np.linalg.norm(offset, axis=1) > tol))
-        if n_hang:
-            raise NotImplementedError(
-                f"mesh has {n_hang} hanging (2:1) faces; the device path currently supports "
-                "single-level meshes"
-            )
+        hang_faces = s_idx[np.linalg.norm(offset, axis=1) > tol]
+        hang_offset = offset[np.linalg.norm(offset, axis=1) > tol]
+        hidx = np.arange(hang_faces.shape[0])
+        move_o = face_centers[hang_faces] - c_o[hang_faces]
+        move_n = face_centers[hang_faces] - c_n[hang_faces]
+        move_o[hidx, axis[hang_faces]] = 0.0
+        move_n[hidx, axis[hang_faces]] = 0.0
 
         # Boundary faces: domain | immersed upper | immersed lower
         iSf = Sf[imm_faces]
@@ -236,6 +240,10 @@ class AxisProjectedGrid:
             bnd_near=bnd_near,
         )
         host.extra["lsq_ata_inv"] = ata_inv
+        host.extra["hang_faces"] = hang_faces
+        host.extra["hang_offset"] = hang_offset
+        host.extra["hang_move_o"] = move_o
+        host.extra["hang_move_n"] = move_n
         return host
 
     def _build_ell(self) -> None:
@@ -332,6 +340,15 @@ class AxisProjectedGrid:
             "face_pos_owner": i32(h.extra["face_pos_owner"]),
             "face_pos_neigh": i32(h.extra["face_pos_neigh"]),
         }
+        hf = h.extra["hang_faces"]
+        face_hang = np.full(self._num_internal_faces, -1, dtype=np.int64)
+        face_hang[hf] = np.arange(hf.shape[0])
+        if hf.shape[0]:
+            t["hang_face"] = i32(hf)
+            t["face_hang"] = i32(face_hang)
+            t["hang_offset"] = f64(h.extra["hang_offset"].T)
+            t["hang_move_o"] = f64(h.extra["hang_move_o"].T)
+            t["hang_move_n"] = f64(h.extra["hang_move_n"].T)
         self.dev = t
         m = GfMesh()
         m.n_cells = self._num_cells
@@ -340,6 +357,7 @@ class AxisProjectedGrid:
         m.n_imm = self._num_immersed_faces
         m.n_bnd = self.num_bnd
         m.ell_width = self._ell_width
+        m.n_hang = int(hf.shape[0])
         for name, tensor in t.items():
             setattr(m, name, ptr(tensor))
         self.cmesh = m
@@ -441,6 +459,11 @@ class AxisProjectedGrid:
     @property
     def num_bnd(self) -> int:
         return self._num_domain_bnd_faces + 2 * self._num_immersed_faces
+
+    @property
+    def num_hanging(self) -> int:
+        """Hanging (coarse-fine) internal faces."""
+        return int(self.cmesh.n_hang)
 
     @property
     def ell_width(self) -> int:

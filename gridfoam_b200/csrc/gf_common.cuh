@@ -87,4 +87,38 @@ __device__ __forceinline__ bool nonassignable(int kind) {
     return kind == GF_BC_DIRICHLET || kind == GF_BC_SLIP;
 }
 
+// Hanging ordinal of internal face f, or -1 (also when the mesh has none).
+__device__ __forceinline__ int hang_of(const gf_mesh_t& m, int f) {
+    return m.n_hang > 0 ? __ldg(m.face_hang + f) : -1;
+}
+
+// Offset correction of the linear face value of component k on hanging face
+// h: (w grad_O + (1 - w) grad_N) . offset (face_interpolation.py:81-96).
+// grad is [ncomp*3][C].
+__device__ __forceinline__ double hang_value_corr(const gf_mesh_t& m, const double* __restrict__ grad, int k,
+                                                  int o, int n, double w, int h) {
+    const int64_t C = m.n_cells, H = m.n_hang;
+    double acc = 0.0;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        const double gf = w * grad[(k * 3 + j) * C + o] + (1.0 - w) * grad[(k * 3 + j) * C + n];
+        acc += gf * __ldg(m.hang_offset + j * H + h);
+    }
+    return acc;
+}
+
+// Skewness correction of the normal gradient of component k on hanging face
+// h: delta (grad_N . move_N - grad_O . move_O) (face_interpolation.py:99-145).
+__device__ __forceinline__ double hang_sn_corr(const gf_mesh_t& m, const double* __restrict__ grad, int k, int o,
+                                               int n, double delta, int h) {
+    const int64_t C = m.n_cells, H = m.n_hang;
+    double cn = 0.0, co = 0.0;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        cn += grad[(k * 3 + j) * C + n] * __ldg(m.hang_move_n + j * H + h);
+        co += grad[(k * 3 + j) * C + o] * __ldg(m.hang_move_o + j * H + h);
+    }
+    return delta * (cn - co);
+}
+
 }  // namespace gf

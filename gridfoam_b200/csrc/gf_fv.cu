@@ -240,6 +240,7 @@ __global__ void k_assemble(gf_mesh_t m, gf_assembly_t a) {
                 const int o = sl.side ? nbr : (int)c;
                 const int n = sl.side ? (int)c : nbr;
                 const double w = __ldg(m.weight + f);
+                const int h = hang_of(m, f);
                 if (conv) {
                     const double flux = a.phi[f];
                     double upper, lower, dO, dN;
@@ -262,6 +263,17 @@ __global__ void k_assemble(gf_mesh_t m, gf_assembly_t a) {
                         val += a.div_sign * lower;
                         diag += a.div_sign * dN;
                     }
+                    if (a.div_scheme == GF_DIV_LINEAR && h >= 0 && a.grad_lsq != nullptr) {
+                        // schemes/div.py:126-137: face-centre offset as an
+                        // explicit deferred source.
+#pragma unroll
+                        for (int k = 0; k < NC; ++k) {
+                            const double base = w * a.psi[k * C + o] + (1.0 - w) * a.psi[k * C + n];
+                            const double corrected = base + hang_value_corr(m, a.grad_lsq, k, o, n, w, h);
+                            const double sf = -flux * (corrected - base);
+                            src[k] += (sl.side == 0 ? a.div_sign : -a.div_sign) * sf;
+                        }
+                    }
                     if (tvd) {
                         // schemes/div.py:240-351 deferred correction.
                         const bool up_o = flux > 0.0;
@@ -276,6 +288,9 @@ __global__ void k_assemble(gf_mesh_t m, gf_assembly_t a) {
                             const double po = a.psi[k * C + o], pn = a.psi[k * C + n];
                             pup[k] = up_o ? po : pn;
                             plin[k] = w * po + (1.0 - w) * pn;
+                            // schemes/div.py:300-305: hanging offset with the
+                            // configured gradient.
+                            if (h >= 0) plin[k] = plin[k] + hang_value_corr(m, a.grad_psi, k, o, n, w, h);
                             const double dg = a.grad_psi[(k * 3 + 0) * C + u] * d0 +
                                               a.grad_psi[(k * 3 + 1) * C + u] * d1 +
                                               a.grad_psi[(k * 3 + 2) * C + u] * d2;
@@ -300,11 +315,29 @@ __global__ void k_assemble(gf_mesh_t m, gf_assembly_t a) {
                         }
                     }
                 }
+                double ffc_k[NC];
+#pragma unroll
+                for (int k = 0; k < NC; ++k) ffc_k[k] = 0.0;
                 if (lap) {
-                    const double coeff =
-                        gamma_face(a, w, o, n) * __ldg(m.mag_sf + f) * __ldg(m.delta + f);
+                    const double gf = gamma_face(a, w, o, n);
+                    const double coeff = gf * __ldg(m.mag_sf + f) * __ldg(m.delta + f);
                     val += a.lap_sign * coeff;
                     diag += a.lap_sign * (-coeff);
+                    if (h >= 0 && a.lap_corrected && a.grad_lsq != nullptr) {
+                        // laplacian.py:162-176: explicit skewness source,
+                        // owner -= corr, neighbour += corr.
+#pragma unroll
+                        for (int k = 0; k < NC; ++k) {
+                            const double corr = hang_sn_corr(m, a.grad_lsq, k, o, n, __ldg(m.delta + f), h);
+                            const double cs = (gf * __ldg(m.mag_sf + f)) * corr;
+                            src[k] += a.lap_sign * (sl.side == 0 ? -cs : cs);
+                            ffc_k[k] = cs;
+                        }
+                    }
+                }
+                if (a.ffc != nullptr && sl.side == 0) {
+#pragma unroll
+                    for (int k = 0; k < NC; ++k) a.ffc[k * F + f] = ffc_k[k];
                 }
             } else if (sl.kind == kBoundary) {
                 const int b = sl.bnd;
@@ -562,7 +595,8 @@ __global__ void k_simplec_ratu(int64_t C, const double* __restrict__ rau, const 
 // ---------------------------------------------------------------------------
 __global__ void k_face_flux(gf_mesh_t m, int mode, const double* __restrict__ vel,
                             const int8_t* __restrict__ u_kind, const double* __restrict__ u_psib,
-                            gf_ddtcorr_t ddt, int has_ddt, double* __restrict__ phi) {
+                            gf_ddtcorr_t ddt, int has_ddt, const double* __restrict__ grad,
+                            double* __restrict__ phi) {
     const int64_t C = m.n_cells;
     const int64_t F = m.n_faces;
     const int64_t nb = m.n_bnd;
@@ -577,11 +611,13 @@ __global__ void k_face_flux(gf_mesh_t m, int mode, const double* __restrict__ ve
             }
             const int o = __ldg(m.owner + f), n = __ldg(m.neighbour + f);
             const double w = __ldg(m.weight + f);
+            const int h = grad ? hang_of(m, f) : -1;
             double flux = 0.0;
             double sf[3];
             for (int k = 0; k < 3; ++k) {
                 sf[k] = __ldg(m.sf + k * F + f);
-                const double vf = w * vel[k * C + o] + (1.0 - w) * vel[k * C + n];
+                double vf = w * vel[k * C + o] + (1.0 - w) * vel[k * C + n];
+                if (h >= 0) vf = vf + hang_value_corr(m, grad, k, o, n, w, h);
                 flux += vf * sf[k];
             }
             if (has_ddt) {
@@ -624,7 +660,7 @@ __global__ void k_face_flux(gf_mesh_t m, int mode, const double* __restrict__ ve
 
 __global__ void k_interpolate(gf_mesh_t m, int nc, const double* __restrict__ psi,
                               const int8_t* __restrict__ kind, const double* __restrict__ psib,
-                              double* __restrict__ out) {
+                              const double* __restrict__ grad, double* __restrict__ out) {
     const int64_t C = m.n_cells;
     const int64_t F = m.n_faces;
     const int64_t nb = m.n_bnd;
@@ -636,8 +672,12 @@ __global__ void k_interpolate(gf_mesh_t m, int nc, const double* __restrict__ ps
             const bool imm = m.imm_index && __ldg(m.imm_index + f) >= 0;
             const int o = __ldg(m.owner + f), n = __ldg(m.neighbour + f);
             const double w = __ldg(m.weight + f);
-            for (int k = 0; k < nc; ++k)
-                out[k * total + f] = imm ? 0.0 : w * psi[k * C + o] + (1.0 - w) * psi[k * C + n];
+            const int h = (grad && !imm) ? hang_of(m, f) : -1;
+            for (int k = 0; k < nc; ++k) {
+                double v = imm ? 0.0 : w * psi[k * C + o] + (1.0 - w) * psi[k * C + n];
+                if (h >= 0) v = v + hang_value_corr(m, grad, k, o, n, w, h);
+                out[k * total + f] = v;
+            }
         } else {
             const int b = (int)(i - F);
             const int c = __ldg(m.bnd_cell + b);
@@ -649,7 +689,8 @@ __global__ void k_interpolate(gf_mesh_t m, int nc, const double* __restrict__ ps
 
 __global__ void k_sn_grad(gf_mesh_t m, int nc, const double* __restrict__ psi, const int8_t* __restrict__ kind,
                           const double* __restrict__ frac, const double* __restrict__ refv,
-                          const double* __restrict__ refg, double* __restrict__ out) {
+                          const double* __restrict__ refg, const double* __restrict__ grad,
+                          double* __restrict__ out) {
     const int64_t C = m.n_cells;
     const int64_t F = m.n_faces;
     const int64_t nb = m.n_bnd;
@@ -661,8 +702,12 @@ __global__ void k_sn_grad(gf_mesh_t m, int nc, const double* __restrict__ psi, c
             const bool imm = m.imm_index && __ldg(m.imm_index + f) >= 0;
             const int o = __ldg(m.owner + f), n = __ldg(m.neighbour + f);
             const double dc = __ldg(m.delta + f);
-            for (int k = 0; k < nc; ++k)
-                out[k * total + f] = imm ? 0.0 : dc * (psi[k * C + n] - psi[k * C + o]);
+            const int h = (grad && !imm) ? hang_of(m, f) : -1;
+            for (int k = 0; k < nc; ++k) {
+                double v = imm ? 0.0 : dc * (psi[k * C + n] - psi[k * C + o]);
+                if (h >= 0) v = v + hang_sn_corr(m, grad, k, o, n, dc, h);
+                out[k * total + f] = v;
+            }
         } else {
             const int b = (int)(i - F);
             const int c = __ldg(m.bnd_cell + b);
@@ -685,6 +730,7 @@ __global__ void k_correct_phi(gf_mesh_t m, const double* __restrict__ pred, cons
                               const double* __restrict__ p, const int8_t* __restrict__ kind,
                               const double* __restrict__ frac, const double* __restrict__ refv,
                               const double* __restrict__ refg, double sign, int simplec,
+                              const double* __restrict__ grad_p, const double* __restrict__ ffc,
                               double* __restrict__ phi) {
     const int64_t F = m.n_faces;
     const int64_t nb = m.n_bnd;
@@ -702,10 +748,15 @@ __global__ void k_correct_phi(gf_mesh_t m, const double* __restrict__ pred, cons
             const double w = __ldg(m.weight + f);
             const double cf = w * coeff[o] + (1.0 - w) * coeff[n];
             if (simplec) {
-                phi[f] = base + cf * __ldg(m.mag_sf + f) * (__ldg(m.delta + f) * (p[n] - p[o]));
+                double sn = __ldg(m.delta + f) * (p[n] - p[o]);
+                const int h = grad_p ? hang_of(m, f) : -1;
+                if (h >= 0) sn = sn + hang_sn_corr(m, grad_p, 0, o, n, __ldg(m.delta + f), h);
+                phi[f] = base + cf * __ldg(m.mag_sf + f) * sn;
             } else {
                 const double g = cf * __ldg(m.mag_sf + f) * __ldg(m.delta + f);
-                phi[f] = base - (g * p[n] - g * p[o]);
+                double flux = g * p[n] - g * p[o];
+                if (ffc) flux = flux + ffc[f];
+                phi[f] = base - flux;
             }
         } else {
             const int b = (int)(i - F);
@@ -888,7 +939,7 @@ __global__ void k_residual_finish(int nparts, const double* __restrict__ part, d
 
 template <int NC>
 __global__ void k_matrix_flux(gf_mesh_t m, const double* __restrict__ val, const double* __restrict__ psi,
-                              double* __restrict__ out) {
+                              const double* __restrict__ ffc, double* __restrict__ out) {
     const int64_t C = m.n_cells;
     const int64_t F = m.n_faces;
     for (int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; f < F;
@@ -898,7 +949,11 @@ __global__ void k_matrix_flux(gf_mesh_t m, const double* __restrict__ val, const
         const double lo = val[__ldg(m.face_pos_neigh + f)];
         const int o = __ldg(m.owner + f), n = __ldg(m.neighbour + f);
 #pragma unroll
-        for (int k = 0; k < NC; ++k) out[k * F + f] = imm ? 0.0 : up * psi[k * C + n] - lo * psi[k * C + o];
+        for (int k = 0; k < NC; ++k) {
+            double v = imm ? 0.0 : up * psi[k * C + n] - lo * psi[k * C + o];
+            if (ffc && !imm) v = v + ffc[k * F + f];
+            out[k * F + f] = v;
+        }
     }
 }
 
@@ -910,6 +965,11 @@ static bool valid_mesh(const gf_mesh_t* m) {
     }
     if (m->n_cells * (int64_t)m->ell_width > 2147483647LL) {
         set_error("mesh too large for 32-bit ELL positions");
+        return false;
+    }
+    if (m->n_hang < 0 || (m->n_hang > 0 && (m->face_hang == nullptr || m->hang_offset == nullptr ||
+                                            m->hang_move_o == nullptr || m->hang_move_n == nullptr))) {
+        set_error("invalid mesh descriptor: hanging-face arrays missing");
         return false;
     }
     return true;
@@ -1057,7 +1117,7 @@ int gf_simplec_rAtU(const gf_mesh_t* m, const double* rau, const double* h1, dou
 }
 
 int gf_face_flux(const gf_mesh_t* m, int32_t mode, const double* vel, const int8_t* u_kind, const double* u_psib,
-                 const gf_ddtcorr_t* ddt, double* phi, void* stream) {
+                 const gf_ddtcorr_t* ddt, const double* grad_vel, double* phi, void* stream) {
     if (!valid_mesh(m) || (mode != 0 && mode != 1) || vel == nullptr || u_kind == nullptr) {
         set_error("gf_face_flux: invalid arguments");
         return GF_ERR_INVALID;
@@ -1074,7 +1134,7 @@ int gf_face_flux(const gf_mesh_t* m, int32_t mode, const double* vel, const int8
         }
     }
     k_face_flux<<<grid_for(m->n_faces + m->n_bnd), kThreads, 0, GF_STREAM(stream)>>>(*m, mode, vel, u_kind, u_psib,
-                                                                                     d, has, phi);
+                                                                                     d, has, grad_vel, phi);
     return check_launch("gf_face_flux");
 }
 
@@ -1085,27 +1145,27 @@ int gf_fvc_div(const gf_mesh_t* m, int32_t ncomp, const double* phi, double* out
 }
 
 int gf_interpolate(const gf_mesh_t* m, int32_t ncomp, const double* psi, const int8_t* bc_kind, const double* psib,
-                   double* out, void* stream) {
+                   const double* grad, double* out, void* stream) {
     if (!valid_mesh(m) || !valid_nc(ncomp)) return GF_ERR_INVALID;
     k_interpolate<<<grid_for(m->n_faces + m->n_bnd), kThreads, 0, GF_STREAM(stream)>>>(*m, ncomp, psi, bc_kind,
-                                                                                       psib, out);
+                                                                                       psib, grad, out);
     return check_launch("gf_interpolate");
 }
 
 int gf_sn_grad(const gf_mesh_t* m, int32_t ncomp, const double* psi, const int8_t* bc_kind, const double* frac,
-               const double* refv, const double* refg, double* out, void* stream) {
+               const double* refv, const double* refg, const double* grad, double* out, void* stream) {
     if (!valid_mesh(m) || !valid_nc(ncomp)) return GF_ERR_INVALID;
     k_sn_grad<<<grid_for(m->n_faces + m->n_bnd), kThreads, 0, GF_STREAM(stream)>>>(*m, ncomp, psi, bc_kind, frac,
-                                                                                   refv, refg, out);
+                                                                                   refv, refg, grad, out);
     return check_launch("gf_sn_grad");
 }
 
 int gf_correct_phi(const gf_mesh_t* m, const double* phi_pred, const double* coeff, const double* p,
                    const int8_t* p_kind, const double* frac, const double* refv, const double* refg, double sign,
-                   int32_t simplec, double* phi, void* stream) {
+                   int32_t simplec, const double* grad_p, const double* ffc, double* phi, void* stream) {
     if (!valid_mesh(m)) return GF_ERR_INVALID;
     k_correct_phi<<<grid_for(m->n_faces + m->n_bnd), kThreads, 0, GF_STREAM(stream)>>>(
-        *m, phi_pred, coeff, p, p_kind, frac, refv, refg, sign, simplec, phi);
+        *m, phi_pred, coeff, p, p_kind, frac, refv, refg, sign, simplec, grad_p, ffc, phi);
     return check_launch("gf_correct_phi");
 }
 
@@ -1190,14 +1250,14 @@ int gf_field_residual(const gf_mesh_t* m, int32_t ncomp, const double* diag, con
     return check_launch("gf_field_residual");
 }
 
-int gf_matrix_flux(const gf_mesh_t* m, int32_t ncomp, const double* val, const double* psi, double* out,
-                   void* stream) {
+int gf_matrix_flux(const gf_mesh_t* m, int32_t ncomp, const double* val, const double* psi, const double* ffc,
+                   double* out, void* stream) {
     if (!valid_mesh(m) || !valid_nc(ncomp)) return GF_ERR_INVALID;
     if (m->n_faces == 0) return GF_OK;
     if (ncomp == 1)
-        k_matrix_flux<1><<<grid_for(m->n_faces), kThreads, 0, GF_STREAM(stream)>>>(*m, val, psi, out);
+        k_matrix_flux<1><<<grid_for(m->n_faces), kThreads, 0, GF_STREAM(stream)>>>(*m, val, psi, ffc, out);
     else
-        k_matrix_flux<3><<<grid_for(m->n_faces), kThreads, 0, GF_STREAM(stream)>>>(*m, val, psi, out);
+        k_matrix_flux<3><<<grid_for(m->n_faces), kThreads, 0, GF_STREAM(stream)>>>(*m, val, psi, ffc, out);
     return check_launch("gf_matrix_flux");
 }
 

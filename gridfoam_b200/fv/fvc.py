@@ -15,7 +15,7 @@ from gridfoam_b200.core.field import (
     get_or_create_facefield,
 )
 from gridfoam_b200.fv import schemes
-from gridfoam_b200.meta.config import GradScheme
+from gridfoam_b200.meta.config import GradScheme, SnGradScheme
 
 
 def _eval_state(field: CellField) -> None:
@@ -39,6 +39,19 @@ def grad(field: CellField) -> CellField:
     return out
 
 
+def _hanging_grad(field: CellField) -> torch.Tensor | None:
+    """Least-squares gradient for the hanging-face corrections, or None on
+    meshes without hanging faces (boundary state must be current)."""
+    grid = field.grid
+    if grid.num_hanging == 0:
+        return None
+    out = torch.empty((field.num_components * 3, grid.num_cells), dtype=torch.float64, device=grid.device)
+    t = field.table
+    call("gf_lsq_grad", ctypes.byref(grid.cmesh), field.num_components, ptr(field.store), ptr(t.kind),
+         ptr(t.psib), ptr(out), stream_ptr())
+    return out
+
+
 def div(phi: FaceField) -> CellField:
     """fv/fvc/div.py:15-64."""
     grid = phi.grid
@@ -54,8 +67,9 @@ def interpolate(field: CellField) -> FaceField:
     _eval_state(field)
     out = get_or_create_facefield(grid, f"{field.name}_f", "local", field.component_shape)
     t = field.table
+    g = _hanging_grad(field)
     call("gf_interpolate", ctypes.byref(grid.cmesh), field.num_components, ptr(field.store), ptr(t.kind),
-         ptr(t.psib), ptr(out.store), stream_ptr())
+         ptr(t.psib), ptr(g), ptr(out.store), stream_ptr())
     return out
 
 
@@ -65,8 +79,10 @@ def sn_grad(field: CellField) -> FaceField:
     _eval_state(field)
     out = get_or_create_facefield(grid, f"snGrad({field.name})", "local", field.component_shape)
     t = field.table
+    corrected = schemes.sn_grad_scheme(grid.sim_config, field.name) == SnGradScheme.CORRECTED
+    g = _hanging_grad(field) if corrected else None
     call("gf_sn_grad", ctypes.byref(grid.cmesh), field.num_components, ptr(field.store), ptr(t.kind),
-         ptr(t.frac), ptr(t.refv), ptr(t.refg), ptr(out.store), stream_ptr())
+         ptr(t.frac), ptr(t.refv), ptr(t.refg), ptr(g), ptr(out.store), stream_ptr())
     return out
 
 
@@ -74,8 +90,9 @@ def face_flux(phi: FaceField, U: CellField) -> None:
     """fv/flux.py:132-162 ``correct_flux(phi, U, update_internal=True)``."""
     _eval_state(U)
     t = U.table
+    g = _hanging_grad(U)
     call("gf_face_flux", ctypes.byref(U.grid.cmesh), 0, ptr(U.store), ptr(t.kind), ptr(t.psib), None,
-         ptr(phi.store), stream_ptr())
+         ptr(g), ptr(phi.store), stream_ptr())
 
 
 def spmv_check(mat, x: torch.Tensor) -> torch.Tensor:

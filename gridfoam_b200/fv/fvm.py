@@ -43,6 +43,17 @@ def _base(field: CellField, mat: FvMatrix) -> GfAssembly:
     return a
 
 
+def _lsq_grad(field: CellField) -> torch.Tensor:
+    if schemes.grad_scheme(field.grid.sim_config, field.name) != GradScheme.LEASTSQUARE:
+        raise NotImplementedError("the device path implements the leastsquare gradient scheme")
+    grad = torch.empty((field.num_components * 3, field.grid.num_cells), dtype=torch.float64,
+                       device=field.grid.device)
+    t = field.table
+    call("gf_lsq_grad", ctypes.byref(field.grid.cmesh), field.num_components, ptr(field.store),
+         ptr(t.kind), ptr(t.psib), ptr(grad), stream_ptr())
+    return grad
+
+
 def _run(field: CellField, a: GfAssembly) -> None:
     call("gf_assemble", ctypes.byref(field.grid.cmesh), ctypes.byref(a), stream_ptr())
 
@@ -70,20 +81,19 @@ def div(phi: FaceField, field: CellField) -> FvMatrix:
     scheme = schemes.div_scheme(field.grid.sim_config, phi.name, field.name)
     code = _lib.DIV_CODES[scheme.value]
     grad = None
-    if code >= _lib.DIV_CODES["vanleer"]:
-        if schemes.grad_scheme(field.grid.sim_config, field.name) != GradScheme.LEASTSQUARE:
-            raise NotImplementedError("the device path implements the leastsquare gradient scheme")
-        grad = torch.empty((field.num_components * 3, field.grid.num_cells), dtype=torch.float64,
-                           device=field.grid.device)
-        t = field.table
-        call("gf_lsq_grad", ctypes.byref(field.grid.cmesh), field.num_components, ptr(field.store),
-             ptr(t.kind), ptr(t.psib), ptr(grad), stream_ptr())
+    hanging = field.grid.num_hanging > 0
+    if code >= _lib.DIV_CODES["vanleer"] or (hanging and code == _lib.DIV_CODES["linear"]):
+        # TVD: the configured gradient; linear on hanging faces: the
+        # least-squares gradient of the offset correction (schemes/div.py).
+        grad = _lsq_grad(field)
     a = _base(field, mat)
     a.div_scheme = code
     a.div_sign = 1.0
     a.phi = ptr(phi.store)
     a.grad_psi = ptr(grad)
+    a.grad_lsq = ptr(grad) if hanging else None
     _run(field, a)
+    mat._keep = grad
     return mat
 
 
@@ -106,6 +116,16 @@ def laplacian(gamma, field: CellField) -> FvMatrix:
         a.gamma = ptr(g_t)
     else:
         a.gamma_scalar = float(gamma)
+    grad = None
+    if grid.num_hanging > 0 and scheme in schemes.CORRECTED:
+        # laplacian.py:162-176: explicit hanging-face skewness correction,
+        # also kept as the matrix's face-flux correction.
+        grad = _lsq_grad(field)
+        a.grad_lsq = ptr(grad)
+        a.lap_corrected = 1
+        mat._ffc = torch.zeros((field.num_components, grid.num_internal_faces), dtype=torch.float64,
+                               device=grid.device)
+        a.ffc = ptr(mat._ffc)
     _run(field, a)
-    mat._keep = g_t
+    mat._keep = (g_t, grad)
     return mat

@@ -23,6 +23,8 @@ LAPLACIAN_ALIASES = {
     LaplacianScheme.GAUSS_LINEAR_UNCORRECTED: LaplacianScheme.UNCORRECTED,
 }
 HARMONIC = {LaplacianScheme.GAUSS_HARMONIC_CORRECTED, LaplacianScheme.GAUSS_HARMONIC_UNCORRECTED}
+# Schemes that add the explicit hanging-face skewness correction.
+CORRECTED = {LaplacianScheme.CORRECTED, LaplacianScheme.GAUSS_HARMONIC_CORRECTED}
 
 
 def _lookup(table, key: str, default, warning: str | None = None):

@@ -103,6 +103,14 @@ typedef struct gf_mesh {
     /* face -> ELL position of the owner / neighbour row [F] */
     const int32_t* face_pos_owner;
     const int32_t* face_pos_neigh;
+    /* Hanging (coarse-fine) faces, fv/kernels/face_geometry.py:141-162: the
+     * H internal faces whose centre is off the owner-neighbour segment. */
+    int64_t n_hang;              /* H (0: no hanging faces, arrays unread) */
+    const int32_t* hang_face;    /* [H] internal face index, ascending */
+    const int32_t* face_hang;    /* [F] hanging ordinal or -1 */
+    const double* hang_offset;   /* [3][H] face centre - linear-weight point */
+    const double* hang_move_o;   /* [3][H] face centre - owner centre, normal part 0 */
+    const double* hang_move_n;   /* [3][H] face centre - neighbour centre, normal part 0 */
 } gf_mesh_t;
 
 /* Per-face boundary-condition table of one field (value-fraction form). */
@@ -155,6 +163,16 @@ typedef struct gf_assembly {
     double* diag;           /* out [C] */
     double* val;            /* out [W][C] */
     double* source;         /* out [ncomp][C] */
+    /* Hanging faces (meshes with n_hang > 0): */
+    int32_t lap_corrected;  /* 1: corrected Laplacian (explicit skewness
+                               source on hanging faces, laplacian.py:162-176) */
+    int32_t reserved;
+    const double* grad_lsq; /* [ncomp*3][C] least-squares gradient of psi
+                               for the hanging corrections of the linear
+                               convection value and the Laplacian */
+    double* ffc;            /* out [ncomp][F] or NULL: the Laplacian's face
+                               flux correction (FvMatrix.face_flux_correction),
+                               0 off hanging faces */
 } gf_assembly_t;
 
 /* Persistent Krylov solve of A x = b for ncomp right-hand sides sharing A
@@ -282,7 +300,9 @@ int gf_simplec_rAtU(const gf_mesh_t* m, const double* rau, const double* h1,
  * velocity BC face value.  mode 1 (compute_phi_hbya): boundary faces take
  * vel_P.Sf, U_b.Sf on non-assignable velocity patches, 0 on uncovered domain
  * faces.  ddt (optional, PISO/PIMPLE): adds interpolate(rAU) * ddtCorr
- * (fv/fvc/ddt_corr.py:13-78) on single-sided faces. */
+ * (fv/fvc/ddt_corr.py:13-78) on single-sided faces.  grad_vel ([9][C]
+ * least-squares gradient of vel, or NULL) adds the hanging-face offset
+ * correction of the interpolated velocity before the dot with Sf. */
 typedef struct gf_ddtcorr {
     const double* rau;        /* [C] */
     const double* u_old;      /* [3][C] */
@@ -294,33 +314,43 @@ typedef struct gf_ddtcorr {
 
 int gf_face_flux(const gf_mesh_t* m, int32_t mode, const double* vel,
                  const int8_t* u_kind, const double* u_psib,
-                 const gf_ddtcorr_t* ddt, double* phi, void* stream);
+                 const gf_ddtcorr_t* ddt, const double* grad_vel, double* phi,
+                 void* stream);
 
 /* fv/fvc/div.py:15-64: div(phi) = face sum / V for ncomp face fields. */
 int gf_fvc_div(const gf_mesh_t* m, int32_t ncomp, const double* phi,
                double* out, void* stream);
 
 /* fv/schemes/interpolate.py:20-63 + fv/boundary_ops.py:545-593: linear face
- * values and boundary face values (BC value or zero-gradient fill). */
+ * values and boundary face values (BC value or zero-gradient fill).  grad
+ * ([ncomp*3][C] least-squares gradient, or NULL) adds the hanging-face
+ * offset correction (fv/kernels/face_interpolation.py:45-96). */
 int gf_interpolate(const gf_mesh_t* m, int32_t ncomp, const double* psi,
-                   const int8_t* bc_kind, const double* psib, double* out,
-                   void* stream);
+                   const int8_t* bc_kind, const double* psib,
+                   const double* grad, double* out, void* stream);
 
-/* fv/fvc/sn_grad.py:16-55 (uncorrected internal part + boundary normal
- * gradient, boundary_ops.py:405-437). */
+/* fv/fvc/sn_grad.py:16-55 (internal part + boundary normal gradient,
+ * boundary_ops.py:405-437).  grad ([ncomp*3][C] least-squares gradient, or
+ * NULL for the uncorrected scheme) adds the hanging-face correction
+ * (fv/kernels/face_interpolation.py:99-145). */
 int gf_sn_grad(const gf_mesh_t* m, int32_t ncomp, const double* psi,
                const int8_t* bc_kind, const double* frac, const double* refv,
-               const double* refg, double* out, void* stream);
+               const double* refg, const double* grad, double* out,
+               void* stream);
 
 /* algorithms/utils/pressure_correction.py:270-305 correct_phi without the
- * fixed-cell closure: phi = phiHbyA - flux(p) on single faces, boundary
- * faces phiHbyA_b + sign coeff_P |Sf| snGrad_b(p).  Also used for the
- * SIMPLEC flux update (pressure_correction.py:257-264) with sign +1 and
- * `internal_coeff` the interpolated (rAtU - rAU). */
+ * fixed-cell closure: phi = phiHbyA - flux(p) on single faces (flux(p)
+ * includes ffc, the pressure Laplacian's hanging-face flux correction, when
+ * not NULL), boundary faces phiHbyA_b + sign coeff_P |Sf| snGrad_b(p).
+ * simplec = 1: the SIMPLEC flux update (pressure_correction.py:257-264),
+ * phiHbyA += interpolate(coeff) snGrad(p) |Sf| with sign +1, coeff =
+ * rAtU - rAU, and snGrad corrected on hanging faces by grad_p (the
+ * least-squares gradient of p, or NULL). */
 int gf_correct_phi(const gf_mesh_t* m, const double* phi_pred,
                    const double* coeff, const double* p, const int8_t* p_kind,
                    const double* frac, const double* refv, const double* refg,
-                   double sign, int32_t simplec, double* phi, void* stream);
+                   double sign, int32_t simplec, const double* grad_p,
+                   const double* ffc, double* phi, void* stream);
 
 /* pressure_correction.py:308-335 fixed-cell flux closure. face_list holds
  * the n_faces boundary faces flagged fixed; area_frac their area share;
@@ -370,9 +400,10 @@ int gf_field_residual(const gf_mesh_t* m, int32_t ncomp, const double* diag,
                       void* stream);
 
 /* fvmatrix.py:424-468 flux on all internal faces (0 on immersed ones):
- * out[f] = upper psi_N - lower psi_O. */
+ * out[f] = upper psi_N - lower psi_O (+ ffc[f] when ffc is not NULL). */
 int gf_matrix_flux(const gf_mesh_t* m, int32_t ncomp, const double* val,
-                   const double* psi, double* out, void* stream);
+                   const double* psi, const double* ffc, double* out,
+                   void* stream);
 
 #ifdef __cplusplus
 }

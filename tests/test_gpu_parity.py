@@ -21,9 +21,10 @@ from tests.golden.oracle_harness import load_golden  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
-CASES = [c for c in STEPS if c not in OCTREE_CASES]
+CASES = list(STEPS)
 # Relative L2 tolerance of whole-step fields against the reference run.
-STEP_TOL = {"cavity8": 1e-10, "channel": 1e-9, "channel_ffp": 1e-9, "ibplane": 1e-10, "pipe10x20": 1e-4}
+STEP_TOL = {"cavity8": 1e-10, "channel": 1e-9, "channel_ffp": 1e-9, "ibplane": 1e-10, "pipe10x20": 1e-4,
+            "cavity_oct": 1e-9, "duct_oct": 1e-8, "ibcyl_oct": 1e-8}
 
 
 def rel(a, b) -> float:
@@ -48,7 +49,7 @@ def test_steps_match_reference(name, algorithm):
         s.variant = 5 if algorithm == "staged" else 0
     np.testing.assert_allclose(to_np(algo.phi.pack()), golden["init_phi"], rtol=0, atol=1e-13)
     tol = STEP_TOL[name]
-    slack = 1 if name.startswith("pipe") else 0
+    slack = 1 if name.startswith("pipe") or name in OCTREE_CASES else 0
     for step in range(STEPS[name]):
         algo.step()
         torch.cuda.synchronize()
