@@ -209,6 +209,9 @@ _SIGNATURES = {
     "gf_ldu_to_ell": ([P, P, P, P, P], ctypes.c_int),
     "gf_field_residual": ([P, I32, P, P, P, P, P, P, P], ctypes.c_int),
     "gf_matrix_flux": ([P, I32, P, P, P, P, P], ctypes.c_int),
+    "gf_adjoint_ldu_grads": ([P, I32, P, P, P, P, P, P], ctypes.c_int),
+    "gf_laplacian_adjoint": ([P, P, P, P, P, P, P, P], ctypes.c_int),
+    "gf_div_adjoint": ([P, P, P, P, P, P, P, P], ctypes.c_int),
 }
 
 EXPORTED = tuple(_SIGNATURES)

@@ -40,6 +40,8 @@ class Equation:
         self.target = target
         cells, values = immersed_dirichlet_constraints(target)
         _, _, mask = target.table.constraints()
+        if cells.numel() and fv_matrix.requires_grad:
+            raise NotImplementedError("gradients through immersed-boundary cell constraints are not implemented")
         self.fv_matrix = fv_matrix.with_fixed_values(cells, values, mask=mask) if cells.numel() else fv_matrix
 
 

@@ -32,6 +32,7 @@ class FvMatrix:
         # Explicit face-flux correction [nc][F] on internal faces (zero off
         # hanging faces), or None: FvMatrix.face_flux_correction.
         self._ffc: torch.Tensor | None = None
+        self._ad: dict | None = None
 
     # ------------------------------------------------------------------
     @property
@@ -49,25 +50,64 @@ class FvMatrix:
     def _src_view(self, store: torch.Tensor) -> torch.Tensor:
         return store[0] if self._field.component_shape == () else store.t()
 
+    # Differentiable coefficients: a tensor that requires grad, assigned
+    # through a setter or produced by a differentiable operator, is kept in
+    # ``_ad`` (reference layout: diag [C], upper/lower [F], source
+    # [C, *comp]) while its values also go to the device stores.  The getters
+    # return it, so torch algebra on the coefficients keeps its graph, and
+    # the solvers' implicit adjoint takes its inputs from it.
+    def _record(self, key: str, value: torch.Tensor) -> None:
+        if isinstance(value, torch.Tensor) and value.requires_grad:
+            if self._ad is None:
+                self._ad = {}
+            self._ad[key] = value
+        elif self._ad is not None:
+            self._ad.pop(key, None)
+
+    @property
+    def requires_grad(self) -> bool:
+        return bool(self._ad) and any(t.requires_grad for t in self._ad.values())
+
+    def autograd_tensors(self) -> tuple[torch.Tensor, torch.Tensor, torch.Tensor, torch.Tensor]:
+        """``(diag, upper, lower, source)`` in the reference layout, the
+        differentiable ones where recorded."""
+        ad = self._ad or {}
+        upper, lower = (None, None)
+        if "upper" not in ad or "lower" not in ad:
+            upper, lower = self._ldu()
+        return (
+            ad.get("diag", self.diag_store),
+            ad.get("upper", upper),
+            ad.get("lower", lower),
+            ad.get("source", self._src_view(self.source_store)),
+        )
+
     @property
     def diag(self) -> torch.Tensor:
+        if self._ad and "diag" in self._ad:
+            return self._ad["diag"]
         return self.diag_store
 
     @diag.setter
     def diag(self, value: torch.Tensor) -> None:
-        self.diag_store.copy_(torch.as_tensor(value, dtype=torch.float64, device=self._grid.device))
+        v = torch.as_tensor(value, dtype=torch.float64, device=self._grid.device)
+        self.diag_store.copy_(v.detach())
+        self._record("diag", v)
 
     @property
     def source(self) -> torch.Tensor:
+        if self._ad and "source" in self._ad:
+            return self._ad["source"]
         return self._src_view(self.source_store)
 
     @source.setter
     def source(self, value: torch.Tensor) -> None:
         value = torch.as_tensor(value, dtype=torch.float64, device=self._grid.device)
         if self._field.component_shape == ():
-            self.source_store[0].copy_(value)
+            self.source_store[0].copy_(value.detach())
         else:
-            self.source_store.copy_(value.t())
+            self.source_store.copy_(value.detach().t())
+        self._record("source", value)
 
     def _ldu(self) -> tuple[torch.Tensor, torch.Tensor]:
         g = self._grid
@@ -78,25 +118,35 @@ class FvMatrix:
 
     @property
     def upper(self) -> torch.Tensor:
+        if self._ad and "upper" in self._ad:
+            return self._ad["upper"]
         return self._ldu()[0]
 
     @upper.setter
     def upper(self, value: torch.Tensor) -> None:
         _, lower = self._ldu()
-        self._set_ldu(torch.as_tensor(value, dtype=torch.float64, device=self._grid.device), lower)
+        v = torch.as_tensor(value, dtype=torch.float64, device=self._grid.device)
+        self._set_ldu(v, lower)
+        self._record("upper", v)
 
     @property
     def lower(self) -> torch.Tensor:
+        if self._ad and "lower" in self._ad:
+            return self._ad["lower"]
         return self._ldu()[1]
 
     @lower.setter
     def lower(self, value: torch.Tensor) -> None:
         upper, _ = self._ldu()
-        self._set_ldu(upper, torch.as_tensor(value, dtype=torch.float64, device=self._grid.device))
+        v = torch.as_tensor(value, dtype=torch.float64, device=self._grid.device)
+        self._set_ldu(upper, v)
+        self._record("lower", v)
 
     def _set_ldu(self, upper: torch.Tensor, lower: torch.Tensor) -> None:
         g = self._grid
-        call("gf_ldu_to_ell", ctypes_ref(g.cmesh), ptr(upper.contiguous()), ptr(lower.contiguous()), ptr(self.val), stream_ptr())
+        up = upper.detach().contiguous()
+        lo = lower.detach().contiguous()
+        call("gf_ldu_to_ell", ctypes_ref(g.cmesh), ptr(up), ptr(lo), ptr(self.val), stream_ptr())
 
     @property
     def face_flux_correction(self):
@@ -129,6 +179,9 @@ class FvMatrix:
         ):
             call("gf_axpby", x.numel(), a, ptr(x), b, ptr(y), ptr(out), s)
         res._ffc = self._combine_ffc(self._ffc, other._ffc, a, b)
+        if self.requires_grad or other.requires_grad:
+            xs, ys = self.autograd_tensors(), other.autograd_tensors()
+            res._ad = {k: a * x + b * y for k, x, y in zip(("diag", "upper", "lower", "source"), xs, ys)}
         return res
 
     def __add__(self, other: "FvMatrix") -> "FvMatrix":

@@ -26,6 +26,8 @@ inline int check_launch(const char* what) {
     return GF_OK;
 }
 
+#define GF_STREAM(s) (reinterpret_cast<cudaStream_t>(s))
+
 inline unsigned grid_for(int64_t n, int threads = kThreads) {
     int64_t g = (n + threads - 1) / threads;
     if (g < 1) g = 1;

@@ -987,7 +987,6 @@ static bool valid_nc(int nc) {
 
 using namespace gf;
 
-#define GF_STREAM(s) (reinterpret_cast<cudaStream_t>(s))
 
 extern "C" {
 

@@ -58,6 +58,53 @@ def _run(field: CellField, a: GfAssembly) -> None:
     call("gf_assemble", ctypes.byref(field.grid.cmesh), ctypes.byref(a), stream_ptr())
 
 
+class _AssemblyAdjoint(torch.autograd.Function):
+    """Differentiable view of an assembled term: forward returns its
+    ``(diag, upper, lower, source)`` in the reference layout; backward runs
+    the hand-written reverse kernel (``gf_laplacian_adjoint`` for the
+    diffusivity, ``gf_div_adjoint`` for the face flux)."""
+
+    @staticmethod
+    def forward(ctx, param, mat, kernel, a, keep):  # noqa: ARG004
+        ctx.mat, ctx.kernel, ctx.a, ctx.keep = mat, kernel, a, keep
+        ctx.param_shape = param.shape
+        upper, lower = mat._ldu()
+        return mat.diag_store.clone(), upper, lower, mat._src_view(mat.source_store).clone()
+
+    @staticmethod
+    def backward(ctx, gd, gu, gl, gs):
+        mat = ctx.mat
+        g = mat.grid
+        nc = mat.num_components
+        z = lambda n: torch.zeros(n, dtype=torch.float64, device=g.device)  # noqa: E731
+        gd = z(g.num_cells) if gd is None else gd.contiguous()
+        gu = z(g.num_internal_faces) if gu is None else gu.contiguous()
+        gl = z(g.num_internal_faces) if gl is None else gl.contiguous()
+        if gs is None:
+            gs = torch.zeros((nc, g.num_cells), dtype=torch.float64, device=g.device)
+        else:
+            gs = gs.reshape(1, -1).contiguous() if nc == 1 else gs.t().contiguous()
+        out = torch.empty(ctx.param_shape, dtype=torch.float64, device=g.device)
+        call(ctx.kernel, ctypes.byref(g.cmesh), ctypes.byref(ctx.a), ptr(gd), ptr(gu), ptr(gl), ptr(gs), ptr(out),
+             stream_ptr())
+        return out, None, None, None, None
+
+
+def _frozen_state(field: CellField, a: GfAssembly) -> tuple:
+    """Copies of the boundary state and field values the reverse kernels
+    read, so later updates of the field do not leak into the backward."""
+    t = field.table
+    keep = (t.kind.clone(), t.frac.clone(), t.refv.clone(), t.refg.clone(), field.store.clone())
+    a.bc_kind, a.frac, a.refv, a.refg, a.psi = (ptr(x) for x in keep)
+    return keep
+
+
+def _attach(mat: FvMatrix, param: torch.Tensor, kernel: str, a: GfAssembly, keep: tuple) -> FvMatrix:
+    d, u, lo, src = _AssemblyAdjoint.apply(param, mat, kernel, a, keep)
+    mat._ad = {"diag": d, "upper": u, "lower": lo, "source": src}
+    return mat
+
+
 def ddt(field: CellField) -> FvMatrix:
     """fv/fvm/ddt.py:7-40."""
     mat = FvMatrix(field)
@@ -94,6 +141,11 @@ def div(phi: FaceField, field: CellField) -> FvMatrix:
     a.grad_lsq = ptr(grad) if hanging else None
     _run(field, a)
     mat._keep = grad
+    if torch.is_grad_enabled() and phi.store.requires_grad:
+        # Reverse with respect to the face flux: the transpose face flux.
+        keep = _frozen_state(field, a) + (grad, phi.store.detach().clone())
+        a.phi = ptr(keep[-1])
+        return _attach(mat, phi.store, "gf_div_adjoint", a, keep)
     return mat
 
 
@@ -110,7 +162,7 @@ def laplacian(gamma, field: CellField) -> FvMatrix:
     if isinstance(gamma, torch.Tensor) and gamma.dim() == 1:
         if gamma.shape[0] != grid.num_cells:
             raise ValueError("diffusivity must have one value per cell")
-        g_t = gamma.to(device=grid.device, dtype=torch.float64).contiguous()
+        g_t = gamma.detach().to(device=grid.device, dtype=torch.float64).contiguous()
         if a.lap_harmonic and not bool(torch.all(torch.isfinite(g_t) & (g_t >= 0))):
             raise ValueError("Harmonic diffusivity must be finite and nonnegative")
         a.gamma = ptr(g_t)
@@ -128,4 +180,9 @@ def laplacian(gamma, field: CellField) -> FvMatrix:
         a.ffc = ptr(mat._ffc)
     _run(field, a)
     mat._keep = (g_t, grad)
+    if torch.is_grad_enabled() and isinstance(gamma, torch.Tensor) and gamma.requires_grad:
+        if a.lap_harmonic:
+            raise NotImplementedError("the diffusivity adjoint covers linear interpolation only")
+        keep = _frozen_state(field, a) + (g_t, grad)
+        return _attach(mat, gamma, "gf_laplacian_adjoint", a, keep)
     return mat

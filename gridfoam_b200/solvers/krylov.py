@@ -16,6 +16,7 @@ import torch
 
 from gridfoam_b200._lib import GfKrylov, call, load, ptr, stream_ptr
 from gridfoam_b200.meta.config import NormType, PrecisionType, PreconditionerType, SolverConfig
+from gridfoam_b200.solvers.adjoint import attach_implicit_adjoint
 from gridfoam_b200.solvers.base import LinearSolver, SolveResult, SolveStats, _StatsBuffer
 
 def workspace(cache: dict, device: torch.device, n: int, ncomp: int, kind: int) -> torch.Tensor:
@@ -140,10 +141,24 @@ class DeviceKrylov(LinearSolver):
         return out
 
     def _solve_matrix(self, A, rhs_store: torch.Tensor, x0_store: torch.Tensor) -> SolveResult:
-        x = x0_store.clone()
+        x = x0_store.contiguous().clone()
         stats = self.solve_arrays(A.grid, A.diag_store, A.val, rhs_store.contiguous(), x)
         sol = x[0] if A.field.component_shape == () else x.t()
         return SolveResult(solution=sol, stats=stats)
+
+    def solve(self, eq) -> SolveResult:
+        """solvers/base.py:96-122: with ``grad_mode="adjoint"`` (default) and
+        differentiable coefficients, the solve is detached and the implicit
+        adjoint attached; the device path has no unrolled mode."""
+        A = eq.fv_matrix
+        if torch.is_grad_enabled() and A.requires_grad:
+            if self.grad_mode != "adjoint":
+                raise NotImplementedError("the device solvers differentiate by the implicit adjoint only")
+            with torch.no_grad():
+                res = self._solve_primal(eq)
+            sol = attach_implicit_adjoint(A, res.solution, solve_transpose=self.solve_transpose)
+            return SolveResult(solution=sol, stats=res.stats)
+        return self._solve_primal(eq)
 
     def _solve_primal(self, eq) -> SolveResult:
         A = eq.fv_matrix
@@ -151,8 +166,8 @@ class DeviceKrylov(LinearSolver):
 
     def solve_transpose(self, A_T, rhs: torch.Tensor) -> torch.Tensor:
         nc = A_T.num_components
-        r = rhs.reshape(1, -1) if nc == 1 else rhs.t()
-        res = self._solve_matrix(A_T, r.contiguous(), torch.zeros_like(r))
+        r = (rhs.reshape(1, -1) if nc == 1 else rhs.t()).contiguous()
+        res = self._solve_matrix(A_T, r, torch.zeros_like(r))
         return res.solution
 
 

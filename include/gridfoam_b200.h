@@ -405,6 +405,34 @@ int gf_matrix_flux(const gf_mesh_t* m, int32_t ncomp, const double* val,
                    const double* psi, const double* ffc, double* out,
                    void* stream);
 
+/* ---- Adjoint (reverse-mode) kernels ---------------------------------- */
+
+/* solvers/adjoint/ldu_grads.py:11-53: for x = A^-1 b and lambda = A^-T xbar
+ * (both [ncomp][C]): grad_diag[c] = -sum_k lambda_kc x_kc,
+ * grad_upper[f] = -sum_k lambda_kO x_kN, grad_lower[f] = -sum_k lambda_kN
+ * x_kO over all F internal faces; the source gradient is lambda itself. */
+int gf_adjoint_ldu_grads(const gf_mesh_t* m, int32_t ncomp, const double* lambda,
+                         const double* x, double* grad_diag, double* grad_upper,
+                         double* grad_lower, void* stream);
+
+/* Reverse of fvm.laplacian(gamma, psi) (fv/fvm/laplacian.py:101-201, the
+ * assembly described by `a` with lap_sign 1, linear gamma interpolation):
+ * given the cotangents of diag [C], upper/lower [F] and source [ncomp][C],
+ * writes the gradient with respect to the per-cell diffusivity, g_gamma [C].
+ * Includes the hanging-face skewness source when a->lap_corrected. */
+int gf_laplacian_adjoint(const gf_mesh_t* m, const gf_assembly_t* a,
+                         const double* g_diag, const double* g_upper,
+                         const double* g_lower, const double* g_source,
+                         double* g_gamma, void* stream);
+
+/* Reverse of fvm.div(phi, psi) (fv/fvm/div.py:15-73 with the scheme in `a`):
+ * the transpose of the face-flux -> coefficient map.  Writes g_phi over the
+ * extended face layout [F internal | Nb boundary]. */
+int gf_div_adjoint(const gf_mesh_t* m, const gf_assembly_t* a,
+                   const double* g_diag, const double* g_upper,
+                   const double* g_lower, const double* g_source,
+                   double* g_phi, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

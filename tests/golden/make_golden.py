@@ -3,6 +3,7 @@
 Run in a container where the reference source tree is available::
 
     GRIDFOAM_REF=/root/reference/src python tests/golden/make_golden.py
+    GRIDFOAM_REF=/root/reference/src python tests/golden/make_golden.py --adjoint
 
 It imports the unmodified reference package (with the import stubs in
 ``tests/golden/refshim`` for its absent optional dependencies), builds each
@@ -238,8 +239,73 @@ def operator_dumps(grid: AxisProjectedGrid, algo) -> dict:
 
 
 
+ADJOINT_CASES = ("cavity8", "cavity_oct")
+
+
+def adjoint_case(name: str) -> dict:
+    """Reference autograd gradients through assembly and implicit-adjoint
+    solves, on the case's state after its golden steps:
+
+    * ``L_p = sum(r * x)``, ``x`` the CG solution of
+      ``-laplacian(gamma, p) x = b`` (pressure-type), gradient in ``gamma``;
+    * ``L_U = sum(r3 * u)``, ``u`` the BiCGStab solution of
+      ``div(phi, U) - laplacian(nu_eff, U) + V/dt``, gradient in ``nu_eff``.
+    """
+    case = ALL_CASES[name]()
+    grid, _ = make_grid(case)
+    algo = create_algorithm(grid)
+    for _ in range(STEPS[name]):
+        with torch.no_grad():
+            algo.step()
+    U, p, phi = algo.U, algo.p, algo.phi
+    C = grid.num_cells
+    rng = np.random.default_rng(7)
+    out: dict[str, np.ndarray] = {}
+    gamma = torch.from_numpy(0.5 + rng.random(C)).requires_grad_(True)
+    src = torch.from_numpy(rng.standard_normal(C))
+    r = torch.from_numpy(rng.standard_normal(C))
+    pmat = -fvm.laplacian(gamma, p)
+    pmat.source = pmat.source - src * grid.cell_volumes
+    if needs_reference_value(p):
+        set_reference_value(pmat, 0, 0.0)
+    with torch.no_grad():
+        p.data.zero_()
+    cg = CGSolver(SolverConfig.model_validate(
+        {"method": "cg", "preconditioner": "jacobi", "tolerance": 1e-13, "rel_tolerance": 0.0, "max_iter": 5000}))
+    x = cg.solve(equation(p, pmat)).solution
+    (r * x).sum().backward()
+    out.update(adj_gamma=gamma.detach().numpy().copy(), adj_src=src.numpy().copy(), adj_r=r.numpy().copy(),
+               adj_x=x.detach().numpy().copy(), adj_grad_gamma=gamma.grad.numpy().copy())
+
+    nu = torch.from_numpy(algo.turbulence.nu_eff().detach().numpy() * (0.5 + rng.random(C))).requires_grad_(True)
+    usrc = torch.from_numpy(rng.standard_normal((C, 3)))
+    r3 = torch.from_numpy(rng.standard_normal((C, 3)))
+    umat = fvm.div(phi, U) - fvm.laplacian(nu, U)
+    umat.diag = umat.diag + grid.cell_volumes / 0.01
+    umat.source = umat.source + usrc * grid.cell_volumes[:, None]
+    with torch.no_grad():
+        U.data.zero_()
+    bi = BiCGSTABSolver(SolverConfig.model_validate(
+        {"method": "bicgstab", "preconditioner": "jacobi", "tolerance": 1e-13, "rel_tolerance": 0.0,
+         "max_iter": 5000}))
+    u = bi.solve(equation(U, umat)).solution
+    (r3 * u).sum().backward()
+    out.update(adj_nu=nu.detach().numpy().copy(), adj_usrc=usrc.numpy().copy(), adj_r3=r3.numpy().copy(),
+               adj_u=u.detach().numpy().copy(), adj_grad_nu=nu.grad.numpy().copy(),
+               adj_phi=packed(phi))
+    return out
+
+
 def main() -> None:
-    names = sys.argv[1:] or list(STEPS)
+    args = sys.argv[1:]
+    if args and args[0] == "--adjoint":
+        for name in args[1:] or ADJOINT_CASES:
+            data = adjoint_case(name)
+            path = HERE / f"adjoint_{name}.npz"
+            np.savez_compressed(path, **data)
+            print(f"adjoint {name}: {len(data)} arrays -> {path} ({path.stat().st_size} B)")
+        return
+    names = args or list(STEPS)
     for name in names:
         data = run_case(name, STEPS[name])
         path = HERE / f"{name}.npz"

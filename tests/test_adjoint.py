@@ -1,0 +1,173 @@
+"""Adjoint (reverse-mode) checks of the device path.
+
+* The implicit adjoint of the CG / BiCGStab solves against finite
+  differences (torch.autograd.gradcheck), as the reference does in
+  test_linear_solver_adjoint.py:141-191.
+* Gradients through the hand-written reverse kernels of ``fvm.laplacian``
+  (diffusivity) and the solves, against the reference's own autograd
+  gradient on the same inputs (``tests/golden/adjoint_*.npz``, written by
+  ``make_golden.py --adjoint``), on a uniform and an octree mesh.
+* The transpose face flux (``fvm.div`` reverse in phi) against central
+  finite differences.
+"""
+
+from __future__ import annotations
+
+import pathlib
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from tests.golden.device_harness import device_case, to_np  # noqa: E402
+from tests.golden.cases import STEPS  # noqa: E402
+from tests.golden.oracle_harness import load_golden  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+HERE = pathlib.Path(__file__).resolve().parent / "golden"
+
+
+@pytest.fixture(autouse=True)
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+
+
+def _state(name):
+    golden = load_golden(name)
+    _, _, grid, algo = device_case(name)
+    step = STEPS[name] - 1
+    algo.U.data = torch.as_tensor(golden[f"step{step}_U"], device="cuda")
+    algo.p.data = torch.as_tensor(golden[f"step{step}_p"], device="cuda")
+    algo.phi.unpack(torch.as_tensor(golden[f"step{step}_phi"], device="cuda"))
+    return grid, algo
+
+
+def _solver(kind, tol=1e-13):
+    from gridfoam_b200.meta.config import SolverConfig
+    from gridfoam_b200.solvers.krylov import BiCGSTABSolver, CGSolver
+
+    cfg = SolverConfig(method=kind, preconditioner="jacobi", tolerance=tol, rel_tolerance=0.0, max_iter=5000)
+    return CGSolver(cfg) if kind == "cg" else BiCGSTABSolver(cfg)
+
+
+@pytest.mark.parametrize(("kind", "symmetric", "seed"), [("cg", True, 0), ("bicgstab", False, 2)])
+def test_krylov_adjoint_gradcheck(kind, symmetric, seed):
+    from gridfoam_b200.core.equation import equation
+    from gridfoam_b200.core.field import CellField
+    from gridfoam_b200.core.fvmatrix import FvMatrix
+
+    _, _, grid, _ = device_case("cavity8")
+    p = CellField(grid, f"p_{kind}_adj", "local", ())
+    A = FvMatrix(p)
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    F, C = grid.num_internal_faces, grid.num_cells
+    upper = (0.1 * torch.rand(F, generator=g, dtype=torch.float64)).cuda()
+    lower = upper.clone() if symmetric else (0.05 * torch.rand(F, generator=g, dtype=torch.float64)).cuda()
+    off = torch.zeros(C, dtype=torch.float64, device="cuda")
+    off.index_add_(0, grid.owner, upper.abs())
+    off.index_add_(0, grid.neighbour, lower.abs())
+    diag = off + 1.0
+    source = torch.randn(C, generator=g, dtype=torch.float64).cuda()
+    eq = equation(p, A)
+    solver = _solver(kind, 1e-12)
+
+    def solve_fn(d, u, lo, s):
+        A.diag, A.upper, A.lower, A.source = d, u, lo, s
+        eq.target.data = torch.zeros(C, dtype=torch.float64, device="cuda")
+        return solver.solve(eq).solution
+
+    inputs = tuple(t.detach().requires_grad_(True) for t in (diag, upper, lower, source))
+    assert torch.autograd.gradcheck(solve_fn, inputs, eps=1e-6, atol=1e-4, rtol=1e-3, fast_mode=True)
+
+
+@pytest.mark.parametrize("name", ["cavity8", "cavity_oct"])
+def test_gradients_match_reference_autograd(name):
+    from gridfoam_b200.core.equation import equation
+    from gridfoam_b200.fv import fvm
+
+    ref = np.load(HERE / f"adjoint_{name}.npz")
+    grid, algo = _state(name)
+    U, p, phi = algo.U, algo.p, algo.phi
+    dev = dict(dtype=torch.float64, device="cuda")
+
+    gamma = torch.as_tensor(ref["adj_gamma"], **dev).requires_grad_(True)
+    pmat = -fvm.laplacian(gamma, p)
+    pmat.source = pmat.source - torch.as_tensor(ref["adj_src"], **dev) * grid.cell_volumes
+    if algo.p_needs_ref:
+        # reference_value.py:33-51: the reference cell's diagonal doubles
+        # (and its gradient with it).
+        d = pmat.diag
+        pmat.diag = d + torch.nn.functional.one_hot(torch.tensor(0), grid.num_cells).cuda() * d[0]
+    p.data = torch.zeros(grid.num_cells, **dev)
+    x = _solver("cg").solve(equation(p, pmat)).solution
+    (torch.as_tensor(ref["adj_r"], **dev) * x).sum().backward()
+    np.testing.assert_allclose(to_np(x), ref["adj_x"], rtol=0, atol=1e-9 * np.abs(ref["adj_x"]).max())
+    g_ref = ref["adj_grad_gamma"]
+    assert np.abs(to_np(gamma.grad) - g_ref).max() <= 1e-7 * np.abs(g_ref).max()
+
+    nu = torch.as_tensor(ref["adj_nu"], **dev).requires_grad_(True)
+    umat = fvm.div(phi, U) - fvm.laplacian(nu, U)
+    umat.diag = umat.diag + grid.cell_volumes / 0.01
+    umat.source = umat.source + torch.as_tensor(ref["adj_usrc"], **dev) * grid.cell_volumes[:, None]
+    U.data = torch.zeros((grid.num_cells, 3), **dev)
+    u = _solver("bicgstab").solve(equation(U, umat)).solution
+    (torch.as_tensor(ref["adj_r3"], **dev) * u).sum().backward()
+    np.testing.assert_allclose(to_np(u), ref["adj_u"], rtol=0, atol=1e-9 * np.abs(ref["adj_u"]).max())
+    g_ref = ref["adj_grad_nu"]
+    assert np.abs(to_np(nu.grad) - g_ref).max() <= 1e-7 * np.abs(g_ref).max()
+
+
+@pytest.mark.parametrize("name", ["cavity8", "duct_oct"])
+@pytest.mark.parametrize("scheme", ["linear", "upwind", "vanleer"])
+def test_transpose_face_flux_matches_finite_differences(name, scheme):
+    """d/dphi of sum(r * u), u solving div(phi, U) - laplacian(nu, U) + V/dt,
+    along random directions: adjoint (transpose face flux + BiCGStab
+    transpose solve) against central differences, h = 1e-6 relative."""
+    from gridfoam_b200.core.equation import equation
+    from gridfoam_b200.fv import fvm
+
+    grid, algo = _state(name)
+    U, phi = algo.U, algo.phi
+    base = grid.sim_config
+    grid.sim_config = base.model_copy(update={"fvSchemes": base.fvSchemes.model_copy(
+        update={"divSchemes": {"default": scheme}})})
+    dev = dict(dtype=torch.float64, device="cuda")
+    rng = np.random.default_rng(3)
+    r3 = torch.as_tensor(rng.standard_normal((grid.num_cells, 3)), **dev)
+    usrc = torch.as_tensor(rng.standard_normal((grid.num_cells, 3)), **dev)
+    solver = _solver("bicgstab")
+    phi0 = phi.store.detach().clone()
+    U0 = U.data.detach().clone()
+
+    def loss():
+        U.data = U0  # the advected field (TVD limiter) and the initial guess
+        m = fvm.div(phi, U) - fvm.laplacian(algo.nu, U)
+        m.diag = m.diag + grid.cell_volumes / 0.01
+        m.source = m.source + usrc * grid.cell_volumes[:, None]
+        return (r3 * solver.solve(equation(U, m)).solution).sum()
+
+    # The face-flux store is the leaf: gradients w.r.t. phi on every face.
+    phi.store.requires_grad_(True)
+    loss().backward()
+    g = phi.store.grad.detach().clone()
+    phi.store.requires_grad_(False)
+    phi.store.grad = None
+    scale = phi0.abs().max().item()
+    for k in range(3):
+        h = 1e-6 * scale
+        # Upwind/TVD are piecewise linear in phi: leave faces whose flux is
+        # within 10 h of zero unperturbed, so no face changes sign.
+        v = torch.as_tensor(rng.standard_normal(phi0.shape), **dev) * (phi0.abs() > 10 * h)
+        with torch.no_grad():
+            phi.store.copy_(phi0 + h * v)
+            lp = loss().item()
+            phi.store.copy_(phi0 - h * v)
+            lm = loss().item()
+            phi.store.copy_(phi0)
+        fd = (lp - lm) / (2 * h)
+        ad = float((g * v).sum())
+        assert abs(ad - fd) <= 1e-5 * max(abs(fd), 1e-12), (k, ad, fd)
+    grid.sim_config = base
