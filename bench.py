@@ -233,6 +233,44 @@ def mixed_variant(args, local: int, ref_algo, torch) -> dict:
     }
 
 
+def octree_variant(args, local: int, torch) -> dict:
+    """Cylinder wake on a 3-level octree (hanging faces, general ELL path):
+    the cylinder-wake config at a 96x64x12 base, refined 2 levels within 2D
+    of the cylinder."""
+    from tests.golden.cases import cylinder_wake_case
+    from tests.golden.device_harness import device_case
+
+    case = cylinder_wake_case()
+    t0 = time.perf_counter()
+    _, _, grid, algo = device_case(case_def=case, device=f"cuda:{local}")
+    setup = time.perf_counter() - t0
+    for _ in range(args.warmup):
+        algo.step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    its = []
+    e0.record()
+    for _ in range(args.steps):
+        algo.step()
+        its.append(algo.last_stats["p"])
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    return {
+        "workload": case["name"] + "_piso",
+        "value": grid.num_cells * args.steps / (ms * 1e-3),
+        "unit": METRIC,
+        "ms_per_step": ms / args.steps,
+        "cells": grid.num_cells,
+        "internal_faces": grid.num_internal_faces,
+        "hanging_faces": grid.num_hanging,
+        "immersed_faces": grid.num_immersed_faces,
+        "ell_width": grid.ell_width,
+        "p_iterations_last_step": [s.iterations for s in its[-1]] if its else None,
+        "setup_s": setup,
+    }
+
+
 def serving_bench(args, local: int) -> dict:
     """Solve-server stream (cavity SIMPLE solves of uneven sizes arriving as
     a Poisson process): the continuous-batching engine (FP64, and FP32-inner
@@ -271,13 +309,15 @@ def serving_bench(args, local: int) -> dict:
     runs["sequential_fp64"] = {r.id: r for r in seq}
     out["sequential_fp64"] = summarize(seq)
     fp = runs["engine_fp64"]
-    same = all(np.array_equal(fp[i].U, runs["sequential_fp64"][i].U) or
-               np.allclose(fp[i].U, runs["sequential_fp64"][i].U, rtol=0, atol=1e-12) for i in fp)
+    seq_d = [float(np.linalg.norm(fp[i].U - runs["sequential_fp64"][i].U) /
+                   max(np.linalg.norm(runs["sequential_fp64"][i].U), 1e-300)) for i in fp]
     errs = []
     for i, r in runs["engine_mixed"].items():
         ref = fp[i].U
         errs.append(float(np.linalg.norm(r.U - ref) / max(np.linalg.norm(ref), 1e-300)))
-    out["engine_fp64"]["matches_sequential"] = bool(same)
+    # Same algorithm and iterations; the engine's block caps change only the
+    # order of the dot-product partial sums.
+    out["engine_fp64"]["max_rel_l2_U_vs_sequential"] = max(seq_d) if seq_d else None
     out["engine_mixed"]["max_rel_l2_U_vs_fp64"] = max(errs) if errs else None
     for k in ("engine_fp64", "engine_mixed"):
         out[k]["speedup_solves_per_s_vs_sequential"] = (
@@ -423,7 +463,8 @@ def run_gpu(args) -> None:
         },
     }
     if not args.no_variants:
-        line["variants"] = {"mixed_fp32_inner": mixed_variant(args, local, algo, torch)}
+        line["variants"] = {"mixed_fp32_inner": mixed_variant(args, local, algo, torch),
+                            "octree_cylinder_wake": octree_variant(args, local, torch)}
     if not args.no_serving and world == 1:
         line["serving"] = serving_bench(args, local)
     if rank == 0 and not args.no_cpu_baseline and world == 1:

@@ -512,6 +512,60 @@ def ibcyl_oct_case() -> dict:
     }
 
 
+def cylinder_wake_case(base: tuple[int, int, int] = (96, 64, 12), levels: int = 2) -> dict:
+    """Cylinder wake on a 3-level octree (the cylinder-wake config, scaled
+    by its base resolution): domain 30D x 20D x 4D, cylinder D = 1 at
+    (10, 10) spanning z, refined ``levels`` levels within 2D of its surface;
+    inflow 1, nu 0.01 (Re 100), PISO at CFL 0.5 on the finest cell."""
+    cyl = {"kind": "cylinder", "center": [10.0, 10.0], "radius": 0.5, "axis": 2, "patch": "cylinder"}
+    dx_fine = 30.0 / base[0] / 2**levels
+    sim = {
+        "control": _control(0.5 * dx_fine / 1.0, 1.0e3),
+        "fvSchemes": {"divSchemes": {"default": "upwind"}},
+        "fvSolution": {
+            "adjustPhi": True,
+            "algorithm": {"type": "piso", "nCorrectors": 2, "pRefCell": 0, "pRefValue": 0.0},
+            "solvers": {
+                "U": {"method": "bicgstab", "preconditioner": "jacobi", "tolerance": 1e-8, "rel_tolerance": 0.1},
+                "p": {"method": "cg", "preconditioner": "jacobi", "tolerance": 1e-7, "rel_tolerance": 0.01},
+                "pFinal": {"method": "cg", "preconditioner": "jacobi", "tolerance": 1e-7, "rel_tolerance": 0.0},
+            },
+        },
+        "conditions": {
+            "U": {
+                "internal": [1.0, 0.0, 0.0],
+                "boundary": {
+                    "inlet": {"type": "dirichlet", "patches": ["x_minus"], "value": [1.0, 0.0, 0.0]},
+                    "outlet": {"type": "inlet_outlet", "patches": ["x_plus"], "value": WALL0},
+                    "sides": {"type": "slip", "patches": ["y_minus", "y_plus", "z_minus", "z_plus"]},
+                    "cyl": {"type": "dirichlet", "patches": ["cylinder"], "value": WALL0},
+                },
+            },
+            "p": {
+                "internal": 0.0,
+                "boundary": {
+                    "outlet": {"type": "dirichlet", "patches": ["x_plus"], "value": 0.0},
+                    "cyl": {"type": "dirichlet", "patches": ["cylinder"], "value": 0.0},
+                    "rest": {"type": "neumann", "patches": ["x_minus", "y_minus", "y_plus", "z_minus", "z_plus"],
+                             "value": 0.0},
+                },
+            },
+        },
+        "properties": _props(0.01),
+        "device": "cpu",
+    }
+    return {
+        "name": f"cylinder_wake_{base[0]}x{base[1]}x{base[2]}",
+        "mesh": {
+            "kind": "octree", "lower": [0, 0, 0], "upper": [30.0, 20.0, 4.0], "res": list(base),
+            "regions": [{"kind": "sdf", "body": cyl, "distance": 2.0, "level": levels}],
+            "bodies": [cyl],
+        },
+        "simulator": sim,
+        "inlet_profile": None,
+    }
+
+
 ALL_CASES = {
     "cavity8": lambda: cavity_case(8),
     "pipe10x20": lambda: pipe_case(10, 20),
