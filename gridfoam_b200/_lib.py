@@ -212,6 +212,7 @@ _SIGNATURES = {
     "gf_adjoint_ldu_grads": ([P, I32, P, P, P, P, P, P], ctypes.c_int),
     "gf_laplacian_adjoint": ([P, P, P, P, P, P, P, P], ctypes.c_int),
     "gf_div_adjoint": ([P, P, P, P, P, P, P, P], ctypes.c_int),
+    "gf_force_integral": ([P, I64, P, P, P, P, P, P, P, P, P, F64, F64, F64, F64, F64, P, P, P], ctypes.c_int),
 }
 
 EXPORTED = tuple(_SIGNATURES)

@@ -240,6 +240,9 @@ class AxisProjectedGrid:
             bnd_near=bnd_near,
         )
         host.extra["lsq_ata_inv"] = ata_inv
+        normals = getattr(ap, "anchor_normal", None)
+        host.extra["anchor_normal"] = (np.asarray(normals, dtype=np.float64).reshape(Fi, 3)
+                                       if normals is not None else None)
         host.extra["hang_faces"] = hang_faces
         host.extra["hang_offset"] = hang_offset
         host.extra["hang_move_o"] = move_o

@@ -50,6 +50,9 @@ class ApPayload:
     owner_near_boundary: np.ndarray
     dist_neighbour_to_bnd: np.ndarray
     neighbour_near_boundary: np.ndarray
+    # [Fi, 3] body-outward unit surface normal per anchor (one anchor per
+    # immersed face); stands in for the surface mesh's face area vectors.
+    anchor_normal: np.ndarray | None = None
 
 
 @dataclass
@@ -241,6 +244,24 @@ def _axis_projected_payload(
     d_nei = (1.0 - t_own[faces]) * seg
     dx_own = sizes[owner[faces], axis[faces]]
     dx_nei = sizes[neighbour[faces], axis[faces]]
+    # Body-outward unit normal at each crossing (the SDF gradient by central
+    # differences; outward for a body occupying sdf < 0): the surface normal
+    # the force integral orients its samples by.
+    normals = np.zeros((faces.shape[0], 3))
+    if faces.shape[0]:
+        pts = p0[faces] + t_own[faces][:, None] * (p1[faces] - p0[faces])
+        h = 1e-6 * extent
+        body_of = patch_of[faces]
+        for body in bodies:
+            sel = body_of == patches.get(body.patch, -1)
+            if not np.any(sel):
+                continue
+            for ax in range(3):
+                e = np.zeros(3)
+                e[ax] = h
+                normals[sel, ax] = (body.sdf(pts[sel] + e) - body.sdf(pts[sel] - e)) / (2 * h)
+        nrm = np.linalg.norm(normals, axis=1)
+        normals = normals / np.where(nrm > 0, nrm, 1.0)[:, None]
     ap = ApPayload(
         is_immersed_face=immersed,
         owner_bnd_patch_id=patch_of[faces].copy(),
@@ -251,6 +272,7 @@ def _axis_projected_payload(
         owner_near_boundary=(d_own / dx_own) <= (dx_own / extent),
         dist_neighbour_to_bnd=d_nei,
         neighbour_near_boundary=(d_nei / dx_nei) <= (dx_nei / extent),
+        anchor_normal=normals,
     )
     return ap, patches
 

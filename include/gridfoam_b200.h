@@ -433,6 +433,24 @@ int gf_div_adjoint(const gf_mesh_t* m, const gf_assembly_t* a,
                    const double* g_lower, const double* g_source,
                    double* g_phi, void* stream);
 
+/* ---- Post-processing -------------------------------------------------- */
+
+/* post/forces/sampling.py:69-168 + integration.py:76-187: force on an
+ * immersed patch from its n axis-projected boundary samples (faces: boundary
+ * face indices, upper and lower sides).  anchor_normal [3][n_imm] is the
+ * body-outward surface normal per anchor (immersed face); a sample is kept
+ * when its outward direction points into the body.  Writes per-sample rows
+ * samples[12][n] (pressure force xyz, viscous force xyz, force xyz, moment
+ * about (cx, cy, cz) xyz; zero for dropped samples) and total[6] (force,
+ * moment), summed in a fixed order.  nu_eff [C] or NULL for nu_scalar. */
+int gf_force_integral(const gf_mesh_t* m, int64_t n, const int32_t* faces,
+                      const double* anchor_normal, const int8_t* p_kind,
+                      const gf_bc_state_t* p_state, const double* p,
+                      const int8_t* u_kind, const gf_bc_state_t* u_state,
+                      const double* U, const double* nu_eff, double nu_scalar,
+                      double rho, double cx, double cy, double cz,
+                      double* samples, double* total, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

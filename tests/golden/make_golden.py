@@ -4,6 +4,7 @@ Run in a container where the reference source tree is available::
 
     GRIDFOAM_REF=/root/reference/src python tests/golden/make_golden.py
     GRIDFOAM_REF=/root/reference/src python tests/golden/make_golden.py --adjoint
+    GRIDFOAM_REF=/root/reference/src python tests/golden/make_golden.py --forces
 
 It imports the unmodified reference package (with the import stubs in
 ``tests/golden/refshim`` for its absent optional dependencies), builds each
@@ -296,8 +297,71 @@ def adjoint_case(name: str) -> dict:
     return out
 
 
+class _StubSurfaceMesh:
+    """Stand-in for the graphlow surface mesh the reference's force
+    integration reads: one face per AP anchor (immersed face) whose area
+    vector is the builder's body-outward unit normal there."""
+
+    class _Geometry:
+        def __init__(self, vectors):
+            self._v = vectors
+
+        def face_area_vectors(self):
+            return self._v
+
+    def __init__(self, normals: np.ndarray):
+        self.geometry = self._Geometry(torch.from_numpy(np.ascontiguousarray(normals)))
+        self.n_cells = normals.shape[0]
+        self.cell_data: dict = {}
+
+
+FORCE_CASES = ("ibcyl_oct",)
+
+
+def force_case(name: str) -> dict:
+    """The reference's immersed-surface force integral
+    (post/forces/integration.py:125-187) on the case's state after its golden
+    steps, with the surface-mesh normals taken from the mesh builder."""
+    from gridfoam.post.forces.integration import integrate_patch_on_surface_mesh, reset_surface_force_data
+
+    case = ALL_CASES[name]()
+    grid, mesh = make_grid(case)
+    algo = create_algorithm(grid)
+    for _ in range(STEPS[name]):
+        with torch.no_grad():
+            algo.step()
+    grid._mesh_path = "builder-normals"
+    grid._surface_mesh_cache = _StubSurfaceMesh(mesh.ap.anchor_normal)
+    reset_surface_force_data(grid)
+    cofr = torch.tensor([0.5, 0.5, 0.25], dtype=torch.float64)
+    nu_eff = algo.turbulence.nu_eff()
+    with torch.no_grad():
+        force, moment = integrate_patch_on_surface_mesh(
+            grid, p=algo.p, U=algo.U, nu_eff=nu_eff, patch_name="cylinder", rho=1.2, center_of_rotation=cofr)
+    cd = grid.surface_mesh.cell_data
+    return {
+        "force": force.numpy().copy(),
+        "moment": moment.numpy().copy(),
+        "pressure_force": cd["pressure_force"].numpy().copy(),
+        "viscous_force": cd["viscous_force"].numpy().copy(),
+        "U": algo.U.data.numpy().copy(),
+        "p": algo.p.data.numpy().copy(),
+        "phi": packed(algo.phi),
+        "nu_eff": nu_eff.detach().numpy().copy() if isinstance(nu_eff, torch.Tensor) else np.array(nu_eff),
+        "rho": np.array(1.2),
+        "cofr": cofr.numpy().copy(),
+    }
+
+
 def main() -> None:
     args = sys.argv[1:]
+    if args and args[0] == "--forces":
+        for name in args[1:] or FORCE_CASES:
+            data = force_case(name)
+            path = HERE / f"forces_{name}.npz"
+            np.savez_compressed(path, **data)
+            print(f"forces {name}: {len(data)} arrays -> {path} ({path.stat().st_size} B)")
+        return
     if args and args[0] == "--adjoint":
         for name in args[1:] or ADJOINT_CASES:
             data = adjoint_case(name)
