@@ -195,6 +195,7 @@ _SIGNATURES = {
     "gf_simplec_rAtU": ([P, P, P, P, P], ctypes.c_int),
     "gf_face_flux": ([P, I32, P, P, P, P, P, P, P], ctypes.c_int),
     "gf_fvc_div": ([P, I32, P, P, P], ctypes.c_int),
+    "gf_reconstruct": ([P, P, P, P], ctypes.c_int),
     "gf_interpolate": ([P, I32, P, P, P, P, P, P], ctypes.c_int),
     "gf_sn_grad": ([P, I32, P, P, P, P, P, P, P, P], ctypes.c_int),
     "gf_correct_phi": ([P, P, P, P, P, P, P, P, F64, I32, P, P, P, P], ctypes.c_int),

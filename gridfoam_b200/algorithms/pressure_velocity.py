@@ -19,7 +19,7 @@ import torch
 
 from gridfoam_b200 import _lib
 from gridfoam_b200._lib import GfAssembly, GfBcAux, GfDdtCorr, call, ptr, stream_ptr
-from gridfoam_b200.core.boundary import DirichletBC, InletOutletBC
+from gridfoam_b200.core.boundary import DirichletBC
 from gridfoam_b200.core.field import (
     CellField,
     FaceField,
@@ -28,6 +28,7 @@ from gridfoam_b200.core.field import (
 )
 from gridfoam_b200.core.fvmatrix import FvMatrix
 from gridfoam_b200.fv import schemes
+from gridfoam_b200.fv.adjust_phi import adjust_classes
 from gridfoam_b200.meta.config import (
     AlgorithmType,
     FieldRole,
@@ -186,16 +187,7 @@ class _PressureVelocity:
 
     def _build_adjust_classes(self) -> torch.Tensor:
         """adjust_phi.py:21-41 classes per domain face: 0 skip, 1 fixed, 2 adjustable."""
-        g = self._grid
-        import numpy as np
-
-        cls = np.zeros(g.num_domain_bnd_faces, dtype=np.int8)
-        for patch, bc in self.U.bcs.items():
-            faces = g.patch_faces(patch)
-            faces = faces[faces < g.num_domain_bnd_faces]
-            fixes = isinstance(bc, DirichletBC) and not isinstance(bc, InletOutletBC)
-            cls[faces] = 1 if fixes else 2
-        return torch.as_tensor(cls, device=g.device)
+        return adjust_classes(self.U)
 
     # ------------------------------------------------------------------
     # boundary states

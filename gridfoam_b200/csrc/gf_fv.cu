@@ -957,6 +957,36 @@ __global__ void k_matrix_flux(gf_mesh_t m, const double* __restrict__ val, const
     }
 }
 
+// fv/fvc/reconstruct.py:28-117: U_c = (sum_f |Sf| n n^T)^-1 sum_f n phi_f over
+// every face of the cell (both sides of internal faces with the same sign;
+// boundary faces with their outward Sf).  Diagonal on axis-aligned grids.
+__global__ void k_reconstruct(gf_mesh_t m, const double* __restrict__ phi, double* __restrict__ U) {
+    const int64_t C = m.n_cells, F = m.n_faces, nb = m.n_bnd;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < C; c += (int64_t)gridDim.x * blockDim.x) {
+        double num[3] = {0.0, 0.0, 0.0}, den[3] = {0.0, 0.0, 0.0};
+        for (int s = 0; s < m.ell_width; ++s) {
+            const Slot sl = decode_slot(m, __ldg(m.ell_code + s * C + c));
+            double sf[3], flux;
+            if (sl.kind == kInternal) {
+                for (int k = 0; k < 3; ++k) sf[k] = __ldg(m.sf + k * F + sl.face);
+                flux = phi[sl.face];
+            } else if (sl.kind == kBoundary) {
+                for (int k = 0; k < 3; ++k) sf[k] = __ldg(m.bnd_sf + k * nb + sl.bnd);
+                flux = phi[F + sl.bnd];
+            } else {
+                continue;
+            }
+            const double mag = sqrt(sf[0] * sf[0] + sf[1] * sf[1] + sf[2] * sf[2]);
+            for (int k = 0; k < 3; ++k) {
+                const double n = sf[k] / mag;
+                num[k] += flux * n;
+                den[k] += mag * n * n;
+            }
+        }
+        for (int k = 0; k < 3; ++k) U[k * C + c] = num[k] / den[k];
+    }
+}
+
 static bool valid_mesh(const gf_mesh_t* m) {
     if (m == nullptr || m->n_cells <= 0 || m->ell_width <= 0 || m->ell_code == nullptr ||
         m->ell_nbr == nullptr || m->volume == nullptr) {
@@ -1135,6 +1165,15 @@ int gf_face_flux(const gf_mesh_t* m, int32_t mode, const double* vel, const int8
     k_face_flux<<<grid_for(m->n_faces + m->n_bnd), kThreads, 0, GF_STREAM(stream)>>>(*m, mode, vel, u_kind, u_psib,
                                                                                      d, has, grad_vel, phi);
     return check_launch("gf_face_flux");
+}
+
+int gf_reconstruct(const gf_mesh_t* m, const double* phi, double* U, void* stream) {
+    if (!valid_mesh(m) || phi == nullptr || U == nullptr || m->sf == nullptr || m->bnd_sf == nullptr) {
+        set_error("gf_reconstruct: invalid arguments");
+        return GF_ERR_INVALID;
+    }
+    k_reconstruct<<<grid_for(m->n_cells), kThreads, 0, GF_STREAM(stream)>>>(*m, phi, U);
+    return check_launch("gf_reconstruct");
 }
 
 int gf_fvc_div(const gf_mesh_t* m, int32_t ncomp, const double* phi, double* out, void* stream) {

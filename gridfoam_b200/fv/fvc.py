@@ -86,6 +86,18 @@ def sn_grad(field: CellField) -> FaceField:
     return out
 
 
+def reconstruct(phi: FaceField, U: CellField) -> torch.Tensor:
+    """fv/fvc/reconstruct.py:28-117: sets and returns ``U.data`` [C, 3]."""
+    if phi.component_shape != ():
+        raise ValueError("phi must be a scalar face flux field.")
+    if U.component_shape != (3,):
+        raise ValueError("U must be a 3-component velocity field.")
+    if phi.grid is not U.grid:
+        raise ValueError("phi and U must share the same grid.")
+    call("gf_reconstruct", ctypes.byref(U.grid.cmesh), ptr(phi.store), ptr(U.store), stream_ptr())
+    return U.data
+
+
 def face_flux(phi: FaceField, U: CellField) -> None:
     """fv/flux.py:132-162 ``correct_flux(phi, U, update_internal=True)``."""
     _eval_state(U)

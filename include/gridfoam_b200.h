@@ -317,6 +317,11 @@ int gf_face_flux(const gf_mesh_t* m, int32_t mode, const double* vel,
                  const gf_ddtcorr_t* ddt, const double* grad_vel, double* phi,
                  void* stream);
 
+/* fv/fvc/reconstruct.py:28-117: cell velocity U [3][C] from the face flux
+ * phi (extended layout [F | Nb]): (sum |Sf| n n^T)^-1 sum n phi over every
+ * face of the cell. */
+int gf_reconstruct(const gf_mesh_t* m, const double* phi, double* U, void* stream);
+
 /* fv/fvc/div.py:15-64: div(phi) = face sum / V for ncomp face fields. */
 int gf_fvc_div(const gf_mesh_t* m, int32_t ncomp, const double* phi,
                double* out, void* stream);

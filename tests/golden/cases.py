@@ -566,6 +566,19 @@ def cylinder_wake_case(base: tuple[int, int, int] = (96, 64, 12), levels: int = 
     }
 
 
+def potential_case(name: str) -> dict:
+    """A case definition with the potential-flow initialisation configured
+    (fvSolution.potentialFlow and a ``Phi`` solver): one non-orthogonal
+    corrector, Jacobi-CG to 1e-11."""
+    case = copy.deepcopy(ALL_CASES[name]())
+    sol = case["simulator"]["fvSolution"]
+    sol["potentialFlow"] = {"nNonOrthogonalCorrectors": 1, "phiRefCell": 0, "phiRefValue": 0.0}
+    sol["solvers"]["Phi"] = {"method": "cg", "preconditioner": "jacobi", "tolerance": 1e-11,
+                             "rel_tolerance": 0.0, "max_iter": 5000}
+    case["name"] = name + "_potential"
+    return case
+
+
 ALL_CASES = {
     "cavity8": lambda: cavity_case(8),
     "pipe10x20": lambda: pipe_case(10, 20),
@@ -578,6 +591,8 @@ ALL_CASES = {
 }
 # Cases on octree meshes (hanging faces).
 OCTREE_CASES = ("cavity_oct", "duct_oct", "ibcyl_oct")
+# Cases whose potential-flow initialisation is pinned to the reference.
+POTENTIAL_CASES = ("duct_oct", "ibcyl_oct")
 
 
 # Steps stored per golden case and the convection schemes dumped per case.

@@ -5,6 +5,7 @@ Run in a container where the reference source tree is available::
     GRIDFOAM_REF=/root/reference/src python tests/golden/make_golden.py
     GRIDFOAM_REF=/root/reference/src python tests/golden/make_golden.py --adjoint
     GRIDFOAM_REF=/root/reference/src python tests/golden/make_golden.py --forces
+    GRIDFOAM_REF=/root/reference/src python tests/golden/make_golden.py --potential
 
 It imports the unmodified reference package (with the import stubs in
 ``tests/golden/refshim`` for its absent optional dependencies), builds each
@@ -353,8 +354,46 @@ def force_case(name: str) -> dict:
     }
 
 
+def potential_run(name: str) -> dict:
+    """The reference's potentialFoam-style initialisation
+    (pre/potential_flow.py:122-214) and fvc.reconstruct of the initial flux
+    on the case's initial fields."""
+    from gridfoam.fv.fvc.reconstruct import reconstruct
+    from gridfoam.fv.flux import correct_flux
+    from gridfoam.pre.potential_flow import PotentialFlow
+
+    from tests.golden.cases import potential_case
+
+    case = potential_case(name)
+    grid, _ = make_grid(case)
+    pf = PotentialFlow(grid)
+    out: dict[str, np.ndarray] = {}
+    with torch.no_grad():
+        correct_flux(pf.phi, pf.U, update_internal=True)
+        out["init_phi"] = packed(pf.phi)
+        out["init_U"] = pf.U.data.numpy().copy()
+        scratch = ref_field.get_or_create_cellfield(grid, "U_reconstructed", ref_field.FieldRole.LOCAL, (3,))
+        out["reconstruct_init"] = reconstruct(pf.phi, scratch).numpy().copy()
+        pf.solve()
+    out["U"] = pf.U.data.numpy().copy()
+    out["phi"] = packed(pf.phi)
+    Phi = grid.get_cellfield("Phi")
+    if Phi is not None:
+        out["Phi"] = Phi.data.numpy().copy()
+    return out
+
+
 def main() -> None:
     args = sys.argv[1:]
+    if args and args[0] == "--potential":
+        from tests.golden.cases import POTENTIAL_CASES
+
+        for name in args[1:] or POTENTIAL_CASES:
+            data = potential_run(name)
+            path = HERE / f"potential_{name}.npz"
+            np.savez_compressed(path, **data)
+            print(f"potential {name}: {sorted(data)} -> {path} ({path.stat().st_size} B)")
+        return
     if args and args[0] == "--forces":
         for name in args[1:] or FORCE_CASES:
             data = force_case(name)
