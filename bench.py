@@ -271,22 +271,36 @@ def octree_variant(args, local: int, torch) -> dict:
     }
 
 
-def serving_bench(args, local: int) -> dict:
+def serving_bench(args, local: int, dist=None, rank: int = 0, world: int = 1) -> dict:
     """Solve-server stream (cavity SIMPLE solves of uneven sizes arriving as
     a Poisson process): the continuous-batching engine (FP64, and FP32-inner
     pressure CG) against one-at-a-time FP64 solves through the plain API,
-    on the same requests."""
+    on the same requests.  With several GPUs each rank serves its share of
+    the one stream (no collective on the data path) and the summaries are
+    merged: solves/s over the whole job, percentiles over every request."""
     import numpy as np
     import torch
 
     from gridfoam_b200.serving import SIZES, ServingEngine, poisson_stream, serve_sequential, summarize
+    from gridfoam_b200.serving.shard import merge_summaries, shard_stream
 
-    reqs = poisson_stream(args.serve_requests, rate=50.0, sizes=SIZES, seed=local)
+    stream = poisson_stream(args.serve_requests, rate=50.0, sizes=SIZES, seed=0)
+    reqs = shard_stream(stream, world, rank)
+
+    def whole(res):
+        if dist is None:
+            return summarize(res)
+        part = ([r.latency for r in res], min((r.arrival for r in res), default=0.0),
+                max((r.finished for r in res), default=0.0))
+        parts = [None] * world
+        dist.all_gather_object(parts, part)
+        return merge_summaries([p[0] for p in parts], [p[1] for p in parts], [p[2] for p in parts])
     common = dict(max_outer=args.serve_end_time, p_tol=1e-6, p_solver_tol=1e-6, keep_fields=True)
     out = {
         "workload": "cavity SIMPLE stream: sizes uniform over 16^3..96^3, Re log-uniform [10,1000], "
                     "lid U uniform [0.5,2], Poisson arrivals 50/s, p cg tol 1e-6, residualControl p 1e-6",
-        "requests": len(reqs),
+        "requests": len(stream),
+        "replicas": world,
         "end_time": args.serve_end_time,
         "sample": f"{len(reqs)} of the 1024-request stream, endTime capped at {args.serve_end_time} iterations",
     }
@@ -301,13 +315,13 @@ def serving_bench(args, local: int) -> dict:
         runs[name] = {r.id: r for r in res}
         if name == "engine_fp64":
             fp_variants = dict(eng.variants)
-        out[name] = {**summarize(res), "prepare_s": prep, "slots": args.serve_slots, "gpu_share": args.serve_share,
+        out[name] = {**whole(res), "prepare_s": prep, "slots": args.serve_slots, "gpu_share": args.serve_share,
                      "autotuned_variants": {str(k): v for k, v in eng.variants.items()}}
         del eng
         torch.cuda.empty_cache()
     seq = serve_sequential(reqs, device=f"cuda:{local}", variants=fp_variants, **common)
     runs["sequential_fp64"] = {r.id: r for r in seq}
-    out["sequential_fp64"] = summarize(seq)
+    out["sequential_fp64"] = whole(seq)
     fp = runs["engine_fp64"]
     seq_d = [float(np.linalg.norm(fp[i].U - runs["sequential_fp64"][i].U) /
                    max(np.linalg.norm(runs["sequential_fp64"][i].U), 1e-300)) for i in fp]
@@ -317,6 +331,10 @@ def serving_bench(args, local: int) -> dict:
         errs.append(float(np.linalg.norm(r.U - ref) / max(np.linalg.norm(ref), 1e-300)))
     # Same algorithm and iterations; the engine's block caps change only the
     # order of the dot-product partial sums.
+    if dist is not None:
+        both = [None] * world
+        dist.all_gather_object(both, (max(seq_d, default=0.0), max(errs, default=0.0)))
+        seq_d, errs = [b[0] for b in both], [b[1] for b in both]
     out["engine_fp64"]["max_rel_l2_U_vs_sequential"] = max(seq_d) if seq_d else None
     out["engine_mixed"]["max_rel_l2_U_vs_fp64"] = max(errs) if errs else None
     for k in ("engine_fp64", "engine_mixed"):
@@ -465,8 +483,8 @@ def run_gpu(args) -> None:
     if not args.no_variants:
         line["variants"] = {"mixed_fp32_inner": mixed_variant(args, local, algo, torch),
                             "octree_cylinder_wake": octree_variant(args, local, torch)}
-    if not args.no_serving and world == 1:
-        line["serving"] = serving_bench(args, local)
+    if not args.no_serving:
+        line["serving"] = serving_bench(args, local, dist, rank, world)
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
     if rank == 0:
