@@ -424,13 +424,17 @@ def run_gpu(args) -> None:
     peak, peak_kind = peaks()
     achieved = total_bytes / total_time / 1e9 if total_time > 0 else 0.0
 
-    # End-to-end through the public API, continuing the same trajectory:
-    # every step takes U and p in from pinned host memory, runs, and reads
-    # its U and p back into the same host buffers (stream-ordered, so the
+    # End-to-end through the public API on the same trajectory as the timed
+    # region: a second case from the same initial state, the same warm-up,
+    # then the same steps, each taking U and p in from pinned host memory
+    # and reading them back into the same buffers (stream-ordered, so the
     # next step's upload sees this step's result).
+    _, _, _, algo = device_case(case_def=pipe_config(), device=f"cuda:{local}")
+    for _ in range(args.warmup):
+        algo.step()
     U_h = algo.U.data.detach().cpu().pin_memory()
     p_h = algo.p.data.detach().cpu().pin_memory()
-    e2e_steps = max(1, args.steps // 2)
+    e2e_steps = args.steps
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()

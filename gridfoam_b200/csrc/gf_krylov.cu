@@ -986,6 +986,10 @@ constexpr int kBoxVariants = 5;
 // FP64 symmetric box CG with shared-memory tiles (k_pcg1_box_staged); falls
 // back to variant 0 when the system does not qualify.
 constexpr int kStagedVariant = 5;
+// FP64 CG with the own-cell vectors in shared memory (pcg1_smem_body), box
+// or ELL, 512-thread (6) or 1024-thread (7) blocks; falls back when the
+// system is too large for it.
+constexpr int kSmemVariant = 6;
 
 template <bool MIXED, bool SYM, int THREADS, int U>
 static BoxVariant box_variant() {
@@ -1390,6 +1394,178 @@ __global__ void __launch_bounds__(THREADS, 1) k_pcg1_box_staged(gf_krylov_t K, i
         o[3] = st.converged;
         o[4] = ok ? st.status : GF_ERR_TIMEOUT;
     }
+}
+
+// ---------------------------------------------------------------------------
+// CG with each block's own-cell vectors resident in shared memory.
+//
+// Every block owns one contiguous chunk of cells for the whole solve and
+// keeps x, r, q = A p and p of those cells in shared memory (4 doubles a
+// cell: the 148 SMs' shared memory together holds them for about a million
+// cells).  Only what neighbours read goes through global memory: z = M r and
+// p (double-buffered), plus the matrix.  The update pass is then shared
+// memory plus one read of the diagonal and one write of z, about half the
+// global traffic of pcg1_body per iteration.  x is read once at the start
+// and written once at the end.  Arithmetic per cell is that of pcg1_body.
+template <int THREADS, int U, bool KEEP_P, class Rows>
+__device__ void pcg1_smem_body(const gf_krylov_t& K, const Rows& rows, int64_t chunk) {
+    __shared__ CgState st;
+    extern __shared__ __align__(16) double sm[];
+    KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
+    barrier_init();
+    double* partials = K.work + kCtlDoubles;
+    double* vec = partials + kPartials;
+    const int64_t n = K.n;
+    double* z = vec;
+    double* pa = vec + n;
+    double* pb = vec + 2 * n;
+    const int64_t c0 = blockIdx.x * chunk;
+    const int64_t c1 = c0 + chunk < n ? c0 + chunk : n;
+    const int m = c1 > c0 ? (int)(c1 - c0) : 0;
+    double* xs = sm;
+    double* rs = sm + chunk;
+    double* qs = sm + 2 * chunk;
+    double* ps = sm + 3 * chunk;  // only with KEEP_P (else p is re-read from global)
+    const bool jac = K.jacobi != 0, linf = K.norm_inf != 0;
+    bool ok = true;
+    {  // r = b - A x, z = M r, p = 0; |r| and r.z
+        double loc[2] = {0.0, 0.0};
+        auto gx = [&](int64_t i) { return __ldcg(K.x + i); };
+        for (int i = threadIdx.x; i < m; i += THREADS) {
+            const int64_t c = c0 + i;
+            const double ax = rows.apply(c, __ldg(K.diag + c), gx);
+            const double rk = __ldg(K.rhs + c) - ax;
+            const double zk = inv_diag(K.diag, c, jac) * rk;
+            xs[i] = __ldcg(K.x + c);
+            rs[i] = rk;
+            __stcg(z + c, zk);
+            __stcg(pa + c, 0.0);
+            loc[0] = norm_acc(loc[0], rk, linf);
+            loc[1] += rk * zk;
+        }
+        ok = grid_reduce<2, THREADS>(ctl, partials, loc, linf ? 1u : 0u);
+        if (threadIdx.x == 0) {
+            const double r0 = norm_fin(loc[0], linf);
+            st.r0 = r0;
+            st.final = r0;
+            st.thresh = fmax(K.atol, K.rtol * r0);
+            st.rz_old = loc[1];
+            st.beta = 0.0;
+            st.its = 0;
+            st.converged = 0;
+            st.status = GF_MAX_ITER;
+            st.done = 0;
+            if (r0 < st.thresh) {
+                st.done = 1;
+                st.converged = 1;
+                st.status = GF_OK;
+            } else if (!isfinite(r0)) {
+                st.done = 1;
+                st.status = GF_NONFINITE;
+            }
+        }
+        __syncthreads();
+    }
+    double* p_old = pa;
+    double* p_new = pb;
+    for (int it = 1; ok && !st.done && it <= K.max_iter; ++it) {
+        {  // p_new = z + p_old beta; q = A p_new; p_new . q
+            const double beta = st.beta;
+            double loc[1] = {0.0};
+            auto gp = [&](int64_t j) { return __ldcg(z + j) + __ldcg(p_old + j) * beta; };
+            // U cells per thread per pass: all their loads are issued before
+            // any store, so U latency chains overlap.
+            for (int i0 = threadIdx.x; i0 < m; i0 += U * THREADS) {
+                double pc[U], ap[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int i = i0 + u * THREADS;
+                    if (i < m) {
+                        const int64_t c = c0 + i;
+                        pc[u] = gp(c);
+                        ap[u] = rows.apply(c, __ldg(K.diag + c), gp);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int i = i0 + u * THREADS;
+                    if (i < m) {
+                        __stcg(p_new + c0 + i, pc[u]);
+                        if (KEEP_P) ps[i] = pc[u];
+                        qs[i] = ap[u];
+                        loc[0] += pc[u] * ap[u];
+                    }
+                }
+            }
+            ok = grid_reduce<1, THREADS>(ctl, partials, loc, 0u);
+            if (!ok) break;
+            if (threadIdx.x == 0) st.alpha = st.rz_old / loc[0];
+            __syncthreads();
+        }
+        {  // x += alpha p; r -= alpha q; z = M r; |r|, r.z (own cells)
+            const double alpha = st.alpha;
+            double loc[2] = {0.0, 0.0};
+            for (int i = threadIdx.x; i < m; i += THREADS) {
+                const int64_t c = c0 + i;
+                xs[i] = xs[i] + alpha * (KEEP_P ? ps[i] : __ldcg(p_new + c));
+                const double rk = rs[i] - alpha * qs[i];
+                const double zk = inv_diag(K.diag, c, jac) * rk;
+                rs[i] = rk;
+                __stcg(z + c, zk);
+                loc[0] = norm_acc(loc[0], rk, linf);
+                loc[1] += rk * zk;
+            }
+            ok = grid_reduce<2, THREADS>(ctl, partials, loc, linf ? 1u : 0u);
+            if (!ok) break;
+            if (threadIdx.x == 0) {
+                const double fin = norm_fin(loc[0], linf);
+                st.final = fin;
+                if (fin < st.thresh) {
+                    st.done = 1;
+                    st.converged = 1;
+                    st.its = it;
+                    st.status = GF_OK;
+                } else if (!isfinite(fin)) {
+                    st.done = 1;
+                    st.its = it;
+                    st.status = GF_NONFINITE;
+                } else {
+                    st.beta = loc[1] / st.rz_old;
+                    st.rz_old = loc[1];
+                }
+            }
+            __syncthreads();
+        }
+        double* tmp = p_old;
+        p_old = p_new;
+        p_new = tmp;
+    }
+    // Every block writes its cells of x once, whatever the outcome.
+    __syncthreads();
+    for (int i = threadIdx.x; i < m; i += THREADS) K.x[c0 + i] = xs[i];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        double* o = K.stats;
+        o[0] = st.r0;
+        o[1] = st.final;
+        o[2] = st.done ? st.its : K.max_iter;
+        o[3] = st.converged;
+        o[4] = ok ? st.status : GF_ERR_TIMEOUT;
+    }
+}
+
+// 512-thread blocks have 128 registers a thread: two cells per pass.
+// KEEP_P: p of the own cells in shared memory too (4 doubles a cell);
+// otherwise 3 doubles a cell, which fits ~1.05M cells on 148 SMs.
+template <bool SYM, int THREADS, bool KEEP_P>
+__global__ void __launch_bounds__(THREADS, 1) k_pcg1_smem_box(gf_krylov_t K, int64_t chunk) {
+    BoxRows<double, SYM, false> rows{K.val, K.n, K.stride_y, K.stride_z};
+    pcg1_smem_body<THREADS, THREADS <= 512 ? 2 : 1, KEEP_P>(K, rows, chunk);
+}
+
+template <int WIDTH, int THREADS, bool KEEP_P>
+__global__ void __launch_bounds__(THREADS, 1) k_pcg1_smem_ell(gf_krylov_t K, int64_t chunk) {
+    EllRows<double, WIDTH> rows{K.val, K.nbr, K.n, K.width};
+    pcg1_smem_body<THREADS, THREADS <= 512 ? 2 : 1, KEEP_P>(K, rows, chunk);
 }
 
 // Tile length for the staged kernel (0: the system does not qualify).
@@ -1834,6 +2010,88 @@ static int launch_staged(const gf_krylov_t* k, int T, void* stream) {
     return GF_OK;
 }
 
+// Cooperative launch of the shared-memory-resident CG: 1, 2 or 4 blocks per
+// SM, whichever most gives each block a chunk whose four vectors fit its
+// shared memory; GF_ERR_INVALID (no launch) when none fits.
+template <int THREADS, bool KEEP_P>
+static const void* smem_kernel(const gf_krylov_t* k) {
+    if (k->stride_y > 0)
+        return k->symmetric ? (const void*)k_pcg1_smem_box<true, THREADS, KEEP_P>
+                            : (const void*)k_pcg1_smem_box<false, THREADS, KEEP_P>;
+    return k->width == 6 ? (const void*)k_pcg1_smem_ell<6, THREADS, KEEP_P>
+                         : (const void*)k_pcg1_smem_ell<0, THREADS, KEEP_P>;
+}
+
+static int launch_smem_arrays(const gf_krylov_t* k, void* stream, int threads, int narr);
+
+static int launch_smem(const gf_krylov_t* k, void* stream, int threads) {
+    const int st = launch_smem_arrays(k, stream, threads, 4);
+    if (st != GF_ERR_INVALID) return st;
+    return launch_smem_arrays(k, stream, threads, 3);
+}
+
+static int launch_smem_arrays(const gf_krylov_t* k, void* stream, int threads, int narr) {
+    const char* what = "gf_pcg_solve";
+    const bool keep = narr == 4;
+    const void* kern = threads == 1024 ? (keep ? smem_kernel<1024, true>(k) : smem_kernel<1024, false>(k))
+                                       : (keep ? smem_kernel<512, true>(k) : smem_kernel<512, false>(k));
+    const int kSmemThreads = threads;
+    int dev = 0, sms = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e != cudaSuccess) {
+        set_error("%s: %s", what, cudaGetErrorString(e));
+        return GF_ERR_CUDA;
+    }
+    cudaFuncAttributes fa;
+    e = cudaFuncGetAttributes(&fa, kern);
+    if (e != cudaSuccess) {
+        set_error("%s: %s", what, cudaGetErrorString(e));
+        return GF_ERR_CUDA;
+    }
+    const int64_t static_smem = (int64_t)fa.sharedSizeBytes;  // CgState and the reduction scratch
+    for (int per_sm : {4, 2, 1}) {
+        int64_t grid = (int64_t)sms * per_sm;
+        const int64_t want = (k->n + kSmemThreads - 1) / kSmemThreads;
+        if (grid > want) grid = want;
+        if (grid > kMaxBlocks) grid = kMaxBlocks;
+        if (k->block_cap > 0 && grid > k->block_cap) grid = k->block_cap;
+        if (grid < 1) grid = 1;
+        int64_t chunk = (k->n + grid - 1) / grid;
+        chunk = (chunk + 1) & ~1LL;
+        const size_t smem = (size_t)(narr * chunk) * sizeof(double);
+        if ((int64_t)smem + static_smem > optin) continue;
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        int occ = 0;
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kSmemThreads, smem);
+        if (e != cudaSuccess) {
+            set_error("%s: shared-memory CG set-up failed: %s", what, cudaGetErrorString(e));
+            return GF_ERR_CUDA;
+        }
+        if ((int64_t)occ * sms < grid) continue;
+        // The chunks must cover n with these many blocks.
+        grid = (k->n + chunk - 1) / chunk;
+        cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+        e = cudaMemsetAsync(k->work, 0, sizeof(KCtl), s);
+        if (e != cudaSuccess) {
+            set_error("%s: %s", what, cudaGetErrorString(e));
+            return GF_ERR_CUDA;
+        }
+        gf_krylov_t arg = *k;
+        int64_t carg = chunk;
+        void* args[] = {&arg, &carg};
+        e = cudaLaunchCooperativeKernel(kern, dim3((unsigned)grid), dim3(kSmemThreads), args, smem, s);
+        if (e != cudaSuccess) {
+            set_error("%s: cooperative launch failed: %s", what, cudaGetErrorString(e));
+            return GF_ERR_CUDA;
+        }
+        return GF_OK;
+    }
+    set_error("%s: system too large for shared-memory-resident CG", what);
+    return GF_ERR_INVALID;
+}
+
 static bool valid_krylov(const gf_krylov_t* k, int nvec, const char* what) {
     if (k == nullptr || k->n <= 0 || k->width <= 0 || k->ncomp < 1 || k->ncomp > 3 || k->nbr == nullptr ||
         k->diag == nullptr || k->val == nullptr || k->rhs == nullptr || k->x == nullptr || k->work == nullptr ||
@@ -1913,12 +2171,18 @@ int gf_pcg_solve(const gf_krylov_t* k, void* stream) {
                 if (k->width == 6) return launch_persistent(k_pcg1_sr<6>, k, stream, "gf_pcg_solve", kCgThreads);
                 return launch_persistent(k_pcg1_sr<0>, k, stream, "gf_pcg_solve", kCgThreads);
             }
+            if (k->variant == kSmemVariant || k->variant == kSmemVariant + 1) {
+                const int st = launch_smem(k, stream, k->variant == kSmemVariant ? 512 : 1024);
+                if (st != GF_ERR_INVALID) return st;
+            }
             if (box && k->variant == kStagedVariant) {
                 const int T = staged_tile(k);
                 if (T > 0) return launch_staged(k, T, stream);
             }
             if (box) {
-                const int v = (k->variant >= 0 && k->variant < kBoxVariants) ? k->variant : 0;
+                // Variants 5-7 that do not qualify fall back to 512-thread blocks.
+                const int v = (k->variant >= 0 && k->variant < kBoxVariants) ? k->variant
+                              : (k->variant >= kStagedVariant ? 2 : 0);
                 const BoxVariant bv = k->symmetric ? box_kernel<false, true>(v) : box_kernel<false, false>(v);
                 return launch_persistent(bv.kern, k, stream, "gf_pcg_solve", bv.threads, bv.unroll);
             }

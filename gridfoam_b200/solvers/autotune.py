@@ -27,7 +27,7 @@ import torch
 
 from gridfoam_b200.meta.config import PrecisionType, PreconditionerType, SolverConfig, SolverType
 
-N_VARIANTS = 6
+N_VARIANTS = 8
 VARIANTS = {
     0: "256 threads x 1 cell/pass",
     1: "256 threads x 2 cells/pass",
@@ -35,6 +35,8 @@ VARIANTS = {
     3: "1024 threads x 1 cell/pass",
     4: "1024 threads x 2 cells/pass",
     5: "512 threads, shared-memory tiles by bulk async copy (symmetric FP64 only)",
+    6: "512 threads, own-cell vectors resident in shared memory (FP64, up to ~1M cells)",
+    7: "1024 threads, own-cell vectors resident in shared memory (FP64, up to ~1M cells)",
 }
 
 _LOCK = threading.Lock()

@@ -36,17 +36,25 @@ def workspace(cache: dict, device: torch.device, n: int, ncomp: int, kind: int) 
     return ws
 
 
-def default_variant(n: int, mixed: bool, symmetric: bool) -> int:
-    """Box CG launch shape by system size, from fixed-iteration timings on
-    B200 (``python -m gridfoam_b200.solvers.autotune``): 256-thread blocks
-    below ~128K cells, where the grid barrier dominates; 512-thread blocks
-    up to ~1.5M; above that the shared-memory tiled kernel (FP64 symmetric
-    systems) or 512-thread blocks."""
-    if n < 131072:
+def default_variant(n: int, mixed: bool, symmetric: bool, box: bool = True) -> int:
+    """CG launch shape by system size, from fixed-iteration timings on B200
+    (``python -m gridfoam_b200.solvers.autotune``).  FP64: 256-thread blocks
+    below ~128K cells, where the grid barrier dominates; then the kernels
+    that keep each block's own-cell vectors in shared memory (512 threads up
+    to ~600K cells, 1024 threads up to ~1.3M, box or ELL); above that the
+    shared-memory tiled kernel for symmetric boxes, else 512-thread blocks.
+    Mixed precision: 256 then 512-thread blocks.  General ELL layouts
+    (octree meshes) keep the register kernel: their wider gathers lose more
+    to the lower occupancy of the shared-memory kernels than they gain."""
+    if n < 131072 or not box:
         return 0
-    if n < 1536000 or mixed or not symmetric:
+    if mixed:
         return 2
-    return 5
+    if n < 600000:
+        return 6
+    if n <= 1300000:
+        return 7
+    return 5 if symmetric else 2
 
 
 class DeviceKrylov(LinearSolver):
@@ -120,7 +128,8 @@ class DeviceKrylov(LinearSolver):
         k.inner_eta = self.inner_eta
         k.block_cap = int(self.block_cap)
         box = getattr(grid, "box_strides", None)
-        k.variant = int(self.variant) if self.variant is not None else default_variant(n, mixed, symmetric)
+        k.variant = (int(self.variant) if self.variant is not None
+                     else default_variant(n, mixed, symmetric, box is not None))
         k.single_reduction = int(self.single_reduction and not mixed and not self.bicgstab and nc == 1)
         if box is not None and not self.bicgstab and nc == 1:
             k.stride_y, k.stride_z = box

@@ -37,7 +37,7 @@ def _cuda():
         pytest.skip("needs a CUDA device")
 
 
-@pytest.mark.parametrize("algorithm", ["pcg", "sr", "staged"])
+@pytest.mark.parametrize("algorithm", ["pcg", "sr", "staged", "smem"])
 @pytest.mark.parametrize("name", CASES)
 def test_steps_match_reference(name, algorithm):
     """pcg: two-reduction fused PCG; sr: single-reduction CG; staged: the
@@ -46,7 +46,7 @@ def test_steps_match_reference(name, algorithm):
     _, _, _, algo = device_case(name)
     for s in algo.solvers.values():
         s.single_reduction = algorithm == "sr"
-        s.variant = 5 if algorithm == "staged" else 0
+        s.variant = {"staged": 5, "smem": 7}.get(algorithm, 0)
     np.testing.assert_allclose(to_np(algo.phi.pack()), golden["init_phi"], rtol=0, atol=1e-13)
     tol = STEP_TOL[name]
     slack = 1 if name.startswith("pipe") or name in OCTREE_CASES else 0
@@ -300,23 +300,25 @@ def test_single_reduction_cg_matches_pcg(layout):
     assert r < 1e-9 * s1.initial_residual
 
 
+@pytest.mark.parametrize("variant", [5, 6, 7])
 @pytest.mark.parametrize("shape", [(24, 20, 28), (64, 64, 40), (7, 5, 6), (130, 3, 4)])
-def test_staged_box_cg_matches_register_kernel(shape):
-    """The shared-memory tiled box kernel (variant 5) against the register
-    kernel (variant 0): same iteration count within one and the same
-    solution to the stopping tolerance, on shapes with partial last tiles,
-    odd strides and a y halo larger than a tile's x extent."""
+def test_staged_box_cg_matches_register_kernel(shape, variant):
+    """The shared-memory variants against the register kernel (variant 0):
+    5 stages tiles by bulk async copy, 6/7 keep each block's own-cell
+    vectors resident (512/1024 threads).  Same iteration count within one and
+    the same solution to the stopping tolerance, on shapes with partial last
+    tiles or chunks, odd strides and a y halo larger than a tile's x extent."""
     from gridfoam_b200.solvers.autotune import BoxSystem, _solver
 
     sysm = BoxSystem(*shape, device=torch.device("cuda"))
     out = {}
-    for v in (0, 5):
+    for v in (0, variant):
         s = _solver(3000, False, v)
         s.atol, s.rtol = 0.0, 1e-10
         x = torch.zeros_like(sysm.rhs)
         st = s.solve_arrays(sysm, sysm.diag, sysm.val, sysm.rhs, x, symmetric=True)
         out[v] = (x.clone(), st[0])
-    (x0, s0), (x1, s1) = out[0], out[5]
+    (x0, s0), (x1, s1) = out[0], out[variant]
     assert s0.converged and s1.converged, (s0.status, s1.status)
     assert abs(s0.iterations - s1.iterations) <= 1, (s0.iterations, s1.iterations)
     assert s0.initial_residual == pytest.approx(s1.initial_residual, rel=1e-13)
@@ -338,3 +340,24 @@ def test_staged_box_cg_fixed_iterations_match_register_kernel():
         assert st[0].iterations == 50 and st[0].status == "max_iter"
         xs.append(to_np(x))
     assert rel(xs[1], xs[0]) < 1e-11
+
+
+@pytest.mark.parametrize("variant", [6, 7])
+def test_smem_resident_cg_on_ell_layout(variant):
+    """The shared-memory-resident CG through the general ELL rows (the
+    octree path), against the register ELL kernel."""
+    from gridfoam_b200.solvers.autotune import BoxSystem, _solver
+
+    sysm = BoxSystem(20, 18, 26, device=torch.device("cuda"))
+    sysm.box_strides = None
+    out = {}
+    for v in (0, variant):
+        s = _solver(3000, False, v)
+        s.atol, s.rtol = 0.0, 1e-10
+        x = torch.zeros_like(sysm.rhs)
+        st = s.solve_arrays(sysm, sysm.diag, sysm.val, sysm.rhs, x, symmetric=True)
+        out[v] = (x.clone(), st[0])
+    (x0, s0), (x1, s1) = out[0], out[variant]
+    assert s0.converged and s1.converged
+    assert abs(s0.iterations - s1.iterations) <= 1
+    assert rel(to_np(x1), to_np(x0)) < 1e-8
