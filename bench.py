@@ -108,12 +108,13 @@ def pcg_bytes_per_iter(C: int, F: int) -> float:
     return 14 * C * 8 + F * (8 + 8)
 
 
-# Measured DRAM bytes (read + write) per iteration of the 512-thread box CG
-# kernel (k_pcg1_box<1, 512, 1>) on a 64x64x256 box: one ncu capture of a
-# 200-iteration launch moved 1.920438 GB + 2.752010 GB.  The CG working set
-# stays largely in the 126 MB L2 at this size, so DRAM sees ~14 % of the
-# algorithmic bytes.
-PCG_DRAM_BYTES_PER_ITER = (1.920438e9 + 2.752010e9) / 200
+# Measured DRAM bytes (read + write) of the pressure CG kernel
+# (k_pcg1_smem_box<1, 1024, 0>) on a 64x64x256 box, from two ncu captures of
+# fixed-length launches: 82.72 MB at 50 iterations, 107.00 MB at 400.  The
+# global working set (~90 MB) stays in the 126 MB L2, so a launch costs a
+# one-time read of its arrays plus a small per-iteration remainder.
+PCG_DRAM_BYTES_PER_ITER = (107002880 - 82719744) / 350
+PCG_DRAM_BYTES_PER_LAUNCH = 82719744 - 50 * PCG_DRAM_BYTES_PER_ITER
 
 
 def pcg_bytes_setup(C: int, F: int) -> float:
@@ -482,9 +483,10 @@ def run_gpu(args) -> None:
             "peak_source": peak_kind,
             "unit": "GB/s",
             "frac": achieved / peak if peak else None,
-            "traffic": (PCG_DRAM_BYTES_PER_ITER * sum(iters) / len(iters)) if iters else None,
-            "traffic_source": "ncu dram bytes of a 200-iteration launch of the same kernel on the same box, "
-                              "scaled to this run's average iterations per launch",
+            "traffic": (PCG_DRAM_BYTES_PER_LAUNCH + PCG_DRAM_BYTES_PER_ITER * sum(iters) / len(iters))
+                       if iters else None,
+            "traffic_source": "ncu dram bytes of 50- and 400-iteration launches of the same kernel on the same box "
+                              "(fixed part + per-iteration slope), at this run's average iterations per launch",
             "note": "working set mostly L2-resident at 1M cells: DRAM traffic is well below the algorithmic "
                     "bytes; the kernel is bound by L2 latency and two grid barriers per iteration",
             "launches": len(durations),

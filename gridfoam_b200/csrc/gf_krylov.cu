@@ -89,7 +89,21 @@ __device__ bool grid_reduce(KCtl* ctl, double* partials, double (&v)[NV], unsign
     __syncthreads();
     const unsigned ep = g_epoch;
     double* part = partials + (ep & 1u) * (kPartials / 2);
-    if (threadIdx.x < NV) {
+    if (THREADS == 1024) {
+        // 32 warp sums: a shuffle tree in warp 0 is shorter than a serial sum.
+        if (warp == 0) {
+#pragma unroll
+            for (int j = 0; j < NV; ++j) {
+                const bool mx = (maxmask >> j) & 1u;
+                double x = sm1[j * 32 + lane];
+                for (int o = 16; o > 0; o >>= 1) {
+                    const double y = __shfl_xor_sync(0xffffffffu, x, o);
+                    x = mx ? nmax(x, y) : x + y;
+                }
+                if (lane == 0) __stcg(part + (int64_t)blockIdx.x * NV + j, x);
+            }
+        }
+    } else if (threadIdx.x < NV) {
         const int j = threadIdx.x;
         const bool mx = (maxmask >> j) & 1u;
         double x = sm1[j * 32];
@@ -155,8 +169,19 @@ __device__ bool grid_reduce(KCtl* ctl, double* partials, double (&v)[NV], unsign
 #pragma unroll
     for (int j = 0; j < NV; ++j) {
         const bool mx = (maxmask >> j) & 1u;
-        double x = sm2[j * 32];
-        for (int w = 1; w < nw; ++w) x = mx ? nmax(x, sm2[j * 32 + w]) : x + sm2[j * 32 + w];
+        double x;
+        if (THREADS == 1024) {
+            // Every warp runs the same butterfly; its additions commute
+            // exactly, so all lanes of all warps hold the same bits.
+            x = sm2[j * 32 + lane];
+            for (int o = 16; o > 0; o >>= 1) {
+                const double t = __shfl_xor_sync(0xffffffffu, x, o);
+                x = mx ? nmax(x, t) : x + t;
+            }
+        } else {
+            x = sm2[j * 32];
+            for (int w = 1; w < nw; ++w) x = mx ? nmax(x, sm2[j * 32 + w]) : x + sm2[j * 32 + w];
+        }
         v[j] = x;
     }
     return true;
@@ -368,14 +393,15 @@ __global__ void __launch_bounds__(kKThreads) k_pcg(gf_krylov_t K) {
 __device__ __forceinline__ double ld_coef(const double* p) { return __ldg(p); }
 __device__ __forceinline__ float ld_coef(const float* p) { return __ldcg(p); }
 
-template <typename T, int WIDTH>
+// I: the cell index type (int32_t where n times the row width fits).
+template <typename T, int WIDTH, typename I = int64_t>
 struct EllRows {
     const T* val;
     const int32_t* nbr;
-    int64_t n;
+    I n;
     int w;
     template <typename A, class G>
-    __device__ __forceinline__ A apply(int64_t c, A dc, const G& g) const {
+    __device__ __forceinline__ A apply(I c, A dc, const G& g) const {
         A acc = dc * g(c);
         if (WIDTH > 0) {
             int nb[WIDTH > 0 ? WIDTH : 1];
@@ -394,20 +420,20 @@ struct EllRows {
     }
 };
 
-template <typename T, bool SYM, bool COMPACT>
+template <typename T, bool SYM, bool COMPACT, typename I = int64_t>
 struct BoxRows {
     const T* val;
-    int64_t n, sy, sz;
+    I n, sy, sz;
     // COMPACT arrays hold only the three '+' slots, which only SYM uses.
-    __device__ __forceinline__ int64_t plus_slot(int a) const { return (COMPACT && SYM) ? a : 2 * a + 1; }
+    __device__ __forceinline__ I plus_slot(int a) const { return (COMPACT && SYM) ? a : 2 * a + 1; }
     template <typename A, class G>
-    __device__ __forceinline__ A apply(int64_t c, A dc, const G& g) const {
-        const int64_t st[3] = {1, sy, sz};
+    __device__ __forceinline__ A apply(I c, A dc, const G& g) const {
+        const I st[3] = {1, sy, sz};
         A ap[3], am[3];
-        int64_t ip[3], im[3];
+        I ip[3], im[3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            const int64_t s = st[a];
+            const I s = st[a];
             const T* pv = val + plus_slot(a) * n;
             ap[a] = (A)ld_coef(pv + c);
             if (SYM) {
@@ -1400,28 +1426,32 @@ __global__ void __launch_bounds__(THREADS, 1) k_pcg1_box_staged(gf_krylov_t K, i
 // CG with each block's own-cell vectors resident in shared memory.
 //
 // Every block owns one contiguous chunk of cells for the whole solve and
-// keeps x, r, q = A p and p of those cells in shared memory (4 doubles a
-// cell: the 148 SMs' shared memory together holds them for about a million
-// cells).  Only what neighbours read goes through global memory: z = M r and
-// p (double-buffered), plus the matrix.  The update pass is then shared
-// memory plus one read of the diagonal and one write of z, about half the
-// global traffic of pcg1_body per iteration.  x is read once at the start
-// and written once at the end.  Arithmetic per cell is that of pcg1_body.
-template <int THREADS, int U, bool KEEP_P, class Rows>
-__device__ void pcg1_smem_body(const gf_krylov_t& K, const Rows& rows, int64_t chunk) {
+// keeps x, r and q = A p of those cells in shared memory (3 doubles a cell,
+// 4 with p: the 148 SMs' shared memory together holds them for about a
+// million cells).  Only what neighbours read goes through global memory:
+// z = M r and p, stored as interleaved pairs {z, p} so the 7-point gather
+// of p_new = z + p_old beta is one 16-byte load a point.  Pair buffer k mod 2
+// holds {z_k, p_(k-1)}: iteration k reads it and writes p_k and z_(k+1)
+// into the other buffer, which no block reads until the grid barrier that
+// ends iteration k.  The inverse diagonal is computed once per solve.  Cell
+// indices are 32-bit (the host launches this kernel only when n times the
+// row width is below 2^31).
+// Arithmetic per cell is that of pcg1_body, so the iterates are the same.
+template <int THREADS, int U, int V, bool KEEP_P, class Rows>
+__device__ void pcg1_smem_body(const gf_krylov_t& K, const Rows& rows, int chunk) {
     __shared__ CgState st;
     extern __shared__ __align__(16) double sm[];
     KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
     barrier_init();
     double* partials = K.work + kCtlDoubles;
     double* vec = partials + kPartials;
-    const int64_t n = K.n;
-    double* z = vec;
-    double* pa = vec + n;
-    double* pb = vec + 2 * n;
-    const int64_t c0 = blockIdx.x * chunk;
-    const int64_t c1 = c0 + chunk < n ? c0 + chunk : n;
-    const int m = c1 > c0 ? (int)(c1 - c0) : 0;
+    const int n = (int)K.n;
+    double2* zp0 = reinterpret_cast<double2*>(vec);
+    double2* zp1 = reinterpret_cast<double2*>(vec + 2 * (int64_t)n);
+    double* inv = vec + 4 * (int64_t)n;
+    const int c0 = blockIdx.x * chunk;
+    const int c1 = c0 + chunk < n ? c0 + chunk : n;
+    const int m = c1 > c0 ? c1 - c0 : 0;
     double* xs = sm;
     double* rs = sm + chunk;
     double* qs = sm + 2 * chunk;
@@ -1430,16 +1460,17 @@ __device__ void pcg1_smem_body(const gf_krylov_t& K, const Rows& rows, int64_t c
     bool ok = true;
     {  // r = b - A x, z = M r, p = 0; |r| and r.z
         double loc[2] = {0.0, 0.0};
-        auto gx = [&](int64_t i) { return __ldcg(K.x + i); };
+        auto gx = [&](int i) { return __ldcg(K.x + i); };
         for (int i = threadIdx.x; i < m; i += THREADS) {
-            const int64_t c = c0 + i;
+            const int c = c0 + i;
             const double ax = rows.apply(c, __ldg(K.diag + c), gx);
             const double rk = __ldg(K.rhs + c) - ax;
-            const double zk = inv_diag(K.diag, c, jac) * rk;
+            const double iv = inv_diag(K.diag, c, jac);
+            const double zk = iv * rk;
             xs[i] = __ldcg(K.x + c);
             rs[i] = rk;
-            __stcg(z + c, zk);
-            __stcg(pa + c, 0.0);
+            inv[c] = iv;
+            __stcg(zp0 + c, make_double2(zk, 0.0));
             loc[0] = norm_acc(loc[0], rk, linf);
             loc[1] += rk * zk;
         }
@@ -1466,13 +1497,19 @@ __device__ void pcg1_smem_body(const gf_krylov_t& K, const Rows& rows, int64_t c
         }
         __syncthreads();
     }
-    double* p_old = pa;
-    double* p_new = pb;
     for (int it = 1; ok && !st.done && it <= K.max_iter; ++it) {
+        const double2* cur = (it & 1) ? zp0 : zp1;
+        double2* nxt = (it & 1) ? zp1 : zp0;
         {  // p_new = z + p_old beta; q = A p_new; p_new . q
             const double beta = st.beta;
             double loc[1] = {0.0};
-            auto gp = [&](int64_t j) { return __ldcg(z + j) + __ldcg(p_old + j) * beta; };
+            // Plain (L1-cacheable) loads: the pair buffer is written only
+            // before the grid barrier, whose acquire makes this SM's L1
+            // coherent again; a stencil's neighbours then mostly hit L1.
+            auto gp = [&](int j) {
+                const double2 v = cur[j];
+                return v.x + v.y * beta;
+            };
             // U cells per thread per pass: all their loads are issued before
             // any store, so U latency chains overlap.
             for (int i0 = threadIdx.x; i0 < m; i0 += U * THREADS) {
@@ -1481,7 +1518,7 @@ __device__ void pcg1_smem_body(const gf_krylov_t& K, const Rows& rows, int64_t c
                 for (int u = 0; u < U; ++u) {
                     const int i = i0 + u * THREADS;
                     if (i < m) {
-                        const int64_t c = c0 + i;
+                        const int c = c0 + i;
                         pc[u] = gp(c);
                         ap[u] = rows.apply(c, __ldg(K.diag + c), gp);
                     }
@@ -1490,7 +1527,7 @@ __device__ void pcg1_smem_body(const gf_krylov_t& K, const Rows& rows, int64_t c
                 for (int u = 0; u < U; ++u) {
                     const int i = i0 + u * THREADS;
                     if (i < m) {
-                        __stcg(p_new + c0 + i, pc[u]);
+                        __stcg(&nxt[c0 + i].y, pc[u]);
                         if (KEEP_P) ps[i] = pc[u];
                         qs[i] = ap[u];
                         loc[0] += pc[u] * ap[u];
@@ -1505,15 +1542,31 @@ __device__ void pcg1_smem_body(const gf_krylov_t& K, const Rows& rows, int64_t c
         {  // x += alpha p; r -= alpha q; z = M r; |r|, r.z (own cells)
             const double alpha = st.alpha;
             double loc[2] = {0.0, 0.0};
-            for (int i = threadIdx.x; i < m; i += THREADS) {
-                const int64_t c = c0 + i;
-                xs[i] = xs[i] + alpha * (KEEP_P ? ps[i] : __ldcg(p_new + c));
-                const double rk = rs[i] - alpha * qs[i];
-                const double zk = inv_diag(K.diag, c, jac) * rk;
-                rs[i] = rk;
-                __stcg(z + c, zk);
-                loc[0] = norm_acc(loc[0], rk, linf);
-                loc[1] += rk * zk;
+            // V cells per thread per pass, global loads first: V L2 latencies
+            // overlap instead of following one another.
+            for (int i0 = threadIdx.x; i0 < m; i0 += V * THREADS) {
+                double pv[V], iv[V];
+#pragma unroll
+                for (int u = 0; u < V; ++u) {
+                    const int i = i0 + u * THREADS;
+                    if (i < m) {
+                        pv[u] = KEEP_P ? ps[i] : __ldcg(&nxt[c0 + i].y);
+                        iv[u] = inv[c0 + i];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < V; ++u) {
+                    const int i = i0 + u * THREADS;
+                    if (i < m) {
+                        xs[i] = xs[i] + alpha * pv[u];
+                        const double rk = rs[i] - alpha * qs[i];
+                        const double zk = iv[u] * rk;
+                        rs[i] = rk;
+                        __stcg(&nxt[c0 + i].x, zk);
+                        loc[0] = norm_acc(loc[0], rk, linf);
+                        loc[1] += rk * zk;
+                    }
+                }
             }
             ok = grid_reduce<2, THREADS>(ctl, partials, loc, linf ? 1u : 0u);
             if (!ok) break;
@@ -1536,9 +1589,6 @@ __device__ void pcg1_smem_body(const gf_krylov_t& K, const Rows& rows, int64_t c
             }
             __syncthreads();
         }
-        double* tmp = p_old;
-        p_old = p_new;
-        p_new = tmp;
     }
     // Every block writes its cells of x once, whatever the outcome.
     __syncthreads();
@@ -1553,19 +1603,24 @@ __device__ void pcg1_smem_body(const gf_krylov_t& K, const Rows& rows, int64_t c
     }
 }
 
-// 512-thread blocks have 128 registers a thread: two cells per pass.
+// Cells per thread per pass: 512-thread blocks (128 registers a thread)
+// gather two cells at once and update four; 1024-thread blocks (64
+// registers) gather one and update two.
 // KEEP_P: p of the own cells in shared memory too (4 doubles a cell);
 // otherwise 3 doubles a cell, which fits ~1.05M cells on 148 SMs.
+__host__ __device__ constexpr int smem_gather_cells(int threads) { return threads <= 512 ? 2 : 1; }
+__host__ __device__ constexpr int smem_update_cells(int threads) { return threads <= 512 ? 4 : 2; }
+
 template <bool SYM, int THREADS, bool KEEP_P>
-__global__ void __launch_bounds__(THREADS, 1) k_pcg1_smem_box(gf_krylov_t K, int64_t chunk) {
-    BoxRows<double, SYM, false> rows{K.val, K.n, K.stride_y, K.stride_z};
-    pcg1_smem_body<THREADS, THREADS <= 512 ? 2 : 1, KEEP_P>(K, rows, chunk);
+__global__ void __launch_bounds__(THREADS, 1) k_pcg1_smem_box(gf_krylov_t K, int chunk) {
+    BoxRows<double, SYM, false, int> rows{K.val, (int)K.n, (int)K.stride_y, (int)K.stride_z};
+    pcg1_smem_body<THREADS, smem_gather_cells(THREADS), smem_update_cells(THREADS), KEEP_P>(K, rows, chunk);
 }
 
 template <int WIDTH, int THREADS, bool KEEP_P>
-__global__ void __launch_bounds__(THREADS, 1) k_pcg1_smem_ell(gf_krylov_t K, int64_t chunk) {
-    EllRows<double, WIDTH> rows{K.val, K.nbr, K.n, K.width};
-    pcg1_smem_body<THREADS, THREADS <= 512 ? 2 : 1, KEEP_P>(K, rows, chunk);
+__global__ void __launch_bounds__(THREADS, 1) k_pcg1_smem_ell(gf_krylov_t K, int chunk) {
+    EllRows<double, WIDTH, int> rows{K.val, K.nbr, (int)K.n, K.width};
+    pcg1_smem_body<THREADS, smem_gather_cells(THREADS), smem_update_cells(THREADS), KEEP_P>(K, rows, chunk);
 }
 
 // Tile length for the staged kernel (0: the system does not qualify).
@@ -2051,6 +2106,13 @@ static int launch_smem_arrays(const gf_krylov_t* k, void* stream, int threads, i
         return GF_ERR_CUDA;
     }
     const int64_t static_smem = (int64_t)fa.sharedSizeBytes;  // CgState and the reduction scratch
+    // 32-bit cell indices (coefficient slot x n included) and 16-byte pair
+    // buffers in the workspace.
+    const int64_t row_span = (int64_t)(k->stride_y > 0 ? 6 : (k->width > 6 ? k->width : 6)) * k->n;
+    if (row_span >= ((int64_t)1 << 31) || (reinterpret_cast<uintptr_t>(k->work) & 15u)) {
+        set_error("%s: system not eligible for shared-memory-resident CG", what);
+        return GF_ERR_INVALID;
+    }
     for (int per_sm : {4, 2, 1}) {
         int64_t grid = (int64_t)sms * per_sm;
         const int64_t want = (k->n + kSmemThreads - 1) / kSmemThreads;
@@ -2079,7 +2141,7 @@ static int launch_smem_arrays(const gf_krylov_t* k, void* stream, int threads, i
             return GF_ERR_CUDA;
         }
         gf_krylov_t arg = *k;
-        int64_t carg = chunk;
+        int carg = (int)chunk;
         void* args[] = {&arg, &carg};
         e = cudaLaunchCooperativeKernel(kern, dim3((unsigned)grid), dim3(kSmemThreads), args, smem, s);
         if (e != cudaSuccess) {

@@ -342,6 +342,28 @@ def test_staged_box_cg_fixed_iterations_match_register_kernel():
     assert rel(xs[1], xs[0]) < 1e-11
 
 
+@pytest.mark.parametrize("box", [True, False])
+@pytest.mark.parametrize("variant", [6, 7])
+def test_smem_resident_cg_fixed_iterations_match_register_kernel(variant, box):
+    """Exactly 60 iterations (tolerances 0) of the shared-memory-resident CG
+    (pair-interleaved z/p, inverse diagonal once per solve, L1-cached
+    gathers) against the register kernel: the iterates differ only through
+    the order of the dot-product partial sums."""
+    from gridfoam_b200.solvers.autotune import BoxSystem, _solver
+
+    sysm = BoxSystem(40, 36, 44, device=torch.device("cuda"))
+    if not box:
+        sysm.box_strides = None
+    xs = []
+    for v in (0, variant):
+        s = _solver(60, False, v)
+        x = torch.zeros_like(sysm.rhs)
+        st = s.solve_arrays(sysm, sysm.diag, sysm.val, sysm.rhs, x, symmetric=True)
+        assert st[0].iterations == 60 and st[0].status == "max_iter"
+        xs.append(to_np(x))
+    assert rel(xs[1], xs[0]) < 1e-11
+
+
 @pytest.mark.parametrize("variant", [6, 7])
 def test_smem_resident_cg_on_ell_layout(variant):
     """The shared-memory-resident CG through the general ELL rows (the
