@@ -214,6 +214,8 @@ _SIGNATURES = {
     "gf_laplacian_adjoint": ([P, P, P, P, P, P, P, P], ctypes.c_int),
     "gf_div_adjoint": ([P, P, P, P, P, P, P, P], ctypes.c_int),
     "gf_force_integral": ([P, I64, P, P, P, P, P, P, P, P, P, F64, F64, F64, F64, F64, P, P, P], ctypes.c_int),
+    "gf_continuity_scratch_doubles": ([], I64),
+    "gf_continuity_sums": ([I64, P, P, P, P, P], ctypes.c_int),
 }
 
 EXPORTED = tuple(_SIGNATURES)
@@ -256,7 +258,7 @@ class GfError(RuntimeError):
 
 
 # Kernels launched per entry point (for launch accounting).
-_LAUNCHES_PER_CALL = {"gf_fixed_values": 3, "gf_close_fixed_flux": 2, "gf_field_residual": 2}
+_LAUNCHES_PER_CALL = {"gf_fixed_values": 3, "gf_close_fixed_flux": 2, "gf_field_residual": 2, "gf_continuity_sums": 2}
 LAUNCHES: collections.Counter = collections.Counter()
 
 

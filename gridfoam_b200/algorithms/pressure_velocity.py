@@ -116,6 +116,8 @@ class _PressureVelocity:
         self._adjust_classes = self._build_adjust_classes()
         self._p_ffp = any(bc.kind == _lib.BC_FIXED_FLUX_P for bc in self.p.bcs.values())
         self.last_stats: dict = {}
+        self._diagnostics = None
+        self._diagnostics_step = 0
         # flux.py:132-162 correct_flux(phi, U, update_internal=True)
         self._eval_U()
         if self._hanging:
@@ -135,6 +137,18 @@ class _PressureVelocity:
     @property
     def solvers(self) -> dict:
         return self._solvers
+
+    def attach_diagnostics(self, diagnostics) -> None:
+        """algorithms/base.py:66-75: record continuity and solver statistics
+        after every step (``post.diagnostics.DiagnosticsCollector``)."""
+        self._diagnostics = diagnostics
+
+    def _finalize_diagnostics(self, phi, solve_stats: dict) -> None:
+        """algorithms/base.py:77-100 (enqueues only: no host round trip)."""
+        if self._diagnostics is None:
+            return
+        self._diagnostics_step += 1
+        self._diagnostics.record_step(self._diagnostics_step, phi, solve_stats)
 
     def set_host_readback(self, enabled: bool) -> None:
         """Switch the per-step pinned host copies on or off (see ``host_readback``)."""
@@ -495,6 +509,7 @@ class SIMPLE(_PressureVelocity):
         if "phi" in self._residual_control:
             self._record("phi", self.continuity_residual())
         self.last_stats = {self.U.name: st_u, self.p.name: st_p}
+        self._finalize_diagnostics(self.phi, self.last_stats)
 
 
 class PISO(_PressureVelocity):
@@ -526,6 +541,7 @@ class PISO(_PressureVelocity):
         self.U.update_history()
         self.phi.update_history()
         self.last_stats = {self.U.name: st_u, self.p.name: st_p}
+        self._finalize_diagnostics(self.phi, self.last_stats)
 
 
 class PIMPLE(_PressureVelocity):
@@ -606,6 +622,7 @@ class PIMPLE(_PressureVelocity):
         self.U.update_history()
         self.phi.update_history()
         self.last_stats = {self.U.name: st_u, self.p.name: st_p}
+        self._finalize_diagnostics(self.phi, self.last_stats)
 
 
 def create_algorithm(grid, phase: str | None = None):

@@ -101,6 +101,50 @@ __global__ void k_force_sum(int64_t n, const double* __restrict__ samples, doubl
     }
 }
 
+// Continuity-error sums over cells: blocks of kContBlocks fixed ranges, then
+// one block over the block partials, both in a fixed order, so the sums are
+// the same bits on every launch and every device.
+constexpr int kContBlocks = 256;
+
+__global__ void k_cont_partials(int64_t n, const double* __restrict__ div, const double* __restrict__ vol,
+                                double* __restrict__ part) {
+    __shared__ double sh[3][kThreads];
+    const int64_t per = (n + kContBlocks - 1) / kContBlocks;
+    const int64_t b0 = blockIdx.x * per;
+    const int64_t b1 = b0 + per < n ? b0 + per : n;
+    double a = 0.0, g = 0.0, v = 0.0;
+    for (int64_t c = b0 + threadIdx.x; c < b1; c += blockDim.x) {
+        const double d = div[c], w = vol[c];
+        a += fabs(d) * w;
+        g += d * w;
+        v += w;
+    }
+    sh[0][threadIdx.x] = a;
+    sh[1][threadIdx.x] = g;
+    sh[2][threadIdx.x] = v;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s)
+            for (int r = 0; r < 3; ++r) sh[r][threadIdx.x] += sh[r][threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x < 3) part[threadIdx.x * kContBlocks + blockIdx.x] = sh[threadIdx.x][0];
+}
+
+__global__ void k_cont_final(const double* __restrict__ part, double* __restrict__ out) {
+    __shared__ double sh[kContBlocks];
+    for (int r = 0; r < 3; ++r) {
+        sh[threadIdx.x] = part[r * kContBlocks + threadIdx.x];
+        __syncthreads();
+        for (int s = kContBlocks / 2; s > 0; s >>= 1) {
+            if ((int)threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[r] = sh[0];
+        __syncthreads();
+    }
+}
+
 }  // namespace gf
 
 using namespace gf;
@@ -123,6 +167,20 @@ int gf_force_integral(const gf_mesh_t* m, int64_t n, const int32_t* faces, const
                                                                          nu_scalar, rho, cx, cy, cz, samples);
     k_force_sum<<<1, kThreads, 0, GF_STREAM(stream)>>>(n, samples, total);
     return check_launch("gf_force_integral");
+}
+
+int64_t gf_continuity_scratch_doubles(void) { return 3 * (int64_t)kContBlocks; }
+
+int gf_continuity_sums(int64_t n, const double* div, const double* vol, double* scratch, double* out,
+                       void* stream) {
+    if (n < 0 || (n > 0 && (div == nullptr || vol == nullptr)) || scratch == nullptr || out == nullptr) {
+        set_error("gf_continuity_sums: invalid arguments");
+        return GF_ERR_INVALID;
+    }
+    static_assert(kContBlocks == kThreads, "one final block reduces one partial per thread");
+    k_cont_partials<<<kContBlocks, kThreads, 0, GF_STREAM(stream)>>>(n, div, vol, scratch);
+    k_cont_final<<<1, kContBlocks, 0, GF_STREAM(stream)>>>(scratch, out);
+    return check_launch("gf_continuity_sums");
 }
 
 }  // extern "C"

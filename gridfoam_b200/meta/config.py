@@ -333,6 +333,29 @@ class ConditionConfig(BaseModel, frozen=True):
         yield from self.boundary.values()
 
 
+class ContinuityErrorConfig(BaseModel, frozen=True):
+    """meta/config.py:768-778: the flux field and the record interval."""
+
+    phi: str = "phi"
+    writeInterval: int = Field(default=1, ge=1)
+
+
+class SolverInfoConfig(BaseModel, frozen=True):
+    """meta/config.py:781-791: fields (default U and p) and the interval."""
+
+    fields: list[str] | None = None
+    writeInterval: int = Field(default=1, ge=1)
+
+
+class PostProcessingConfig(BaseModel, frozen=True):
+    """meta/config.py:794-811.  ``forceCoeff`` stays the raw mapping that
+    ``post.forces.ForceEvaluator`` reads."""
+
+    forceCoeff: dict[str, Any] | None = None
+    continuityError: ContinuityErrorConfig | None = None
+    solverInfo: SolverInfoConfig | None = None
+
+
 class SimulatorConfig(BaseModel, frozen=True):
     control: ControlConfig
     fvSchemes: fvSchemesConfig

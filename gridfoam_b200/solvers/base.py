@@ -38,6 +38,12 @@ class _StatsBuffer:
         self.event.record()
         self._ready = False
 
+    def ready(self) -> bool:
+        """True once the copy has landed (never blocks)."""
+        if not self._ready and self.event.query():
+            self._ready = True
+        return self._ready
+
     def row(self, k: int) -> torch.Tensor:
         if not self._ready:
             self.event.synchronize()
@@ -58,6 +64,10 @@ class SolveStats:
         self.solver = solver
         self._buf = buffer
         self._k = k
+
+    def ready(self) -> bool:
+        """True once the statistics are on the host (never blocks)."""
+        return self._buf.ready()
 
     @property
     def initial_residual(self) -> float:

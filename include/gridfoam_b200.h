@@ -456,6 +456,16 @@ int gf_force_integral(const gf_mesh_t* m, int64_t n, const int32_t* faces,
                       double rho, double cx, double cy, double cz,
                       double* samples, double* total, void* stream);
 
+/* post/diagnostics/continuity.py:11-49 (the sums of compute_continuity_error,
+ * without its host round trip): from div = fvc.div(phi) [n] and the cell
+ * volumes [n], out[0] = sum |div| V, out[1] = sum div V, out[2] = sum V, each
+ * summed in a fixed order (the same bits on every launch).  scratch holds
+ * gf_continuity_scratch_doubles() doubles.  The caller forms
+ * local = dt out[0] / out[2] and global = dt out[1] / out[2]. */
+int64_t gf_continuity_scratch_doubles(void);
+int gf_continuity_sums(int64_t n, const double* div, const double* vol,
+                       double* scratch, double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -6,6 +6,7 @@ Run in a container where the reference source tree is available::
     GRIDFOAM_REF=/root/reference/src python tests/golden/make_golden.py --adjoint
     GRIDFOAM_REF=/root/reference/src python tests/golden/make_golden.py --forces
     GRIDFOAM_REF=/root/reference/src python tests/golden/make_golden.py --potential
+    GRIDFOAM_REF=/root/reference/src python tests/golden/make_golden.py --diagnostics
 
 It imports the unmodified reference package (with the import stubs in
 ``tests/golden/refshim`` for its absent optional dependencies), builds each
@@ -383,8 +384,109 @@ def potential_run(name: str) -> dict:
     return out
 
 
+# Post-processing settings of the diagnostics fixtures: continuity every
+# step, solver statistics every DIAG_SOLVER_INTERVAL steps (and the last).
+DIAG_CASES = ("cavity8", "pipe10x20")
+DIAG_SOLVER_INTERVAL = 3
+
+
+class _CaptureUnstructuredGrid:
+    """Records what the reference's io/vtu.py hands to pyvista."""
+
+    def __init__(self, cells, cell_types, points):
+        self.cells = np.asarray(cells)
+        self.cell_types = np.asarray(cell_types)
+        self.points = np.asarray(points)
+        self.cell_data: dict = {}
+
+    def save(self, path):
+        pass
+
+
+def diagnostics_run(name: str) -> dict:
+    """The reference's DiagnosticsCollector (post/diagnostics/collector.py)
+    attached to the case's algorithm for its golden steps, and its VTU export
+    (io/vtu.py) of the final state through a pyvista stand-in that records
+    the points, cells, cell types and cell data it is given."""
+    import csv
+    import tempfile
+    import types
+
+    import gridfoam.io.vtu as ref_vtu
+    from gridfoam.meta.config import PostProcessingConfig
+    from gridfoam.post.diagnostics import DiagnosticsCollector
+
+    case = ALL_CASES[name]()
+    profile = case["inlet_profile"]
+    original = bc_factory.create_boundary_condition
+
+    def patched(bc_config, dtype, device):
+        if profile is not None and [str(p) for p in bc_config.patches] == [
+            profile["patch"]
+        ] and bc_config.type == "dirichlet" and bc_config.value is not None and len(
+            np.atleast_1d(bc_config.value)
+        ) == 3:
+            return ParabolicInletBC(profile)
+        return original(bc_config, dtype, device)
+
+    ref_field.boundary_factory.create_boundary_condition = patched
+    try:
+        grid, _ = make_grid(case)
+        algo = create_algorithm(grid)
+    finally:
+        ref_field.boundary_factory.create_boundary_condition = original
+    n_steps = STEPS[name]
+    dt = float(grid.sim_config.control.deltaT)
+    cfg = PostProcessingConfig.model_validate(
+        {"continuityError": {"writeInterval": 1}, "solverInfo": {"writeInterval": DIAG_SOLVER_INTERVAL}})
+    out: dict[str, np.ndarray] = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        diag = DiagnosticsCollector.from_config(grid, cfg, pathlib.Path(tmp), n_steps=n_steps, delta_t=dt)
+        algo.attach_diagnostics(diag)
+        for k in range(n_steps):
+            with torch.no_grad():
+                algo.step()
+            out[f"step{k}_phi"] = packed(algo.phi)
+        diag.close()
+        with open(pathlib.Path(tmp) / "continuity_error.csv") as fh:
+            rows = list(csv.reader(fh))
+        out["continuity_header"] = np.array(rows[0])
+        out["continuity"] = np.array(rows[1:], dtype=np.float64)
+        with open(pathlib.Path(tmp) / "solver_info.csv") as fh:
+            rows = list(csv.reader(fh))
+        out["solver_info_header"] = np.array(rows[0])
+        out["solver_info"] = np.array(rows[1:])
+    saved = (ref_vtu.pv.UnstructuredGrid, getattr(ref_vtu.pv, "CellType", None))
+    ref_vtu.pv.UnstructuredGrid = _CaptureUnstructuredGrid
+    ref_vtu.pv.CellType = types.SimpleNamespace(HEXAHEDRON=12)
+    try:
+        ug = ref_vtu.save_export_fields_as_vtu(grid, "unused.vtu")
+    finally:
+        ref_vtu.pv.UnstructuredGrid = saved[0]
+        if saved[1] is None:
+            del ref_vtu.pv.CellType
+        else:
+            ref_vtu.pv.CellType = saved[1]
+    out["vtu_points"] = ug.points
+    out["vtu_cells"] = ug.cells
+    out["vtu_cell_types"] = ug.cell_types
+    out["vtu_fields"] = np.array(sorted(ug.cell_data))
+    for key, val in ug.cell_data.items():
+        out[f"vtu_data_{key}"] = np.asarray(val)
+    out["delta_t"] = np.array(dt)
+    out["n_steps"] = np.array(n_steps)
+    return out
+
+
 def main() -> None:
     args = sys.argv[1:]
+    if args and args[0] == "--diagnostics":
+        for name in args[1:] or DIAG_CASES:
+            data = diagnostics_run(name)
+            path = HERE / f"diagnostics_{name}.npz"
+            np.savez_compressed(path, **data)
+            print(f"diagnostics {name}: {sorted(data)} -> {path} ({path.stat().st_size} B)")
+        return
     if args and args[0] == "--potential":
         from tests.golden.cases import POTENTIAL_CASES
 
