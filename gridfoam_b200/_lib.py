@@ -78,6 +78,7 @@ class GfMesh(ctypes.Structure):
         ("hang_offset", P),
         ("hang_move_o", P),
         ("hang_move_n", P),
+        ("face_axis", P),
     ]
 
 

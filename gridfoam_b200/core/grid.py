@@ -342,6 +342,7 @@ class AxisProjectedGrid:
             "bnd_near": torch.as_tensor(h.bnd_near.astype(np.uint8), device=dev),
             "face_pos_owner": i32(h.extra["face_pos_owner"]),
             "face_pos_neigh": i32(h.extra["face_pos_neigh"]),
+            "face_axis": torch.as_tensor(np.ascontiguousarray(h.axis, dtype=np.int8), device=dev),
         }
         hf = h.extra["hang_faces"]
         face_hang = np.full(self._num_internal_faces, -1, dtype=np.int64)

@@ -612,9 +612,14 @@ __global__ void k_face_flux(gf_mesh_t m, int mode, const double* __restrict__ ve
             const int o = __ldg(m.owner + f), n = __ldg(m.neighbour + f);
             const double w = __ldg(m.weight + f);
             const int h = grad ? hang_of(m, f) : -1;
+            // Sf has one non-zero component (the face axis) on this grid:
+            // with face_axis only that component is read, and the products
+            // of the two zero components (exact zeros) are not formed.
+            const int k0 = m.face_axis ? __ldg(m.face_axis + f) : 0;
+            const int k1 = m.face_axis ? k0 + 1 : 3;
             double flux = 0.0;
-            double sf[3];
-            for (int k = 0; k < 3; ++k) {
+            double sf[3] = {0.0, 0.0, 0.0};
+            for (int k = k0; k < k1; ++k) {
                 sf[k] = __ldg(m.sf + k * F + f);
                 double vf = w * vel[k * C + o] + (1.0 - w) * vel[k * C + n];
                 if (h >= 0) vf = vf + hang_value_corr(m, grad, k, o, n, w, h);
@@ -622,14 +627,14 @@ __global__ void k_face_flux(gf_mesh_t m, int mode, const double* __restrict__ ve
             }
             if (has_ddt) {
                 double u0f_sf = 0.0;
-                for (int k = 0; k < 3; ++k)
+                for (int k = k0; k < k1; ++k)
                     u0f_sf += (w * ddt.u_old[k * C + o] + (1.0 - w) * ddt.u_old[k * C + n]) * sf[k];
                 const double phi0 = ddt.phi_old[f];
                 const double corr = phi0 - u0f_sf;
                 double hist = ddt.b * corr;
                 if (ddt.c != 0.0) {
                     double u00f_sf = 0.0;
-                    for (int k = 0; k < 3; ++k)
+                    for (int k = k0; k < k1; ++k)
                         u00f_sf += (w * ddt.u_older[k * C + o] + (1.0 - w) * ddt.u_older[k * C + n]) * sf[k];
                     hist = hist - ddt.c * (ddt.phi_older[f] - u00f_sf);
                 }

@@ -1623,6 +1623,229 @@ __global__ void __launch_bounds__(THREADS, 1) k_pcg1_smem_ell(gf_krylov_t K, int
     pcg1_smem_body<THREADS, smem_gather_cells(THREADS), smem_update_cells(THREADS), KEEP_P>(K, rows, chunk);
 }
 
+// ---------------------------------------------------------------------------
+// FP32-inner CG in FP64 refinement (the algorithm of pcg1_mixed_body) with
+// each block's own-cell FP32 vectors resident in shared memory: r, q, the
+// correction d, the Jacobi inverse and (KEEP_P) p, 4-5 floats a cell.  What
+// neighbours read goes through global memory as in pcg1_smem_body: FP32
+// pairs {z, p} (8 bytes a stencil point) double-buffered by iteration
+// parity, plus the FP32 matrix copy and, once per refinement cycle, x (FP64)
+// for the true residual.  Per cell the arithmetic is that of
+// pcg1_mixed_body, so only the order of the reduction partial sums differs.
+//
+// Global layout after the header: n doubles (unused), then floats: the two
+// pair buffers (4n), the FP32 coefficients (ncoef n) and diagonal (n).
+template <int THREADS, int U, int V, bool KEEP_P, class Rows64, class Rows32>
+__device__ void pcg1_mixed_smem_body(const gf_krylov_t& K, const Rows64& rows64, Rows32 rows32, int ncoef,
+                                     int chunk) {
+    __shared__ CgState st;
+    __shared__ double s_target;
+    __shared__ int s_cycle_done;
+    extern __shared__ __align__(16) double sm[];
+    KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
+    barrier_init();
+    double* partials = K.work + kCtlDoubles;
+    double* base = partials + kPartials;
+    const int n = (int)K.n;
+    float* f = reinterpret_cast<float*>(base + n);
+    float2* zp0 = reinterpret_cast<float2*>(f);
+    float2* zp1 = zp0 + n;
+    float* val32 = f + 4 * (int64_t)n;
+    float* diag32 = val32 + (int64_t)ncoef * n;
+    rows32.val = val32;
+    const int c0 = blockIdx.x * chunk;
+    const int c1 = c0 + chunk < n ? c0 + chunk : n;
+    const int m = c1 > c0 ? c1 - c0 : 0;
+    float* smf = reinterpret_cast<float*>(sm);
+    float* rs = smf;
+    float* qs = smf + chunk;
+    float* ds = smf + 2 * chunk;
+    float* ivs = smf + 3 * chunk;
+    float* ps = smf + 4 * chunk;  // only with KEEP_P
+    double* x = K.x;
+    const bool jac = K.jacobi != 0, linf = K.norm_inf != 0;
+    const bool sym_box = K.stride_y > 0 && K.symmetric;
+    bool ok = true;
+    int its = 0;
+
+    for (int i = threadIdx.x; i < m; i += THREADS) {
+        const int c = c0 + i;
+        for (int s = 0; s < ncoef; ++s) {
+            const int src = sym_box ? (2 * s + 1) : s;
+            __stcg(val32 + (int64_t)s * n + c, (float)__ldg(K.val + (int64_t)src * n + c));
+        }
+        __stcg(diag32 + c, (float)__ldg(K.diag + c));
+        ivs[i] = (float)inv_diag(K.diag, c, jac);
+    }
+    if (threadIdx.x == 0) {
+        st.its = 0;
+        st.converged = 0;
+        st.status = GF_MAX_ITER;
+        st.done = 0;
+    }
+    bool pending = false;
+    // max_outer inner cycles, each preceded by a true-residual evaluation,
+    // plus a final evaluation that verifies the last correction.
+    for (int cycle = 0; ok && cycle <= K.max_outer; ++cycle) {
+        {  // fold the pending correction, then the true residual in FP64
+            double loc[2] = {0.0, 0.0};
+            if (pending) {
+                for (int i = threadIdx.x; i < m; i += THREADS) x[c0 + i] = x[c0 + i] + (double)ds[i];
+                pending = false;
+            }
+            // The barrier also publishes x and (cycle 0) the FP32 matrix.
+            double dummy[1] = {0.0};
+            ok = grid_reduce<1, THREADS>(ctl, partials, dummy, 0u);
+            if (!ok) break;
+            auto gx = [&](int i) { return __ldcg(x + i); };
+            for (int i = threadIdx.x; i < m; i += THREADS) {
+                const int c = c0 + i;
+                const double ax = rows64.apply(c, __ldg(K.diag + c), gx);
+                const double rk = __ldg(K.rhs + c) - ax;
+                const float r32 = (float)rk;
+                const float z32 = ivs[i] * r32;
+                rs[i] = r32;
+                ds[i] = 0.0f;
+                __stcg(zp0 + c, make_float2(z32, 0.0f));
+                loc[0] = norm_acc(loc[0], rk, linf);
+                loc[1] += (double)r32 * (double)z32;
+            }
+            ok = grid_reduce<2, THREADS>(ctl, partials, loc, linf ? 1u : 0u);
+            if (!ok) break;
+            if (threadIdx.x == 0) {
+                const double nr = norm_fin(loc[0], linf);
+                if (cycle == 0) {
+                    st.r0 = nr;
+                    st.thresh = fmax(K.atol, K.rtol * nr);
+                }
+                st.final = nr;
+                if (nr < st.thresh) {
+                    st.done = 1;
+                    st.converged = 1;
+                    st.status = GF_OK;
+                } else if (!isfinite(nr)) {
+                    st.done = 1;
+                    st.status = GF_NONFINITE;
+                }
+                st.rz_old = loc[1];
+                st.beta = 0.0;
+                s_target = fmax(K.inner_eta * nr, 0.5 * st.thresh);
+                s_cycle_done = 0;
+            }
+            __syncthreads();
+            if (st.done || cycle == K.max_outer || its >= K.max_iter) break;
+        }
+        pending = true;
+        int k = 0;  // inner iteration of this cycle: pair buffer parity
+        while (ok && !s_cycle_done && its < K.max_iter) {
+            ++its;
+            ++k;
+            const float2* cur = (k & 1) ? zp0 : zp1;
+            float2* nxt = (k & 1) ? zp1 : zp0;
+            {  // p_new = z + p_old beta; q = A p_new; p_new . q
+                const float beta = (float)st.beta;
+                double loc[1] = {0.0};
+                // Plain (L1-cacheable) loads: see pcg1_smem_body.
+                auto gp = [&](int j) {
+                    const float2 v = cur[j];
+                    return v.x + v.y * beta;
+                };
+                for (int i0 = threadIdx.x; i0 < m; i0 += U * THREADS) {
+                    float pc[U], ap[U];
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const int i = i0 + u * THREADS;
+                        if (i < m) {
+                            const int c = c0 + i;
+                            pc[u] = gp(c);
+                            ap[u] = rows32.apply(c, __ldcg(diag32 + c), gp);
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const int i = i0 + u * THREADS;
+                        if (i < m) {
+                            __stcg(&nxt[c0 + i].y, pc[u]);
+                            if (KEEP_P) ps[i] = pc[u];
+                            qs[i] = ap[u];
+                            loc[0] += (double)pc[u] * (double)ap[u];
+                        }
+                    }
+                }
+                ok = grid_reduce<1, THREADS>(ctl, partials, loc, 0u);
+                if (!ok) break;
+                if (threadIdx.x == 0) st.alpha = st.rz_old / loc[0];
+                __syncthreads();
+            }
+            {  // d += alpha p; r -= alpha q; z = M r; |r|, r.z (own cells)
+                const float alpha = (float)st.alpha;
+                double loc[2] = {0.0, 0.0};
+                for (int i0 = threadIdx.x; i0 < m; i0 += V * THREADS) {
+                    float pv[V];
+#pragma unroll
+                    for (int u = 0; u < V; ++u) {
+                        const int i = i0 + u * THREADS;
+                        if (i < m) pv[u] = KEEP_P ? ps[i] : __ldcg(&nxt[c0 + i].y);
+                    }
+#pragma unroll
+                    for (int u = 0; u < V; ++u) {
+                        const int i = i0 + u * THREADS;
+                        if (i < m) {
+                            ds[i] = ds[i] + alpha * pv[u];
+                            const float rk = rs[i] - alpha * qs[i];
+                            const float zk = ivs[i] * rk;
+                            rs[i] = rk;
+                            __stcg(&nxt[c0 + i].x, zk);
+                            loc[0] = norm_acc(loc[0], (double)rk, linf);
+                            loc[1] += (double)rk * (double)zk;
+                        }
+                    }
+                }
+                ok = grid_reduce<2, THREADS>(ctl, partials, loc, linf ? 1u : 0u);
+                if (!ok) break;
+                if (threadIdx.x == 0) {
+                    const double nr = norm_fin(loc[0], linf);
+                    if (!(nr >= s_target) || !isfinite(nr)) {
+                        s_cycle_done = 1;
+                    } else {
+                        st.beta = loc[1] / st.rz_old;
+                        st.rz_old = loc[1];
+                    }
+                }
+                __syncthreads();
+            }
+        }
+    }
+    if (ok && pending) {
+        // iteration budget spent inside a cycle: keep its correction
+        for (int i = threadIdx.x; i < m; i += THREADS) x[c0 + i] = x[c0 + i] + (double)ds[i];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        double* o = K.stats;
+        o[0] = st.r0;
+        o[1] = st.final;
+        o[2] = its;
+        o[3] = st.converged;
+        o[4] = ok ? st.status : GF_ERR_TIMEOUT;
+    }
+}
+
+template <bool SYM, int THREADS, bool KEEP_P>
+__global__ void __launch_bounds__(THREADS, 1) k_pcg1_mixed_smem_box(gf_krylov_t K, int chunk) {
+    BoxRows<double, SYM, false, int> rows64{K.val, (int)K.n, (int)K.stride_y, (int)K.stride_z};
+    BoxRows<float, SYM, SYM, int> rows32{nullptr, (int)K.n, (int)K.stride_y, (int)K.stride_z};
+    pcg1_mixed_smem_body<THREADS, smem_gather_cells(THREADS), smem_update_cells(THREADS), KEEP_P>(
+        K, rows64, rows32, SYM ? 3 : 6, chunk);
+}
+
+template <int WIDTH, int THREADS, bool KEEP_P>
+__global__ void __launch_bounds__(THREADS, 1) k_pcg1_mixed_smem_ell(gf_krylov_t K, int chunk) {
+    EllRows<double, WIDTH, int> rows64{K.val, K.nbr, (int)K.n, K.width};
+    EllRows<float, WIDTH, int> rows32{nullptr, K.nbr, (int)K.n, K.width};
+    pcg1_mixed_smem_body<THREADS, smem_gather_cells(THREADS), smem_update_cells(THREADS), KEEP_P>(
+        K, rows64, rows32, K.width, chunk);
+}
+
 // Tile length for the staged kernel (0: the system does not qualify).
 static int staged_tile(const gf_krylov_t* k) {
     if (!k->symmetric || k->stride_y < 1 || (k->n & 1)) return 0;
@@ -2077,19 +2300,36 @@ static const void* smem_kernel(const gf_krylov_t* k) {
                          : (const void*)k_pcg1_smem_ell<0, THREADS, KEEP_P>;
 }
 
-static int launch_smem_arrays(const gf_krylov_t* k, void* stream, int threads, int narr);
-
-static int launch_smem(const gf_krylov_t* k, void* stream, int threads) {
-    const int st = launch_smem_arrays(k, stream, threads, 4);
-    if (st != GF_ERR_INVALID) return st;
-    return launch_smem_arrays(k, stream, threads, 3);
+template <int THREADS, bool KEEP_P>
+static const void* mixed_smem_kernel(const gf_krylov_t* k) {
+    if (k->stride_y > 0)
+        return k->symmetric ? (const void*)k_pcg1_mixed_smem_box<true, THREADS, KEEP_P>
+                            : (const void*)k_pcg1_mixed_smem_box<false, THREADS, KEEP_P>;
+    return k->width == 6 ? (const void*)k_pcg1_mixed_smem_ell<6, THREADS, KEEP_P>
+                         : (const void*)k_pcg1_mixed_smem_ell<0, THREADS, KEEP_P>;
 }
 
-static int launch_smem_arrays(const gf_krylov_t* k, void* stream, int threads, int narr) {
+static int launch_smem_arrays(const gf_krylov_t* k, void* stream, int threads, int narr, bool mixed);
+
+// FP64: 4 doubles a cell with p kept, else 3.  Mixed: 5 floats, else 4.
+static int launch_smem(const gf_krylov_t* k, void* stream, int threads) {
+    const bool mixed = k->mixed != 0;
+    const int st = launch_smem_arrays(k, stream, threads, mixed ? 5 : 4, mixed);
+    if (st != GF_ERR_INVALID) return st;
+    return launch_smem_arrays(k, stream, threads, mixed ? 4 : 3, mixed);
+}
+
+static int launch_smem_arrays(const gf_krylov_t* k, void* stream, int threads, int narr, bool mixed) {
     const char* what = "gf_pcg_solve";
-    const bool keep = narr == 4;
-    const void* kern = threads == 1024 ? (keep ? smem_kernel<1024, true>(k) : smem_kernel<1024, false>(k))
-                                       : (keep ? smem_kernel<512, true>(k) : smem_kernel<512, false>(k));
+    const bool keep = narr == (mixed ? 5 : 4);
+    const size_t elem = mixed ? sizeof(float) : sizeof(double);
+    const void* kern;
+    if (mixed)
+        kern = threads == 1024 ? (keep ? mixed_smem_kernel<1024, true>(k) : mixed_smem_kernel<1024, false>(k))
+                               : (keep ? mixed_smem_kernel<512, true>(k) : mixed_smem_kernel<512, false>(k));
+    else
+        kern = threads == 1024 ? (keep ? smem_kernel<1024, true>(k) : smem_kernel<1024, false>(k))
+                               : (keep ? smem_kernel<512, true>(k) : smem_kernel<512, false>(k));
     const int kSmemThreads = threads;
     int dev = 0, sms = 0, optin = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -2122,7 +2362,7 @@ static int launch_smem_arrays(const gf_krylov_t* k, void* stream, int threads, i
         if (grid < 1) grid = 1;
         int64_t chunk = (k->n + grid - 1) / grid;
         chunk = (chunk + 1) & ~1LL;
-        const size_t smem = (size_t)(narr * chunk) * sizeof(double);
+        const size_t smem = (size_t)(narr * chunk) * elem;
         if ((int64_t)smem + static_smem > optin) continue;
         e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         int occ = 0;
@@ -2213,8 +2453,14 @@ int gf_pcg_solve(const gf_krylov_t* k, void* stream) {
                       (long long)need);
             return GF_ERR_INVALID;
         }
+        if (k->variant == kSmemVariant || k->variant == kSmemVariant + 1) {
+            const int st = launch_smem(k, stream, k->variant == kSmemVariant ? 512 : 1024);
+            if (st != GF_ERR_INVALID) return st;
+        }
         if (box) {
-            const int v = (k->variant >= 0 && k->variant < kBoxVariants) ? k->variant : 0;
+            // Variants 5-7 that do not qualify fall back to 512-thread blocks.
+            const int v = (k->variant >= 0 && k->variant < kBoxVariants) ? k->variant
+                          : (k->variant >= kStagedVariant ? 2 : 0);
             const BoxVariant bv = k->symmetric ? box_kernel<true, true>(v) : box_kernel<true, false>(v);
             return launch_persistent(bv.kern, k, stream, "gf_pcg_solve", bv.threads, bv.unroll);
         }

@@ -35,8 +35,8 @@ VARIANTS = {
     3: "1024 threads x 1 cell/pass",
     4: "1024 threads x 2 cells/pass",
     5: "512 threads, shared-memory tiles by bulk async copy (symmetric FP64 only)",
-    6: "512 threads, own-cell vectors resident in shared memory (FP64, up to ~1M cells)",
-    7: "1024 threads, own-cell vectors resident in shared memory (FP64, up to ~1M cells)",
+    6: "512 threads, own-cell vectors resident in shared memory (up to ~1.3M cells)",
+    7: "1024 threads, own-cell vectors resident in shared memory (up to ~1.3M cells)",
 }
 
 _LOCK = threading.Lock()

@@ -38,19 +38,17 @@ def workspace(cache: dict, device: torch.device, n: int, ncomp: int, kind: int) 
 
 def default_variant(n: int, mixed: bool, symmetric: bool, box: bool = True) -> int:
     """CG launch shape by system size, from fixed-iteration timings on B200
-    (``python -m gridfoam_b200.solvers.autotune``).  FP64: 256-thread blocks
-    below ~128K cells, where the grid barrier dominates; then the kernel
-    that keeps each block's own-cell vectors in shared memory (1024-thread
-    blocks, box or ELL rows) up to ~1.3M cells; above that the shared-memory
-    tiled kernel for symmetric boxes, else 512-thread blocks.  Mixed
-    precision: 256 then 512-thread blocks."""
+    (``python -m gridfoam_b200.solvers.autotune``).  Below ~128K cells
+    256-thread blocks, where the grid barrier dominates; then the kernels
+    that keep each block's own-cell vectors in shared memory (1024-thread
+    blocks, box or ELL rows, FP64 or FP32-inner) up to ~1.3M cells; above
+    that the shared-memory tiled kernel for symmetric FP64 boxes, else
+    512-thread blocks."""
     if n < 131072:
         return 0
-    if mixed:
-        return 2 if box else 0
     if n <= 1300000:
         return 7
-    return 5 if symmetric and box else 2
+    return 5 if symmetric and box and not mixed else 2
 
 
 class DeviceKrylov(LinearSolver):

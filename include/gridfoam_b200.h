@@ -111,6 +111,10 @@ typedef struct gf_mesh {
     const double* hang_offset;   /* [3][H] face centre - linear-weight point */
     const double* hang_move_o;   /* [3][H] face centre - owner centre, normal part 0 */
     const double* hang_move_n;   /* [3][H] face centre - neighbour centre, normal part 0 */
+    /* Axis (0, 1, 2) of every internal face [F], or NULL.  Faces of the
+     * axis-projected grid are axis-aligned: sf[k][f] = 0 for k != axis, so
+     * kernels given this array read and gather one component per face. */
+    const int8_t* face_axis;
 } gf_mesh_t;
 
 /* Per-face boundary-condition table of one field (value-fraction form). */

@@ -209,10 +209,13 @@ def test_cavity32_against_oracle():
         assert [s.iterations for s in dalgo.last_stats["p"]] == [s.iterations for s in oalgo.last_stats["p"]]
 
 
-def test_mixed_precision_pcg_meets_fp64_criterion():
+@pytest.mark.parametrize("layout", ["box", "ell"])
+@pytest.mark.parametrize("variant", [None, 6, 7])
+def test_mixed_precision_pcg_meets_fp64_criterion(variant, layout):
     """FP32 inner CG inside FP64 refinement reaches the same FP64 true-residual
     threshold as the FP64 solver, and its solution agrees with the FP64
-    solution to the accuracy that threshold implies."""
+    solution to the accuracy that threshold implies.  Variants 6/7: the
+    kernels with each block's FP32 vectors resident in shared memory."""
     from gridfoam_b200.fv import fvm
     from gridfoam_b200.meta.config import SolverConfig
     from gridfoam_b200.solvers.krylov import CGSolver
@@ -224,24 +227,37 @@ def test_mixed_precision_pcg_meets_fp64_criterion():
     A = -fvm.laplacian(gamma, algo.p)
     gen = torch.Generator(device="cpu").manual_seed(1)
     rhs = torch.randn((1, grid.num_cells), generator=gen, dtype=torch.float64).cuda() * 1e-3
-    for tol, rel_tol in ((1e-9, 0.0), (1e-7, 0.01)):
-        base = dict(method="cg", preconditioner="jacobi", tolerance=tol, rel_tolerance=rel_tol, max_iter=5000)
-        x64 = torch.zeros_like(rhs)
-        s64 = CGSolver(SolverConfig(**base)).solve_arrays(grid, A.diag_store, A.val, rhs, x64)
-        x32 = torch.zeros_like(rhs)
-        s32 = CGSolver(SolverConfig(**base, inner_precision="float32")).solve_arrays(
-            grid, A.diag_store, A.val, rhs, x32)
-        assert s64[0].converged and s32[0].converged, (s64, s32)
-        # true FP64 residual of the mixed solution meets the same threshold
-        r = rhs - A.multiply(x32[0]).reshape(1, -1)
-        thresh = max(tol, rel_tol * s64[0].initial_residual)
-        assert float(torch.linalg.vector_norm(r)) < thresh
-        assert abs(s32[0].initial_residual - s64[0].initial_residual) <= 1e-12 * s64[0].initial_residual
+    strides = grid.box_strides
+    if layout == "ell":
+        grid.box_strides = None
+    try:
+        for tol, rel_tol in ((1e-9, 0.0), (1e-7, 0.01)):
+            base = dict(method="cg", preconditioner="jacobi", tolerance=tol, rel_tolerance=rel_tol, max_iter=5000)
+            x64 = torch.zeros_like(rhs)
+            s64 = CGSolver(SolverConfig(**base)).solve_arrays(grid, A.diag_store, A.val, rhs, x64)
+            x32 = torch.zeros_like(rhs)
+            mixed = CGSolver(SolverConfig(**base, inner_precision="float32"))
+            mixed.variant = variant
+            s32 = mixed.solve_arrays(grid, A.diag_store, A.val, rhs, x32, symmetric=layout == "box")
+            _check_mixed(A, rhs, x32, s32, s64, tol, rel_tol)
+    finally:
+        grid.box_strides = strides
 
 
-def test_box_layout_matches_ell_layout():
+def _check_mixed(A, rhs, x32, s32, s64, tol, rel_tol):
+    assert s64[0].converged and s32[0].converged, (s64, s32)
+    # true FP64 residual of the mixed solution meets the same threshold
+    r = rhs - A.multiply(x32[0]).reshape(1, -1)
+    thresh = max(tol, rel_tol * s64[0].initial_residual)
+    assert float(torch.linalg.vector_norm(r)) < thresh
+    assert abs(s32[0].initial_residual - s64[0].initial_residual) <= 1e-12 * s64[0].initial_residual
+
+
+@pytest.mark.parametrize("variant", [None, 7])
+def test_box_layout_matches_ell_layout(variant):
     """On a uniform box, CG with implicit neighbours (symmetric three-array
-    coefficient reads) gives the same solve as the generic ELL path."""
+    coefficient reads) gives the same solve as the generic ELL path, in the
+    register kernels and in the shared-memory-resident ones (7)."""
     from gridfoam_b200.fv import fvm
     from gridfoam_b200.meta.config import SolverConfig
     from gridfoam_b200.solvers.krylov import CGSolver
@@ -258,11 +274,13 @@ def test_box_layout_matches_ell_layout():
         cfg = SolverConfig(method="cg", preconditioner="jacobi", tolerance=1e-10, rel_tolerance=0.0,
                            max_iter=4000, inner_precision=precision)
         x_box = torch.zeros_like(rhs)
-        s_box = CGSolver(cfg).solve_arrays(grid, A.diag_store, A.val, rhs, x_box, symmetric=True)
+        solver = CGSolver(cfg)
+        solver.variant = variant
+        s_box = solver.solve_arrays(grid, A.diag_store, A.val, rhs, x_box, symmetric=True)
         strides, grid.box_strides = grid.box_strides, None
         try:
             x_ell = torch.zeros_like(rhs)
-            s_ell = CGSolver(cfg).solve_arrays(grid, A.diag_store, A.val, rhs, x_ell)
+            s_ell = solver.solve_arrays(grid, A.diag_store, A.val, rhs, x_ell)
         finally:
             grid.box_strides = strides
         assert s_box[0].converged and s_ell[0].converged
