@@ -593,15 +593,17 @@ __global__ void k_simplec_ratu(int64_t C, const double* __restrict__ rau, const 
 // ---------------------------------------------------------------------------
 // Face fluxes (fv/flux.py:32-162, fv/fvc/ddt_corr.py:13-78)
 // ---------------------------------------------------------------------------
+// Rows first .. F + Nb of the extended face layout (first = F: boundary
+// faces only, the internal ones done by k_face_flux_axis).
 __global__ void k_face_flux(gf_mesh_t m, int mode, const double* __restrict__ vel,
                             const int8_t* __restrict__ u_kind, const double* __restrict__ u_psib,
                             gf_ddtcorr_t ddt, int has_ddt, const double* __restrict__ grad,
-                            double* __restrict__ phi) {
+                            double* __restrict__ phi, int64_t first) {
     const int64_t C = m.n_cells;
     const int64_t F = m.n_faces;
     const int64_t nb = m.n_bnd;
     const int64_t total = F + nb;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+    for (int64_t i = first + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
          i += (int64_t)gridDim.x * blockDim.x) {
         if (i < F) {
             const int f = (int)i;
@@ -615,27 +617,34 @@ __global__ void k_face_flux(gf_mesh_t m, int mode, const double* __restrict__ ve
             // Sf has one non-zero component (the face axis) on this grid:
             // with face_axis only that component is read, and the products
             // of the two zero components (exact zeros) are not formed.
-            const int k0 = m.face_axis ? __ldg(m.face_axis + f) : 0;
-            const int k1 = m.face_axis ? k0 + 1 : 3;
+            const int ax = m.face_axis ? __ldg(m.face_axis + f) : -1;
             double flux = 0.0;
-            double sf[3] = {0.0, 0.0, 0.0};
-            for (int k = k0; k < k1; ++k) {
-                sf[k] = __ldg(m.sf + k * F + f);
-                double vf = w * vel[k * C + o] + (1.0 - w) * vel[k * C + n];
-                if (h >= 0) vf = vf + hang_value_corr(m, grad, k, o, n, w, h);
-                flux += vf * sf[k];
+            double sf[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const bool on = ax < 0 || k == ax;
+                sf[k] = on ? __ldg(m.sf + k * F + f) : 0.0;
+                if (on) {
+                    double vf = w * vel[k * C + o] + (1.0 - w) * vel[k * C + n];
+                    if (h >= 0) vf = vf + hang_value_corr(m, grad, k, o, n, w, h);
+                    flux += vf * sf[k];
+                }
             }
             if (has_ddt) {
                 double u0f_sf = 0.0;
-                for (int k = k0; k < k1; ++k)
-                    u0f_sf += (w * ddt.u_old[k * C + o] + (1.0 - w) * ddt.u_old[k * C + n]) * sf[k];
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                    if (ax < 0 || k == ax)
+                        u0f_sf += (w * ddt.u_old[k * C + o] + (1.0 - w) * ddt.u_old[k * C + n]) * sf[k];
                 const double phi0 = ddt.phi_old[f];
                 const double corr = phi0 - u0f_sf;
                 double hist = ddt.b * corr;
                 if (ddt.c != 0.0) {
                     double u00f_sf = 0.0;
-                    for (int k = k0; k < k1; ++k)
-                        u00f_sf += (w * ddt.u_older[k * C + o] + (1.0 - w) * ddt.u_older[k * C + n]) * sf[k];
+#pragma unroll
+                    for (int k = 0; k < 3; ++k)
+                        if (ax < 0 || k == ax)
+                            u00f_sf += (w * ddt.u_older[k * C + o] + (1.0 - w) * ddt.u_older[k * C + n]) * sf[k];
                     hist = hist - ddt.c * (ddt.phi_older[f] - u00f_sf);
                 }
                 const double tiny = 2.2250738585072014e-308;
@@ -659,6 +668,81 @@ __global__ void k_face_flux(gf_mesh_t m, int mode, const double* __restrict__ ve
                 for (int k = 0; k < 3; ++k) flux += vel[k * C + c] * __ldg(m.bnd_sf + k * nb + b);
             }
             phi[i] = flux;
+        }
+    }
+}
+
+// Internal faces of an axis-aligned grid without hanging faces
+// (face_axis given, no gradient correction): the arithmetic of k_face_flux
+// for the one non-zero Sf component, two faces per thread per pass with
+// every load of both faces issued before the loads that depend on them
+// (indices, then gathers), and no branch between the two levels.
+template <bool DDT>
+__global__ void __launch_bounds__(256, 3) k_face_flux_axis(gf_mesh_t m, const double* __restrict__ vel,
+                                                        gf_ddtcorr_t ddt, double* __restrict__ phi) {
+    constexpr int U = 2;
+    const int64_t C = m.n_cells;
+    const int F = (int)m.n_faces;
+    const int stride = gridDim.x * blockDim.x;
+    const bool older = DDT && ddt.c != 0.0;
+    for (int f0 = blockIdx.x * blockDim.x + threadIdx.x; f0 < F; f0 += U * stride) {
+        int f[U], o[U], n[U], ax[U], imm[U];
+        double w[U], p0[U], p00[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            f[u] = f0 + u * stride;
+            const int g = f[u] < F ? f[u] : f0;  // the tail re-reads face f0
+            o[u] = __ldg(m.owner + g);
+            n[u] = __ldg(m.neighbour + g);
+            w[u] = __ldg(m.weight + g);
+            ax[u] = __ldg(m.face_axis + g);
+            imm[u] = m.imm_index ? __ldg(m.imm_index + g) : -1;
+            if (DDT) {
+                p0[u] = __ldg(ddt.phi_old + g);
+                p00[u] = older ? __ldg(ddt.phi_older + g) : 0.0;
+            }
+        }
+        double sfa[U], vo[U], vn[U], uo[U], un[U], uoo[U], unn[U], ro[U], rn[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int g = f[u] < F ? f[u] : f0;
+            const int64_t kC = (int64_t)ax[u] * C;
+            sfa[u] = __ldg(m.sf + (int64_t)ax[u] * F + g);
+            vo[u] = __ldg(vel + kC + o[u]);
+            vn[u] = __ldg(vel + kC + n[u]);
+            if (DDT) {
+                uo[u] = __ldg(ddt.u_old + kC + o[u]);
+                un[u] = __ldg(ddt.u_old + kC + n[u]);
+                ro[u] = __ldg(ddt.rau + o[u]);
+                rn[u] = __ldg(ddt.rau + n[u]);
+                if (older) {
+                    uoo[u] = __ldg(ddt.u_older + kC + o[u]);
+                    unn[u] = __ldg(ddt.u_older + kC + n[u]);
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (f[u] >= F) continue;
+            double flux = 0.0;
+            const double vf = w[u] * vo[u] + (1.0 - w[u]) * vn[u];
+            flux += vf * sfa[u];
+            if (DDT) {
+                double u0f_sf = 0.0;
+                u0f_sf += (w[u] * uo[u] + (1.0 - w[u]) * un[u]) * sfa[u];
+                const double corr = p0[u] - u0f_sf;
+                double hist = ddt.b * corr;
+                if (older) {
+                    double u00f_sf = 0.0;
+                    u00f_sf += (w[u] * uoo[u] + (1.0 - w[u]) * unn[u]) * sfa[u];
+                    hist = hist - ddt.c * (p00[u] - u00f_sf);
+                }
+                const double tiny = 2.2250738585072014e-308;
+                const double coupling = 1.0 - fmin(fabs(corr) / (fabs(p0[u]) + tiny), 1.0);
+                const double rau_f = w[u] * ro[u] + (1.0 - w[u]) * rn[u];
+                flux = flux + rau_f * (coupling * hist / ddt.dt);
+            }
+            phi[f[u]] = imm[u] >= 0 ? 0.0 : flux;
         }
     }
 }
@@ -1167,8 +1251,20 @@ int gf_face_flux(const gf_mesh_t* m, int32_t mode, const double* vel, const int8
             return GF_ERR_INVALID;
         }
     }
-    k_face_flux<<<grid_for(m->n_faces + m->n_bnd), kThreads, 0, GF_STREAM(stream)>>>(*m, mode, vel, u_kind, u_psib,
-                                                                                     d, has, grad_vel, phi);
+    cudaStream_t st = GF_STREAM(stream);
+    if (m->face_axis != nullptr && grad_vel == nullptr && m->n_faces > 0 && m->n_faces < (int64_t)INT32_MAX) {
+        const unsigned g = grid_for((m->n_faces + 1) / 2);
+        if (has)
+            k_face_flux_axis<true><<<g, kThreads, 0, st>>>(*m, vel, d, phi);
+        else
+            k_face_flux_axis<false><<<g, kThreads, 0, st>>>(*m, vel, d, phi);
+        if (m->n_bnd > 0)
+            k_face_flux<<<grid_for(m->n_bnd), kThreads, 0, st>>>(*m, mode, vel, u_kind, u_psib, d, has, grad_vel,
+                                                                  phi, m->n_faces);
+    } else {
+        k_face_flux<<<grid_for(m->n_faces + m->n_bnd), kThreads, 0, st>>>(*m, mode, vel, u_kind, u_psib, d, has,
+                                                                          grad_vel, phi, 0);
+    }
     return check_launch("gf_face_flux");
 }
 
