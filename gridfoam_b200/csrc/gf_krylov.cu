@@ -187,14 +187,17 @@ __device__ bool grid_reduce(KCtl* ctl, double* partials, double (&v)[NV], unsign
     return true;
 }
 
-// y_k(c) = diag(c) * g(k, c) + sum_s val(s, c) * g(k, nbr(s, c))
-template <int NC, class G>
+// y_k(c) = diag(c) * g(k, c) + sum_s val(s, c) * g(k, nbr(s, c)); WIDTH > 0
+// fixes the row width at compile time (the slots are unrolled).
+template <int NC, int WIDTH = 0, class G>
 __device__ __forceinline__ void row_apply(const gf_krylov_t& K, int64_t c, const G& g, double (&out)[NC]) {
     const int64_t n = K.n;
     const double d = __ldg(K.diag + c);
+    const int W = WIDTH > 0 ? WIDTH : K.width;
 #pragma unroll
     for (int k = 0; k < NC; ++k) out[k] = d * g(k, c);
-    for (int s = 0; s < K.width; ++s) {
+#pragma unroll
+    for (int s = 0; s < W; ++s) {
         const double a = __ldg(K.val + s * n + c);
         const int nb = __ldg(K.nbr + s * n + c);
 #pragma unroll
@@ -1892,7 +1895,10 @@ __device__ __forceinline__ void breakdown(BiState& s, int it, int max_restart) {
     }
 }
 
-template <int NC>
+// WIDTH: the ELL row width at compile time (6) or 0 (any).  The Jacobi
+// inverse of every cell is computed once per solve into the workspace (after
+// the six vectors) and gathered from there by the preconditioned SpMVs.
+template <int NC, int WIDTH>
 __global__ void __launch_bounds__(kKThreads) k_bicgstab(gf_krylov_t K) {
     __shared__ BiState st[NC];
     __shared__ int s_any;
@@ -1907,20 +1913,22 @@ __global__ void __launch_bounds__(kKThreads) k_bicgstab(gf_krylov_t K) {
     double* v = vec + 3 * NC * n;
     double* s = vec + 4 * NC * n;
     double* t = vec + 5 * NC * n;
+    double* inv = vec + 6 * NC * n;
     double* x = K.x;
     const bool jac = K.jacobi != 0, linf = K.norm_inf != 0;
     const int64_t t0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     bool ok = true;
 
-    {  // r = b - A x; r_hat = p = r; |r|, r.r
+    {  // r = b - A x; r_hat = p = r; |r|, r.r; the Jacobi inverse
         double loc[2 * NC];
 #pragma unroll
         for (int j = 0; j < 2 * NC; ++j) loc[j] = 0.0;
         auto gx = [&](int k, int64_t i) { return __ldcg(x + k * n + i); };
         for (int64_t c = t0; c < n; c += stride) {
+            __stcg(inv + c, inv_diag(K.diag, c, jac));
             double ax[NC];
-            row_apply<NC>(K, c, gx, ax);
+            row_apply<NC, WIDTH>(K, c, gx, ax);
 #pragma unroll
             for (int k = 0; k < NC; ++k) {
                 const double rk = __ldg(K.rhs + k * n + c) - ax[k];
@@ -1975,10 +1983,10 @@ __global__ void __launch_bounds__(kKThreads) k_bicgstab(gf_krylov_t K) {
             double loc[3 * NC];
 #pragma unroll
             for (int j = 0; j < 3 * NC; ++j) loc[j] = 0.0;
-            auto gy = [&](int k, int64_t i) { return inv_diag(K.diag, i, jac) * __ldcg(p + k * n + i); };
+            auto gy = [&](int k, int64_t i) { return __ldcg(inv + i) * __ldcg(p + k * n + i); };
             for (int64_t c = t0; c < n; c += stride) {
                 double av[NC];
-                row_apply<NC>(K, c, gy, av);
+                row_apply<NC, WIDTH>(K, c, gy, av);
 #pragma unroll
                 for (int k = 0; k < NC; ++k) {
                     if (st[k].mode != kRun) continue;
@@ -2056,11 +2064,11 @@ __global__ void __launch_bounds__(kKThreads) k_bicgstab(gf_krylov_t K) {
             double loc[2 * NC];
 #pragma unroll
             for (int j = 0; j < 2 * NC; ++j) loc[j] = 0.0;
-            auto gz = [&](int k, int64_t i) { return inv_diag(K.diag, i, jac) * __ldcg(s + k * n + i); };
+            auto gz = [&](int k, int64_t i) { return __ldcg(inv + i) * __ldcg(s + k * n + i); };
             for (int64_t c = t0; c < n; c += stride) {
                 double at[NC];
-                row_apply<NC>(K, c, gz, at);
-                const double ic = inv_diag(K.diag, c, jac);
+                row_apply<NC, WIDTH>(K, c, gz, at);
+                const double ic = __ldcg(inv + c);
 #pragma unroll
                 for (int k = 0; k < NC; ++k) {
                     const int md = st[k].mode;
@@ -2102,7 +2110,7 @@ __global__ void __launch_bounds__(kKThreads) k_bicgstab(gf_krylov_t K) {
 #pragma unroll
             for (int j = 0; j < 4 * NC; ++j) loc[j] = 0.0;
             for (int64_t c = t0; c < n; c += stride) {
-                const double ic = inv_diag(K.diag, c, jac);
+                const double ic = __ldcg(inv + c);
 #pragma unroll
                 for (int k = 0; k < NC; ++k) {
                     const int md = st[k].mode;
@@ -2394,14 +2402,15 @@ static int launch_smem_arrays(const gf_krylov_t* k, void* stream, int threads, i
     return GF_ERR_INVALID;
 }
 
-static bool valid_krylov(const gf_krylov_t* k, int nvec, const char* what) {
+// nvec vectors of ncomp x n doubles plus `extra` doubles after the header.
+static bool valid_krylov(const gf_krylov_t* k, int nvec, const char* what, int64_t extra = 0) {
     if (k == nullptr || k->n <= 0 || k->width <= 0 || k->ncomp < 1 || k->ncomp > 3 || k->nbr == nullptr ||
         k->diag == nullptr || k->val == nullptr || k->rhs == nullptr || k->x == nullptr || k->work == nullptr ||
         k->stats == nullptr || k->max_iter < 0) {
         set_error("%s: invalid arguments", what);
         return false;
     }
-    const int64_t need = kHeader + (int64_t)nvec * k->ncomp * k->n;
+    const int64_t need = kHeader + (int64_t)nvec * k->ncomp * k->n + extra;
     if (k->work_len < need) {
         set_error("%s: workspace holds %lld doubles, %lld needed", what, (long long)k->work_len, (long long)need);
         return false;
@@ -2428,7 +2437,8 @@ int64_t gf_krylov_workspace_size(int64_t n, int32_t ncomp, int32_t kind) {
     }
     const int bicgstab = kind == 1;
     const int nvec = bicgstab ? 6 : (ncomp == 1 ? 7 : 3);
-    return kHeader + (int64_t)nvec * ncomp * n;
+    // BiCGStab keeps the Jacobi inverse (n doubles) after its six vectors.
+    return kHeader + (int64_t)nvec * ncomp * n + (bicgstab ? n : 0);
 }
 
 int gf_pcg_solve(const gf_krylov_t* k, void* stream) {
@@ -2504,14 +2514,18 @@ int gf_pcg_solve(const gf_krylov_t* k, void* stream) {
 }
 
 int gf_bicgstab_solve(const gf_krylov_t* k, void* stream) {
-    if (!valid_krylov(k, 6, "gf_bicgstab_solve")) return GF_ERR_INVALID;
+    if (!valid_krylov(k, 6, "gf_bicgstab_solve", k ? k->n : 0)) return GF_ERR_INVALID;
+    const bool w6 = k->width == 6;
     switch (k->ncomp) {
         case 1:
-            return launch_persistent(k_bicgstab<1>, k, stream, "gf_bicgstab_solve");
+            return w6 ? launch_persistent(k_bicgstab<1, 6>, k, stream, "gf_bicgstab_solve")
+                      : launch_persistent(k_bicgstab<1, 0>, k, stream, "gf_bicgstab_solve");
         case 2:
-            return launch_persistent(k_bicgstab<2>, k, stream, "gf_bicgstab_solve");
+            return w6 ? launch_persistent(k_bicgstab<2, 6>, k, stream, "gf_bicgstab_solve")
+                      : launch_persistent(k_bicgstab<2, 0>, k, stream, "gf_bicgstab_solve");
         default:
-            return launch_persistent(k_bicgstab<3>, k, stream, "gf_bicgstab_solve");
+            return w6 ? launch_persistent(k_bicgstab<3, 6>, k, stream, "gf_bicgstab_solve")
+                      : launch_persistent(k_bicgstab<3, 0>, k, stream, "gf_bicgstab_solve");
     }
 }
 
