@@ -527,8 +527,8 @@ def main() -> None:
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--serve-requests", type=int, default=64)
     ap.add_argument("--serve-end-time", type=int, default=100)
-    ap.add_argument("--serve-slots", type=int, default=16)
-    ap.add_argument("--serve-share", type=float, default=0.25)
+    ap.add_argument("--serve-slots", type=int, default=8)
+    ap.add_argument("--serve-share", type=float, default=1.0)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

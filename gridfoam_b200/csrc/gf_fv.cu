@@ -171,6 +171,99 @@ __global__ void k_lsq_grad(gf_mesh_t m, const double* __restrict__ psi,
     }
 }
 
+// k_lsq_grad for six-slot rows: the slot codes and neighbours, then the
+// immersed ordinals and the neighbours' centres and values (at the slot's
+// own neighbour index, valid for every slot) are loaded for all six slots
+// before any is used; the slots are then accumulated in order with the
+// arithmetic of k_lsq_grad (same bits).  Boundary slots take its branch.
+template <int NC>
+__global__ void __launch_bounds__(256, 2) k_lsq_grad6(gf_mesh_t m, const double* __restrict__ psi,
+                                                      const int8_t* __restrict__ kind,
+                                                      const double* __restrict__ psib, double* __restrict__ grad) {
+    constexpr int W = 6;
+    const int64_t C = m.n_cells;
+    const int64_t nb = m.n_bnd;
+    const int F = (int)m.n_faces;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < C;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        int code[W], nbr[W], imm[W];
+#pragma unroll
+        for (int s = 0; s < W; ++s) {
+            code[s] = __ldg(m.ell_code + s * C + c);
+            nbr[s] = __ldg(m.ell_nbr + s * C + c);
+        }
+        double cn[W][3], pn[W][NC];
+#pragma unroll
+        for (int s = 0; s < W; ++s) {
+            const int f = code[s] >> 1;
+            const int fc = (code[s] >= 0 && f < F) ? f : 0;
+            imm[s] = m.imm_index ? __ldg(m.imm_index + fc) : -1;
+#pragma unroll
+            for (int j = 0; j < 3; ++j) cn[s][j] = __ldg(m.center + j * C + nbr[s]);
+#pragma unroll
+            for (int k = 0; k < NC; ++k) pn[s][k] = psi[k * C + nbr[s]];
+        }
+        double atb[NC][3];
+#pragma unroll
+        for (int k = 0; k < NC; ++k) atb[k][0] = atb[k][1] = atb[k][2] = 0.0;
+        const double cx = __ldg(m.center + c), cy = __ldg(m.center + C + c), cz = __ldg(m.center + 2 * C + c);
+        double pc[NC];
+#pragma unroll
+        for (int k = 0; k < NC; ++k) pc[k] = psi[k * C + c];
+#pragma unroll
+        for (int s = 0; s < W; ++s) {
+            const int f = code[s] >> 1;
+            const int side = code[s] & 1;
+            if (code[s] < 0) continue;
+            if (f < F && imm[s] < 0) {
+                double d0 = cn[s][0] - cx, d1 = cn[s][1] - cy, d2 = cn[s][2] - cz;
+                if (side == 1) {
+                    d0 = -d0;
+                    d1 = -d1;
+                    d2 = -d2;
+                }
+                const double dd = d0 * d0 + d1 * d1 + d2 * d2;
+                const double w2 = 1.0 / (dd > 0.0 ? dd : 1.0);
+                const double wd0 = w2 * d0, wd1 = w2 * d1, wd2 = w2 * d2;
+#pragma unroll
+                for (int k = 0; k < NC; ++k) {
+                    double dpsi = pn[s][k] - pc[k];
+                    if (side == 1) dpsi = -dpsi;
+                    atb[k][0] += dpsi * wd0;
+                    atb[k][1] += dpsi * wd1;
+                    atb[k][2] += dpsi * wd2;
+                }
+            } else {
+                const int b = f >= F ? f - F : (int)m.n_domain + (side ? (int)m.n_imm : 0) + imm[s];
+                if (kind[b] == GF_BC_NONE) continue;
+                const double d0 = __ldg(m.bnd_d + b), d1 = __ldg(m.bnd_d + nb + b),
+                             d2 = __ldg(m.bnd_d + 2 * nb + b);
+                const double dd = d0 * d0 + d1 * d1 + d2 * d2;
+                const double w2 = 1.0 / (dd > 0.0 ? dd : 1.0);
+                const double wd0 = w2 * d0, wd1 = w2 * d1, wd2 = w2 * d2;
+#pragma unroll
+                for (int k = 0; k < NC; ++k) {
+                    const double dpsi = psib[k * nb + b] - pc[k];
+                    atb[k][0] += dpsi * wd0;
+                    atb[k][1] += dpsi * wd1;
+                    atb[k][2] += dpsi * wd2;
+                }
+            }
+        }
+        double inv[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) inv[i] = __ldg(m.lsq_ata_inv + i * C + c);
+#pragma unroll
+        for (int k = 0; k < NC; ++k) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                grad[(k * 3 + i) * C + c] =
+                    inv[i * 3 + 0] * atb[k][0] + inv[i * 3 + 1] * atb[k][1] + inv[i * 3 + 2] * atb[k][2];
+            }
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Matrix assembly: ddt + div_sign div(phi, psi) + lap_sign laplacian(gamma, psi)
 // (fv/fvm/ddt.py:7-40, fv/fvm/div.py:15-73, fv/schemes/div.py:36-351,
@@ -369,6 +462,153 @@ __global__ void k_assemble(gf_mesh_t m, gf_assembly_t a) {
             }
             a.val[s * C + c] = val;
         }
+        a.diag[c] = diag;
+#pragma unroll
+        for (int k = 0; k < NC; ++k) a.source[k * C + c] = src[k];
+    }
+}
+
+// k_assemble for the common case: six slots a row, no hanging faces, no
+// TVD correction and no face-flux correction output.  The loads of all six
+// slots are staged (slot codes and neighbours, then immersed ordinals, then
+// the face data at clamped indices) before any of them is used, so a row's
+// gathers are in flight together; the slots' contributions are then added
+// in slot order with the arithmetic of k_assemble, so the matrix is the
+// same bits.  Boundary slots (rare) take the branchy path of k_assemble.
+// CONV / LAP: whether the convection / Laplacian term is assembled (fixed at
+// compile time so a row's staged face data holds only what is used).
+template <int NC, bool CONV, bool LAP>
+__global__ void __launch_bounds__(256, 2) k_assemble6(gf_mesh_t m, gf_assembly_t a) {
+    constexpr int W = 6;
+    const int64_t C = m.n_cells;
+    const int F = (int)m.n_faces;
+    const int64_t nb = m.n_bnd;
+    constexpr bool conv = CONV;
+    constexpr bool lap = LAP;
+    const bool linear = a.div_scheme == GF_DIV_LINEAR;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < C;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        int code[W], nbr[W], fc[W], imm[W];
+#pragma unroll
+        for (int s = 0; s < W; ++s) {
+            code[s] = __ldg(m.ell_code + s * C + c);
+            nbr[s] = __ldg(m.ell_nbr + s * C + c);
+        }
+#pragma unroll
+        for (int s = 0; s < W; ++s) {
+            const int f = code[s] >> 1;
+            fc[s] = (code[s] >= 0 && f < F) ? f : 0;
+            imm[s] = m.imm_index ? __ldg(m.imm_index + fc[s]) : -1;
+        }
+        double w[W], phi[W], msf[W], dl[W], go[W], gn[W];
+#pragma unroll
+        for (int s = 0; s < W; ++s) {
+            const int side = code[s] & 1;
+            const int o = side ? nbr[s] : (int)c;
+            const int n = side ? (int)c : nbr[s];
+            w[s] = __ldg(m.weight + fc[s]);
+            if (CONV) phi[s] = __ldg(a.phi + fc[s]);
+            if (LAP) {
+                msf[s] = __ldg(m.mag_sf + fc[s]);
+                dl[s] = __ldg(m.delta + fc[s]);
+                go[s] = a.gamma ? __ldg(a.gamma + o) : 0.0;
+                gn[s] = a.gamma ? __ldg(a.gamma + n) : 0.0;
+            }
+        }
+        double diag = 0.0;
+        double src[NC];
+#pragma unroll
+        for (int k = 0; k < NC; ++k) src[k] = 0.0;
+        if (a.use_ddt) {
+            const double vdt = __ldg(m.volume + c) / a.dt;
+            diag += a.ddt_a * vdt;
+#pragma unroll
+            for (int k = 0; k < NC; ++k) {
+                double hist = a.ddt_b * a.psi_old[k * C + c];
+                if (a.ddt_c != 0.0) hist = hist - a.ddt_c * a.psi_older[k * C + c];
+                src[k] += vdt * hist;
+            }
+        }
+        double vals[W];
+#pragma unroll
+        for (int s = 0; s < W; ++s) {
+            double val = 0.0;
+            const int f = code[s] >> 1;
+            const int side = code[s] & 1;
+            const bool empty = code[s] < 0;
+            const bool internal = !empty && f < F && imm[s] < 0;
+            if (internal) {
+                if (conv) {
+                    const double flux = phi[s], ww = w[s];
+                    double upper, lower, dO, dN;
+                    if (linear) {
+                        upper = flux * (1.0 - ww);
+                        lower = -flux * ww;
+                        dO = flux * ww;
+                        dN = -flux * (1.0 - ww);
+                    } else {
+                        const double pos = fmax(flux, 0.0), neg = fmin(flux, 0.0);
+                        upper = neg;
+                        lower = -pos;
+                        dO = pos;
+                        dN = -neg;
+                    }
+                    if (side == 0) {
+                        val += a.div_sign * upper;
+                        diag += a.div_sign * dO;
+                    } else {
+                        val += a.div_sign * lower;
+                        diag += a.div_sign * dN;
+                    }
+                }
+                if (lap) {
+                    double gf;
+                    if (a.gamma == nullptr) {
+                        gf = a.gamma_scalar;
+                    } else if (!a.lap_harmonic) {
+                        gf = w[s] * go[s] + (1.0 - w[s]) * gn[s];
+                    } else {
+                        const double scale = fmax(go[s], gn[s]);
+                        const double safe = scale > 0.0 ? scale : 1.0;
+                        const double den = w[s] * (go[s] / safe) + (1.0 - w[s]) * (gn[s] / safe);
+                        gf = fmin(go[s], gn[s]) / (den > 0.0 ? den : 1.0);
+                    }
+                    const double coeff = gf * msf[s] * dl[s];
+                    val += a.lap_sign * coeff;
+                    diag += a.lap_sign * (-coeff);
+                }
+            } else if (!empty) {
+                const int b = f >= F ? f - F : (int)m.n_domain + (side ? (int)m.n_imm : 0) + imm[s];
+                if (a.bc_kind[b] != GF_BC_NONE) {
+                    const double fr = a.frac[b];
+                    const double mag_d = __ldg(m.bnd_mag_d + b);
+                    if (conv) {
+                        const double flux = a.phi[F + b];
+                        diag += a.div_sign * (flux * (1.0 - fr));
+#pragma unroll
+                        for (int k = 0; k < NC; ++k) {
+                            const double bsrc = fr * a.refv[k * nb + b] + (1.0 - fr) * mag_d * a.refg[k * nb + b];
+                            src[k] += -a.div_sign * (flux * bsrc);
+                        }
+                    }
+                    if (lap) {
+                        const double g = a.gamma ? a.gamma[c] : a.gamma_scalar;
+                        const double cond = g * __ldg(m.bnd_mag_sf + b);
+                        const double cv = cond * value_grad_coeff(m, b, fr);
+                        const double cg = cond * (1.0 - fr);
+                        diag += a.lap_sign * (-cv);
+#pragma unroll
+                        for (int k = 0; k < NC; ++k) {
+                            const double ls = cv * a.refv[k * nb + b] + cg * a.refg[k * nb + b];
+                            src[k] += a.lap_sign * (-ls);
+                        }
+                    }
+                }
+            }
+            vals[s] = val;
+        }
+#pragma unroll
+        for (int s = 0; s < W; ++s) a.val[s * C + c] = vals[s];
         a.diag[c] = diag;
 #pragma unroll
         for (int k = 0; k < NC; ++k) a.source[k * C + c] = src[k];
@@ -1129,10 +1369,18 @@ int gf_bc_state(const gf_mesh_t* m, const gf_bc_t* bc, const double* psi, const 
 int gf_lsq_grad(const gf_mesh_t* m, int32_t ncomp, const double* psi, const int8_t* bc_kind, const double* psib,
                 double* grad, void* stream) {
     if (!valid_mesh(m) || !valid_nc(ncomp) || m->lsq_ata_inv == nullptr) return GF_ERR_INVALID;
-    if (ncomp == 1)
-        k_lsq_grad<1><<<grid_for(m->n_cells), kThreads, 0, GF_STREAM(stream)>>>(*m, psi, bc_kind, psib, grad);
-    else
-        k_lsq_grad<3><<<grid_for(m->n_cells), kThreads, 0, GF_STREAM(stream)>>>(*m, psi, bc_kind, psib, grad);
+    const unsigned g = grid_for(m->n_cells);
+    cudaStream_t st = GF_STREAM(stream);
+    const bool six = m->ell_width == 6 && m->n_faces < (int64_t)INT32_MAX;
+    // One component: the per-slot kernel is as fast (fewer registers).
+    if (ncomp == 1) {
+        k_lsq_grad<1><<<g, kThreads, 0, st>>>(*m, psi, bc_kind, psib, grad);
+    } else {
+        if (six)
+            k_lsq_grad6<3><<<g, kThreads, 0, st>>>(*m, psi, bc_kind, psib, grad);
+        else
+            k_lsq_grad<3><<<g, kThreads, 0, st>>>(*m, psi, bc_kind, psib, grad);
+    }
     return check_launch("gf_lsq_grad");
 }
 
@@ -1154,10 +1402,26 @@ int gf_assemble(const gf_mesh_t* m, const gf_assembly_t* a, void* stream) {
         set_error("gf_assemble: ddt term needs history and dt > 0");
         return GF_ERR_INVALID;
     }
-    if (a->ncomp == 1)
-        k_assemble<1><<<grid_for(m->n_cells), kThreads, 0, GF_STREAM(stream)>>>(*m, *a);
-    else
-        k_assemble<3><<<grid_for(m->n_cells), kThreads, 0, GF_STREAM(stream)>>>(*m, *a);
+    const bool fast = m->ell_width == 6 && m->n_hang == 0 && a->ffc == nullptr &&
+                      a->div_scheme <= GF_DIV_LINEAR && m->n_faces < (int64_t)INT32_MAX;
+    const bool conv = a->div_scheme != GF_DIV_NONE, lap = a->lap_sign != 0.0;
+    cudaStream_t st = GF_STREAM(stream);
+    const unsigned g = grid_for(m->n_cells);
+    if (fast) {
+        if (a->ncomp == 1) {
+            if (conv && lap) k_assemble6<1, true, true><<<g, kThreads, 0, st>>>(*m, *a);
+            else if (conv) k_assemble6<1, true, false><<<g, kThreads, 0, st>>>(*m, *a);
+            else k_assemble6<1, false, true><<<g, kThreads, 0, st>>>(*m, *a);
+        } else {
+            if (conv && lap) k_assemble6<3, true, true><<<g, kThreads, 0, st>>>(*m, *a);
+            else if (conv) k_assemble6<3, true, false><<<g, kThreads, 0, st>>>(*m, *a);
+            else k_assemble6<3, false, true><<<g, kThreads, 0, st>>>(*m, *a);
+        }
+    } else if (a->ncomp == 1) {
+        k_assemble<1><<<g, kThreads, 0, st>>>(*m, *a);
+    } else {
+        k_assemble<3><<<g, kThreads, 0, st>>>(*m, *a);
+    }
     return check_launch("gf_assemble");
 }
 
