@@ -161,6 +161,7 @@ class GfKrylov(ctypes.Structure):
         ("block_cap", I32),
         ("variant", I32),
         ("single_reduction", I32),
+        ("inner_margin", F64),
     ]
 
 

@@ -886,7 +886,7 @@ __device__ void pcg1_mixed_body(const gf_krylov_t& K, const Rows64& rows64, Rows
                 }
                 st.rz_old = loc[1];
                 st.beta = 0.0;
-                s_target = fmax(K.inner_eta * nr, 0.5 * st.thresh);
+                s_target = fmax(K.inner_eta * nr, (K.inner_margin > 0.0 ? K.inner_margin : 0.5) * st.thresh);
                 s_cycle_done = 0;
             }
             __syncthreads();
@@ -1019,6 +1019,9 @@ constexpr int kStagedVariant = 5;
 // or ELL, 512-thread (6) or 1024-thread (7) blocks; falls back when the
 // system is too large for it.
 constexpr int kSmemVariant = 6;
+// q-recurrence CG with shared-memory-resident vectors (pcg1_qrec_body),
+// 1024-thread blocks, one (8) or two (9) cells per thread per gather pass.
+constexpr int kQrecVariant = 8;
 
 template <bool MIXED, bool SYM, int THREADS, int U>
 static BoxVariant box_variant() {
@@ -1627,6 +1630,180 @@ __global__ void __launch_bounds__(THREADS, 1) k_pcg1_smem_ell(gf_krylov_t K, int
 }
 
 // ---------------------------------------------------------------------------
+// Shared-memory-resident CG with the direction product updated by recurrence:
+// q = A p is formed as q_k = A z_k + beta q_(k-1) (equal to A (z_k + beta
+// p_(k-1)) in exact arithmetic), so the stencil gathers z alone and only z
+// crosses L2 between blocks.  Each block keeps r, q and p of its cells in
+// shared memory and updates its cells of x in place in global memory.  The
+// iterates differ from pcg1_smem_body by the rounding of the recurrence.
+template <int THREADS, int U, int V, class Rows>
+__device__ void pcg1_qrec_body(const gf_krylov_t& K, const Rows& rows, int chunk) {
+    __shared__ CgState st;
+    extern __shared__ __align__(16) double sm[];
+    KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
+    barrier_init();
+    double* partials = K.work + kCtlDoubles;
+    double* vec = partials + kPartials;
+    const int n = (int)K.n;
+    double* z = vec;
+    double* inv = vec + n;
+    double* x = K.x;
+    const int c0 = blockIdx.x * chunk;
+    const int c1 = c0 + chunk < n ? c0 + chunk : n;
+    const int m = c1 > c0 ? c1 - c0 : 0;
+    double* rs = sm;
+    double* qs = sm + chunk;
+    double* ps = sm + 2 * chunk;
+    const bool jac = K.jacobi != 0, linf = K.norm_inf != 0;
+    bool ok = true;
+    {  // r = b - A x, z = M r, p = q = 0; |r| and r.z
+        double loc[2] = {0.0, 0.0};
+        auto gx = [&](int i) { return __ldcg(x + i); };
+        for (int i = threadIdx.x; i < m; i += THREADS) {
+            const int c = c0 + i;
+            const double ax = rows.apply(c, __ldg(K.diag + c), gx);
+            const double rk = __ldg(K.rhs + c) - ax;
+            const double iv = inv_diag(K.diag, c, jac);
+            const double zk = iv * rk;
+            rs[i] = rk;
+            qs[i] = 0.0;
+            ps[i] = 0.0;
+            inv[c] = iv;
+            __stcg(z + c, zk);
+            loc[0] = norm_acc(loc[0], rk, linf);
+            loc[1] += rk * zk;
+        }
+        ok = grid_reduce<2, THREADS>(ctl, partials, loc, linf ? 1u : 0u);
+        if (threadIdx.x == 0) {
+            const double r0 = norm_fin(loc[0], linf);
+            st.r0 = r0;
+            st.final = r0;
+            st.thresh = fmax(K.atol, K.rtol * r0);
+            st.rz_old = loc[1];
+            st.beta = 0.0;
+            st.its = 0;
+            st.converged = 0;
+            st.status = GF_MAX_ITER;
+            st.done = 0;
+            if (r0 < st.thresh) {
+                st.done = 1;
+                st.converged = 1;
+                st.status = GF_OK;
+            } else if (!isfinite(r0)) {
+                st.done = 1;
+                st.status = GF_NONFINITE;
+            }
+        }
+        __syncthreads();
+    }
+    for (int it = 1; ok && !st.done && it <= K.max_iter; ++it) {
+        {  // w = A z; p = z + beta p; q = w + beta q; p . q
+            const double beta = st.beta;
+            double loc[1] = {0.0};
+            // Plain (L1-cacheable) loads: z is written only before the grid
+            // barrier that precedes this pass (see pcg1_smem_body).
+            auto gz = [&](int j) { return z[j]; };
+            for (int i0 = threadIdx.x; i0 < m; i0 += U * THREADS) {
+                double zc[U], w[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int i = i0 + u * THREADS;
+                    if (i < m) {
+                        const int c = c0 + i;
+                        zc[u] = z[c];
+                        w[u] = rows.apply(c, __ldg(K.diag + c), gz);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int i = i0 + u * THREADS;
+                    if (i < m) {
+                        const double pk = zc[u] + ps[i] * beta;
+                        const double qk = w[u] + qs[i] * beta;
+                        ps[i] = pk;
+                        qs[i] = qk;
+                        loc[0] += pk * qk;
+                    }
+                }
+            }
+            ok = grid_reduce<1, THREADS>(ctl, partials, loc, 0u);
+            if (!ok) break;
+            if (threadIdx.x == 0) st.alpha = st.rz_old / loc[0];
+            __syncthreads();
+        }
+        {  // x += alpha p; r -= alpha q; z = M r; |r|, r.z (own cells)
+            const double alpha = st.alpha;
+            double loc[2] = {0.0, 0.0};
+            for (int i0 = threadIdx.x; i0 < m; i0 += V * THREADS) {
+                double xv[V], iv[V];
+#pragma unroll
+                for (int u = 0; u < V; ++u) {
+                    const int i = i0 + u * THREADS;
+                    if (i < m) {
+                        xv[u] = __ldcg(x + c0 + i);
+                        iv[u] = inv[c0 + i];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < V; ++u) {
+                    const int i = i0 + u * THREADS;
+                    if (i < m) {
+                        const int c = c0 + i;
+                        __stcg(x + c, xv[u] + alpha * ps[i]);
+                        const double rk = rs[i] - alpha * qs[i];
+                        const double zk = iv[u] * rk;
+                        rs[i] = rk;
+                        __stcg(z + c, zk);
+                        loc[0] = norm_acc(loc[0], rk, linf);
+                        loc[1] += rk * zk;
+                    }
+                }
+            }
+            ok = grid_reduce<2, THREADS>(ctl, partials, loc, linf ? 1u : 0u);
+            if (!ok) break;
+            if (threadIdx.x == 0) {
+                const double fin = norm_fin(loc[0], linf);
+                st.final = fin;
+                if (fin < st.thresh) {
+                    st.done = 1;
+                    st.converged = 1;
+                    st.its = it;
+                    st.status = GF_OK;
+                } else if (!isfinite(fin)) {
+                    st.done = 1;
+                    st.its = it;
+                    st.status = GF_NONFINITE;
+                } else {
+                    st.beta = loc[1] / st.rz_old;
+                    st.rz_old = loc[1];
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        double* o = K.stats;
+        o[0] = st.r0;
+        o[1] = st.final;
+        o[2] = st.done ? st.its : K.max_iter;
+        o[3] = st.converged;
+        o[4] = ok ? st.status : GF_ERR_TIMEOUT;
+    }
+}
+
+template <bool SYM, int THREADS, int U>
+__global__ void __launch_bounds__(THREADS, 1) k_pcg1_qrec_box(gf_krylov_t K, int chunk) {
+    BoxRows<double, SYM, false, int> rows{K.val, (int)K.n, (int)K.stride_y, (int)K.stride_z};
+    pcg1_qrec_body<THREADS, U, 2>(K, rows, chunk);
+}
+
+template <int WIDTH, int THREADS, int U>
+__global__ void __launch_bounds__(THREADS, 1) k_pcg1_qrec_ell(gf_krylov_t K, int chunk) {
+    EllRows<double, WIDTH, int> rows{K.val, K.nbr, (int)K.n, K.width};
+    pcg1_qrec_body<THREADS, U, 2>(K, rows, chunk);
+}
+
+// ---------------------------------------------------------------------------
 // FP32-inner CG in FP64 refinement (the algorithm of pcg1_mixed_body) with
 // each block's own-cell FP32 vectors resident in shared memory: r, q, the
 // correction d, the Jacobi inverse and (KEEP_P) p, 4-5 floats a cell.  What
@@ -1732,7 +1909,7 @@ __device__ void pcg1_mixed_smem_body(const gf_krylov_t& K, const Rows64& rows64,
                 }
                 st.rz_old = loc[1];
                 st.beta = 0.0;
-                s_target = fmax(K.inner_eta * nr, 0.5 * st.thresh);
+                s_target = fmax(K.inner_eta * nr, (K.inner_margin > 0.0 ? K.inner_margin : 0.5) * st.thresh);
                 s_cycle_done = 0;
             }
             __syncthreads();
@@ -2317,27 +2494,44 @@ static const void* mixed_smem_kernel(const gf_krylov_t* k) {
                          : (const void*)k_pcg1_mixed_smem_ell<0, THREADS, KEEP_P>;
 }
 
-static int launch_smem_arrays(const gf_krylov_t* k, void* stream, int threads, int narr, bool mixed);
+template <int U>
+static const void* qrec_kernel(const gf_krylov_t* k) {
+    if (k->stride_y > 0)
+        return k->symmetric ? (const void*)k_pcg1_qrec_box<true, 1024, U> : (const void*)k_pcg1_qrec_box<false, 1024, U>;
+    return k->width == 6 ? (const void*)k_pcg1_qrec_ell<6, 1024, U> : (const void*)k_pcg1_qrec_ell<0, 1024, U>;
+}
+
+static int launch_smem_arrays(const gf_krylov_t* k, void* stream, int threads, int narr, size_t elem,
+                              const void* kern);
 
 // FP64: 4 doubles a cell with p kept, else 3.  Mixed: 5 floats, else 4.
 static int launch_smem(const gf_krylov_t* k, void* stream, int threads) {
     const bool mixed = k->mixed != 0;
-    const int st = launch_smem_arrays(k, stream, threads, mixed ? 5 : 4, mixed);
-    if (st != GF_ERR_INVALID) return st;
-    return launch_smem_arrays(k, stream, threads, mixed ? 4 : 3, mixed);
+    const size_t elem = mixed ? sizeof(float) : sizeof(double);
+    for (int keep = 1; keep >= 0; --keep) {
+        const void* kern;
+        if (mixed)
+            kern = threads == 1024 ? (keep ? mixed_smem_kernel<1024, true>(k) : mixed_smem_kernel<1024, false>(k))
+                                   : (keep ? mixed_smem_kernel<512, true>(k) : mixed_smem_kernel<512, false>(k));
+        else
+            kern = threads == 1024 ? (keep ? smem_kernel<1024, true>(k) : smem_kernel<1024, false>(k))
+                                   : (keep ? smem_kernel<512, true>(k) : smem_kernel<512, false>(k));
+        const int narr = (mixed ? 4 : 3) + keep;
+        const int st = launch_smem_arrays(k, stream, threads, narr, elem, kern);
+        if (st != GF_ERR_INVALID) return st;
+    }
+    return GF_ERR_INVALID;
 }
 
-static int launch_smem_arrays(const gf_krylov_t* k, void* stream, int threads, int narr, bool mixed) {
+// The q-recurrence form (FP64, 1024 threads): r, q and p in shared memory.
+static int launch_qrec(const gf_krylov_t* k, void* stream, int unroll) {
+    const void* kern = unroll == 2 ? qrec_kernel<2>(k) : qrec_kernel<1>(k);
+    return launch_smem_arrays(k, stream, 1024, 3, sizeof(double), kern);
+}
+
+static int launch_smem_arrays(const gf_krylov_t* k, void* stream, int threads, int narr, size_t elem,
+                              const void* kern) {
     const char* what = "gf_pcg_solve";
-    const bool keep = narr == (mixed ? 5 : 4);
-    const size_t elem = mixed ? sizeof(float) : sizeof(double);
-    const void* kern;
-    if (mixed)
-        kern = threads == 1024 ? (keep ? mixed_smem_kernel<1024, true>(k) : mixed_smem_kernel<1024, false>(k))
-                               : (keep ? mixed_smem_kernel<512, true>(k) : mixed_smem_kernel<512, false>(k));
-    else
-        kern = threads == 1024 ? (keep ? smem_kernel<1024, true>(k) : smem_kernel<1024, false>(k))
-                               : (keep ? smem_kernel<512, true>(k) : smem_kernel<512, false>(k));
     const int kSmemThreads = threads;
     int dev = 0, sms = 0, optin = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -2491,6 +2685,10 @@ int gf_pcg_solve(const gf_krylov_t* k, void* stream) {
             }
             if (k->variant == kSmemVariant || k->variant == kSmemVariant + 1) {
                 const int st = launch_smem(k, stream, k->variant == kSmemVariant ? 512 : 1024);
+                if (st != GF_ERR_INVALID) return st;
+            }
+            if (k->variant == kQrecVariant || k->variant == kQrecVariant + 1) {
+                const int st = launch_qrec(k, stream, k->variant == kQrecVariant ? 1 : 2);
                 if (st != GF_ERR_INVALID) return st;
             }
             if (box && k->variant == kStagedVariant) {

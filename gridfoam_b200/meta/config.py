@@ -209,11 +209,14 @@ class SolverConfig(BaseModel, frozen=True):
     # Extension (not in the reference schema; defaults keep its behaviour):
     # ``inner_precision: float32`` runs CG's inner iterations in FP32 inside
     # FP64 iterative refinement; the stopping test stays the FP64 true
-    # residual.  ``max_outer`` bounds the refinement cycles and
-    # ``inner_eta`` is the relative reduction of one FP32 cycle.
+    # residual.  ``max_outer`` bounds the refinement cycles,
+    # ``inner_eta`` is the relative reduction of one FP32 cycle, and a cycle
+    # also ends once its FP32 residual is below ``inner_margin`` times the
+    # stopping threshold (margin for the FP32 rounding of that residual).
     inner_precision: PrecisionType = PrecisionType.FLOAT64
     max_outer: int = Field(default=10, ge=1)
     inner_eta: float = Field(default=1e-4, gt=0.0, lt=1.0)
+    inner_margin: float = Field(default=0.9, gt=0.0, le=1.0)
 
 
 class PotentialFlowConfig(BaseModel, frozen=True):

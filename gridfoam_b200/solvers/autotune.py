@@ -27,6 +27,9 @@ import torch
 
 from gridfoam_b200.meta.config import PrecisionType, PreconditionerType, SolverConfig, SolverType
 
+# best_variant chooses among the first N_VARIANTS (the iterates of these
+# differ only by the order of the dot-product partial sums); 8 and 9 form
+# q = A p by recurrence and are used when asked for.
 N_VARIANTS = 8
 VARIANTS = {
     0: "256 threads x 1 cell/pass",
@@ -37,6 +40,8 @@ VARIANTS = {
     5: "512 threads, shared-memory tiles by bulk async copy (symmetric FP64 only)",
     6: "512 threads, own-cell vectors resident in shared memory (up to ~1.3M cells)",
     7: "1024 threads, own-cell vectors resident in shared memory (up to ~1.3M cells)",
+    8: "1024 threads, shared-memory vectors, q = A z + beta q recurrence, 1 cell/pass (FP64)",
+    9: "1024 threads, shared-memory vectors, q = A z + beta q recurrence, 2 cells/pass (FP64)",
 }
 
 _LOCK = threading.Lock()

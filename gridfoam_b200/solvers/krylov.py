@@ -68,6 +68,7 @@ class DeviceKrylov(LinearSolver):
         self.mixed = config.inner_precision == PrecisionType.FLOAT32
         self.max_outer = int(config.max_outer)
         self.inner_eta = float(config.inner_eta)
+        self.inner_margin = float(config.inner_margin)
         self._stats_dev: dict[tuple, torch.Tensor] = {}
         self._workspaces: dict[tuple, torch.Tensor] = {}
         # Optional list receiving (start event, end event, stats) per solve.
@@ -120,6 +121,7 @@ class DeviceKrylov(LinearSolver):
         k.mixed = int(mixed)
         k.max_outer = self.max_outer
         k.inner_eta = self.inner_eta
+        k.inner_margin = self.inner_margin
         k.block_cap = int(self.block_cap)
         box = getattr(grid, "box_strides", None)
         k.variant = (int(self.variant) if self.variant is not None

@@ -209,10 +209,12 @@ typedef struct gf_krylov {
     int64_t stride_z;
     int32_t symmetric;    /* 1 (box only): A is symmetric, only + slots read */
     int32_t block_cap;    /* > 0: at most this many persistent blocks (tuning) */
-    int32_t variant;      /* box CG kernel variant (0..4, see gf_krylov.cu) */
+    int32_t variant;      /* CG launch shape (0..7, see gf_krylov.cu) */
     int32_t single_reduction; /* 1 (FP64 CG, one system): Chronopoulos-Gear
                              CG, one grid reduction per iteration; needs the
                              kind-0 workspace (7 vectors) */
+    double inner_margin;  /* mixed: an FP32 cycle also ends once its residual
+                             is below margin * threshold, in (0, 1]; 0: 0.5 */
 } gf_krylov_t;
 
 const char* gf_last_error(void);

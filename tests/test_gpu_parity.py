@@ -37,16 +37,18 @@ def _cuda():
         pytest.skip("needs a CUDA device")
 
 
-@pytest.mark.parametrize("algorithm", ["pcg", "sr", "staged", "smem"])
+@pytest.mark.parametrize("algorithm", ["pcg", "sr", "staged", "smem", "qrec"])
 @pytest.mark.parametrize("name", CASES)
 def test_steps_match_reference(name, algorithm):
     """pcg: two-reduction fused PCG; sr: single-reduction CG; staged: the
-    shared-memory tiled box kernel (box grids; ELL grids fall back)."""
+    shared-memory tiled box kernel (box grids; ELL grids fall back); smem:
+    own-cell vectors in shared memory; qrec: the same with q = A p formed
+    by recurrence."""
     golden = load_golden(name)
     _, _, _, algo = device_case(name)
     for s in algo.solvers.values():
         s.single_reduction = algorithm == "sr"
-        s.variant = {"staged": 5, "smem": 7}.get(algorithm, 0)
+        s.variant = {"staged": 5, "smem": 7, "qrec": 9}.get(algorithm, 0)
     np.testing.assert_allclose(to_np(algo.phi.pack()), golden["init_phi"], rtol=0, atol=1e-13)
     tol = STEP_TOL[name]
     slack = 1 if name.startswith("pipe") or name in OCTREE_CASES else 0
@@ -318,12 +320,13 @@ def test_single_reduction_cg_matches_pcg(layout):
     assert r < 1e-9 * s1.initial_residual
 
 
-@pytest.mark.parametrize("variant", [5, 6, 7])
+@pytest.mark.parametrize("variant", [5, 6, 7, 8, 9])
 @pytest.mark.parametrize("shape", [(24, 20, 28), (64, 64, 40), (7, 5, 6), (130, 3, 4)])
 def test_staged_box_cg_matches_register_kernel(shape, variant):
     """The shared-memory variants against the register kernel (variant 0):
     5 stages tiles by bulk async copy, 6/7 keep each block's own-cell
-    vectors resident (512/1024 threads).  Same iteration count within one and
+    vectors resident (512/1024 threads), 8/9 also form q = A p by
+    recurrence.  Same iteration count within one and
     the same solution to the stopping tolerance, on shapes with partial last
     tiles or chunks, odd strides and a y halo larger than a tile's x extent."""
     from gridfoam_b200.solvers.autotune import BoxSystem, _solver
@@ -382,7 +385,7 @@ def test_smem_resident_cg_fixed_iterations_match_register_kernel(variant, box):
     assert rel(xs[1], xs[0]) < 1e-11
 
 
-@pytest.mark.parametrize("variant", [6, 7])
+@pytest.mark.parametrize("variant", [6, 7, 8, 9])
 def test_smem_resident_cg_on_ell_layout(variant):
     """The shared-memory-resident CG through the general ELL rows (the
     octree path), against the register ELL kernel."""
