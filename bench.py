@@ -109,12 +109,13 @@ def pcg_bytes_per_iter(C: int, F: int) -> float:
 
 
 # Measured DRAM bytes (read + write) of the pressure CG kernel
-# (k_pcg1_smem_box<1, 1024, 0>) on a 64x64x256 box, from two ncu captures of
-# fixed-length launches: 82.72 MB at 50 iterations, 107.00 MB at 400.  The
-# global working set (~90 MB) stays in the 126 MB L2, so a launch costs a
-# one-time read of its arrays plus a small per-iteration remainder.
-PCG_DRAM_BYTES_PER_ITER = (107002880 - 82719744) / 350
-PCG_DRAM_BYTES_PER_LAUNCH = 82719744 - 50 * PCG_DRAM_BYTES_PER_ITER
+# (k_pcg1_qrec_box<1, 1024, 1>) on a 64x64x256 box, from two ncu captures of
+# fixed-length launches: 51.96 MB at 50 iterations, 182.87 MB at 400.  The
+# global working set stays in the 126 MB L2, so a launch costs a one-time
+# read of its arrays plus the write-back of the x updated in place each
+# iteration.
+PCG_DRAM_BYTES_PER_ITER = (182874112 - 51962368) / 350
+PCG_DRAM_BYTES_PER_LAUNCH = 51962368 - 50 * PCG_DRAM_BYTES_PER_ITER
 
 
 def pcg_bytes_setup(C: int, F: int) -> float:
@@ -476,7 +477,7 @@ def run_gpu(args) -> None:
             "p_iterations_per_solve": (sum(iters) / len(iters)) if iters else None,
         },
         "roofline": {
-            "kernel": "k_pcg (persistent Jacobi-PCG, fp64)",
+            "kernel": "k_pcg1_qrec_box (persistent Jacobi-PCG, fp64, q by recurrence)",
             "bound": "hbm",
             "achieved": achieved,
             "peak": peak,

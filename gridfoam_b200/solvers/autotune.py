@@ -27,10 +27,10 @@ import torch
 
 from gridfoam_b200.meta.config import PrecisionType, PreconditionerType, SolverConfig, SolverType
 
-# best_variant chooses among the first N_VARIANTS (the iterates of these
-# differ only by the order of the dot-product partial sums); 8 and 9 form
-# q = A p by recurrence and are used when asked for.
-N_VARIANTS = 8
+# Variants 0-7 differ only in launch shape and memory placement (their
+# iterates differ by the order of the dot-product partial sums); 8 and 9
+# form q = A p by recurrence (FP64 only: mixed solves fall back to 2).
+N_VARIANTS = 10
 VARIANTS = {
     0: "256 threads x 1 cell/pass",
     1: "256 threads x 2 cells/pass",

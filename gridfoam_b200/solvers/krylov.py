@@ -39,15 +39,17 @@ def workspace(cache: dict, device: torch.device, n: int, ncomp: int, kind: int) 
 def default_variant(n: int, mixed: bool, symmetric: bool, box: bool = True) -> int:
     """CG launch shape by system size, from fixed-iteration timings on B200
     (``python -m gridfoam_b200.solvers.autotune``).  Below ~128K cells
-    256-thread blocks, where the grid barrier dominates; then the kernels
-    that keep each block's own-cell vectors in shared memory (1024-thread
-    blocks, box or ELL rows, FP64 or FP32-inner) up to ~1.3M cells; above
-    that the shared-memory tiled kernel for symmetric FP64 boxes, else
-    512-thread blocks."""
+    256-thread blocks, where the grid barrier dominates; then, up to ~1.3M
+    cells, kernels that keep each block's own-cell vectors in shared memory
+    (1024-thread blocks, box or ELL rows): for FP64 the form that updates
+    q = A p by recurrence and gathers z alone (15.8 against 20.4 us an
+    iteration at 1M cells), for FP32-inner solves the plain one; above that
+    the shared-memory tiled kernel for symmetric FP64 boxes, else 512-thread
+    blocks."""
     if n < 131072:
         return 0
     if n <= 1300000:
-        return 7
+        return 7 if mixed else 8
     return 5 if symmetric and box and not mixed else 2
 
 

@@ -490,3 +490,25 @@ def test_staged_assembly_matches_generic_kernel(name):
         a.ffc = None
         for x, y in zip(*outs):
             assert torch.equal(x, y), field.name
+
+
+@pytest.mark.parametrize("variant", [8, 9])
+@pytest.mark.parametrize("box", [True, False])
+def test_qrec_cg_true_residual(variant, box):
+    """The q-recurrence CG updates r from q = A z + beta q rather than from
+    A p: after a solve to 1e-10 relative, the true residual b - A x must sit
+    at the reported one (no residual gap beyond rounding)."""
+    from gridfoam_b200.solvers.autotune import BoxSystem, _solver
+
+    sysm = BoxSystem(48, 40, 96, device=torch.device("cuda"))
+    if not box:
+        sysm.box_strides = None
+    s = _solver(6000, False, variant)
+    s.atol, s.rtol = 0.0, 1e-10
+    x = torch.zeros_like(sysm.rhs)
+    st = s.solve_arrays(sysm, sysm.diag, sysm.val, sysm.rhs, x, symmetric=True)[0]
+    assert st.converged
+    nb = sysm.dev["ell_nbr"].long()
+    ax = sysm.diag * x[0] + (sysm.val * x[0][nb]).sum(0)
+    true = torch.linalg.vector_norm(sysm.rhs[0] - ax).item()
+    assert true < 2e-10 * st.initial_residual, (true / st.initial_residual, st.iterations)
