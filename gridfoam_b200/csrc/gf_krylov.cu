@@ -2026,6 +2026,207 @@ __global__ void __launch_bounds__(THREADS, 1) k_pcg1_mixed_smem_ell(gf_krylov_t 
         K, rows64, rows32, K.width, chunk);
 }
 
+// ---------------------------------------------------------------------------
+// FP32-inner CG in FP64 refinement with shared-memory-resident FP32 vectors
+// and q = A p formed by recurrence (q_k = A z_k + beta q_(k-1), as in
+// pcg1_qrec_body): the stencil gathers the FP32 z alone.  Each block keeps
+// r, q, p, the correction d and the Jacobi inverse of its cells in shared
+// memory (5 floats a cell) and folds d into the FP64 x once per refinement
+// cycle.  Cycle control, true residuals and stopping rule are those of
+// pcg1_mixed_body.
+//
+// Global layout after the header: n doubles (unused), then floats: z (n),
+// the FP32 coefficients (ncoef n) and diagonal (n).
+template <int THREADS, int U, int V, class Rows64, class Rows32>
+__device__ void pcg1_mixed_qrec_body(const gf_krylov_t& K, const Rows64& rows64, Rows32 rows32, int ncoef,
+                                     int chunk) {
+    __shared__ CgState st;
+    __shared__ double s_target;
+    __shared__ int s_cycle_done;
+    extern __shared__ __align__(16) double sm[];
+    KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
+    barrier_init();
+    double* partials = K.work + kCtlDoubles;
+    double* base = partials + kPartials;
+    const int n = (int)K.n;
+    float* f = reinterpret_cast<float*>(base + n);
+    float* z = f;
+    float* val32 = f + (int64_t)n;
+    float* diag32 = val32 + (int64_t)ncoef * n;
+    rows32.val = val32;
+    const int c0 = blockIdx.x * chunk;
+    const int c1 = c0 + chunk < n ? c0 + chunk : n;
+    const int m = c1 > c0 ? c1 - c0 : 0;
+    float* smf = reinterpret_cast<float*>(sm);
+    float* rs = smf;
+    float* qs = smf + chunk;
+    float* ds = smf + 2 * chunk;
+    float* ivs = smf + 3 * chunk;
+    float* ps = smf + 4 * chunk;
+    double* x = K.x;
+    const bool jac = K.jacobi != 0, linf = K.norm_inf != 0;
+    const bool sym_box = K.stride_y > 0 && K.symmetric;
+    bool ok = true;
+    int its = 0;
+
+    for (int i = threadIdx.x; i < m; i += THREADS) {
+        const int c = c0 + i;
+        for (int s = 0; s < ncoef; ++s) {
+            const int src = sym_box ? (2 * s + 1) : s;
+            __stcg(val32 + (int64_t)s * n + c, (float)__ldg(K.val + (int64_t)src * n + c));
+        }
+        __stcg(diag32 + c, (float)__ldg(K.diag + c));
+        ivs[i] = (float)inv_diag(K.diag, c, jac);
+    }
+    if (threadIdx.x == 0) {
+        st.its = 0;
+        st.converged = 0;
+        st.status = GF_MAX_ITER;
+        st.done = 0;
+    }
+    bool pending = false;
+    for (int cycle = 0; ok && cycle <= K.max_outer; ++cycle) {
+        {  // fold the pending correction, then the true residual in FP64
+            double loc[2] = {0.0, 0.0};
+            if (pending) {
+                for (int i = threadIdx.x; i < m; i += THREADS) x[c0 + i] = x[c0 + i] + (double)ds[i];
+                pending = false;
+            }
+            // The barrier also publishes x and (cycle 0) the FP32 matrix.
+            double dummy[1] = {0.0};
+            ok = grid_reduce<1, THREADS>(ctl, partials, dummy, 0u);
+            if (!ok) break;
+            auto gx = [&](int i) { return __ldcg(x + i); };
+            for (int i = threadIdx.x; i < m; i += THREADS) {
+                const int c = c0 + i;
+                const double ax = rows64.apply(c, __ldg(K.diag + c), gx);
+                const double rk = __ldg(K.rhs + c) - ax;
+                const float r32 = (float)rk;
+                const float z32 = ivs[i] * r32;
+                rs[i] = r32;
+                ds[i] = 0.0f;
+                ps[i] = 0.0f;
+                qs[i] = 0.0f;
+                __stcg(z + c, z32);
+                loc[0] = norm_acc(loc[0], rk, linf);
+                loc[1] += (double)r32 * (double)z32;
+            }
+            ok = grid_reduce<2, THREADS>(ctl, partials, loc, linf ? 1u : 0u);
+            if (!ok) break;
+            if (threadIdx.x == 0) {
+                const double nr = norm_fin(loc[0], linf);
+                if (cycle == 0) {
+                    st.r0 = nr;
+                    st.thresh = fmax(K.atol, K.rtol * nr);
+                }
+                st.final = nr;
+                if (nr < st.thresh) {
+                    st.done = 1;
+                    st.converged = 1;
+                    st.status = GF_OK;
+                } else if (!isfinite(nr)) {
+                    st.done = 1;
+                    st.status = GF_NONFINITE;
+                }
+                st.rz_old = loc[1];
+                st.beta = 0.0;
+                s_target = fmax(K.inner_eta * nr, (K.inner_margin > 0.0 ? K.inner_margin : 0.5) * st.thresh);
+                s_cycle_done = 0;
+            }
+            __syncthreads();
+            if (st.done || cycle == K.max_outer || its >= K.max_iter) break;
+        }
+        pending = true;
+        while (ok && !s_cycle_done && its < K.max_iter) {
+            ++its;
+            {  // w = A z; p = z + beta p; q = w + beta q; p . q
+                const float beta = (float)st.beta;
+                double loc[1] = {0.0};
+                // Plain (L1-cacheable) loads: see pcg1_smem_body.
+                auto gz = [&](int j) { return z[j]; };
+                for (int i0 = threadIdx.x; i0 < m; i0 += U * THREADS) {
+                    float zc[U], w[U];
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const int i = i0 + u * THREADS;
+                        if (i < m) {
+                            const int c = c0 + i;
+                            zc[u] = z[c];
+                            w[u] = rows32.apply(c, __ldcg(diag32 + c), gz);
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const int i = i0 + u * THREADS;
+                        if (i < m) {
+                            const float pk = zc[u] + ps[i] * beta;
+                            const float qk = w[u] + qs[i] * beta;
+                            ps[i] = pk;
+                            qs[i] = qk;
+                            loc[0] += (double)pk * (double)qk;
+                        }
+                    }
+                }
+                ok = grid_reduce<1, THREADS>(ctl, partials, loc, 0u);
+                if (!ok) break;
+                if (threadIdx.x == 0) st.alpha = st.rz_old / loc[0];
+                __syncthreads();
+            }
+            {  // d += alpha p; r -= alpha q; z = M r; |r|, r.z (own cells)
+                const float alpha = (float)st.alpha;
+                double loc[2] = {0.0, 0.0};
+                for (int i = threadIdx.x; i < m; i += THREADS) {
+                    ds[i] = ds[i] + alpha * ps[i];
+                    const float rk = rs[i] - alpha * qs[i];
+                    const float zk = ivs[i] * rk;
+                    rs[i] = rk;
+                    __stcg(z + c0 + i, zk);
+                    loc[0] = norm_acc(loc[0], (double)rk, linf);
+                    loc[1] += (double)rk * (double)zk;
+                }
+                ok = grid_reduce<2, THREADS>(ctl, partials, loc, linf ? 1u : 0u);
+                if (!ok) break;
+                if (threadIdx.x == 0) {
+                    const double nr = norm_fin(loc[0], linf);
+                    if (!(nr >= s_target) || !isfinite(nr)) {
+                        s_cycle_done = 1;
+                    } else {
+                        st.beta = loc[1] / st.rz_old;
+                        st.rz_old = loc[1];
+                    }
+                }
+                __syncthreads();
+            }
+        }
+    }
+    if (ok && pending) {
+        // iteration budget spent inside a cycle: keep its correction
+        for (int i = threadIdx.x; i < m; i += THREADS) x[c0 + i] = x[c0 + i] + (double)ds[i];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        double* o = K.stats;
+        o[0] = st.r0;
+        o[1] = st.final;
+        o[2] = its;
+        o[3] = st.converged;
+        o[4] = ok ? st.status : GF_ERR_TIMEOUT;
+    }
+}
+
+template <bool SYM, int U>
+__global__ void __launch_bounds__(1024, 1) k_pcg1_mixed_qrec_box(gf_krylov_t K, int chunk) {
+    BoxRows<double, SYM, false, int> rows64{K.val, (int)K.n, (int)K.stride_y, (int)K.stride_z};
+    BoxRows<float, SYM, SYM, int> rows32{nullptr, (int)K.n, (int)K.stride_y, (int)K.stride_z};
+    pcg1_mixed_qrec_body<1024, U, 1>(K, rows64, rows32, SYM ? 3 : 6, chunk);
+}
+
+template <int WIDTH, int U>
+__global__ void __launch_bounds__(1024, 1) k_pcg1_mixed_qrec_ell(gf_krylov_t K, int chunk) {
+    EllRows<double, WIDTH, int> rows64{K.val, K.nbr, (int)K.n, K.width};
+    EllRows<float, WIDTH, int> rows32{nullptr, K.nbr, (int)K.n, K.width};
+    pcg1_mixed_qrec_body<1024, U, 1>(K, rows64, rows32, K.width, chunk);
+}
+
 // Tile length for the staged kernel (0: the system does not qualify).
 static int staged_tile(const gf_krylov_t* k) {
     if (!k->symmetric || k->stride_y < 1 || (k->n & 1)) return 0;
@@ -2523,8 +2724,20 @@ static int launch_smem(const gf_krylov_t* k, void* stream, int threads) {
     return GF_ERR_INVALID;
 }
 
-// The q-recurrence form (FP64, 1024 threads): r, q and p in shared memory.
+template <int U>
+static const void* mixed_qrec_kernel(const gf_krylov_t* k) {
+    if (k->stride_y > 0)
+        return k->symmetric ? (const void*)k_pcg1_mixed_qrec_box<true, U> : (const void*)k_pcg1_mixed_qrec_box<false, U>;
+    return k->width == 6 ? (const void*)k_pcg1_mixed_qrec_ell<6, U> : (const void*)k_pcg1_mixed_qrec_ell<0, U>;
+}
+
+// The q-recurrence forms (1024 threads): FP64 keeps r, q and p in shared
+// memory (3 doubles a cell), FP32-inner r, q, p, d and the inverse (5 floats).
 static int launch_qrec(const gf_krylov_t* k, void* stream, int unroll) {
+    if (k->mixed) {
+        const void* kern = unroll == 2 ? mixed_qrec_kernel<2>(k) : mixed_qrec_kernel<1>(k);
+        return launch_smem_arrays(k, stream, 1024, 5, sizeof(float), kern);
+    }
     const void* kern = unroll == 2 ? qrec_kernel<2>(k) : qrec_kernel<1>(k);
     return launch_smem_arrays(k, stream, 1024, 3, sizeof(double), kern);
 }
@@ -2661,8 +2874,12 @@ int gf_pcg_solve(const gf_krylov_t* k, void* stream) {
             const int st = launch_smem(k, stream, k->variant == kSmemVariant ? 512 : 1024);
             if (st != GF_ERR_INVALID) return st;
         }
+        if (k->variant == kQrecVariant || k->variant == kQrecVariant + 1) {
+            const int st = launch_qrec(k, stream, k->variant == kQrecVariant ? 1 : 2);
+            if (st != GF_ERR_INVALID) return st;
+        }
         if (box) {
-            // Variants 5-7 that do not qualify fall back to 512-thread blocks.
+            // Variants 5-9 that do not qualify fall back to 512-thread blocks.
             const int v = (k->variant >= 0 && k->variant < kBoxVariants) ? k->variant
                           : (k->variant >= kStagedVariant ? 2 : 0);
             const BoxVariant bv = k->symmetric ? box_kernel<true, true>(v) : box_kernel<true, false>(v);

@@ -29,7 +29,7 @@ from gridfoam_b200.meta.config import PrecisionType, PreconditionerType, SolverC
 
 # Variants 0-7 differ only in launch shape and memory placement (their
 # iterates differ by the order of the dot-product partial sums); 8 and 9
-# form q = A p by recurrence (FP64 only: mixed solves fall back to 2).
+# form q = A p by recurrence.
 N_VARIANTS = 10
 VARIANTS = {
     0: "256 threads x 1 cell/pass",
@@ -40,8 +40,8 @@ VARIANTS = {
     5: "512 threads, shared-memory tiles by bulk async copy (symmetric FP64 only)",
     6: "512 threads, own-cell vectors resident in shared memory (up to ~1.3M cells)",
     7: "1024 threads, own-cell vectors resident in shared memory (up to ~1.3M cells)",
-    8: "1024 threads, shared-memory vectors, q = A z + beta q recurrence, 1 cell/pass (FP64)",
-    9: "1024 threads, shared-memory vectors, q = A z + beta q recurrence, 2 cells/pass (FP64)",
+    8: "1024 threads, shared-memory vectors, q = A z + beta q recurrence, 1 cell/pass",
+    9: "1024 threads, shared-memory vectors, q = A z + beta q recurrence, 2 cells/pass",
 }
 
 _LOCK = threading.Lock()

@@ -40,16 +40,16 @@ def default_variant(n: int, mixed: bool, symmetric: bool, box: bool = True) -> i
     """CG launch shape by system size, from fixed-iteration timings on B200
     (``python -m gridfoam_b200.solvers.autotune``).  Below ~128K cells
     256-thread blocks, where the grid barrier dominates; then, up to ~1.3M
-    cells, kernels that keep each block's own-cell vectors in shared memory
-    (1024-thread blocks, box or ELL rows): for FP64 the form that updates
-    q = A p by recurrence and gathers z alone (15.8 against 20.4 us an
-    iteration at 1M cells), for FP32-inner solves the plain one; above that
-    the shared-memory tiled kernel for symmetric FP64 boxes, else 512-thread
-    blocks."""
+    cells, the kernels that keep each block's own-cell vectors in shared
+    memory and form q = A p by recurrence, gathering z alone (1024-thread
+    blocks, box or ELL rows; at 1M cells 15.7 against 20.4 us an FP64
+    iteration for the plain shared-memory form, 12.0 against 13.2 FP32);
+    above that the shared-memory tiled kernel for symmetric FP64 boxes,
+    else 512-thread blocks."""
     if n < 131072:
         return 0
     if n <= 1300000:
-        return 7 if mixed else 8
+        return 8
     return 5 if symmetric and box and not mixed else 2
 
 

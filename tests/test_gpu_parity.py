@@ -212,7 +212,7 @@ def test_cavity32_against_oracle():
 
 
 @pytest.mark.parametrize("layout", ["box", "ell"])
-@pytest.mark.parametrize("variant", [None, 6, 7])
+@pytest.mark.parametrize("variant", [None, 6, 7, 8, 9])
 def test_mixed_precision_pcg_meets_fp64_criterion(variant, layout):
     """FP32 inner CG inside FP64 refinement reaches the same FP64 true-residual
     threshold as the FP64 solver, and its solution agrees with the FP64
@@ -255,7 +255,7 @@ def _check_mixed(A, rhs, x32, s32, s64, tol, rel_tol):
     assert abs(s32[0].initial_residual - s64[0].initial_residual) <= 1e-12 * s64[0].initial_residual
 
 
-@pytest.mark.parametrize("variant", [None, 7])
+@pytest.mark.parametrize("variant", [None, 7, 8])
 def test_box_layout_matches_ell_layout(variant):
     """On a uniform box, CG with implicit neighbours (symmetric three-array
     coefficient reads) gives the same solve as the generic ELL path, in the
