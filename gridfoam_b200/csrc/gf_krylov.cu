@@ -69,12 +69,43 @@ __device__ __forceinline__ double inv_diag(const double* __restrict__ diag, int6
 
 // Grid-wide reduction of NV values per thread (sum, or max where maxmask
 // has the bit set), fused with the grid barrier.  Returns false when the
-// barrier wait expired or another block reported an error.
-template <int NV, int THREADS = kKThreads>
-__device__ bool grid_reduce(KCtl* ctl, double* partials, double (&v)[NV], unsigned maxmask) {
-    __shared__ double sm1[NV * 32];
-    __shared__ double sm2[NV * 32];
-    __shared__ int s_err;
+// barrier wait expired or another block reported an error.  Every block
+// sums the per-block partials in the same fixed order, so all blocks hold
+// the same bits.  The cost is in the CTA barriers, the shuffle trees and
+// the L2 round trips; an empty reduction of 148 x 1024 threads measured
+// 2.26 / 2.83 / 3.42 us (NV = 1 / 2 / 3) with grid_reduce_all and 2.07 /
+// 2.75 us (NV = 1 / 3) with grid_reduce_w0, against 1.33 us for the bare
+// counter barrier.
+constexpr int kW0Loads = 5;
+constexpr int kW0Blocks = 32 * kW0Loads;
+
+__device__ __forceinline__ double comb(double x, double y, bool mx) { return mx ? nmax(x, y) : x + y; }
+
+// Staging of the partials in grid_reduce_w0 (warp 0 only, between its wait
+// and the CTA barrier that ends the reduction).
+__shared__ __align__(16) double g_stage[3 * kW0Blocks + 2];
+
+// Reduction scratch, one per NV, shared by the two forms.
+template <int NV>
+struct RedBuf {
+    double sm1[NV * 32];
+    double sm2[NV * 32];
+    int err;
+};
+template <int NV>
+__device__ __forceinline__ RedBuf<NV>& red_buf() {
+    __shared__ RedBuf<NV> b;
+    return b;
+}
+
+// All threads load the partials: the general form (any block size, any
+// grid, any NV).
+template <int NV, int THREADS>
+__device__ bool grid_reduce_all(KCtl* ctl, double* partials, double (&v)[NV], unsigned maxmask) {
+    RedBuf<NV>& rb = red_buf<NV>();
+    double* sm1 = rb.sm1;
+    double* sm2 = rb.sm2;
+    int& s_err = rb.err;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
     for (int j = 0; j < NV; ++j) {
@@ -185,6 +216,136 @@ __device__ bool grid_reduce(KCtl* ctl, double* partials, double (&v)[NV], unsign
         v[j] = x;
     }
     return true;
+}
+
+// 1024-thread blocks on grids of at most kW0Blocks (one block an SM) and a
+// 16-byte aligned workspace: one warp on the critical path after the warp
+// sums.  Warp 0 forms the block partial, thread 0 publishes it, warp 0
+// waits, copies every partial to shared memory with all copies in flight
+// and sums them in a fixed order; a second CTA barrier hands the result out
+// (grid_reduce_all: four CTA barriers, and every warp runs two more shuffle
+// trees).  The shuffle trees of the NV values are interleaved level by
+// level.
+template <int NV>
+__device__ bool grid_reduce_w0(KCtl* ctl, double* partials, double (&v)[NV], unsigned maxmask) {
+    RedBuf<NV>& rb = red_buf<NV>();
+    double* sm1 = rb.sm1;
+    double* sm2 = rb.sm2;
+    int& s_err = rb.err;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    double x[NV];
+#pragma unroll
+    for (int j = 0; j < NV; ++j) x[j] = v[j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int j = 0; j < NV; ++j) x[j] = comb(x[j], __shfl_xor_sync(0xffffffffu, x[j], o), (maxmask >> j) & 1u);
+    if (lane == 0)
+#pragma unroll
+        for (int j = 0; j < NV; ++j) sm1[j * 32 + warp] = x[j];
+    __syncthreads();
+    if (warp == 0) {
+        // Only warp 0 uses the epoch; lane 0 reads it (after the CTA barrier
+        // that follows barrier_init) and advances it after its wait.
+        const unsigned ep = __shfl_sync(0xffffffffu, lane == 0 ? g_epoch : 0u, 0);
+        double* part = partials + (ep & 1u) * (kPartials / 2);
+        // Block partial (0 is the identity of both: the max values are norms).
+#pragma unroll
+        for (int j = 0; j < NV; ++j) x[j] = lane < nw ? sm1[j * 32 + lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+            for (int j = 0; j < NV; ++j)
+                x[j] = comb(x[j], __shfl_xor_sync(0xffffffffu, x[j], o), (maxmask >> j) & 1u);
+        if (lane == 0) {
+#pragma unroll
+            for (int j = 0; j < NV; ++j) __stcg(part + (int64_t)blockIdx.x * NV + j, x[j]);
+            // The CTA barrier above orders the other warps' writes before
+            // this release (cumulativity).
+            arrive_release(&ctl->count);
+        }
+        __syncwarp();
+        {
+            // The whole warp polls (one request a poll).  Lane 0 polling
+            // alone with __nanosleep while the other lanes waited at a warp
+            // barrier left the blocks microseconds apart on leaving (CG
+            // iterations 40-60 % slower).
+            const unsigned long long target = (unsigned long long)(ep + 1u) * gridDim.x;
+            int err = 0;
+            long long it = 0;
+            while (true) {
+                const unsigned long long c = load_acquire(&ctl->count);
+                if (__all_sync(0xffffffffu, c >= target)) break;
+                __nanosleep(20);
+                ++it;
+                if ((it & 255) == 0 && __any_sync(0xffffffffu, vload(&ctl->error) != 0)) {
+                    err = 1;
+                    break;
+                }
+                if (it > kSpinLimit) {
+                    if (lane == 0) atomicExch(&ctl->error, 1);
+                    err = 1;
+                    break;
+                }
+            }
+            // A block that gave up raised the flag; the others see it at
+            // their next wait (checked every 256 polls) and leave as well.
+            if (lane == 0) {
+                s_err = err;
+                g_epoch = ep + 1u;
+            }
+        }
+        __syncwarp();
+        if (!s_err) {
+            // All partials in flight at once through 16-byte L2 copies into
+            // shared memory (register loads would be serialised in the
+            // register-capped CG kernels).  The last copy may read one
+            // double past the partials, inside the same half.
+            const int nd = (int)gridDim.x * NV;
+            for (int q = lane; 2 * q < nd; q += 32) {
+                const unsigned dst = (unsigned)__cvta_generic_to_shared(g_stage + 2 * q);
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(part + 2 * q) : "memory");
+            }
+            asm volatile("cp.async.commit_group;\n\tcp.async.wait_all;" ::: "memory");
+            __syncwarp();
+#pragma unroll
+            for (int j = 0; j < NV; ++j) x[j] = lane < (int)gridDim.x ? g_stage[lane * NV + j] : 0.0;
+#pragma unroll
+            for (int k = 1; k < kW0Loads; ++k) {
+                const int b = lane + 32 * k;
+                if (b < (int)gridDim.x)
+#pragma unroll
+                    for (int j = 0; j < NV; ++j) x[j] = comb(x[j], g_stage[b * NV + j], (maxmask >> j) & 1u);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                for (int j = 0; j < NV; ++j)
+                    x[j] = comb(x[j], __shfl_xor_sync(0xffffffffu, x[j], o), (maxmask >> j) & 1u);
+            if (lane == 0)
+#pragma unroll
+                for (int j = 0; j < NV; ++j) sm2[j] = x[j];
+        }
+    }
+    __syncthreads();
+    // No trailing barrier: sm1 is read only before the barrier above (the
+    // next call writes it before its first one), and sm2 is next written
+    // after the next call's first barrier, which every thread reaches only
+    // after reading it here.
+    if (s_err) return false;
+#pragma unroll
+    for (int j = 0; j < NV; ++j) v[j] = sm2[j];
+    return true;
+}
+
+template <int NV, int THREADS = kKThreads>
+__device__ __forceinline__ bool grid_reduce(KCtl* ctl, double* partials, double (&v)[NV], unsigned maxmask) {
+    if constexpr (THREADS == 1024 && NV <= 3) {
+        // (the 16-byte copies of the partials need a 16-byte aligned workspace)
+        if (gridDim.x <= (unsigned)kW0Blocks && (reinterpret_cast<uintptr_t>(partials) & 15u) == 0)
+            return grid_reduce_w0<NV>(ctl, partials, v, maxmask);
+    }
+    return grid_reduce_all<NV, THREADS>(ctl, partials, v, maxmask);
 }
 
 // y_k(c) = diag(c) * g(k, c) + sum_s val(s, c) * g(k, nbr(s, c)); WIDTH > 0
@@ -421,6 +582,16 @@ struct EllRows {
         }
         return acc;
     }
+    // Smallest and largest cell index that apply(c) reads, folded into lo/hi.
+    __device__ __forceinline__ void span(I c, I& lo, I& hi) const {
+        lo = c < lo ? c : lo;
+        hi = c > hi ? c : hi;
+        for (int s = 0; s < w; ++s) {
+            const I j = __ldg(nbr + s * n + c);
+            lo = j < lo ? j : lo;
+            hi = j > hi ? j : hi;
+        }
+    }
 };
 
 template <typename T, bool SYM, bool COMPACT, typename I = int64_t>
@@ -456,6 +627,16 @@ struct BoxRows {
             acc += ap[a] * g(ip[a]);
         }
         return acc;
+    }
+    __device__ __forceinline__ void span(I c, I& lo, I& hi) const {
+        const I st[3] = {1, sy, sz};
+        lo = c < lo ? c : lo;
+        hi = c > hi ? c : hi;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            if (c >= st[a] && c - st[a] < lo) lo = c - st[a];
+            if (c + st[a] < n && c + st[a] > hi) hi = c + st[a];
+        }
     }
 };
 
@@ -1022,6 +1203,10 @@ constexpr int kSmemVariant = 6;
 // q-recurrence CG with shared-memory-resident vectors (pcg1_qrec_body),
 // 1024-thread blocks, one (8) or two (9) cells per thread per gather pass.
 constexpr int kQrecVariant = 8;
+// Single-reduction CG with a halo sync (pcg1_halo_body), 1024-thread
+// blocks, one (10) or two (11) cells per thread per gather pass; falls back
+// to variant 8 when its four vectors do not fit.
+constexpr int kHaloVariant = 10;
 
 template <bool MIXED, bool SYM, int THREADS, int U>
 static BoxVariant box_variant() {
@@ -1801,6 +1986,262 @@ template <int WIDTH, int THREADS, int U>
 __global__ void __launch_bounds__(THREADS, 1) k_pcg1_qrec_ell(gf_krylov_t K, int chunk) {
     EllRows<double, WIDTH, int> rows{K.val, K.nbr, (int)K.n, K.width};
     pcg1_qrec_body<THREADS, U, 2>(K, rows, chunk);
+}
+
+// ---------------------------------------------------------------------------
+// Single-reduction CG with shared-memory-resident vectors and a halo sync.
+// The recurrences are those of pcg1_sr_body (Chronopoulos and Gear): with
+// z = M r and w = A z, gamma = r.z, delta = w.z, beta = gamma / gamma_old,
+// alpha = gamma / (delta - beta gamma / alpha_old), p = z + beta p,
+// q = w + beta q (q = A p), x += alpha p, r -= alpha q.  An iteration is two
+// passes: gather w = A z and reduce (|r|, gamma, delta) in ONE grid
+// reduction (|r| and gamma of the previous update ride along with delta),
+// then update the own cells and publish the new z.  The gather of the next
+// iteration needs the new z of the neighbouring blocks only, so the second
+// synchronisation is point to point: each block waits for the blocks that
+// hold the cells its rows read (found once, from the row structure), not
+// for the whole grid.  A block cannot overwrite z before every block has
+// finished reading it: the overwrite follows the grid reduction, which
+// follows every block's gather.  The stopping test sees |r_k| one gather
+// later than pcg1_qrec_body; iteration count, statistics and final x are
+// those of a PCG run (one extra gather at the end, no extra update).  Each
+// block keeps r, p, q and w of its cells in shared memory (4 doubles a
+// cell) and updates its cells of x in place in global memory.
+
+// Halo flags: one 64-bit epoch per block, one per 128-byte line (flags of
+// neighbouring blocks sharing a line cost ~1.7 us an iteration at 262K
+// cells), after z and the Jacobi inverse in the workspace.
+constexpr int64_t kHaloFlagStride = 16;
+constexpr int64_t kHaloFlagDoubles = kMaxBlocks * kHaloFlagStride;
+
+// Publish epoch ep for this block, then wait (bounded, like grid_reduce)
+// until blocks blo..bhi have published it.  The CTA barrier before the
+// release makes it cumulative over the whole block's writes; the acquires
+// and the CTA barrier after them order every thread's later reads.
+__device__ bool halo_sync(KCtl* ctl, unsigned long long* flags, unsigned long long ep, int blo, int bhi) {
+    __syncthreads();
+    if (threadIdx.x == 0)
+        asm volatile("fence.acq_rel.gpu;\n\tst.relaxed.gpu.global.u64 [%0], %1;" ::"l"(
+                         flags + kHaloFlagStride * blockIdx.x),
+                     "l"(ep)
+                     : "memory");
+    int err = 0;
+    for (int b = blo + (int)threadIdx.x; b <= bhi && !err; b += blockDim.x) {
+        if (b == (int)blockIdx.x) continue;
+        long long it = 0;
+        while (load_acquire(flags + kHaloFlagStride * b) < ep) {
+            __nanosleep(20);
+            ++it;
+            if ((it & 255) == 0 && vload(&ctl->error) != 0) {
+                err = 1;
+                break;
+            }
+            if (it > kSpinLimit) {
+                atomicExch(&ctl->error, 1);
+                err = 1;
+                break;
+            }
+        }
+    }
+    return __syncthreads_or(err) == 0;
+}
+
+template <int THREADS, int U, int V, class Rows>
+__device__ void pcg1_halo_body(const gf_krylov_t& K, const Rows& rows, int chunk) {
+    __shared__ CgState st;
+    __shared__ int s_lo, s_hi;
+    extern __shared__ __align__(16) double sm[];
+    KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
+    barrier_init();
+    double* partials = K.work + kCtlDoubles;
+    double* vec = partials + kPartials;
+    const int n = (int)K.n;
+    double* z = vec;
+    double* inv = vec + n;
+    unsigned long long* flags = reinterpret_cast<unsigned long long*>(vec + 2 * (int64_t)n);
+    double* x = K.x;
+    const int c0 = blockIdx.x * chunk;
+    const int c1 = c0 + chunk < n ? c0 + chunk : n;
+    const int m = c1 > c0 ? c1 - c0 : 0;
+    double* rs = sm;
+    double* ps = sm + chunk;
+    double* qs = sm + 2 * chunk;
+    double* ws = sm + 3 * chunk;
+    const bool jac = K.jacobi != 0, linf = K.norm_inf != 0;
+    if (threadIdx.x == 0) {
+        s_lo = n;
+        s_hi = -1;
+        // Visible to every block after the first grid reduction below.
+        flags[kHaloFlagStride * blockIdx.x] = 0ull;
+    }
+    __syncthreads();
+    bool ok = true;
+    {  // r = b - A x, z = M r, p = q = 0; |r| and r.z; the cells the rows read
+        double loc[2] = {0.0, 0.0};
+        int lo = n, hi = -1;
+        auto gx = [&](int i) { return __ldcg(x + i); };
+        for (int i = threadIdx.x; i < m; i += THREADS) {
+            const int c = c0 + i;
+            const double ax = rows.apply(c, __ldg(K.diag + c), gx);
+            const double rk = __ldg(K.rhs + c) - ax;
+            const double iv = inv_diag(K.diag, c, jac);
+            const double zk = iv * rk;
+            rows.span(c, lo, hi);
+            rs[i] = rk;
+            ps[i] = 0.0;
+            qs[i] = 0.0;
+            inv[c] = iv;
+            __stcg(z + c, zk);
+            loc[0] = norm_acc(loc[0], rk, linf);
+            loc[1] += rk * zk;
+        }
+        lo = __reduce_min_sync(0xffffffffu, lo);
+        hi = __reduce_max_sync(0xffffffffu, hi);
+        if ((threadIdx.x & 31) == 0) {
+            atomicMin(&s_lo, lo);
+            atomicMax(&s_hi, hi);
+        }
+        ok = grid_reduce<2, THREADS>(ctl, partials, loc, linf ? 1u : 0u);
+        if (threadIdx.x == 0) {
+            const double r0 = norm_fin(loc[0], linf);
+            st.r0 = r0;
+            st.final = r0;
+            st.thresh = fmax(K.atol, K.rtol * r0);
+            st.rz_old = loc[1];
+            st.alpha = 1.0;
+            st.beta = 0.0;
+            st.its = 0;
+            st.converged = 0;
+            st.status = GF_MAX_ITER;
+            st.done = 0;
+            if (r0 < st.thresh) {
+                st.done = 1;
+                st.converged = 1;
+                st.status = GF_OK;
+            } else if (!isfinite(r0)) {
+                st.done = 1;
+                st.status = GF_NONFINITE;
+            }
+            // Blocks holding the cells this block's rows read (itself when it has none).
+            s_lo = m > 0 ? s_lo / chunk : (int)blockIdx.x;
+            s_hi = m > 0 ? s_hi / chunk : (int)blockIdx.x;
+        }
+        __syncthreads();
+    }
+    double rn = 0.0, gm = 0.0;  // this thread's |r| and r.z of the last update
+    for (int it = 1; ok && !st.done && K.max_iter > 0; ++it) {
+        {  // w = A z; delta = w.z; one reduction with |r| and gamma of the last update
+            double loc[3] = {rn, gm, 0.0};
+            auto gz = [&](int j) { return z[j]; };
+            for (int i0 = threadIdx.x; i0 < m; i0 += U * THREADS) {
+                double zc[U], w[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int i = i0 + u * THREADS;
+                    if (i < m) {
+                        const int c = c0 + i;
+                        zc[u] = z[c];
+                        w[u] = rows.apply(c, __ldg(K.diag + c), gz);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int i = i0 + u * THREADS;
+                    if (i < m) {
+                        ws[i] = w[u];
+                        loc[2] += w[u] * zc[u];
+                    }
+                }
+            }
+            ok = grid_reduce<3, THREADS>(ctl, partials, loc, linf ? 1u : 0u);
+            if (!ok) break;
+            if (threadIdx.x == 0) {
+                if (it > 1) {
+                    const double fin = norm_fin(loc[0], linf);
+                    st.final = fin;
+                    if (fin < st.thresh) {
+                        st.done = 1;
+                        st.converged = 1;
+                        st.its = it - 1;
+                        st.status = GF_OK;
+                    } else if (!isfinite(fin)) {
+                        st.done = 1;
+                        st.its = it - 1;
+                        st.status = GF_NONFINITE;
+                    } else if (it - 1 >= K.max_iter) {
+                        st.done = 1;
+                        st.its = K.max_iter;
+                    }
+                }
+                if (!st.done) {
+                    const double g = it > 1 ? loc[1] : st.rz_old;
+                    const double b = it > 1 ? g / st.rz_old : 0.0;
+                    st.alpha = g / (it > 1 ? loc[2] - b * g / st.alpha : loc[2]);
+                    st.beta = b;
+                    st.rz_old = g;
+                }
+            }
+            __syncthreads();
+            if (st.done) break;
+        }
+        {  // p = z + beta p; q = w + beta q; x += alpha p; r -= alpha q; z = M r
+            // The own z is recomputed as inv r: the bits it was stored with.
+            const double alpha = st.alpha, beta = st.beta;
+            rn = 0.0;
+            gm = 0.0;
+            for (int i0 = threadIdx.x; i0 < m; i0 += V * THREADS) {
+                double xv[V], iv[V];
+#pragma unroll
+                for (int u = 0; u < V; ++u) {
+                    const int i = i0 + u * THREADS;
+                    if (i < m) {
+                        const int c = c0 + i;
+                        xv[u] = __ldcg(x + c);
+                        iv[u] = inv[c];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < V; ++u) {
+                    const int i = i0 + u * THREADS;
+                    if (i < m) {
+                        const int c = c0 + i;
+                        const double pk = iv[u] * rs[i] + ps[i] * beta;
+                        const double qk = ws[i] + qs[i] * beta;
+                        ps[i] = pk;
+                        qs[i] = qk;
+                        __stcg(x + c, xv[u] + alpha * pk);
+                        const double rk = rs[i] - alpha * qk;
+                        const double zk = iv[u] * rk;
+                        rs[i] = rk;
+                        __stcg(z + c, zk);
+                        rn = norm_acc(rn, rk, linf);
+                        gm += rk * zk;
+                    }
+                }
+            }
+            ok = halo_sync(ctl, flags, (unsigned long long)it, s_lo, s_hi);
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        double* o = K.stats;
+        o[0] = st.r0;
+        o[1] = st.final;
+        o[2] = st.done ? st.its : K.max_iter;
+        o[3] = st.converged;
+        o[4] = ok ? st.status : GF_ERR_TIMEOUT;
+    }
+}
+
+template <bool SYM, int U>
+__global__ void __launch_bounds__(1024, 1) k_pcg1_halo_box(gf_krylov_t K, int chunk) {
+    BoxRows<double, SYM, false, int> rows{K.val, (int)K.n, (int)K.stride_y, (int)K.stride_z};
+    pcg1_halo_body<1024, U, 2>(K, rows, chunk);
+}
+
+template <int WIDTH, int U>
+__global__ void __launch_bounds__(1024, 1) k_pcg1_halo_ell(gf_krylov_t K, int chunk) {
+    EllRows<double, WIDTH, int> rows{K.val, K.nbr, (int)K.n, K.width};
+    pcg1_halo_body<1024, U, 2>(K, rows, chunk);
 }
 
 // ---------------------------------------------------------------------------
@@ -2742,6 +3183,25 @@ static int launch_qrec(const gf_krylov_t* k, void* stream, int unroll) {
     return launch_smem_arrays(k, stream, 1024, 3, sizeof(double), kern);
 }
 
+template <int U>
+static const void* halo_kernel(const gf_krylov_t* k) {
+    if (k->stride_y > 0)
+        return k->symmetric ? (const void*)k_pcg1_halo_box<true, U> : (const void*)k_pcg1_halo_box<false, U>;
+    return k->width == 6 ? (const void*)k_pcg1_halo_ell<6, U> : (const void*)k_pcg1_halo_ell<0, U>;
+}
+
+// FP64 single-reduction form: r, p, q and w in shared memory (4 doubles a
+// cell), the halo flags after z and the inverse in the workspace; the
+// q-recurrence form (variant 8) when either does not fit.
+static int launch_halo(const gf_krylov_t* k, void* stream, int unroll) {
+    if (k->work_len >= kHeader + 2 * k->n + kHaloFlagDoubles) {
+        const void* kern = unroll == 2 ? halo_kernel<2>(k) : halo_kernel<1>(k);
+        const int st = launch_smem_arrays(k, stream, 1024, 4, sizeof(double), kern);
+        if (st != GF_ERR_INVALID) return st;
+    }
+    return launch_qrec(k, stream, 1);
+}
+
 static int launch_smem_arrays(const gf_krylov_t* k, void* stream, int threads, int narr, size_t elem,
                               const void* kern) {
     const char* what = "gf_pcg_solve";
@@ -2874,8 +3334,8 @@ int gf_pcg_solve(const gf_krylov_t* k, void* stream) {
             const int st = launch_smem(k, stream, k->variant == kSmemVariant ? 512 : 1024);
             if (st != GF_ERR_INVALID) return st;
         }
-        if (k->variant == kQrecVariant || k->variant == kQrecVariant + 1) {
-            const int st = launch_qrec(k, stream, k->variant == kQrecVariant ? 1 : 2);
+        if (k->variant >= kQrecVariant && k->variant <= kHaloVariant + 1) {
+            const int st = launch_qrec(k, stream, (k->variant - kQrecVariant) % 2 == 0 ? 1 : 2);
             if (st != GF_ERR_INVALID) return st;
         }
         if (box) {
@@ -2906,6 +3366,10 @@ int gf_pcg_solve(const gf_krylov_t* k, void* stream) {
             }
             if (k->variant == kQrecVariant || k->variant == kQrecVariant + 1) {
                 const int st = launch_qrec(k, stream, k->variant == kQrecVariant ? 1 : 2);
+                if (st != GF_ERR_INVALID) return st;
+            }
+            if (k->variant == kHaloVariant || k->variant == kHaloVariant + 1) {
+                const int st = launch_halo(k, stream, k->variant == kHaloVariant ? 1 : 2);
                 if (st != GF_ERR_INVALID) return st;
             }
             if (box && k->variant == kStagedVariant) {

@@ -30,7 +30,7 @@ from gridfoam_b200.meta.config import PrecisionType, PreconditionerType, SolverC
 # Variants 0-7 differ only in launch shape and memory placement (their
 # iterates differ by the order of the dot-product partial sums); 8 and 9
 # form q = A p by recurrence.
-N_VARIANTS = 10
+N_VARIANTS = 12
 VARIANTS = {
     0: "256 threads x 1 cell/pass",
     1: "256 threads x 2 cells/pass",
@@ -42,6 +42,8 @@ VARIANTS = {
     7: "1024 threads, own-cell vectors resident in shared memory (up to ~1.3M cells)",
     8: "1024 threads, shared-memory vectors, q = A z + beta q recurrence, 1 cell/pass",
     9: "1024 threads, shared-memory vectors, q = A z + beta q recurrence, 2 cells/pass",
+    10: "1024 threads, shared-memory vectors, one grid reduction and a halo sync per iteration, 1 cell/pass",
+    11: "1024 threads, shared-memory vectors, one grid reduction and a halo sync per iteration, 2 cells/pass",
 }
 
 _LOCK = threading.Lock()

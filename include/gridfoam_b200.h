@@ -209,7 +209,7 @@ typedef struct gf_krylov {
     int64_t stride_z;
     int32_t symmetric;    /* 1 (box only): A is symmetric, only + slots read */
     int32_t block_cap;    /* > 0: at most this many persistent blocks (tuning) */
-    int32_t variant;      /* CG launch shape (0..7, see gf_krylov.cu) */
+    int32_t variant;      /* CG launch shape (0..11, see gf_krylov.cu) */
     int32_t single_reduction; /* 1 (FP64 CG, one system): Chronopoulos-Gear
                              CG, one grid reduction per iteration; needs the
                              kind-0 workspace (7 vectors) */

@@ -320,13 +320,14 @@ def test_single_reduction_cg_matches_pcg(layout):
     assert r < 1e-9 * s1.initial_residual
 
 
-@pytest.mark.parametrize("variant", [5, 6, 7, 8, 9])
+@pytest.mark.parametrize("variant", [5, 6, 7, 8, 9, 10, 11])
 @pytest.mark.parametrize("shape", [(24, 20, 28), (64, 64, 40), (7, 5, 6), (130, 3, 4)])
 def test_staged_box_cg_matches_register_kernel(shape, variant):
     """The shared-memory variants against the register kernel (variant 0):
     5 stages tiles by bulk async copy, 6/7 keep each block's own-cell
     vectors resident (512/1024 threads), 8/9 also form q = A p by
-    recurrence.  Same iteration count within one and
+    recurrence, 10/11 take one grid reduction and a halo sync with the
+    neighbouring blocks per iteration.  Same iteration count within one and
     the same solution to the stopping tolerance, on shapes with partial last
     tiles or chunks, odd strides and a y halo larger than a tile's x extent."""
     from gridfoam_b200.solvers.autotune import BoxSystem, _solver
@@ -385,7 +386,7 @@ def test_smem_resident_cg_fixed_iterations_match_register_kernel(variant, box):
     assert rel(xs[1], xs[0]) < 1e-11
 
 
-@pytest.mark.parametrize("variant", [6, 7, 8, 9])
+@pytest.mark.parametrize("variant", [6, 7, 8, 9, 10, 11])
 def test_smem_resident_cg_on_ell_layout(variant):
     """The shared-memory-resident CG through the general ELL rows (the
     octree path), against the register ELL kernel."""
@@ -403,6 +404,60 @@ def test_smem_resident_cg_on_ell_layout(variant):
     (x0, s0), (x1, s1) = out[0], out[variant]
     assert s0.converged and s1.converged
     assert abs(s0.iterations - s1.iterations) <= 1
+    assert rel(to_np(x1), to_np(x0)) < 1e-8
+
+
+@pytest.mark.parametrize("box", [True, False])
+@pytest.mark.parametrize("variant", [10, 11])
+def test_halo_cg_fixed_iterations_match_register_kernel(variant, box):
+    """Exactly 60 iterations (tolerances 0) of the single-reduction CG with
+    the halo sync against the register kernel: the same iterates up to the
+    rounding of alpha = gamma / (delta - beta gamma / alpha_old) instead of
+    gamma / p.Ap and of the partial-sum order."""
+    from gridfoam_b200.solvers.autotune import BoxSystem, _solver
+
+    sysm = BoxSystem(40, 36, 44, device=torch.device("cuda"))
+    if not box:
+        sysm.box_strides = None
+    xs = []
+    for v in (0, variant):
+        s = _solver(60, False, v)
+        x = torch.zeros_like(sysm.rhs)
+        st = s.solve_arrays(sysm, sysm.diag, sysm.val, sysm.rhs, x, symmetric=True)
+        assert st[0].iterations == 60 and st[0].status == "max_iter"
+        xs.append(to_np(x))
+    assert rel(xs[1], xs[0]) < 1e-9
+
+
+def test_halo_cg_on_scrambled_ell():
+    """A randomly renumbered system: every block's rows read cells of
+    nearly every other block, so each halo sync waits on ~all blocks (one
+    polling thread each).  Same iterations within one and the same solution
+    as the register kernel, mapped back to the original numbering."""
+    from gridfoam_b200.solvers.autotune import BoxSystem, _solver
+
+    sysm = BoxSystem(48, 40, 60, device=torch.device("cuda"))
+    sysm.box_strides = None
+    n = sysm.num_cells
+    g = torch.Generator(device="cpu").manual_seed(11)
+    perm = torch.randperm(n, generator=g).cuda()  # new -> old
+    inv = torch.empty_like(perm)
+    inv[perm] = torch.arange(n, device=perm.device)
+    nbr = sysm.dev["ell_nbr"].long()
+    sysm.dev["ell_nbr"] = inv[nbr[:, perm]].to(torch.int32).contiguous()
+    sysm.val = sysm.val[:, perm].contiguous()
+    sysm.diag = sysm.diag[perm].contiguous()
+    sysm.rhs = sysm.rhs[:, perm].contiguous()
+    out = {}
+    for v in (0, 10):
+        s = _solver(4000, False, v)
+        s.atol, s.rtol = 0.0, 1e-10
+        x = torch.zeros_like(sysm.rhs)
+        st = s.solve_arrays(sysm, sysm.diag, sysm.val, sysm.rhs, x, symmetric=True)
+        out[v] = (x.clone(), st[0])
+    (x0, s0), (x1, s1) = out[0], out[10]
+    assert s0.converged and s1.converged
+    assert abs(s0.iterations - s1.iterations) <= 1, (s0.iterations, s1.iterations)
     assert rel(to_np(x1), to_np(x0)) < 1e-8
 
 
@@ -492,7 +547,7 @@ def test_staged_assembly_matches_generic_kernel(name):
             assert torch.equal(x, y), field.name
 
 
-@pytest.mark.parametrize("variant", [8, 9])
+@pytest.mark.parametrize("variant", [8, 9, 10, 11])
 @pytest.mark.parametrize("box", [True, False])
 def test_qrec_cg_true_residual(variant, box):
     """The q-recurrence CG updates r from q = A z + beta q rather than from
