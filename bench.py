@@ -110,12 +110,12 @@ def pcg_bytes_per_iter(C: int, F: int) -> float:
 
 # Measured DRAM bytes (read + write) of the pressure CG kernel
 # (k_pcg1_qrec_box<1, 1024, 1>) on a 64x64x256 box, from two ncu captures of
-# fixed-length launches: 51.96 MB at 50 iterations, 182.87 MB at 400.  The
+# fixed-length launches: 51.98 MB at 50 iterations, 165.41 MB at 400.  The
 # global working set stays in the 126 MB L2, so a launch costs a one-time
 # read of its arrays plus the write-back of the x updated in place each
 # iteration.
-PCG_DRAM_BYTES_PER_ITER = (182874112 - 51962368) / 350
-PCG_DRAM_BYTES_PER_LAUNCH = 51962368 - 50 * PCG_DRAM_BYTES_PER_ITER
+PCG_DRAM_BYTES_PER_ITER = (165412096 - 51979264) / 350
+PCG_DRAM_BYTES_PER_LAUNCH = 51979264 - 50 * PCG_DRAM_BYTES_PER_ITER
 
 
 def pcg_bytes_setup(C: int, F: int) -> float:

@@ -1881,20 +1881,27 @@ __device__ void pcg1_qrec_body(const gf_krylov_t& K, const Rows& rows, int chunk
         }
         __syncthreads();
     }
+    // x += alpha p of an iteration is applied in the next iteration's gather
+    // pass (which reads the old p anyway), off the path between the two
+    // reductions; the same additions in the same order, so the same bits.
+    bool pending = false;
     for (int it = 1; ok && !st.done && it <= K.max_iter; ++it) {
-        {  // w = A z; p = z + beta p; q = w + beta q; p . q
+        {  // x += alpha_prev p; w = A z; p = z + beta p; q = w + beta q; p . q
             const double beta = st.beta;
+            const double alpha_prev = st.alpha;
+            const bool upd = pending;
             double loc[1] = {0.0};
             // Plain (L1-cacheable) loads: z is written only before the grid
             // barrier that precedes this pass (see pcg1_smem_body).
             auto gz = [&](int j) { return z[j]; };
             for (int i0 = threadIdx.x; i0 < m; i0 += U * THREADS) {
-                double zc[U], w[U];
+                double zc[U], w[U], xo[U];
 #pragma unroll
                 for (int u = 0; u < U; ++u) {
                     const int i = i0 + u * THREADS;
                     if (i < m) {
                         const int c = c0 + i;
+                        if (upd) xo[u] = __ldcg(x + c);
                         zc[u] = z[c];
                         w[u] = rows.apply(c, __ldg(K.diag + c), gz);
                     }
@@ -1903,7 +1910,9 @@ __device__ void pcg1_qrec_body(const gf_krylov_t& K, const Rows& rows, int chunk
                 for (int u = 0; u < U; ++u) {
                     const int i = i0 + u * THREADS;
                     if (i < m) {
-                        const double pk = zc[u] + ps[i] * beta;
+                        const double pold = ps[i];
+                        if (upd) __stcg(x + c0 + i, xo[u] + alpha_prev * pold);
+                        const double pk = zc[u] + pold * beta;
                         const double qk = w[u] + qs[i] * beta;
                         ps[i] = pk;
                         qs[i] = qk;
@@ -1911,30 +1920,29 @@ __device__ void pcg1_qrec_body(const gf_krylov_t& K, const Rows& rows, int chunk
                     }
                 }
             }
+            pending = false;
+            // alpha_prev is read above by every thread before this barrier.
             ok = grid_reduce<1, THREADS>(ctl, partials, loc, 0u);
             if (!ok) break;
             if (threadIdx.x == 0) st.alpha = st.rz_old / loc[0];
             __syncthreads();
+            pending = true;
         }
-        {  // x += alpha p; r -= alpha q; z = M r; |r|, r.z (own cells)
+        {  // r -= alpha q; z = M r; |r|, r.z (own cells); x follows next pass
             const double alpha = st.alpha;
             double loc[2] = {0.0, 0.0};
             for (int i0 = threadIdx.x; i0 < m; i0 += V * THREADS) {
-                double xv[V], iv[V];
+                double iv[V];
 #pragma unroll
                 for (int u = 0; u < V; ++u) {
                     const int i = i0 + u * THREADS;
-                    if (i < m) {
-                        xv[u] = __ldcg(x + c0 + i);
-                        iv[u] = inv[c0 + i];
-                    }
+                    if (i < m) iv[u] = inv[c0 + i];
                 }
 #pragma unroll
                 for (int u = 0; u < V; ++u) {
                     const int i = i0 + u * THREADS;
                     if (i < m) {
                         const int c = c0 + i;
-                        __stcg(x + c, xv[u] + alpha * ps[i]);
                         const double rk = rs[i] - alpha * qs[i];
                         const double zk = iv[u] * rk;
                         rs[i] = rk;
@@ -1965,6 +1973,10 @@ __device__ void pcg1_qrec_body(const gf_krylov_t& K, const Rows& rows, int chunk
             }
             __syncthreads();
         }
+    }
+    if (pending) {
+        const double alpha = st.alpha;
+        for (int i = threadIdx.x; i < m; i += THREADS) __stcg(x + c0 + i, __ldcg(x + c0 + i) + alpha * ps[i]);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         double* o = K.stats;
@@ -2129,17 +2141,23 @@ __device__ void pcg1_halo_body(const gf_krylov_t& K, const Rows& rows, int chunk
         __syncthreads();
     }
     double rn = 0.0, gm = 0.0;  // this thread's |r| and r.z of the last update
+    // x += alpha p of an update is applied in the next gather pass (as in
+    // pcg1_qrec_body): the same additions in the same order.
+    bool pending = false;
     for (int it = 1; ok && !st.done && K.max_iter > 0; ++it) {
-        {  // w = A z; delta = w.z; one reduction with |r| and gamma of the last update
+        {  // x += alpha p; w = A z; delta = w.z; one reduction with |r| and gamma of the last update
+            const double alpha_prev = st.alpha;
+            const bool upd = pending;
             double loc[3] = {rn, gm, 0.0};
             auto gz = [&](int j) { return z[j]; };
             for (int i0 = threadIdx.x; i0 < m; i0 += U * THREADS) {
-                double zc[U], w[U];
+                double zc[U], w[U], xo[U];
 #pragma unroll
                 for (int u = 0; u < U; ++u) {
                     const int i = i0 + u * THREADS;
                     if (i < m) {
                         const int c = c0 + i;
+                        if (upd) xo[u] = __ldcg(x + c);
                         zc[u] = z[c];
                         w[u] = rows.apply(c, __ldg(K.diag + c), gz);
                     }
@@ -2148,11 +2166,14 @@ __device__ void pcg1_halo_body(const gf_krylov_t& K, const Rows& rows, int chunk
                 for (int u = 0; u < U; ++u) {
                     const int i = i0 + u * THREADS;
                     if (i < m) {
+                        if (upd) __stcg(x + c0 + i, xo[u] + alpha_prev * ps[i]);
                         ws[i] = w[u];
                         loc[2] += w[u] * zc[u];
                     }
                 }
             }
+            pending = false;
+            // alpha_prev is read above by every thread before this barrier.
             ok = grid_reduce<3, THREADS>(ctl, partials, loc, linf ? 1u : 0u);
             if (!ok) break;
             if (threadIdx.x == 0) {
@@ -2184,21 +2205,18 @@ __device__ void pcg1_halo_body(const gf_krylov_t& K, const Rows& rows, int chunk
             __syncthreads();
             if (st.done) break;
         }
-        {  // p = z + beta p; q = w + beta q; x += alpha p; r -= alpha q; z = M r
+        {  // p = z + beta p; q = w + beta q; r -= alpha q; z = M r; x follows next pass
             // The own z is recomputed as inv r: the bits it was stored with.
             const double alpha = st.alpha, beta = st.beta;
+            pending = true;
             rn = 0.0;
             gm = 0.0;
             for (int i0 = threadIdx.x; i0 < m; i0 += V * THREADS) {
-                double xv[V], iv[V];
+                double iv[V];
 #pragma unroll
                 for (int u = 0; u < V; ++u) {
                     const int i = i0 + u * THREADS;
-                    if (i < m) {
-                        const int c = c0 + i;
-                        xv[u] = __ldcg(x + c);
-                        iv[u] = inv[c];
-                    }
+                    if (i < m) iv[u] = inv[c0 + i];
                 }
 #pragma unroll
                 for (int u = 0; u < V; ++u) {
@@ -2209,7 +2227,6 @@ __device__ void pcg1_halo_body(const gf_krylov_t& K, const Rows& rows, int chunk
                         const double qk = ws[i] + qs[i] * beta;
                         ps[i] = pk;
                         qs[i] = qk;
-                        __stcg(x + c, xv[u] + alpha * pk);
                         const double rk = rs[i] - alpha * qk;
                         const double zk = iv[u] * rk;
                         rs[i] = rk;
@@ -2221,6 +2238,10 @@ __device__ void pcg1_halo_body(const gf_krylov_t& K, const Rows& rows, int chunk
             }
             ok = halo_sync(ctl, flags, (unsigned long long)it, s_lo, s_hi);
         }
+    }
+    if (pending) {
+        const double alpha = st.alpha;
+        for (int i = threadIdx.x; i < m; i += THREADS) __stcg(x + c0 + i, __ldcg(x + c0 + i) + alpha * ps[i]);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         double* o = K.stats;

@@ -38,19 +38,27 @@ def workspace(cache: dict, device: torch.device, n: int, ncomp: int, kind: int) 
 
 def default_variant(n: int, mixed: bool, symmetric: bool, box: bool = True) -> int:
     """CG launch shape by system size, from fixed-iteration timings on B200
-    (``python -m gridfoam_b200.solvers.autotune``).  Below ~128K cells
-    256-thread blocks, where the grid barrier dominates; then, up to ~1.3M
-    cells, the kernels that keep each block's own-cell vectors in shared
-    memory and form q = A p by recurrence, gathering z alone (1024-thread
-    blocks, box or ELL rows; at 1M cells 15.7 against 20.4 us an FP64
-    iteration for the plain shared-memory form, 12.0 against 13.2 FP32);
-    above that the shared-memory tiled kernel for symmetric FP64 boxes,
-    else 512-thread blocks."""
-    if n < 131072:
-        return 0
+    (``python -m gridfoam_b200.solvers.autotune``).  FP64 up to ~400K cells:
+    one grid reduction and a halo sync with the neighbouring blocks per
+    iteration, vectors in shared memory (6.9 against 9.8 us an iteration
+    for 256-thread register blocks at 48^3, 8.0 against 8.2 for the
+    q-recurrence form at 64^3); then, up to ~1.3M cells, the q-recurrence
+    form (q = A z + beta q, z alone gathered; 14.7 us at 1M cells); above
+    that the shared-memory tiled kernel for symmetric boxes, else
+    512-thread blocks.  FP32-inner (mixed) solves: 256-thread register
+    blocks below ~32K cells (6.5 us an inner iteration at 24^3 either way),
+    the q-recurrence form up to ~1.3M cells (7.0 against 8.8 us at 48^3,
+    12.0 against 13.2 for the plain shared-memory form at 1M cells), then
+    512-thread blocks."""
+    if mixed:
+        if n < 32768:
+            return 0
+        return 8 if n <= 1300000 else 2
+    if n <= 400000:
+        return 10
     if n <= 1300000:
         return 8
-    return 5 if symmetric and box and not mixed else 2
+    return 5 if symmetric and box else 2
 
 
 class DeviceKrylov(LinearSolver):
