@@ -226,8 +226,17 @@ __device__ bool grid_reduce_all(KCtl* ctl, double* partials, double (&v)[NV], un
 // (grid_reduce_all: four CTA barriers, and every warp runs two more shuffle
 // trees).  The shuffle trees of the NV values are interleaved level by
 // level.
-template <int NV>
-__device__ bool grid_reduce_w0(KCtl* ctl, double* partials, double (&v)[NV], unsigned maxmask) {
+//
+// SIDE(t, nt) runs on the other 31 warps (t = threadIdx.x - 32 of nt =
+// blockDim.x - 32) while warp 0 waits for the grid: block-local work that
+// needs neither the reduction's result nor other blocks' data.
+struct NoSide {
+    __device__ __forceinline__ void operator()(int, int) const {}
+};
+
+template <int NV, class SIDE = NoSide>
+__device__ bool grid_reduce_w0(KCtl* ctl, double* partials, double (&v)[NV], unsigned maxmask,
+                               const SIDE& side = SIDE()) {
     RedBuf<NV>& rb = red_buf<NV>();
     double* sm1 = rb.sm1;
     double* sm2 = rb.sm2;
@@ -326,6 +335,8 @@ __device__ bool grid_reduce_w0(KCtl* ctl, double* partials, double (&v)[NV], uns
 #pragma unroll
                 for (int j = 0; j < NV; ++j) sm2[j] = x[j];
         }
+    } else {
+        side((int)threadIdx.x - 32, (int)blockDim.x - 32);
     }
     __syncthreads();
     // No trailing barrier: sm1 is read only before the barrier above (the
@@ -336,6 +347,19 @@ __device__ bool grid_reduce_w0(KCtl* ctl, double* partials, double (&v)[NV], uns
 #pragma unroll
     for (int j = 0; j < NV; ++j) v[j] = sm2[j];
     return true;
+}
+
+// With side work (see grid_reduce_w0); the general form runs it first on
+// every thread.
+template <int NV, int THREADS, class SIDE>
+__device__ __forceinline__ bool grid_reduce_side(KCtl* ctl, double* partials, double (&v)[NV], unsigned maxmask,
+                                                 const SIDE& side) {
+    if constexpr (THREADS == 1024 && NV <= 3) {
+        if (gridDim.x <= (unsigned)kW0Blocks && (reinterpret_cast<uintptr_t>(partials) & 15u) == 0)
+            return grid_reduce_w0<NV>(ctl, partials, v, maxmask, side);
+    }
+    side((int)threadIdx.x, (int)blockDim.x);
+    return grid_reduce_all<NV, THREADS>(ctl, partials, v, maxmask);
 }
 
 template <int NV, int THREADS = kKThreads>
@@ -1881,27 +1905,23 @@ __device__ void pcg1_qrec_body(const gf_krylov_t& K, const Rows& rows, int chunk
         }
         __syncthreads();
     }
-    // x += alpha p of an iteration is applied in the next iteration's gather
-    // pass (which reads the old p anyway), off the path between the two
-    // reductions; the same additions in the same order, so the same bits.
-    bool pending = false;
+    // x += alpha p of an iteration runs as side work of the second
+    // reduction (the other warps while warp 0 waits for the grid), off the
+    // passes; the same additions in the same order, so the same bits.
     for (int it = 1; ok && !st.done && it <= K.max_iter; ++it) {
-        {  // x += alpha_prev p; w = A z; p = z + beta p; q = w + beta q; p . q
+        {  // w = A z; p = z + beta p; q = w + beta q; p . q
             const double beta = st.beta;
-            const double alpha_prev = st.alpha;
-            const bool upd = pending;
             double loc[1] = {0.0};
             // Plain (L1-cacheable) loads: z is written only before the grid
             // barrier that precedes this pass (see pcg1_smem_body).
             auto gz = [&](int j) { return z[j]; };
             for (int i0 = threadIdx.x; i0 < m; i0 += U * THREADS) {
-                double zc[U], w[U], xo[U];
+                double zc[U], w[U];
 #pragma unroll
                 for (int u = 0; u < U; ++u) {
                     const int i = i0 + u * THREADS;
                     if (i < m) {
                         const int c = c0 + i;
-                        if (upd) xo[u] = __ldcg(x + c);
                         zc[u] = z[c];
                         w[u] = rows.apply(c, __ldg(K.diag + c), gz);
                     }
@@ -1911,7 +1931,6 @@ __device__ void pcg1_qrec_body(const gf_krylov_t& K, const Rows& rows, int chunk
                     const int i = i0 + u * THREADS;
                     if (i < m) {
                         const double pold = ps[i];
-                        if (upd) __stcg(x + c0 + i, xo[u] + alpha_prev * pold);
                         const double pk = zc[u] + pold * beta;
                         const double qk = w[u] + qs[i] * beta;
                         ps[i] = pk;
@@ -1920,15 +1939,12 @@ __device__ void pcg1_qrec_body(const gf_krylov_t& K, const Rows& rows, int chunk
                     }
                 }
             }
-            pending = false;
-            // alpha_prev is read above by every thread before this barrier.
             ok = grid_reduce<1, THREADS>(ctl, partials, loc, 0u);
             if (!ok) break;
             if (threadIdx.x == 0) st.alpha = st.rz_old / loc[0];
             __syncthreads();
-            pending = true;
         }
-        {  // r -= alpha q; z = M r; |r|, r.z (own cells); x follows next pass
+        {  // r -= alpha q; z = M r; |r|, r.z (own cells); x += alpha p during the reduction
             const double alpha = st.alpha;
             double loc[2] = {0.0, 0.0};
             for (int i0 = threadIdx.x; i0 < m; i0 += V * THREADS) {
@@ -1952,7 +1968,10 @@ __device__ void pcg1_qrec_body(const gf_krylov_t& K, const Rows& rows, int chunk
                     }
                 }
             }
-            ok = grid_reduce<2, THREADS>(ctl, partials, loc, linf ? 1u : 0u);
+            auto xupd = [&](int t, int nt) {
+                for (int i = t; i < m; i += nt) __stcg(x + c0 + i, __ldcg(x + c0 + i) + alpha * ps[i]);
+            };
+            ok = grid_reduce_side<2, THREADS>(ctl, partials, loc, linf ? 1u : 0u, xupd);
             if (!ok) break;
             if (threadIdx.x == 0) {
                 const double fin = norm_fin(loc[0], linf);
@@ -1973,10 +1992,6 @@ __device__ void pcg1_qrec_body(const gf_krylov_t& K, const Rows& rows, int chunk
             }
             __syncthreads();
         }
-    }
-    if (pending) {
-        const double alpha = st.alpha;
-        for (int i = threadIdx.x; i < m; i += THREADS) __stcg(x + c0 + i, __ldcg(x + c0 + i) + alpha * ps[i]);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         double* o = K.stats;
@@ -2634,11 +2649,10 @@ __device__ void pcg1_mixed_qrec_body(const gf_krylov_t& K, const Rows64& rows64,
                 if (threadIdx.x == 0) st.alpha = st.rz_old / loc[0];
                 __syncthreads();
             }
-            {  // d += alpha p; r -= alpha q; z = M r; |r|, r.z (own cells)
+            {  // r -= alpha q; z = M r; |r|, r.z (own cells); d += alpha p during the reduction
                 const float alpha = (float)st.alpha;
                 double loc[2] = {0.0, 0.0};
                 for (int i = threadIdx.x; i < m; i += THREADS) {
-                    ds[i] = ds[i] + alpha * ps[i];
                     const float rk = rs[i] - alpha * qs[i];
                     const float zk = ivs[i] * rk;
                     rs[i] = rk;
@@ -2646,7 +2660,10 @@ __device__ void pcg1_mixed_qrec_body(const gf_krylov_t& K, const Rows64& rows64,
                     loc[0] = norm_acc(loc[0], (double)rk, linf);
                     loc[1] += (double)rk * (double)zk;
                 }
-                ok = grid_reduce<2, THREADS>(ctl, partials, loc, linf ? 1u : 0u);
+                auto dupd = [&](int t, int nt) {
+                    for (int i = t; i < m; i += nt) ds[i] = ds[i] + alpha * ps[i];
+                };
+                ok = grid_reduce_side<2, THREADS>(ctl, partials, loc, linf ? 1u : 0u, dupd);
                 if (!ok) break;
                 if (threadIdx.x == 0) {
                     const double nr = norm_fin(loc[0], linf);
