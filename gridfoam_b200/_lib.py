@@ -218,6 +218,7 @@ _SIGNATURES = {
     "gf_force_integral": ([P, I64, P, P, P, P, P, P, P, P, P, F64, F64, F64, F64, F64, P, P, P], ctypes.c_int),
     "gf_continuity_scratch_doubles": ([], I64),
     "gf_continuity_sums": ([I64, P, P, P, P, P], ctypes.c_int),
+    "gf_octree_face_keys": ([P, I64, I64, I64, P, I64, I32, P, P], ctypes.c_int),
 }
 
 EXPORTED = tuple(_SIGNATURES)

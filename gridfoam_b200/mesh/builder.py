@@ -350,24 +350,7 @@ def build_octree_mesh(
     FX, FY, FZ = rx * f, ry * f, rz * f
     hf = (hi - lo) / np.array([FX, FY, FZ], dtype=np.float64)
 
-    # Required level per finest cell (max over regions).
-    req = np.zeros((FX, FY, FZ), dtype=np.int8)
-    if regions:
-        xs = lo[0] + (np.arange(FX) + 0.5) * hf[0]
-        ys = lo[1] + (np.arange(FY) + 0.5) * hf[1]
-        zs = lo[2] + (np.arange(FZ) + 0.5) * hf[2]
-        for r in regions:
-            if isinstance(r, BoxRegion):
-                mx = (xs >= r.lo[0]) & (xs <= r.hi[0])
-                my = (ys >= r.lo[1]) & (ys <= r.hi[1])
-                mz = (zs >= r.lo[2]) & (zs <= r.hi[2])
-                m = mx[:, None, None] & my[None, :, None] & mz[None, None, :]
-            elif isinstance(r, SdfRegion):
-                P = np.stack(np.meshgrid(xs, ys, zs, indexing="ij"), axis=-1)
-                m = r.sdf(P) <= r.distance
-            else:
-                raise TypeError(f"unknown refinement region {r!r}")
-            req = np.maximum(req, np.where(m, np.int8(r.level), np.int8(0)))
+    req = _required_levels(lo, hf, (FX, FY, FZ), regions)
 
     # Level of the leaf covering each finest cell; refine level by level.
     lev = np.zeros((FX, FY, FZ), dtype=np.int8)
@@ -410,8 +393,6 @@ def build_octree_mesh(
     bits = int(np.ceil(np.log2(max(FX, FY, FZ, 2))))
     order = np.lexsort((_morton(li, lj, lk, bits), ll))
     li, lj, lk, ll = li[order], lj[order], lk[order], ll[order]
-    n_cells = li.shape[0]
-    size_f = (1 << (L - ll)).astype(np.int64)  # leaf edge in finest cells
 
     ids = np.empty((FX, FY, FZ), dtype=np.int64)
     for level in range(L + 1):
@@ -424,11 +405,6 @@ def build_octree_mesh(
         full = np.repeat(np.repeat(np.repeat(blk, s, 0), s, 1), s, 2)
         m = full >= 0
         ids[m] = full[m]
-
-    centers = np.stack(
-        [lo[0] + (li + 0.5 * size_f) * hf[0], lo[1] + (lj + 0.5 * size_f) * hf[1],
-         lo[2] + (lk + 0.5 * size_f) * hf[2]], axis=1)
-    sizes = size_f[:, None] * hf[None, :]
 
     owners, neighbours, axes = [], [], []
     for ax in range(3):
@@ -456,14 +432,60 @@ def build_octree_mesh(
         bnd_dir.append(np.full(cells.shape, direction, dtype=np.int64))
     domain_owner = np.concatenate(bnd_owner)
     domain_dir = np.concatenate(bnd_dir)
+    return _octree_mesh(lo, hi, hf, L, (rx, ry, rz), (li, lj, lk, ll), (owner, neighbour, axis_arr),
+                        (domain_owner, domain_dir), bodies)
 
+
+def _required_levels(lo: np.ndarray, hf: np.ndarray, shape: tuple[int, int, int], regions: list,
+                     slab: int = 32) -> np.ndarray:
+    """Required level per finest cell (max over the refinement regions).
+
+    Signed-distance regions are evaluated on slabs of ``slab`` finest x
+    planes (the same per-point expressions as one whole-grid evaluation, in
+    bounded memory)."""
+    FX, FY, FZ = shape
+    req = np.zeros((FX, FY, FZ), dtype=np.int8)
+    if not regions:
+        return req
+    xs = lo[0] + (np.arange(FX) + 0.5) * hf[0]
+    ys = lo[1] + (np.arange(FY) + 0.5) * hf[1]
+    zs = lo[2] + (np.arange(FZ) + 0.5) * hf[2]
+    for r in regions:
+        if isinstance(r, BoxRegion):
+            mx = (xs >= r.lo[0]) & (xs <= r.hi[0])
+            my = (ys >= r.lo[1]) & (ys <= r.hi[1])
+            mz = (zs >= r.lo[2]) & (zs <= r.hi[2])
+            m = mx[:, None, None] & my[None, :, None] & mz[None, None, :]
+            req = np.maximum(req, np.where(m, np.int8(r.level), np.int8(0)))
+        elif isinstance(r, SdfRegion):
+            for x0 in range(0, FX, slab):
+                P = np.stack(np.meshgrid(xs[x0:x0 + slab], ys, zs, indexing="ij"), axis=-1)
+                m = r.sdf(P) <= r.distance
+                req[x0:x0 + slab] = np.maximum(req[x0:x0 + slab], np.where(m, np.int8(r.level), np.int8(0)))
+        else:
+            raise TypeError(f"unknown refinement region {r!r}")
+    return req
+
+
+def _octree_mesh(lo, hi, hf, L, root, leaves, faces, domain, bodies) -> FluxelMesh:
+    """The fluxel mesh from the leaves (finest-level lower corners and
+    levels, in cell order) and the face lists: cell geometry and the AP-IBM
+    payload."""
+    li, lj, lk, ll = leaves
+    owner, neighbour, axis_arr = faces
+    domain_owner, domain_dir = domain
+    size_f = (1 << (L - ll)).astype(np.int64)  # leaf edge in finest cells
+    centers = np.stack(
+        [lo[0] + (li + 0.5 * size_f) * hf[0], lo[1] + (lj + 0.5 * size_f) * hf[1],
+         lo[2] + (lk + 0.5 * size_f) * hf[2]], axis=1)
+    sizes = size_f[:, None] * hf[None, :]
     extent = float(np.max(hi - lo))
     ap, patches = _axis_projected_payload(centers, sizes, owner, neighbour, axis_arr, bodies or [], extent)
     imm = np.nonzero(ap.is_immersed_face)[0]
     if imm.size and np.any(ll[owner[imm]] != ll[neighbour[imm]]):
         raise ValueError("an immersed face lies on a coarse-fine interface; refine around the body")
     return FluxelMesh(
-        n_cells=n_cells,
+        n_cells=int(li.shape[0]),
         internal_faces_owner=owner,
         internal_faces_neighbour=neighbour,
         internal_faces_axis=axis_arr,
@@ -473,6 +495,136 @@ def build_octree_mesh(
         cell_centers=centers,
         cell_sizes=sizes,
         ap=ap,
-        resolution=None if L > 0 else (rx, ry, rz),
-        meta={"lower": tuple(lo), "upper": tuple(hi), "levels": ll, "root_resolution": (rx, ry, rz)},
+        resolution=None if L > 0 else root,
+        meta={"lower": tuple(lo), "upper": tuple(hi), "levels": ll, "root_resolution": root},
     )
+
+
+def build_octree_mesh_device(
+    lower: tuple[float, float, float],
+    upper: tuple[float, float, float],
+    root_resolution: tuple[int, int, int],
+    regions: list | None = None,
+    *,
+    bodies: list[Body] | None = None,
+    device: str = "cuda",
+) -> FluxelMesh:
+    """``build_octree_mesh`` with the finest-level work on the GPU; the same
+    mesh, array for array.
+
+    The required levels come from the same host expressions.  The 2:1
+    refinement, the leaves, their level-then-Morton order, the finest-level
+    leaf ids and the domain-boundary cells are integer tensor work on
+    ``device``.  The internal faces come from ``gf_octree_face_keys``: each
+    owner/neighbour pair is emitted once as ``owner * n_cells +
+    neighbour``, and a device sort gives the (owner, neighbour) order of the
+    host builder's ``np.unique``.  Cell geometry and the immersed-boundary
+    payload are then computed on the host from the same integer arrays with
+    the same expressions as the host builder.
+    """
+    import torch
+
+    from gridfoam_b200._lib import call, ptr, stream_ptr
+
+    dev = torch.device(device)
+    regions = list(regions or [])
+    rx, ry, rz = (int(v) for v in root_resolution)
+    lo = np.asarray(lower, dtype=np.float64)
+    hi = np.asarray(upper, dtype=np.float64)
+    L = max([r.level for r in regions], default=0)
+    f = 1 << L
+    FX, FY, FZ = rx * f, ry * f, rz * f
+    hf = (hi - lo) / np.array([FX, FY, FZ], dtype=np.float64)
+    req = torch.from_numpy(_required_levels(lo, hf, (FX, FY, FZ), regions)).to(dev)
+
+    def bmax(a, s):
+        return a.reshape(FX // s, s, FY // s, s, FZ // s, s).amax(dim=(1, 3, 5))
+
+    def expand(a, s):
+        return a.repeat_interleave(s, 0).repeat_interleave(s, 1).repeat_interleave(s, 2)
+
+    lev = torch.zeros((FX, FY, FZ), dtype=torch.int8, device=dev)
+    for _ in range(64):
+        changed = False
+        nb = lev.clone()
+        for ax in range(3):
+            lo_sl = [slice(None)] * 3
+            hi_sl = [slice(None)] * 3
+            lo_sl[ax], hi_sl[ax] = slice(None, -1), slice(1, None)
+            v = nb[tuple(lo_sl)]
+            v.copy_(torch.maximum(v, lev[tuple(hi_sl)]))
+            v = nb[tuple(hi_sl)]
+            v.copy_(torch.maximum(v, lev[tuple(lo_sl)]))
+        for level in range(L):
+            s = 1 << (L - level)
+            at = (bmax(lev, s) == level) & (-bmax(-lev, s) == level)
+            want = (bmax(req, s) > level) | (bmax(nb, s) > level + 1)
+            grow = at & want
+            if bool(grow.any()):
+                changed = True
+                lev.masked_fill_(expand(grow, s), level + 1)
+        if not changed:
+            break
+    else:
+        raise RuntimeError("octree refinement did not settle")
+
+    li, lj, lk, ll = [], [], [], []
+    for level in range(L + 1):
+        s = 1 << (L - level)
+        blk = (bmax(lev, s) == level) & (-bmax(-lev, s) == level)
+        I, J, K = torch.nonzero(blk, as_tuple=True)
+        li.append(I * s)
+        lj.append(J * s)
+        lk.append(K * s)
+        ll.append(torch.full_like(I, level))
+    li, lj, lk, ll = (torch.cat(a) for a in (li, lj, lk, ll))
+    bits = int(np.ceil(np.log2(max(FX, FY, FZ, 2))))
+    code = torch.zeros_like(li)
+    for b in range(bits):
+        code |= ((li >> b) & 1) << (3 * b)
+        code |= ((lj >> b) & 1) << (3 * b + 1)
+        code |= ((lk >> b) & 1) << (3 * b + 2)
+    # np.lexsort((code, ll)): level first, then Morton code (unique per level).
+    o1 = torch.argsort(code, stable=True)
+    order = o1[torch.argsort(ll[o1], stable=True)]
+    li, lj, lk, ll = li[order], lj[order], lk[order], ll[order]
+    n = int(li.shape[0])
+
+    ids = torch.full((FX, FY, FZ), -1, dtype=torch.int64, device=dev)
+    for level in range(L + 1):
+        s = 1 << (L - level)
+        sel = torch.nonzero(ll == level, as_tuple=True)[0]
+        if sel.numel() == 0:
+            continue
+        blk = torch.full((FX // s, FY // s, FZ // s), -1, dtype=torch.int64, device=dev)
+        blk[li[sel] // s, lj[sel] // s, lk[sel] // s] = sel
+        full = expand(blk, s)
+        ids = torch.where(full >= 0, full, ids)
+
+    corner = torch.stack([li, lj, lk]).contiguous()
+    owners, neighbours, axes = [], [], []
+    for ax in range(3):
+        shape = [FX, FY, FZ]
+        shape[ax] -= 1
+        keys = torch.empty(int(np.prod(shape)), dtype=torch.int64, device=dev)
+        call("gf_octree_face_keys", ptr(ids), FX, FY, FZ, ptr(corner), n, ax, ptr(keys), stream_ptr())
+        if bool((keys == -2).any()):
+            raise RuntimeError("gf_octree_face_keys: a finest cell is not covered by a leaf")
+        keys = torch.sort(keys[keys >= 0]).values
+        owners.append(keys // n)
+        neighbours.append(keys % n)
+        axes.append(torch.full_like(keys, ax))
+    bnd_owner, bnd_dir = [], []
+    for direction in range(6):
+        ax, side_max = direction // 2, direction % 2 == 1
+        cells = torch.unique(ids.select(ax, -1 if side_max else 0))
+        bnd_owner.append(cells)
+        bnd_dir.append(torch.full_like(cells, direction))
+
+    def host(parts):
+        return torch.cat(parts).cpu().numpy()
+
+    leaves = tuple(t.cpu().numpy() for t in (li, lj, lk, ll))
+    faces = (host(owners), host(neighbours), host(axes))
+    domain = (host(bnd_owner), host(bnd_dir))
+    return _octree_mesh(lo, hi, hf, L, (rx, ry, rz), leaves, faces, domain, bodies)

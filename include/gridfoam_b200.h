@@ -472,6 +472,21 @@ int64_t gf_continuity_scratch_doubles(void);
 int gf_continuity_sums(int64_t n, const double* div, const double* vol,
                        double* scratch, double* out, void* stream);
 
+/* No counterpart in the reference, which takes its mesh from the external
+ * fluxel package (core/grid/factory.py:32-65; hanging-face contract
+ * core/grid/axis_projected.py:715-767).  Internal faces of a 2:1-balanced
+ * octree along `axis` (0..2): ids [fx][fy][fz] (C order) is the leaf covering
+ * each finest-level cell, corner [3][n_cells] the leaves' finest-level lower
+ * corners.  keys gets one entry per face position of the [fx - (axis == 0)]
+ * [fy - (axis == 1)][fz - (axis == 2)] lower cells: owner * n_cells +
+ * neighbour at the one position that emits each leaf pair (the corner of
+ * their shared rectangle with the smallest tangential coordinates), -1
+ * elsewhere, -2 where an id lies outside [0, n_cells).  Sorting the
+ * non-negative keys gives the faces in (owner, neighbour) order. */
+int gf_octree_face_keys(const int64_t* ids, int64_t fx, int64_t fy, int64_t fz,
+                        const int64_t* corner, int64_t n_cells, int32_t axis,
+                        int64_t* keys, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

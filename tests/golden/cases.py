@@ -17,6 +17,7 @@ from gridfoam_b200.mesh.builder import (
     BoxRegion,
     SdfRegion,
     build_octree_mesh,
+    build_octree_mesh_device,
     build_uniform_mesh,
     cylinder_sdf,
     plane_sdf,
@@ -361,8 +362,9 @@ def _sdf(b: dict):
     raise ValueError(b["kind"])
 
 
-def build_mesh(spec: dict):
-    """Build the mesh described by a case's ``mesh`` entry."""
+def build_mesh(spec: dict, device: str | None = None):
+    """Build the mesh described by a case's ``mesh`` entry (octrees on
+    ``device`` when it is a CUDA device: the same mesh, built on the GPU)."""
     bodies = [Body(sdf=_sdf(b), patch=b["patch"]) for b in spec.get("bodies", [])]
     if spec["kind"] == "octree":
         regions = []
@@ -371,9 +373,10 @@ def build_mesh(spec: dict):
                 regions.append(BoxRegion(tuple(r["lo"]), tuple(r["hi"]), r["level"]))
             else:
                 regions.append(SdfRegion(_sdf(r["body"]), r["distance"], r["level"]))
-        return build_octree_mesh(
-            tuple(spec["lower"]), tuple(spec["upper"]), tuple(spec["res"]), regions, bodies=bodies
-        )
+        args = (tuple(spec["lower"]), tuple(spec["upper"]), tuple(spec["res"]), regions)
+        if device is not None and str(device).startswith("cuda"):
+            return build_octree_mesh_device(*args, bodies=bodies, device=device)
+        return build_octree_mesh(*args, bodies=bodies)
     return build_uniform_mesh(
         tuple(spec["lower"]), tuple(spec["upper"]), tuple(spec["res"]), bodies=bodies
     )

@@ -21,7 +21,7 @@ def device_case(name: str | None = None, case_def: dict | None = None, device: s
     from gridfoam_b200.meta.config import FieldRole, SimulatorConfig
 
     case_def = copy.deepcopy(case_def or ALL_CASES[name]())
-    mesh = build_mesh(case_def["mesh"])
+    mesh = build_mesh(case_def["mesh"], device=device)
     sim = SimulatorConfig.model_validate(case_def["simulator"])
     grid = AxisProjectedGrid(sim, mesh, device=device)
     kind = case_def["simulator"]["fvSolution"]["algorithm"]["type"]
