@@ -110,12 +110,11 @@ def pcg_bytes_per_iter(C: int, F: int) -> float:
 
 # Measured DRAM bytes (read + write) of the pressure CG kernel
 # (k_pcg1_qrec_box<1, 1024, 1>) on a 64x64x256 box, from two ncu captures of
-# fixed-length launches: 51.98 MB at 50 iterations, 165.41 MB at 400.  The
-# global working set stays in the 126 MB L2, so a launch costs a one-time
-# read of its arrays plus the write-back of the x updated in place each
-# iteration.
-PCG_DRAM_BYTES_PER_ITER = (165412096 - 51979264) / 350
-PCG_DRAM_BYTES_PER_LAUNCH = 51979264 - 50 * PCG_DRAM_BYTES_PER_ITER
+# fixed-length launches: 51.91 MB at 50 iterations, 51.88 MB at 400.  The
+# global working set, x included, stays in the 126 MB L2, so a launch costs
+# a one-time read of its arrays and no DRAM traffic per iteration.
+PCG_DRAM_BYTES_PER_ITER = 0.0
+PCG_DRAM_BYTES_PER_LAUNCH = (51905280 + 51882240) / 2
 
 
 def pcg_bytes_setup(C: int, F: int) -> float:
@@ -487,7 +486,7 @@ def run_gpu(args) -> None:
             "traffic": (PCG_DRAM_BYTES_PER_LAUNCH + PCG_DRAM_BYTES_PER_ITER * sum(iters) / len(iters))
                        if iters else None,
             "traffic_source": "ncu dram bytes of 50- and 400-iteration launches of the same kernel on the same box "
-                              "(fixed part + per-iteration slope), at this run's average iterations per launch",
+                              "(equal within 0.05 %: a fixed part per launch, nothing per iteration)",
             "note": "working set mostly L2-resident at 1M cells: DRAM traffic is well below the algorithmic "
                     "bytes; the kernel is bound by L2 latency and two grid barriers per iteration",
             "launches": len(durations),
