@@ -2706,6 +2706,222 @@ __global__ void __launch_bounds__(1024, 1) k_pcg1_mixed_qrec_ell(gf_krylov_t K, 
     pcg1_mixed_qrec_body<1024, U, 1>(K, rows64, rows32, K.width, chunk);
 }
 
+// ---------------------------------------------------------------------------
+// FP32-inner CG in FP64 refinement (the cycles of pcg1_mixed_qrec_body) with
+// the inner iterations in the single-reduction form of pcg1_halo_body: one
+// grid reduction of |r|, gamma = r.z and delta = w.z and one halo sync with
+// the neighbouring blocks per inner iteration.  Each block keeps the FP32
+// r, q, d, Jacobi inverse, p and w = A z of its cells in shared memory (6
+// floats a cell).  The halo flags use the first kHaloFlagDoubles doubles
+// of the workspace's vector region, which the FP32-inner forms leave
+// unused (n >= kHaloFlagDoubles).  A cycle ends when the FP32 residual of
+// the last update is below the cycle target, seen at the next reduction,
+// or when the iteration budget is spent; the same updates as
+// pcg1_mixed_qrec_body up to the rounding of alpha.
+template <int THREADS, class Rows64, class Rows32>
+__device__ void pcg1_mixed_halo_body(const gf_krylov_t& K, const Rows64& rows64, Rows32 rows32, int ncoef,
+                                     int chunk) {
+    __shared__ CgState st;
+    __shared__ double s_target;
+    __shared__ int s_cycle_done;
+    __shared__ int s_lo, s_hi;
+    extern __shared__ __align__(16) double sm[];
+    KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
+    barrier_init();
+    double* partials = K.work + kCtlDoubles;
+    double* base = partials + kPartials;
+    unsigned long long* flags = reinterpret_cast<unsigned long long*>(base);
+    const int n = (int)K.n;
+    float* f = reinterpret_cast<float*>(base + n);
+    float* z = f;
+    float* val32 = f + (int64_t)n;
+    float* diag32 = val32 + (int64_t)ncoef * n;
+    rows32.val = val32;
+    const int c0 = blockIdx.x * chunk;
+    const int c1 = c0 + chunk < n ? c0 + chunk : n;
+    const int m = c1 > c0 ? c1 - c0 : 0;
+    float* smf = reinterpret_cast<float*>(sm);
+    float* rs = smf;
+    float* qs = smf + chunk;
+    float* ds = smf + 2 * chunk;
+    float* ivs = smf + 3 * chunk;
+    float* ps = smf + 4 * chunk;
+    float* ws = smf + 5 * chunk;
+    double* x = K.x;
+    const bool jac = K.jacobi != 0, linf = K.norm_inf != 0;
+    const bool sym_box = K.stride_y > 0 && K.symmetric;
+    bool ok = true;
+    int its = 0;
+
+    if (threadIdx.x == 0) {
+        st.its = 0;
+        st.converged = 0;
+        st.status = GF_MAX_ITER;
+        st.done = 0;
+        s_lo = n;
+        s_hi = -1;
+        // Visible to every block after the first grid reduction below.
+        flags[kHaloFlagStride * blockIdx.x] = 0ull;
+    }
+    __syncthreads();
+    {
+        int lo = n, hi = -1;
+        for (int i = threadIdx.x; i < m; i += THREADS) {
+            const int c = c0 + i;
+            for (int sl = 0; sl < ncoef; ++sl) {
+                const int src = sym_box ? (2 * sl + 1) : sl;
+                __stcg(val32 + (int64_t)sl * n + c, (float)__ldg(K.val + (int64_t)src * n + c));
+            }
+            __stcg(diag32 + c, (float)__ldg(K.diag + c));
+            ivs[i] = (float)inv_diag(K.diag, c, jac);
+            rows64.span(c, lo, hi);
+        }
+        lo = __reduce_min_sync(0xffffffffu, lo);
+        hi = __reduce_max_sync(0xffffffffu, hi);
+        if ((threadIdx.x & 31) == 0) {
+            atomicMin(&s_lo, lo);
+            atomicMax(&s_hi, hi);
+        }
+    }
+    unsigned long long hep = 0;
+    bool pending = false;
+    for (int cycle = 0; ok && cycle <= K.max_outer; ++cycle) {
+        {  // fold the pending correction, then the true residual in FP64
+            double loc[2] = {0.0, 0.0};
+            if (pending) {
+                for (int i = threadIdx.x; i < m; i += THREADS) x[c0 + i] = x[c0 + i] + (double)ds[i];
+                pending = false;
+            }
+            // The barrier also publishes x, the halo flags and (cycle 0) the FP32 matrix.
+            double dummy[1] = {0.0};
+            ok = grid_reduce<1, THREADS>(ctl, partials, dummy, 0u);
+            if (!ok) break;
+            auto gx = [&](int i) { return __ldcg(x + i); };
+            for (int i = threadIdx.x; i < m; i += THREADS) {
+                const int c = c0 + i;
+                const double ax = rows64.apply(c, __ldg(K.diag + c), gx);
+                const double rk = __ldg(K.rhs + c) - ax;
+                const float r32 = (float)rk;
+                const float z32 = ivs[i] * r32;
+                rs[i] = r32;
+                ds[i] = 0.0f;
+                ps[i] = 0.0f;
+                qs[i] = 0.0f;
+                __stcg(z + c, z32);
+                loc[0] = norm_acc(loc[0], rk, linf);
+                loc[1] += (double)r32 * (double)z32;
+            }
+            ok = grid_reduce<2, THREADS>(ctl, partials, loc, linf ? 1u : 0u);
+            if (!ok) break;
+            if (threadIdx.x == 0) {
+                const double nr = norm_fin(loc[0], linf);
+                if (cycle == 0) {
+                    st.r0 = nr;
+                    st.thresh = fmax(K.atol, K.rtol * nr);
+                    // Blocks holding the cells this block's rows read.
+                    s_lo = m > 0 ? s_lo / chunk : (int)blockIdx.x;
+                    s_hi = m > 0 ? s_hi / chunk : (int)blockIdx.x;
+                }
+                st.final = nr;
+                if (nr < st.thresh) {
+                    st.done = 1;
+                    st.converged = 1;
+                    st.status = GF_OK;
+                } else if (!isfinite(nr)) {
+                    st.done = 1;
+                    st.status = GF_NONFINITE;
+                }
+                st.rz_old = loc[1];
+                st.alpha = 1.0;
+                s_target = fmax(K.inner_eta * nr, (K.inner_margin > 0.0 ? K.inner_margin : 0.5) * st.thresh);
+                s_cycle_done = 0;
+            }
+            __syncthreads();
+            if (st.done || cycle == K.max_outer || its >= K.max_iter) break;
+        }
+        pending = true;
+        double rn = 0.0, gm = 0.0;  // this thread's |r| and r.z of the last update
+        for (int k = 1; ok; ++k) {
+            {  // w = A z; delta = w.z; one reduction with |r| and gamma of the last update
+                double loc[3] = {rn, gm, 0.0};
+                auto gz = [&](int j) { return z[j]; };
+                for (int i = threadIdx.x; i < m; i += THREADS) {
+                    const int c = c0 + i;
+                    const float zc = z[c];
+                    const float w = rows32.apply(c, __ldcg(diag32 + c), gz);
+                    ws[i] = w;
+                    loc[2] += (double)w * (double)zc;
+                }
+                ok = grid_reduce<3, THREADS>(ctl, partials, loc, linf ? 1u : 0u);
+                if (!ok) break;
+                if (threadIdx.x == 0) {
+                    if (k > 1) {
+                        const double nr = norm_fin(loc[0], linf);
+                        if (!(nr >= s_target) || !isfinite(nr)) s_cycle_done = 1;
+                    }
+                    if (its >= K.max_iter) s_cycle_done = 1;
+                    if (!s_cycle_done) {
+                        const double g = k > 1 ? loc[1] : st.rz_old;
+                        const double b = k > 1 ? g / st.rz_old : 0.0;
+                        st.alpha = g / (k > 1 ? loc[2] - b * g / st.alpha : loc[2]);
+                        st.beta = b;
+                        st.rz_old = g;
+                    }
+                }
+                __syncthreads();
+                if (s_cycle_done) break;
+            }
+            ++its;
+            {  // p = z + beta p; q = w + beta q; d += alpha p; r -= alpha q; z = M r
+                // The own z is recomputed as inv r: the bits it was stored with.
+                const float alpha = (float)st.alpha, beta = (float)st.beta;
+                rn = 0.0;
+                gm = 0.0;
+                for (int i = threadIdx.x; i < m; i += THREADS) {
+                    const float pk = ivs[i] * rs[i] + ps[i] * beta;
+                    const float qk = ws[i] + qs[i] * beta;
+                    ps[i] = pk;
+                    qs[i] = qk;
+                    ds[i] = ds[i] + alpha * pk;
+                    const float rk = rs[i] - alpha * qk;
+                    const float zk = ivs[i] * rk;
+                    rs[i] = rk;
+                    __stcg(z + c0 + i, zk);
+                    rn = norm_acc(rn, (double)rk, linf);
+                    gm += (double)rk * (double)zk;
+                }
+                ok = halo_sync(ctl, flags, ++hep, s_lo, s_hi);
+            }
+        }
+    }
+    if (ok && pending) {
+        // iteration budget spent inside a cycle: keep its correction
+        for (int i = threadIdx.x; i < m; i += THREADS) x[c0 + i] = x[c0 + i] + (double)ds[i];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        double* o = K.stats;
+        o[0] = st.r0;
+        o[1] = st.final;
+        o[2] = its;
+        o[3] = st.converged;
+        o[4] = ok ? st.status : GF_ERR_TIMEOUT;
+    }
+}
+
+template <bool SYM>
+__global__ void __launch_bounds__(1024, 1) k_pcg1_mixed_halo_box(gf_krylov_t K, int chunk) {
+    BoxRows<double, SYM, false, int> rows64{K.val, (int)K.n, (int)K.stride_y, (int)K.stride_z};
+    BoxRows<float, SYM, SYM, int> rows32{nullptr, (int)K.n, (int)K.stride_y, (int)K.stride_z};
+    pcg1_mixed_halo_body<1024>(K, rows64, rows32, SYM ? 3 : 6, chunk);
+}
+
+template <int WIDTH>
+__global__ void __launch_bounds__(1024, 1) k_pcg1_mixed_halo_ell(gf_krylov_t K, int chunk) {
+    EllRows<double, WIDTH, int> rows64{K.val, K.nbr, (int)K.n, K.width};
+    EllRows<float, WIDTH, int> rows32{nullptr, K.nbr, (int)K.n, K.width};
+    pcg1_mixed_halo_body<1024>(K, rows64, rows32, K.width, chunk);
+}
+
 // Tile length for the staged kernel (0: the system does not qualify).
 static int staged_tile(const gf_krylov_t* k) {
     if (!k->symmetric || k->stride_y < 1 || (k->n & 1)) return 0;
@@ -3240,6 +3456,20 @@ static int launch_halo(const gf_krylov_t* k, void* stream, int unroll) {
     return launch_qrec(k, stream, 1);
 }
 
+// FP32-inner single-reduction form (variants 10/11): r, q, d, inverse, p and
+// w in shared memory (6 floats a cell), the halo flags at the start of the
+// workspace's vector region; GF_ERR_INVALID (no launch) when n is too small
+// for the flags or the arrays do not fit.
+static int launch_mixed_halo(const gf_krylov_t* k, void* stream) {
+    if (k->n < kHaloFlagDoubles) return GF_ERR_INVALID;
+    const void* kern;
+    if (k->stride_y > 0)
+        kern = k->symmetric ? (const void*)k_pcg1_mixed_halo_box<true> : (const void*)k_pcg1_mixed_halo_box<false>;
+    else
+        kern = k->width == 6 ? (const void*)k_pcg1_mixed_halo_ell<6> : (const void*)k_pcg1_mixed_halo_ell<0>;
+    return launch_smem_arrays(k, stream, 1024, 6, sizeof(float), kern);
+}
+
 static int launch_smem_arrays(const gf_krylov_t* k, void* stream, int threads, int narr, size_t elem,
                               const void* kern) {
     const char* what = "gf_pcg_solve";
@@ -3373,7 +3603,9 @@ int gf_pcg_solve(const gf_krylov_t* k, void* stream) {
             if (st != GF_ERR_INVALID) return st;
         }
         if (k->variant >= kQrecVariant && k->variant <= kHaloVariant + 1) {
-            const int st = launch_qrec(k, stream, (k->variant - kQrecVariant) % 2 == 0 ? 1 : 2);
+            int st = GF_ERR_INVALID;
+            if (k->variant >= kHaloVariant) st = launch_mixed_halo(k, stream);
+            if (st == GF_ERR_INVALID) st = launch_qrec(k, stream, (k->variant - kQrecVariant) % 2 == 0 ? 1 : 2);
             if (st != GF_ERR_INVALID) return st;
         }
         if (box) {

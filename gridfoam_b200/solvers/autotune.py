@@ -42,7 +42,7 @@ VARIANTS = {
     7: "1024 threads, own-cell vectors resident in shared memory (up to ~1.3M cells)",
     8: "1024 threads, shared-memory vectors, q = A z + beta q recurrence, 1 cell/pass",
     9: "1024 threads, shared-memory vectors, q = A z + beta q recurrence, 2 cells/pass",
-    10: "1024 threads, shared-memory vectors, one grid reduction and a halo sync per iteration, 1 cell/pass",
+    10: "1024 threads, shared-memory vectors, one grid reduction and a halo sync per iteration, 1 cell/pass (FP32-inner: same form)",
     11: "1024 threads, shared-memory vectors, one grid reduction and a halo sync per iteration, 2 cells/pass",
 }
 

@@ -46,14 +46,16 @@ def default_variant(n: int, mixed: bool, symmetric: bool, box: bool = True) -> i
     form (q = A z + beta q, z alone gathered; 14.7 us at 1M cells); above
     that the shared-memory tiled kernel for symmetric boxes, else
     512-thread blocks.  FP32-inner (mixed) solves: 256-thread register
-    blocks below ~32K cells (6.5 us an inner iteration at 24^3 either way),
-    the q-recurrence form up to ~1.3M cells (7.0 against 8.8 us at 48^3,
-    12.0 against 13.2 for the plain shared-memory form at 1M cells), then
-    512-thread blocks."""
+    blocks below ~32K cells (6.5 us an inner iteration at 24^3, as for the
+    shared-memory forms); then, up to ~1.3M cells, the single-reduction
+    form with the halo sync (6.7 against 7.0 us for the q-recurrence form
+    and 8.9 for the register blocks at 48^3, 7.5 against 7.8 at 64^3, 11.6
+    either way at 1M cells; it falls back to the q-recurrence form where its
+    six shared-memory arrays do not fit); then 512-thread blocks."""
     if mixed:
         if n < 32768:
             return 0
-        return 8 if n <= 1300000 else 2
+        return 10 if n <= 1300000 else 2
     if n <= 400000:
         return 10
     if n <= 1300000:

@@ -218,13 +218,25 @@ def test_mixed_precision_pcg_meets_fp64_criterion(variant, layout):
     threshold as the FP64 solver, and its solution agrees with the FP64
     solution to the accuracy that threshold implies.  Variants 6/7: the
     kernels with each block's FP32 vectors resident in shared memory."""
+    _mixed_case(variant, layout, 16, 32)
+
+
+@pytest.mark.parametrize("layout", ["box", "ell"])
+@pytest.mark.parametrize("variant", [10, 11])
+def test_mixed_halo_pcg_meets_fp64_criterion(variant, layout):
+    """The FP32-inner solve in the single-reduction form with a halo sync
+    (27,648 cells: enough for its flags) meets the same FP64 criterion."""
+    _mixed_case(variant, layout, 24, 48)
+
+
+def _mixed_case(variant, layout, nxy, nz):
     from gridfoam_b200.fv import fvm
     from gridfoam_b200.meta.config import SolverConfig
     from gridfoam_b200.solvers.krylov import CGSolver
 
     from tests.golden.cases import pipe_case
 
-    _, _, grid, algo = device_case(case_def=pipe_case(16, 32))
+    _, _, grid, algo = device_case(case_def=pipe_case(nxy, nz))
     gamma = torch.full((grid.num_cells,), 0.3, dtype=torch.float64, device="cuda")
     A = -fvm.laplacian(gamma, algo.p)
     gen = torch.Generator(device="cpu").manual_seed(1)
