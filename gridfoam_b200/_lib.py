@@ -162,6 +162,7 @@ class GfKrylov(ctypes.Structure):
         ("variant", I32),
         ("single_reduction", I32),
         ("inner_margin", F64),
+        ("spin_limit", I64),
     ]
 
 

@@ -60,12 +60,18 @@ def build(verbose: bool = False, force: bool = False) -> pathlib.Path:
     ]
     if verbose:
         common += ["-Xptxas", "-v"]
-    objs = []
-    for src in sources():
-        obj = obj_dir / (src.stem + ".o")
-        cmd = [nvcc, *common, "-dc", str(src), "-o", str(obj)]
-        subprocess.run(cmd, check=True)
-        objs.append(obj)
+    from concurrent.futures import ThreadPoolExecutor
+
+    objs = [obj_dir / (src.stem + ".o") for src in sources()]
+
+    def compile_one(pair):
+        src, obj = pair
+        subprocess.run([nvcc, *common, "-dc", str(src), "-o", str(obj)], check=True)
+
+    # The translation units are independent (relocatable device code,
+    # linked below), so they compile in parallel.
+    with ThreadPoolExecutor(max_workers=max(1, min(len(objs), os.cpu_count() or 1))) as pool:
+        list(pool.map(compile_one, zip(sources(), objs)))
     tmp = LIB_PATH.with_suffix(".so.tmp")
     cmd = [nvcc, *ARCH, "-shared", "-cudart", "static", "-o", str(tmp), *map(str, objs)]
     subprocess.run(cmd, check=True)

@@ -34,12 +34,17 @@ struct KCtl {
     int pad;
 };
 
-// Barriers this block has passed since the kernel started; barrier_init()
-// must run at the top of every kernel that calls grid_reduce.
+// Barriers this block has passed since the kernel started, and the poll
+// limit of every bounded wait of this launch; barrier_init() must run at the
+// top of every kernel that waits on other blocks.
 __shared__ unsigned g_epoch;
+__shared__ long long g_spin;
 
-__device__ __forceinline__ void barrier_init() {
-    if (threadIdx.x == 0) g_epoch = 0;
+__device__ __forceinline__ void barrier_init(const gf_krylov_t& K) {
+    if (threadIdx.x == 0) {
+        g_epoch = 0;
+        g_spin = K.spin_limit > 0 ? K.spin_limit : kSpinLimit;
+    }
 }
 
 __device__ __forceinline__ int vload(const int* p) { return *(const volatile int*)p; }
@@ -154,7 +159,7 @@ __device__ bool grid_reduce_all(KCtl* ctl, double* partials, double (&v)[NV], un
                 err = 1;
                 break;
             }
-            if (it > kSpinLimit) {
+            if (it > g_spin) {
                 atomicExch(&ctl->error, 1);
                 err = 1;
                 break;
@@ -291,7 +296,7 @@ __device__ bool grid_reduce_w0(KCtl* ctl, double* partials, double (&v)[NV], uns
                     err = 1;
                     break;
                 }
-                if (it > kSpinLimit) {
+                if (it > g_spin) {
                     if (lane == 0) atomicExch(&ctl->error, 1);
                     err = 1;
                     break;
@@ -406,7 +411,7 @@ __global__ void __launch_bounds__(kKThreads) k_pcg(gf_krylov_t K) {
     __shared__ CgState st[NC];
     __shared__ int s_all_done;
     KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
-    barrier_init();
+    barrier_init(K);
     double* partials = K.work + kCtlDoubles;
     double* vec = partials + kPartials;
     const int64_t n = K.n;
@@ -673,7 +678,7 @@ template <int THREADS, int U, class Rows>
 __device__ void pcg1_body(const gf_krylov_t& K, const Rows& rows) {
     __shared__ CgState st;
     KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
-    barrier_init();
+    barrier_init(K);
     double* partials = K.work + kCtlDoubles;
     double* vec = partials + kPartials;
     const int64_t n = K.n;
@@ -846,7 +851,7 @@ template <int THREADS, class Rows>
 __device__ void pcg1_sr_body(const gf_krylov_t& K, const Rows& rows) {
     __shared__ CgState st;
     KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
-    barrier_init();
+    barrier_init(K);
     double* partials = K.work + kCtlDoubles;
     double* vec = partials + kPartials;
     const int64_t n = K.n;
@@ -1008,7 +1013,7 @@ __device__ void pcg1_mixed_body(const gf_krylov_t& K, const Rows64& rows64, Rows
     __shared__ double s_target;
     __shared__ int s_cycle_done;
     KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
-    barrier_init();
+    barrier_init(K);
     double* partials = K.work + kCtlDoubles;
     double* base = partials + kPartials;
     const int64_t n = K.n;
@@ -1304,7 +1309,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity) {
     long long it = 0;
     while (!mbar_test(b, parity)) {
         if (++it > 1024) __nanosleep(20);
-        if (it > kSpinLimit) return false;
+        if (it > g_spin) return false;
     }
     return true;
 }
@@ -1458,7 +1463,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_pcg1_box_staged(gf_krylov_t K, i
     __shared__ int s_stage_err;
     extern __shared__ __align__(16) double smem[];
     KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
-    barrier_init();
+    barrier_init(K);
     double* partials = K.work + kCtlDoubles;
     double* vec = partials + kPartials;
     const int64_t n = K.n, sy = K.stride_y, sz = K.stride_z;
@@ -1657,7 +1662,7 @@ __device__ void pcg1_smem_body(const gf_krylov_t& K, const Rows& rows, int chunk
     __shared__ CgState st;
     extern __shared__ __align__(16) double sm[];
     KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
-    barrier_init();
+    barrier_init(K);
     double* partials = K.work + kCtlDoubles;
     double* vec = partials + kPartials;
     const int n = (int)K.n;
@@ -1850,7 +1855,7 @@ __device__ void pcg1_qrec_body(const gf_krylov_t& K, const Rows& rows, int chunk
     __shared__ CgState st;
     extern __shared__ __align__(16) double sm[];
     KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
-    barrier_init();
+    barrier_init(K);
     double* partials = K.work + kCtlDoubles;
     double* vec = partials + kPartials;
     const int n = (int)K.n;
@@ -2063,7 +2068,7 @@ __device__ bool halo_sync(KCtl* ctl, unsigned long long* flags, unsigned long lo
                 err = 1;
                 break;
             }
-            if (it > kSpinLimit) {
+            if (it > g_spin) {
                 atomicExch(&ctl->error, 1);
                 err = 1;
                 break;
@@ -2079,7 +2084,7 @@ __device__ void pcg1_halo_body(const gf_krylov_t& K, const Rows& rows, int chunk
     __shared__ int s_lo, s_hi;
     extern __shared__ __align__(16) double sm[];
     KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
-    barrier_init();
+    barrier_init(K);
     double* partials = K.work + kCtlDoubles;
     double* vec = partials + kPartials;
     const int n = (int)K.n;
@@ -2300,7 +2305,7 @@ __device__ void pcg1_mixed_smem_body(const gf_krylov_t& K, const Rows64& rows64,
     __shared__ int s_cycle_done;
     extern __shared__ __align__(16) double sm[];
     KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
-    barrier_init();
+    barrier_init(K);
     double* partials = K.work + kCtlDoubles;
     double* base = partials + kPartials;
     const int n = (int)K.n;
@@ -2522,7 +2527,7 @@ __device__ void pcg1_mixed_qrec_body(const gf_krylov_t& K, const Rows64& rows64,
     __shared__ int s_cycle_done;
     extern __shared__ __align__(16) double sm[];
     KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
-    barrier_init();
+    barrier_init(K);
     double* partials = K.work + kCtlDoubles;
     double* base = partials + kPartials;
     const int n = (int)K.n;
@@ -2727,7 +2732,7 @@ __device__ void pcg1_mixed_halo_body(const gf_krylov_t& K, const Rows64& rows64,
     __shared__ int s_lo, s_hi;
     extern __shared__ __align__(16) double sm[];
     KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
-    barrier_init();
+    barrier_init(K);
     double* partials = K.work + kCtlDoubles;
     double* base = partials + kPartials;
     unsigned long long* flags = reinterpret_cast<unsigned long long*>(base);
@@ -2976,7 +2981,7 @@ __global__ void __launch_bounds__(kKThreads) k_bicgstab(gf_krylov_t K) {
     __shared__ BiState st[NC];
     __shared__ int s_any;
     KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
-    barrier_init();
+    barrier_init(K);
     double* partials = K.work + kCtlDoubles;
     double* vec = partials + kPartials;
     const int64_t n = K.n;
@@ -3757,7 +3762,10 @@ int gf_pcg_solve_static(const gf_krylov_t* k, void* stream) {
     if (st != GF_OK) return st;
     gf_krylov_t local = *k;
     local.work = scratch;
-    local.work_len = kStaticScratchDoubles;
+    // The system's own workspace size, not the whole array: the launch
+    // shape depends on work_len, and this keeps it the one gf_pcg_solve
+    // picks for a workspace sized by gf_krylov_workspace_size.
+    local.work_len = need;
     // gf_pcg_solve clears the barrier control block before its launch; the
     // partials and vectors are written before they are read.
     return gf_pcg_solve(&local, stream);

@@ -95,6 +95,9 @@ class DeviceKrylov(LinearSolver):
         # False: no pinned statistics copy per solve (stream capture into a
         # CUDA graph); the statistics stay in the device buffer.
         self.host_stats = True
+        # > 0: polls after which a device-side wait gives up and the solve
+        # reports status "timeout" (0: the library default, about a second).
+        self.spin_limit = 0
 
     def solve_arrays(self, grid, diag: torch.Tensor, val: torch.Tensor, rhs: torch.Tensor,
                      x: torch.Tensor, *, symmetric: bool = False) -> tuple[SolveStats, ...]:
@@ -135,6 +138,7 @@ class DeviceKrylov(LinearSolver):
         k.inner_eta = self.inner_eta
         k.inner_margin = self.inner_margin
         k.block_cap = int(self.block_cap)
+        k.spin_limit = int(self.spin_limit)
         box = getattr(grid, "box_strides", None)
         k.variant = (int(self.variant) if self.variant is not None
                      else default_variant(n, mixed, symmetric, box is not None))

@@ -215,6 +215,10 @@ typedef struct gf_krylov {
                              kind-0 workspace (7 vectors) */
     double inner_margin;  /* mixed: an FP32 cycle also ends once its residual
                              is below margin * threshold, in (0, 1]; 0: 0.5 */
+    int64_t spin_limit;   /* > 0: polls after which every bounded device wait
+                             (grid barrier, halo flag, copy stage) gives up and
+                             the solve ends with GF_ERR_TIMEOUT; 0: the
+                             default, about a second of polling */
 } gf_krylov_t;
 
 const char* gf_last_error(void);
@@ -275,9 +279,13 @@ int gf_pcg_solve(const gf_krylov_t* k, void* stream);
  * time (a host framework that owns the device pool through its own caching
  * allocator, or a serving loop that must not allocate after start-up).
  * k->work and k->work_len are ignored: the scratch is a file-scope device
- * array of gf_pcg_static_scratch_doubles() doubles (14.3 MiB; one FP64
- * system of up to 262,144 cells) that every GPU loading this library holds
- * until exit.  Larger systems are rejected with GF_ERR_INVALID.  The first
+ * array of gf_pcg_static_scratch_doubles() doubles (14.3 MiB) that every GPU
+ * loading this library holds until exit.  It fits one FP64 system of up to
+ * 262,144 cells, or one FP32-inner (mixed) system of up to 229,376 cells at
+ * ELL width 6 (fewer for wider rows: 166,830 at width 12).  A system fits
+ * when gf_krylov_workspace_size(n, 1, kind) <= gf_pcg_static_scratch_doubles()
+ * with kind 0 (FP64) or 2 + 100 * width (mixed).  Larger systems are
+ * rejected with GF_ERR_INVALID.  The first
  * call on a device looks up the array's device address
  * (cudaGetSymbolAddress); make that first call before any stream capture.
  * All calls share the one array, so calls that overlap on the GPU (other

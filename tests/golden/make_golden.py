@@ -1,12 +1,13 @@
 """Generate golden fixtures by running the reference gridfoam on CPU.
 
-Run in a container where the reference source tree is available::
+Run where the reference source tree is available, with ``GRIDFOAM_REF``
+naming its ``src`` directory (required; there is no default)::
 
-    GRIDFOAM_REF=/root/reference/src python tests/golden/make_golden.py
-    GRIDFOAM_REF=/root/reference/src python tests/golden/make_golden.py --adjoint
-    GRIDFOAM_REF=/root/reference/src python tests/golden/make_golden.py --forces
-    GRIDFOAM_REF=/root/reference/src python tests/golden/make_golden.py --potential
-    GRIDFOAM_REF=/root/reference/src python tests/golden/make_golden.py --diagnostics
+    GRIDFOAM_REF=<reference>/src python tests/golden/make_golden.py
+    GRIDFOAM_REF=<reference>/src python tests/golden/make_golden.py --adjoint
+    GRIDFOAM_REF=<reference>/src python tests/golden/make_golden.py --forces
+    GRIDFOAM_REF=<reference>/src python tests/golden/make_golden.py --potential
+    GRIDFOAM_REF=<reference>/src python tests/golden/make_golden.py --diagnostics
 
 It imports the unmodified reference package (with the import stubs in
 ``tests/golden/refshim`` for its absent optional dependencies), builds each
@@ -24,7 +25,9 @@ import sys
 
 HERE = pathlib.Path(__file__).resolve().parent
 REPO = HERE.parents[1]
-REF_SRC = os.environ.get("GRIDFOAM_REF", "/root/reference/src")
+REF_SRC = os.environ.get("GRIDFOAM_REF")
+if not REF_SRC:
+    raise SystemExit("set GRIDFOAM_REF to the reference's src directory")
 os.environ.setdefault("GRIDFOAM_RUNTIME_TYPE_CHECKS", "0")
 sys.path[:0] = [str(HERE / "refshim"), REF_SRC, str(REPO)]
 

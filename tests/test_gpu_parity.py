@@ -193,6 +193,51 @@ def test_krylov_zero_rhs_and_limits():
         assert not st[0].converged and st[0].status == "nonfinite"
 
 
+@pytest.mark.parametrize("method,variant", [("cg", 0), ("cg", 10), ("cg", 8), ("bicgstab", None)])
+def test_krylov_wait_timeout_reports_and_recovers(method, variant):
+    """A device wait that runs out ends the solve with status "timeout"
+    (GF_ERR_TIMEOUT) and returns; the next solve on the same stream runs
+    normally.  The poll limit is cut to two polls, so some block gives up
+    at a grid barrier or halo flag: the kernel sets the error flag, every
+    other block leaves at its next bounded wait, nothing traps."""
+    from gridfoam_b200.fv import fvm
+    from gridfoam_b200.meta.config import SolverConfig
+    from gridfoam_b200.solvers.krylov import BiCGSTABSolver, CGSolver
+    from tests.golden.cases import pipe_case
+
+    _, _, grid, algo = device_case(case_def=pipe_case(24, 48))
+    A = -fvm.laplacian(1.0, algo.p)
+    A.diag = A.diag + 1e-3 * grid.cell_volumes
+    n = grid.num_cells
+    rhs = torch.linspace(-1.0, 1.0, n, dtype=torch.float64, device="cuda").reshape(1, n)
+    cls = CGSolver if method == "cg" else BiCGSTABSolver
+    cfg = SolverConfig(method=method, preconditioner="jacobi", tolerance=1e-10, rel_tolerance=0.0, max_iter=5000)
+    ref = cls(cfg)
+    ref.variant = variant
+    x_ref = torch.zeros_like(rhs)
+    st = ref.solve_arrays(grid, A.diag_store, A.val, rhs, x_ref, symmetric=True)
+    assert st[0].converged and st[0].iterations > 20
+
+    s = cls(cfg)
+    s.variant = variant
+    s.spin_limit = 2
+    statuses = []
+    for _ in range(5):  # a timeout needs one block to arrive > 2 polls early
+        x = torch.zeros_like(rhs)
+        st = s.solve_arrays(grid, A.diag_store, A.val, rhs, x, symmetric=True)
+        statuses.append(st[0].status)
+        if st[0].status == "timeout":
+            break
+    assert "timeout" in statuses, statuses
+    assert not st[0].converged
+    s.spin_limit = 0
+    x = torch.zeros_like(rhs)
+    st = s.solve_arrays(grid, A.diag_store, A.val, rhs, x, symmetric=True)
+    torch.cuda.synchronize()
+    assert st[0].status == "ok" and st[0].converged
+    torch.testing.assert_close(x, x_ref, rtol=1e-12, atol=1e-14)
+
+
 def test_cavity32_against_oracle():
     """Full-size cavity config (32^3, SIMPLE, linear): two steps against the
     oracle (the reference restatement) on the same mesh."""

@@ -18,12 +18,12 @@ torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
 
-def _system():
+def _system(n: int, nz: int):
     from gridfoam_b200.fv import fvm
     from tests.golden.cases import pipe_case
     from tests.golden.device_harness import device_case
 
-    _, _, grid, algo = device_case(case_def=pipe_case(24, 48))
+    _, _, grid, algo = device_case(case_def=pipe_case(n, nz))
     gamma = torch.linspace(0.2, 0.5, grid.num_cells, dtype=torch.float64, device="cuda")
     A = -fvm.laplacian(gamma, algo.p)
     gen = torch.Generator(device="cpu").manual_seed(5)
@@ -31,7 +31,7 @@ def _system():
     return grid, A, rhs
 
 
-def _descriptor(grid, A, rhs, x, stats, work=None):
+def _descriptor(grid, A, rhs, x, stats, variant, mixed, work=None):
     from gridfoam_b200 import _lib
 
     k = _lib.GfKrylov()
@@ -53,33 +53,51 @@ def _descriptor(grid, A, rhs, x, stats, work=None):
     if work is not None:
         k.work = _lib.ptr(work)
         k.work_len = work.numel()
-    k.max_outer = 1
+    k.variant = variant
+    k.mixed = mixed
+    k.max_outer = 20 if mixed else 1
     k.inner_eta = 1e-4
     return k
 
 
-def test_static_scratch_matches_workspace_solve():
+# (CG launch shape, FP32 inner iterations): the register kernel, and the
+# single-reduction halo kernels of the FP64 and the FP32-inner solve, whose
+# halo flags live in the scratch and must be reset by every call.
+SHAPES = [(0, 0), (10, 0), (10, 1)]
+
+
+@pytest.mark.parametrize("variant,mixed", SHAPES, ids=["v0-fp64", "v10-fp64", "v10-fp32inner"])
+def test_static_scratch_matches_workspace_solve(variant, mixed):
     if not torch.cuda.is_available():
         pytest.skip("needs a CUDA device")
     from gridfoam_b200 import _lib
 
     lib = _lib.load()
-    grid, A, rhs = _system()
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
-    n = grid.num_cells
-    assert lib.gf_krylov_workspace_size(n, 1, 0) <= lib.gf_pcg_static_scratch_doubles()
+    # Two systems of different sizes (both >= 16,384 cells, where the
+    # FP32-inner halo kernel applies), solved with a sized workspace first.
+    systems = [_system(24, 48), _system(20, 44)]
+    refs = []
+    for grid, A, rhs in systems:
+        n = grid.num_cells
+        kind = 2 + 100 * grid.ell_width if mixed else 0
+        assert lib.gf_krylov_workspace_size(n, 1, kind) <= lib.gf_pcg_static_scratch_doubles()
+        work = torch.empty(lib.gf_krylov_workspace_size(n, 1, kind), dtype=torch.float64, device="cuda")
+        x_ref = torch.zeros_like(rhs)
+        st_ref = torch.zeros((1, 5), dtype=torch.float64, device="cuda")
+        _lib.call("gf_pcg_solve", ctypes.byref(_descriptor(grid, A, rhs, x_ref, st_ref, variant, mixed, work)),
+                  stream)
+        torch.cuda.synchronize()
+        assert int(st_ref[0, 3]) == 1
+        refs.append((x_ref, st_ref))
 
-    work = torch.empty(lib.gf_krylov_workspace_size(n, 1, 0), dtype=torch.float64, device="cuda")
-    x_ref = torch.zeros_like(rhs)
-    st_ref = torch.zeros((1, 5), dtype=torch.float64, device="cuda")
-    _lib.call("gf_pcg_solve", ctypes.byref(_descriptor(grid, A, rhs, x_ref, st_ref, work)), stream)
-    torch.cuda.synchronize()
-    assert int(st_ref[0, 3]) == 1
-
-    for _ in range(2):  # two calls in a row share the static scratch
+    # Calls in a row on the one shared array, alternating sizes.
+    for i in (0, 1, 0, 1):
+        grid, A, rhs = systems[i]
+        x_ref, st_ref = refs[i]
         x = torch.zeros_like(rhs)
         st = torch.zeros((1, 5), dtype=torch.float64, device="cuda")
-        _lib.call("gf_pcg_solve_static", ctypes.byref(_descriptor(grid, A, rhs, x, st)), stream)
+        _lib.call("gf_pcg_solve_static", ctypes.byref(_descriptor(grid, A, rhs, x, st, variant, mixed)), stream)
         torch.cuda.synchronize()
         assert int(st[0, 2]) == int(st_ref[0, 2]) and int(st[0, 3]) == 1
         torch.testing.assert_close(x, x_ref, rtol=1e-12, atol=1e-14)
