@@ -1,13 +1,17 @@
-"""Benchmark: cell-iterations/s of the immersed-boundary Hagen-Poiseuille
-pipe (box 1x1x4 on 64x64x256 cells, cylindrical IB r = 0.4 along z,
-parabolic inlet with mean velocity 1, nu = 0.02, PISO dt = 1e-3, two
-correctors, upwind convection), float64 on one B200.
+"""Benchmark: cell-iterations/s of the cylinder wake on a 3-level octree
+(domain 30D x 20D x 4D, base 256 x 160 x 32 cells refined two levels within
+2D of an immersed cylinder of diameter D = 1: 4,079,808 cells, 12.2M
+internal faces, hanging faces at both level interfaces), inflow 1,
+nu = 0.01 (Re 100), PISO at CFL 0.5 on the finest cell, two correctors,
+float64, on one B200.
 
 One step is one PISO time step (momentum BiCGStab + 2 pressure CG solves to
 tolerance).  ``value`` is device-timed with inputs resident in HBM; ``e2e``
 times the public API with the step's state copied host->device from pinned
 memory and the result read back every step.  ``--impl reference`` times the
-CPU oracle (the reference algorithm restated in numpy) on a bounded sample.
+CPU path (the reference algorithm restated in numpy with its Krylov solves
+and repeated scatter-adds in multi-threaded C) on the same mesh and case,
+on every host core.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 """
@@ -28,13 +32,34 @@ REPO = pathlib.Path(__file__).resolve().parent
 sys.path.insert(0, str(REPO))
 
 METRIC = "cell-iters/s"
-WORKLOAD = "ib_pipe_64x64x256_piso"
+BASE = (256, 160, 32)
+WORKLOAD = f"cylinder_wake_{BASE[0]}x{BASE[1]}x{BASE[2]}_piso"
+ALGORITHM = ("piso nCorrectors=2, dt=CFL 0.5 on the finest cell, upwind, p cg+jacobi tol 1e-7 rel 0.01 "
+             "(pFinal rel 0), U bicgstab+jacobi tol 1e-8 rel 0.1")
 
 
-def pipe_config(n: int = 64, nz: int = 256, length: float = 4.0) -> dict:
-    from tests.golden.cases import pipe_case
+def workload_case() -> dict:
+    from gridfoam_b200.cases import cylinder_wake_case
 
-    return pipe_case(n, nz, length)
+    return cylinder_wake_case(BASE)
+
+
+def workload_config(mesh, world: int) -> dict:
+    """The bench line's ``config``: a function of the mesh and the case only,
+    so the GPU arm and the reference arm print the same dictionary."""
+    import numpy as np
+
+    F = int(np.asarray(mesh.internal_faces_owner).shape[0])
+    imm = int(np.asarray(mesh.ap.is_immersed_face).sum())
+    return {
+        "workload": WORKLOAD,
+        "cells": int(mesh.n_cells),
+        "internal_faces": F,
+        "immersed_faces": imm,
+        "algorithm": ALGORITHM,
+        "l2": "working set (8 GB) larger than L2 (126 MB), no flush",
+        "parallelism": f"replicas x{world}",
+    }
 
 
 def peaks() -> tuple[float, str]:
@@ -102,83 +127,95 @@ class ClockSampler:
         }
 
 
-def pcg_bytes_per_iter(C: int, F: int) -> float:
-    """Algorithmic bytes of one fused Jacobi-PCG iteration (fp64, int32 indices):
-    14 C s + F (s + 8), s = 8."""
-    return 14 * C * 8 + F * (8 + 8)
+def pcg_bytes_per_iter(C: int, F: int, s: int = 8) -> float:
+    """Algorithmic bytes of one fused Jacobi-PCG iteration (int32 indices):
+    14 C s + F (s + 8)."""
+    return 14 * C * s + F * (s + 8)
 
 
-# Measured DRAM bytes (read + write) of the pressure CG kernel
-# (k_pcg1_qrec_box<1, 1024, 1>) on a 64x64x256 box, from two ncu captures of
-# fixed-length launches: 51.91 MB at 50 iterations, 51.88 MB at 400.  The
-# global working set, x included, stays in the 126 MB L2, so a launch costs
-# a one-time read of its arrays and no DRAM traffic per iteration.
-PCG_DRAM_BYTES_PER_ITER = 0.0
-PCG_DRAM_BYTES_PER_LAUNCH = (51905280 + 51882240) / 2
-
-
-def pcg_bytes_setup(C: int, F: int) -> float:
+def pcg_bytes_setup(C: int, F: int, s: int = 8) -> float:
     """Initial residual pass: x, b, diag read; r, p written; matrix once."""
-    return 5 * C * 8 + F * (8 + 8)
+    return 5 * C * s + F * (s + 8)
 
 
-def cpu_baseline(seconds: float = 15.0) -> dict:
-    """The CPU oracle on a bounded sample: a 16x16x64 downscale of the pipe."""
-    import numpy as np  # noqa: F401
-
-    from tests.golden.oracle_harness import oracle_case
-
-    case = pipe_config(16, 64, 4.0)
-    _, mesh, _, algo = oracle_case("pipe_cpu", case_def=case)
-    algo.step()
-    steps, t0 = 0, time.perf_counter()
-    while True:
-        algo.step()
-        steps += 1
-        el = time.perf_counter() - t0
-        if el > seconds or steps >= 200:
-            break
-    return {
-        "value": mesh.n_cells * steps / el,
-        "unit": METRIC,
-        "cores": 1,
-        "kind": "port",
-        "sample": f"numpy oracle, pipe 16x16x64 ({mesh.n_cells} cells) PISO, {steps} steps in {el:.1f} s",
-    }
+# Measured DRAM bytes (read + write) per cell per iteration of the pressure
+# CG on the cylinder-wake octree, from ncu captures of fixed-length launches
+# on the 192x120x24 base (1,729,632 cells; the working set exceeds L2, so
+# the traffic grows in proportion to the cells).
+PCG_DRAM_BYTES_PER_CELL_ITER = None
 
 
-def _reference_worker(steps: int, warmup: int) -> tuple[int, float]:
-    """One CPU replica of the reference arm: the oracle pipe downscale,
-    ``warmup`` untimed and ``steps`` timed PISO steps; returns (cells, s)."""
-    from tests.golden.oracle_harness import oracle_case
+def _oracle_threads() -> int:
+    from oracle import native
 
-    case = pipe_config(32, 128, 4.0)
-    _, mesh, _, algo = oracle_case("pipe_ref", case_def=case)
-    for _ in range(warmup):
-        algo.step()
+    return native.num_threads()
+
+
+def oracle_step_sample(mesh, case_def: dict, steps: int = 1):
+    """The CPU oracle (numpy restatement, Krylov solves and repeated
+    scatter-adds in multi-threaded C) on ``mesh``: ``steps`` PISO steps from
+    the initial state.  Returns (seconds, algorithm)."""
+    from oracle import native
+    from oracle.algorithms import create_algorithm
+    from oracle.case import Case, CellField
+
+    native.enable()
+    case = Case(mesh, case_def["simulator"])
+    CellField(case, "U", "transient", (3,))
+    algo = create_algorithm(case)
     t0 = time.perf_counter()
     for _ in range(steps):
         algo.step()
-    return int(mesh.n_cells), time.perf_counter() - t0
+    return time.perf_counter() - t0, algo
+
+
+def cpu_baseline(mesh, case_def: dict) -> tuple[dict, object]:
+    """One PISO step of the workload itself (full mesh, from the initial
+    state) on the host: a bounded sample of about half a minute."""
+    el, algo = oracle_step_sample(mesh, case_def, 1)
+    its = [s.iterations for s in algo.last_stats["p"]]
+    line = {
+        "value": mesh.n_cells / el,
+        "unit": METRIC,
+        "cores": _oracle_threads(),
+        "kind": "port",
+        "sample": f"oracle (reference algorithm restated; Krylov and scatter-adds in OpenMP C), {WORKLOAD}, "
+                  f"the first PISO step from the initial state on the full mesh ({mesh.n_cells} cells) in "
+                  f"{el:.1f} s, pFinal CG iterations {its}",
+    }
+    return line, algo
 
 
 def run_reference(args) -> None:
-    """The reference arm: the reference algorithm (the numpy oracle port)
-    on every host core at once, one independent replica per core (numpy's
-    scatter-heavy steps are single-threaded), spawned processes."""
+    """The reference arm: the reference algorithm (the oracle port) on the
+    same mesh and case as the GPU arm, every host core, W untimed and K
+    timed PISO steps.  Under torchrun rank 0 alone runs it."""
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
-    import multiprocessing as mp
+    from oracle import native
 
-    cores = max(1, min(os.cpu_count() or 1, 64))
-    for var in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
-        os.environ.setdefault(var, "1")
-    with mp.get_context("spawn").Pool(cores) as pool:
-        res = pool.starmap(_reference_worker, [(args.steps, args.warmup)] * cores)
-    cells = res[0][0]
-    el = max(r[1] for r in res)
-    value = cells * args.steps * cores / el
+    native.build()
+    from gridfoam_b200.cases import build_mesh
+
+    case = workload_case()
+    mesh = build_mesh(case["mesh"])
+    from oracle.algorithms import create_algorithm
+    from oracle.case import Case, CellField
+
+    native.enable()
+    ocase = Case(mesh, case["simulator"])
+    CellField(ocase, "U", "transient", (3,))
+    algo = create_algorithm(ocase)
+    for _ in range(args.warmup):
+        algo.step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        algo.step()
+    el = time.perf_counter() - t0
+    value = mesh.n_cells * args.steps / el
+    cores = _oracle_threads()
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -193,98 +230,67 @@ def run_reference(args) -> None:
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample": f"pipe 32x32x128 per step, {cores} replicas (bounded sample)"},
+        "config": workload_config(mesh, world),
         "cpu_baseline": {
             "value": value,
             "unit": METRIC,
             "cores": cores,
             "kind": "port",
-            "sample": f"numpy oracle (reference algorithm restated), pipe 32x32x128 ({cells} cells) PISO, "
-                      f"{args.steps} steps on each of {cores} cores; slowest replica's time",
+            "sample": f"the whole run: {args.warmup} untimed and {args.steps} timed PISO steps of {WORKLOAD} on the "
+                      f"full mesh, oracle port (numpy; Krylov and scatter-adds in OpenMP C on {cores} threads)",
         },
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
 
 
-def mixed_variant(args, local: int, ref_algo, torch) -> dict:
-    """Same workload with the pressure CG in FP32 inside FP64 refinement.
+def _timed_steps(algo, steps: int, torch) -> float:
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        algo.step()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
 
-    Both runs start from the same initial state and take the same number of
-    steps; the reported errors are relative L2 norms against the FP64 run.
-    """
-    from tests.golden.device_harness import device_case
 
-    case = pipe_config()
+def _rel(a, b) -> float:
+    import numpy as np
+
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(np.asarray(b)), 1e-300))
+
+
+def mixed_variant(args, local: int, torch, first_fp64, oracle_first) -> dict:
+    """The workload with FP32 inner iterations of the pressure CG inside FP64
+    iterative refinement.  Errors: after the first step against the FP64
+    oracle (when it ran) and the FP64 GPU path; after warm-up plus the timed
+    steps against the FP64 GPU path run over the same steps."""
+    from gridfoam_b200.cases import create_case
+
+    case = workload_case()
     for key in ("p", "pFinal"):
         case["simulator"]["fvSolution"]["solvers"][key]["inner_precision"] = "float32"
-    _, _, grid, algo = device_case(case_def=case, device=f"cuda:{local}")
-    _, _, _, ref = device_case(case_def=pipe_config(), device=f"cuda:{local}")
-    n_steps = args.warmup + args.steps
-    for _ in range(args.warmup):
+    _, grid, algo = create_case(case, device=f"cuda:{local}")
+    algo.step()
+    torch.cuda.synchronize()
+    U1, p1 = algo.U.data.cpu().numpy(), algo.p.data.cpu().numpy()
+    out = {"rel_l2_U_vs_fp64_gpu_step1": _rel(U1, first_fp64[0]),
+           "rel_l2_p_vs_fp64_gpu_step1": _rel(p1, first_fp64[1])}
+    if oracle_first is not None:
+        out["rel_l2_U_vs_fp64_oracle_step1"] = _rel(U1, oracle_first[0])
+        out["rel_l2_p_vs_fp64_oracle_step1"] = _rel(p1, oracle_first[1])
+    for _ in range(max(0, args.warmup - 1)):
         algo.step()
-        ref.step()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(args.steps):
-        algo.step()
-    e1.record()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    for _ in range(args.steps):
-        ref.step()
-    torch.cuda.synchronize()
-    du = torch.linalg.vector_norm(algo.U.data - ref.U.data) / torch.linalg.vector_norm(ref.U.data)
-    dp = torch.linalg.vector_norm(algo.p.data - ref.p.data) / torch.linalg.vector_norm(ref.p.data)
+    ms = _timed_steps(algo, args.steps, torch)
     its = [s.iterations for s in algo.last_stats["p"]]
-    return {
+    out.update({
         "value": grid.num_cells * args.steps / (ms * 1e-3),
         "unit": METRIC,
         "ms_per_step": ms / args.steps,
-        "steps_compared": n_steps,
-        "rel_l2_U_vs_fp64": float(du),
-        "rel_l2_p_vs_fp64": float(dp),
-        "last_p_iterations": its,
-    }
-
-
-def octree_variant(args, local: int, torch) -> dict:
-    """Cylinder wake on a 3-level octree (hanging faces, general ELL path):
-    the cylinder-wake config at a 96x64x12 base, refined 2 levels within 2D
-    of the cylinder."""
-    from tests.golden.cases import cylinder_wake_case
-    from tests.golden.device_harness import device_case
-
-    case = cylinder_wake_case()
-    t0 = time.perf_counter()
-    _, _, grid, algo = device_case(case_def=case, device=f"cuda:{local}")
-    setup = time.perf_counter() - t0
-    for _ in range(args.warmup):
-        algo.step()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    its = []
-    e0.record()
-    for _ in range(args.steps):
-        algo.step()
-        its.append(algo.last_stats["p"])
-    e1.record()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    return {
-        "workload": case["name"] + "_piso",
-        "value": grid.num_cells * args.steps / (ms * 1e-3),
-        "unit": METRIC,
-        "ms_per_step": ms / args.steps,
-        "cells": grid.num_cells,
-        "internal_faces": grid.num_internal_faces,
-        "hanging_faces": grid.num_hanging,
-        "immersed_faces": grid.num_immersed_faces,
-        "ell_width": grid.ell_width,
-        "p_iterations_last_step": [s.iterations for s in its[-1]] if its else None,
-        "setup_s": setup,
-    }
+        "last_pfinal_iterations": its,
+    })
+    return out, algo
 
 
 def serving_bench(args, local: int, dist=None, rank: int = 0, world: int = 1) -> dict:
@@ -359,11 +365,86 @@ def serving_bench(args, local: int, dist=None, rank: int = 0, world: int = 1) ->
     return out
 
 
+def pipe_variant(args, local: int, torch) -> dict:
+    """The immersed Hagen-Poiseuille pipe (64x64x256 cells, PISO dt 1e-3),
+    FP64 and FP32-inner: cell-iters/s over the timed steps, the pressure CG
+    per iteration (its working set is L2-resident: against the measured
+    floor of its two grid reductions, not HBM), and after ``pipe_steps``
+    steps the relative L2 error of u_z against the analytic profile
+    2 (1 - r^2 / 0.16) over the cells in the last quarter of the pipe."""
+    import numpy as np
+
+    from gridfoam_b200.cases import create_case, pipe_analytic_uz, pipe_case
+
+    out = {}
+    finals = {}
+    for name, prec in (("fp64", "float64"), ("fp32_inner", "float32")):
+        case = pipe_case(64, 256, 4.0)
+        for key in ("p", "pFinal"):
+            case["simulator"]["fvSolution"]["solvers"][key]["inner_precision"] = prec
+        mesh, grid, algo = create_case(case, device=f"cuda:{local}")
+        psolvers = [s for n, s in algo.solvers.items() if n.startswith("p")]
+        for _ in range(args.warmup):
+            algo.step()
+        events: list = []
+        for s in psolvers:
+            s.profile_events = events
+        ms = _timed_steps(algo, args.steps, torch)
+        for s in psolvers:
+            s.profile_events = None
+        cg_ms = sum(a.elapsed_time(b) for a, b, _ in events)
+        cg_its = sum(st[0].iterations for _, _, st in events)
+        done = args.warmup + args.steps
+        t0 = time.perf_counter()
+        for _ in range(max(0, args.pipe_steps - done)):
+            algo.step()
+        torch.cuda.synchronize()
+        run_s = time.perf_counter() - t0
+        c = mesh.cell_centers
+        uz = algo.U.data[:, 2].cpu().numpy()
+        ref = pipe_analytic_uz(mesh, case["inlet_profile"])
+        sel = (c[:, 2] > 3.0) & (ref > 0.0)
+        finals[name] = algo.U.data.cpu().numpy()
+        out[name] = {
+            "value": grid.num_cells * args.steps / (ms * 1e-3),
+            "unit": METRIC,
+            "ms_per_step": ms / args.steps,
+            "p_cg_us_per_iteration": 1e3 * cg_ms / max(1, cg_its),
+            "steps_run": max(done, args.pipe_steps),
+            "wall_s_after_timed": run_s,
+            "rel_l2_uz_vs_analytic_last_quarter": float(np.linalg.norm(uz[sel] - ref[sel]) / np.linalg.norm(ref[sel])),
+        }
+        del algo, grid
+        torch.cuda.empty_cache()
+    out["workload"] = "ib_pipe_64x64x256_piso (1,048,576 cells)"
+    out["p_cg_sync_floor_us"] = 4.7
+    out["p_cg_sync_floor_note"] = ("two grid reductions of 1024-thread blocks on 148 SMs measured at 2.07 + 2.66 us "
+                                   "(empty loop); the CG working set (~90 MB) is L2-resident at this size")
+    out["rel_l2_U_fp32_inner_vs_fp64_gpu_final"] = _rel(finals["fp32_inner"], finals["fp64"])
+    return out
+
+
+def cavity_variant(local: int, torch) -> dict:
+    """The lid-driven cavity at 32^3, SIMPLE for 300 iterations (the
+    CPU-runnable config): wall time and cell-iters/s on the device."""
+    from gridfoam_b200.cases import cavity_case, create_case
+
+    case = cavity_case(32)
+    _, grid, algo = create_case(case, device=f"cuda:{local}")
+    algo.step()
+    ms = _timed_steps(algo, 299, torch)
+    return {"workload": "cavity_32^3_simple_300_iterations", "value": grid.num_cells * 299 / (ms * 1e-3),
+            "unit": METRIC, "ms_per_iteration": ms / 299,
+            "last_p_iterations": [s.iterations for s in algo.last_stats["p"]]}
+
+
 def run_gpu(args) -> None:
+    import numpy as np
     import torch
 
     import gridfoam_b200._lib as gl
-    from tests.golden.device_harness import device_case
+    from gridfoam_b200.cases import create_case
+    from gridfoam_b200.solvers.krylov import default_variant
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -377,10 +458,16 @@ def run_gpu(args) -> None:
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
-    case = pipe_config()
-    _, mesh, grid, algo = device_case(case_def=case, device=f"cuda:{local}")
+    case = workload_case()
+    t0 = time.perf_counter()
+    mesh, grid, algo = create_case(case, device=f"cuda:{local}")
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
     C, F = grid.num_cells, grid.num_internal_faces
-    for _ in range(args.warmup):
+    algo.step()
+    torch.cuda.synchronize()
+    first = (algo.U.data.cpu().numpy(), algo.p.data.cpu().numpy())
+    for _ in range(max(0, args.warmup - 1)):
         algo.step()
     torch.cuda.synchronize()
 
@@ -398,11 +485,9 @@ def run_gpu(args) -> None:
     torch.cuda.synchronize()
     gl.LAUNCHES.clear()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    stats = []
     start.record()
     for _ in range(args.steps):
         algo.step()
-        stats.append(algo.last_stats)
     stop.record()
     torch.cuda.synchronize()
     launches = sum(gl.LAUNCHES.values())
@@ -414,8 +499,9 @@ def run_gpu(args) -> None:
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
+    final = (algo.U.data.cpu().numpy(), algo.p.data.cpu().numpy())
 
-    # Roofline of the pressure PCG launches.
+    # Roofline of the pressure CG launches (HBM-bound at this size).
     durations, iters = [], []
     for ev0, ev1, st in events:
         durations.append(ev0.elapsed_time(ev1) * 1e-3)
@@ -424,32 +510,37 @@ def run_gpu(args) -> None:
     total_time = sum(durations)
     peak, peak_kind = peaks()
     achieved = total_bytes / total_time / 1e9 if total_time > 0 else 0.0
+    variant = default_variant(C, False, True, False)
+    step_bytes = total_bytes / args.steps
 
-    # End-to-end through the public API on the same trajectory as the timed
-    # region: a second case from the same initial state, the same warm-up,
-    # then the same steps, each taking U and p in from pinned host memory
-    # and reading them back into the same buffers (stream-ordered, so the
-    # next step's upload sees this step's result).
-    _, _, _, algo = device_case(case_def=pipe_config(), device=f"cuda:{local}")
+    # End-to-end through the public API on the same trajectory: a second
+    # case from the same initial state, the same warm-up, then the same
+    # steps, each taking U and p in from pinned host memory and reading them
+    # back into the same buffers (stream-ordered).
+    _, _, algo2 = create_case(workload_case(), device=f"cuda:{local}")
     for _ in range(args.warmup):
-        algo.step()
-    U_h = algo.U.data.detach().cpu().pin_memory()
-    p_h = algo.p.data.detach().cpu().pin_memory()
-    e2e_steps = args.steps
+        algo2.step()
+    U_h = algo2.U.data.detach().cpu().pin_memory()
+    p_h = algo2.p.data.detach().cpu().pin_memory()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    for _ in range(e2e_steps):
-        algo.U.data = U_h.to(algo.U.store.device, non_blocking=True)
-        algo.p.data = p_h.to(algo.p.store.device, non_blocking=True)
-        algo.step()
-        U_h.copy_(algo.U.data, non_blocking=True)
-        p_h.copy_(algo.p.data, non_blocking=True)
+    for _ in range(args.steps):
+        algo2.U.data = U_h.to(algo2.U.store.device, non_blocking=True)
+        algo2.p.data = p_h.to(algo2.p.store.device, non_blocking=True)
+        algo2.step()
+        U_h.copy_(algo2.U.data, non_blocking=True)
+        p_h.copy_(algo2.p.data, non_blocking=True)
     e1.record()
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    e2e_ms = e0.elapsed_time(e1) / args.steps
     h2d = U_h.numel() * 8 + p_h.numel() * 8
+    del algo2
+    torch.cuda.empty_cache()
 
+    per_launch_traffic = None
+    if PCG_DRAM_BYTES_PER_CELL_ITER is not None and iters:
+        per_launch_traffic = PCG_DRAM_BYTES_PER_CELL_ITER * C * sum(iters) / len(iters)
     value = C * world * args.steps / (ms * 1e-3)
     line = {
         "metric": METRIC,
@@ -464,31 +555,29 @@ def run_gpu(args) -> None:
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": {
-            "workload": WORKLOAD,
-            "cells": C,
-            "internal_faces": F,
-            "immersed_faces": grid.num_immersed_faces,
-            "algorithm": "piso nCorrectors=2, dt=1e-3, upwind, p cg+jacobi tol 1e-7 rel 0.01 (pFinal rel 0), "
-                         "U bicgstab+jacobi tol 1e-8 rel 0.1",
-            "l2": "working set larger than L2 (126 MB), no flush",
-            "parallelism": f"replicas x{world}",
+        "config": workload_config(mesh, world),
+        "workload_detail": {
+            "hanging_faces": grid.num_hanging,
+            "ell_width": grid.ell_width,
+            "setup_s": setup_s,
             "p_iterations_per_solve": (sum(iters) / len(iters)) if iters else None,
+            "p_solve_share_of_step": total_time * 1e3 / ms if ms > 0 else None,
+            "algorithmic_bytes_per_step_pcg": step_bytes,
+            "algorithmic_GBps_per_step_pcg": step_bytes / (ms / args.steps * 1e-3) / 1e9,
         },
         "roofline": {
-            "kernel": "k_pcg1_qrec_box (persistent Jacobi-PCG, fp64, q by recurrence)",
+            "kernel": f"pressure CG, variant {variant} (persistent Jacobi-PCG on the octree ELL rows, fp64)",
             "bound": "hbm",
             "achieved": achieved,
             "peak": peak,
             "peak_source": peak_kind,
             "unit": "GB/s",
             "frac": achieved / peak if peak else None,
-            "traffic": (PCG_DRAM_BYTES_PER_LAUNCH + PCG_DRAM_BYTES_PER_ITER * sum(iters) / len(iters))
-                       if iters else None,
-            "traffic_source": "ncu dram bytes of 50- and 400-iteration launches of the same kernel on the same box "
-                              "(equal within 0.05 %: a fixed part per launch, nothing per iteration)",
-            "note": "working set mostly L2-resident at 1M cells: DRAM traffic is well below the algorithmic "
-                    "bytes; the kernel is bound by L2 latency and two grid barriers per iteration",
+            "traffic": per_launch_traffic,
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per cell-iteration of fixed-length "
+                              "launches on the 192x120x24-base wake (1.73M cells, above L2), scaled to this "
+                              "launch's cells and mean iterations",
+            "bytes_model": "per iteration 14 C s + F (s + 8), s = 8, plus one initial pass 5 C s + F (s + 8)",
             "launches": len(durations),
             "avg_launch_ms": 1e3 * total_time / max(1, len(durations)),
         },
@@ -501,13 +590,31 @@ def run_gpu(args) -> None:
             "d2h_bytes_per_step": h2d,
         },
     }
+    oracle_first = None
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        cpu, oalgo = cpu_baseline(mesh, case)
+        line["cpu_baseline"] = cpu
+        oracle_first = (oalgo.U.data, oalgo.p.data)
+        line["parity_first_step_vs_fp64_oracle"] = {
+            "rel_l2_U": _rel(first[0], oracle_first[0]),
+            "rel_l2_p": _rel(first[1], oracle_first[1]),
+            "note": "full mesh, first PISO step from the initial state; p solves stop at rel_tolerance 0.01 "
+                    "(p) and 1e-7 absolute (pFinal), so two correct implementations differ inside that band",
+        }
+        del oalgo
     if not args.no_variants:
-        line["variants"] = {"mixed_fp32_inner": mixed_variant(args, local, algo, torch),
-                            "octree_cylinder_wake": octree_variant(args, local, torch)}
+        mixed, malgo = mixed_variant(args, local, torch, first, oracle_first)
+        mixed["rel_l2_U_vs_fp64_gpu_after_all_steps"] = _rel(malgo.U.data.cpu().numpy(), final[0])
+        mixed["rel_l2_p_vs_fp64_gpu_after_all_steps"] = _rel(malgo.p.data.cpu().numpy(), final[1])
+        del malgo
+        torch.cuda.empty_cache()
+        line["variants"] = {"mixed_fp32_inner": mixed,
+                            "ib_pipe_64x64x256": pipe_variant(args, local, torch),
+                            "cavity_32": cavity_variant(local, torch)}
+    del algo
+    torch.cuda.empty_cache()
     if not args.no_serving:
         line["serving"] = serving_bench(args, local, dist, rank, world)
-    if rank == 0 and not args.no_cpu_baseline and world == 1:
-        line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
     if rank == 0:
         print(json.dumps(line))
     if dist is not None:
@@ -519,12 +626,13 @@ def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="gridfoam_b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--pipe-steps", type=int, default=2000,
+                    help="PISO steps of the pipe variant before its error against the analytic profile")
     ap.add_argument("--serve-requests", type=int, default=64)
     ap.add_argument("--serve-end-time", type=int, default=100)
     ap.add_argument("--serve-slots", type=int, default=8)

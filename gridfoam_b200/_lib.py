@@ -79,6 +79,7 @@ class GfMesh(ctypes.Structure):
         ("hang_move_o", P),
         ("hang_move_n", P),
         ("face_axis", P),
+        ("ell_len", P),
     ]
 
 
@@ -163,6 +164,7 @@ class GfKrylov(ctypes.Structure):
         ("single_reduction", I32),
         ("inner_margin", F64),
         ("spin_limit", I64),
+        ("row_len", P),
     ]
 
 
@@ -200,6 +202,7 @@ _SIGNATURES = {
     "gf_fvc_div": ([P, I32, P, P, P], ctypes.c_int),
     "gf_reconstruct": ([P, P, P, P], ctypes.c_int),
     "gf_interpolate": ([P, I32, P, P, P, P, P, P], ctypes.c_int),
+    "gf_gauss_grad": ([P, I32, P, P, P], ctypes.c_int),
     "gf_sn_grad": ([P, I32, P, P, P, P, P, P, P, P], ctypes.c_int),
     "gf_correct_phi": ([P, P, P, P, P, P, P, P, F64, I32, P, P, P, P], ctypes.c_int),
     "gf_close_fixed_flux": ([P, I64, P, P, P, P, P], ctypes.c_int),

@@ -109,9 +109,9 @@ class _PressureVelocity:
         # gradients of U, p and HbyA (fv/kernels/face_interpolation.py).
         self._hanging = g.num_hanging > 0
         self._div_code = _lib.DIV_CODES[schemes.div_scheme(sim, self.phi.name, self.U.name).value]
-        for fld in (self.U, self.p):
-            if schemes.grad_scheme(sim, fld.name) != GradScheme.LEASTSQUARE:
-                raise NotImplementedError("the device path implements the leastsquare gradient scheme")
+        # Configured gradient scheme per field (fvc.grad, the TVD limiter);
+        # the hanging-face corrections always take the least-squares one.
+        self._gg = {fld.name: schemes.grad_scheme(sim, fld.name) == GradScheme.LINEAR for fld in (self.U, self.p)}
         self._alloc()
         self._adjust_classes = self._build_adjust_classes()
         self._p_ffp = any(bc.kind == _lib.BC_FIXED_FLUX_P for bc in self.p.bcs.values())
@@ -178,8 +178,17 @@ class _PressureVelocity:
         self.pEqn = FvMatrix(self.p)
         self.pSolve = FvMatrix(self.p)
         self.pred_source = torch.zeros((3, C), **f64)
+        # grad_p / grad_U_cfg: the configured gradients; grad_p_lsq / grad_U:
+        # the least-squares ones of the hanging-face corrections (the same
+        # buffers when the configured scheme is least squares).
         self.grad_p = torch.zeros((3, C), **f64)
         self.grad_U = torch.zeros((9, C), **f64)
+        gg_u, gg_p = self._gg[self.U.name], self._gg[self.p.name]
+        self.grad_U_cfg = torch.zeros((9, C), **f64) if gg_u else self.grad_U
+        self.grad_p_lsq = torch.zeros((3, C), **f64) if gg_p else self.grad_p
+        rows = g.num_internal_faces + g.num_bnd
+        self._gg_faces = {self.U.name: torch.zeros((3, rows), **f64) if gg_u else None,
+                          self.p.name: torch.zeros((1, rows), **f64) if gg_p else None}
         # Hanging faces: HbyA gradient and the pressure Laplacian's face flux
         # correction (zero off hanging faces).
         self.grad_H = torch.zeros((9, C) if self._hanging else (9, 1), **f64)
@@ -228,13 +237,29 @@ class _PressureVelocity:
         call("gf_lsq_grad", byref(self._grid.cmesh), field.num_components, ptr(field.store),
              ptr(t.kind), ptr(t.psib), ptr(out), stream_ptr())
 
+    def _grad_cfg(self, field: CellField, out: torch.Tensor, lsq: torch.Tensor) -> None:
+        """The configured gradient into ``out`` (fv/schemes/grad.py): least
+        squares, or Green-Gauss over the linear face values, whose hanging
+        correction needs the least-squares gradient (written to ``lsq``;
+        ``out`` is ``lsq`` itself when the scheme is least squares)."""
+        if not self._gg[field.name]:
+            self._grad(field, out)
+            return
+        from gridfoam_b200.fv.fvc import configured_grad
+
+        configured_grad(field, out, self._gg_faces[field.name], lsq)
+
     # ------------------------------------------------------------------
     # momentum predictor
     # ------------------------------------------------------------------
     def _assemble_momentum(self, relax: float) -> None:
         g = self._grid
         self._eval_U()
-        if self._div_code >= _lib.DIV_CODES["vanleer"] or self._hanging:
+        tvd = self._div_code >= _lib.DIV_CODES["vanleer"]
+        if tvd:
+            # also fills grad_U (the hanging corrections') on a hanging mesh
+            self._grad_cfg(self.U, self.grad_U_cfg, self.grad_U)
+        elif self._hanging:
             self._grad(self.U, self.grad_U)
         a = GfAssembly()
         a.ncomp = 3
@@ -246,7 +271,7 @@ class _PressureVelocity:
         a.gamma = None
         a.phi = ptr(self.phi.store)
         a.psi = ptr(self.U.store)
-        a.grad_psi = ptr(self.grad_U)
+        a.grad_psi = ptr(self.grad_U_cfg)
         if self.transient:
             ca, cb, cc = schemes.ddt_coefficients(self.U)
             a.use_ddt = 1
@@ -271,7 +296,7 @@ class _PressureVelocity:
                  ptr(self.UEqn.diag_store), ptr(self.UEqn.source_store), None, s)
         # predictor source b - V grad(p)
         self._eval_p()
-        self._grad(self.p, self.grad_p)
+        self._grad_cfg(self.p, self.grad_p, self.grad_p_lsq)
         call("gf_momentum_finalize", byref(g.cmesh), 3, 0.0, None, ptr(self.grad_p),
              ptr(self.UEqn.diag_store), ptr(self.UEqn.source_store), ptr(self.pred_source), s)
 
@@ -355,10 +380,12 @@ class _PressureVelocity:
             call("gf_axpby", g.num_cells, 1.0, ptr(self.rAtU.store), -1.0, ptr(self.rAU.store), ptr(self.d_r), s)
             self._eval_p()
             t = self.p.table
-            self._grad(self.p, self.grad_p)
+            # (with Green-Gauss on a hanging mesh this also leaves the
+            # least-squares gradient of the correction in grad_p_lsq)
+            self._grad_cfg(self.p, self.grad_p, self.grad_p_lsq)
             call("gf_correct_phi", byref(g.cmesh), ptr(self.phi_hbya.store), ptr(self.d_r), ptr(self.p.store),
                  ptr(t.kind), ptr(t.frac), ptr(t.refv), ptr(t.refg), 1.0, 1,
-                 ptr(self.grad_p) if self._hanging else None, None, ptr(self.phi_hbya.store), s)
+                 ptr(self.grad_p_lsq) if self._hanging else None, None, ptr(self.phi_hbya.store), s)
             call("gf_axpby", g.num_cells, 1.0, ptr(self.rAU.store), -1.0, ptr(self.rAtU.store), ptr(self.d_r), s)
             call("gf_correct_velocity", byref(g.cmesh), ptr(self.HbyA.store), ptr(self.d_r), ptr(self.grad_p),
                  ptr(self.HbyA.store), s)
@@ -388,8 +415,8 @@ class _PressureVelocity:
             a.val = ptr(self.pEqn.val)
             a.source = ptr(self.pEqn.source_store)
             if self._hanging:
-                self._grad(self.p, self.grad_p)
-                a.grad_lsq = ptr(self.grad_p)
+                self._grad(self.p, self.grad_p_lsq)
+                a.grad_lsq = ptr(self.grad_p_lsq)
                 a.lap_corrected = self._p_corrected
                 a.ffc = ptr(self.p_ffc)
             call("gf_assemble", byref(g.cmesh), byref(a), s)
@@ -428,7 +455,7 @@ class _PressureVelocity:
         """pressure_correction.py:338-363."""
         g = self._grid
         self._eval_p()
-        self._grad(self.p, self.grad_p)
+        self._grad_cfg(self.p, self.grad_p, self.grad_p_lsq)
         call("gf_correct_velocity", byref(g.cmesh), ptr(self.HbyA.store), ptr(self.rAtU.store), ptr(self.grad_p),
              ptr(self.U.store), stream_ptr())
         if self.u_cells.numel():

@@ -250,7 +250,19 @@ class AxisProjectedGrid:
         return host
 
     def _build_ell(self) -> None:
-        """Cell-centric slot table sorted by (cell, direction, face)."""
+        """Cell-centric slot table sorted by (cell, direction, face).
+
+        On meshes that are not uniform boxes the slots of a row are sorted
+        internal faces first, then domain faces, so the matrix entries of a
+        row lead it and ``ell_len`` (one past the last internal-face slot)
+        lets the Krylov kernels stop at the row's last entry instead of
+        reading the padding of the widest row.
+        """
+        self._build_ell_order(couplings_first=False)
+        if self.box_strides is None:
+            self._build_ell_order(couplings_first=True)
+
+    def _build_ell_order(self, *, couplings_first: bool) -> None:
         h = self.host
         C, F, Fb = self._num_cells, self._num_internal_faces, self._num_domain_bnd_faces
         fidx = np.arange(F, dtype=np.int64)
@@ -258,7 +270,10 @@ class AxisProjectedGrid:
         direction = np.concatenate([2 * h.axis + 1, 2 * h.axis, h.domain_dir])
         code = np.concatenate([fidx * 2, fidx * 2 + 1, (F + np.arange(Fb, dtype=np.int64)) * 2])
         nbr = np.concatenate([h.neighbour, h.owner, h.domain_owner])
-        order = np.lexsort((code, direction, cells))
+        if couplings_first:
+            order = np.lexsort((code, direction, code >= 2 * F, cells))
+        else:
+            order = np.lexsort((code, direction, cells))
         cells, code, nbr = cells[order], code[order], nbr[order]
         counts = np.bincount(cells, minlength=C)
         W = int(counts.max()) if counts.size else 1
@@ -277,10 +292,16 @@ class AxisProjectedGrid:
         p_int = pos[is_int]
         pos_owner[face_of[side_of == 0]] = p_int[side_of == 0]
         pos_neigh[face_of[side_of == 1]] = p_int[side_of == 1]
+        # One past the last internal-face slot of each row: later slots hold
+        # boundary faces or nothing, whose matrix coefficients are zero.
+        ell_len = np.zeros(C, dtype=np.int64)
+        np.maximum.at(ell_len, cells[is_int], rank[is_int] + 1)
         self._ell_width = W
-        self.box_strides = self._detect_box(ell_code, ell_nbr, W)
+        if not couplings_first:
+            self.box_strides = self._detect_box(ell_code, ell_nbr, W)
         h.extra.update(
-            ell_code=ell_code, ell_nbr=ell_nbr, face_pos_owner=pos_owner, face_pos_neigh=pos_neigh
+            ell_code=ell_code, ell_nbr=ell_nbr, face_pos_owner=pos_owner, face_pos_neigh=pos_neigh,
+            ell_len=ell_len,
         )
 
     def _detect_box(self, ell_code: np.ndarray, ell_nbr: np.ndarray, W: int) -> tuple[int, int] | None:
@@ -334,6 +355,7 @@ class AxisProjectedGrid:
             "lsq_ata_inv": f64(h.extra["lsq_ata_inv"].T),
             "ell_code": i32(h.extra["ell_code"]),
             "ell_nbr": i32(h.extra["ell_nbr"]),
+            "ell_len": torch.as_tensor(np.ascontiguousarray(h.extra["ell_len"], dtype=np.uint8), device=dev),
             "bnd_cell": i32(h.bnd_cell),
             "bnd_sf": f64(h.bnd_sf.T),
             "bnd_mag_sf": f64(h.bnd_mag_sf),

@@ -682,6 +682,53 @@ __global__ void k_fvc_div(gf_mesh_t m, int nc, const double* __restrict__ phi, d
     }
 }
 
+// Green-Gauss gradient from face values (fv/kernels/gauss_gradient.py:15-73):
+// grad(c) = sum over the faces of c of psi_f Sf (Sf outward from c) / V.
+// psi_f is a face field in the extended layout [F | Nb] (fvc.interpolate);
+// internal faces enter with +Sf on the owner side and -Sf on the neighbour
+// side, boundary and immersed faces with their outward Sf.
+template <int NC>
+__global__ void k_gauss_grad(gf_mesh_t m, const double* __restrict__ psif, double* __restrict__ grad) {
+    const int64_t C = m.n_cells;
+    const int64_t F = m.n_faces;
+    const int64_t Nb = m.n_bnd;
+    const int64_t rows = F + Nb;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < C;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        double g[NC][3];
+#pragma unroll
+        for (int k = 0; k < NC; ++k) g[k][0] = g[k][1] = g[k][2] = 0.0;
+        for (int s = 0; s < m.ell_width; ++s) {
+            const Slot sl = decode_slot(m, __ldg(m.ell_code + s * C + c));
+            double S[3];
+            int64_t row;
+            if (sl.kind == kInternal) {
+                const double sign = sl.side ? -1.0 : 1.0;
+#pragma unroll
+                for (int j = 0; j < 3; ++j) S[j] = sign * __ldg(m.sf + j * F + sl.face);
+                row = sl.face;
+            } else if (sl.kind == kBoundary) {
+#pragma unroll
+                for (int j = 0; j < 3; ++j) S[j] = __ldg(m.bnd_sf + j * Nb + sl.bnd);
+                row = F + sl.bnd;
+            } else {
+                continue;
+            }
+#pragma unroll
+            for (int k = 0; k < NC; ++k) {
+                const double v = psif[k * rows + row];
+#pragma unroll
+                for (int j = 0; j < 3; ++j) g[k][j] += v * S[j];
+            }
+        }
+        const double vol = __ldg(m.volume + c);
+#pragma unroll
+        for (int k = 0; k < NC; ++k)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) grad[(k * 3 + j) * C + c] = g[k][j] / vol;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Deterministic reductions (single pass of block partials + one final block)
 // ---------------------------------------------------------------------------
@@ -773,7 +820,8 @@ __global__ void k_spmv(gf_mesh_t m, const double* __restrict__ diag, const doubl
         double acc[NC];
 #pragma unroll
         for (int k = 0; k < NC; ++k) acc[k] = d * x[k * C + c];
-        for (int s = 0; s < W; ++s) {
+        const int Wc = m.ell_len ? (int)__ldg(m.ell_len + c) : W;
+        for (int s = 0; s < Wc; ++s) {
             const double v = val[s * C + c];
             const int n = __ldg(m.ell_nbr + s * C + c);
 #pragma unroll
@@ -798,7 +846,8 @@ __global__ void k_rau_hbya(gf_mesh_t m, const double* __restrict__ diag, const d
         double hsum = 0.0;
 #pragma unroll
         for (int k = 0; k < NC; ++k) off[k] = 0.0;
-        for (int s = 0; s < W; ++s) {
+        const int Wc = m.ell_len ? (int)__ldg(m.ell_len + c) : W;
+        for (int s = 0; s < Wc; ++s) {
             const double a = val[s * C + c];
             const int n = __ldg(m.ell_nbr + s * C + c);
             hsum += -a;
@@ -1230,7 +1279,8 @@ __global__ void k_residual_partial(gf_mesh_t m, const double* __restrict__ diag,
         double acc[NC];
 #pragma unroll
         for (int k = 0; k < NC; ++k) acc[k] = d * psi[k * C + c];
-        for (int s = 0; s < W; ++s) {
+        const int Wc = m.ell_len ? (int)__ldg(m.ell_len + c) : W;
+        for (int s = 0; s < Wc; ++s) {
             const double v = val[s * C + c];
             const int n = __ldg(m.ell_nbr + s * C + c);
 #pragma unroll
@@ -1545,6 +1595,20 @@ int gf_fvc_div(const gf_mesh_t* m, int32_t ncomp, const double* phi, double* out
     if (!valid_mesh(m) || !valid_nc(ncomp)) return GF_ERR_INVALID;
     k_fvc_div<<<grid_for(m->n_cells), kThreads, 0, GF_STREAM(stream)>>>(*m, ncomp, phi, out);
     return check_launch("gf_fvc_div");
+}
+
+int gf_gauss_grad(const gf_mesh_t* m, int32_t ncomp, const double* psi_f, double* grad, void* stream) {
+    if (!valid_mesh(m) || !valid_nc(ncomp) || psi_f == nullptr || grad == nullptr || m->sf == nullptr ||
+        m->bnd_sf == nullptr) {
+        set_error("gf_gauss_grad: invalid arguments");
+        return GF_ERR_INVALID;
+    }
+    const unsigned g = grid_for(m->n_cells);
+    cudaStream_t st = GF_STREAM(stream);
+    if (ncomp == 1) k_gauss_grad<1><<<g, kThreads, 0, st>>>(*m, psi_f, grad);
+    else if (ncomp == 2) k_gauss_grad<2><<<g, kThreads, 0, st>>>(*m, psi_f, grad);
+    else k_gauss_grad<3><<<g, kThreads, 0, st>>>(*m, psi_f, grad);
+    return check_launch("gf_gauss_grad");
 }
 
 int gf_interpolate(const gf_mesh_t* m, int32_t ncomp, const double* psi, const int8_t* bc_kind, const double* psib,

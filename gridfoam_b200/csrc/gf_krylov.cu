@@ -21,6 +21,8 @@ constexpr int kMaxBlocks = 1024;
 constexpr int kMaxNV = 16;
 constexpr int kCtlDoubles = 32;
 constexpr long long kSpinLimit = 30000000LL;  // x ~40 ns polls: about a second
+// Slots of a runtime-width matrix row whose loads are issued together.
+constexpr int kSlotGroup = 8;
 
 // Partial sums are double-buffered by barrier parity: a block may write the
 // next barrier's partials while a slower block still reads this one's, but
@@ -383,15 +385,34 @@ template <int NC, int WIDTH = 0, class G>
 __device__ __forceinline__ void row_apply(const gf_krylov_t& K, int64_t c, const G& g, double (&out)[NC]) {
     const int64_t n = K.n;
     const double d = __ldg(K.diag + c);
-    const int W = WIDTH > 0 ? WIDTH : K.width;
 #pragma unroll
     for (int k = 0; k < NC; ++k) out[k] = d * g(k, c);
+    if (WIDTH > 0) {
 #pragma unroll
-    for (int s = 0; s < W; ++s) {
-        const double a = __ldg(K.val + s * n + c);
-        const int nb = __ldg(K.nbr + s * n + c);
+        for (int s = 0; s < (WIDTH > 0 ? WIDTH : 1); ++s) {
+            const double a = __ldg(K.val + s * n + c);
+            const int nb = __ldg(K.nbr + s * n + c);
 #pragma unroll
-        for (int k = 0; k < NC; ++k) out[k] += a * g(k, nb);
+            for (int k = 0; k < NC; ++k) out[k] += a * g(k, nb);
+        }
+        return;
+    }
+    // Runtime row length: loads of a slot group first (see EllRows).
+    const int W = K.row_len ? (int)__ldg(K.row_len + c) : K.width;
+    for (int s0 = 0; s0 < W; s0 += kSlotGroup) {
+        int nb[kSlotGroup];
+        double a[kSlotGroup];
+#pragma unroll
+        for (int j = 0; j < kSlotGroup; ++j) {
+            const int s = s0 + j;
+            nb[j] = s < W ? __ldg(K.nbr + s * n + c) : (int)c;
+            a[j] = s < W ? __ldg(K.val + s * n + c) : 0.0;
+        }
+#pragma unroll
+        for (int j = 0; j < kSlotGroup; ++j)
+            if (s0 + j < W)
+#pragma unroll
+                for (int k = 0; k < NC; ++k) out[k] += a[j] * g(k, nb[j]);
     }
 }
 
@@ -593,6 +614,8 @@ struct EllRows {
     const int32_t* nbr;
     I n;
     int w;
+    // Row lengths (gf_krylov_t row_len) or nullptr: row c stops at len[c].
+    const uint8_t* len = nullptr;
     template <typename A, class G>
     __device__ __forceinline__ A apply(I c, A dc, const G& g) const {
         A acc = dc * g(c);
@@ -607,7 +630,28 @@ struct EllRows {
 #pragma unroll
             for (int s = 0; s < (WIDTH > 0 ? WIDTH : 1); ++s) acc += a[s] * g(nb[s]);
         } else {
-            for (int s = 0; s < w; ++s) acc += (A)ld_coef(val + s * n + c) * g(__ldg(nbr + s * n + c));
+            // Slots in groups of kSlotGroup: every coefficient and index load
+            // of a group is issued before its gathers, so a thread keeps
+            // many loads in flight (a plain loop over a runtime row length
+            // waits for each slot's index before its gather).  The products
+            // are added in slot order, as in the plain loop.
+            const int ws = len ? (int)__ldg(len + c) : w;
+            for (int s0 = 0; s0 < ws; s0 += kSlotGroup) {
+                int nb[kSlotGroup];
+                A a[kSlotGroup];
+#pragma unroll
+                for (int j = 0; j < kSlotGroup; ++j) {
+                    const int s = s0 + j;
+                    nb[j] = s < ws ? __ldg(nbr + s * n + c) : (int)c;
+                    a[j] = s < ws ? (A)ld_coef(val + s * n + c) : (A)0;
+                }
+                A gv[kSlotGroup];
+#pragma unroll
+                for (int j = 0; j < kSlotGroup; ++j) gv[j] = s0 + j < ws ? g(nb[j]) : (A)0;
+#pragma unroll
+                for (int j = 0; j < kSlotGroup; ++j)
+                    if (s0 + j < ws) acc += a[j] * gv[j];
+            }
         }
         return acc;
     }
@@ -831,7 +875,7 @@ __device__ void pcg1_body(const gf_krylov_t& K, const Rows& rows) {
 
 template <int WIDTH>
 __global__ void __launch_bounds__(kCgThreads, 4) k_pcg1(gf_krylov_t K) {
-    EllRows<double, WIDTH> rows{K.val, K.nbr, K.n, K.width};
+    EllRows<double, WIDTH> rows{K.val, K.nbr, K.n, K.width, K.row_len};
     pcg1_body<kCgThreads, 1>(K, rows);
 }
 
@@ -980,7 +1024,7 @@ __device__ void pcg1_sr_body(const gf_krylov_t& K, const Rows& rows) {
 
 template <int WIDTH>
 __global__ void __launch_bounds__(kCgThreads, 4) k_pcg1_sr(gf_krylov_t K) {
-    EllRows<double, WIDTH> rows{K.val, K.nbr, K.n, K.width};
+    EllRows<double, WIDTH> rows{K.val, K.nbr, K.n, K.width, K.row_len};
     pcg1_sr_body<kCgThreads>(K, rows);
 }
 
@@ -1202,8 +1246,8 @@ __device__ void pcg1_mixed_body(const gf_krylov_t& K, const Rows64& rows64, Rows
 
 template <int WIDTH>
 __global__ void __launch_bounds__(kCgThreads, 4) k_pcg1_mixed(gf_krylov_t K) {
-    EllRows<double, WIDTH> rows64{K.val, K.nbr, K.n, K.width};
-    EllRows<float, WIDTH> rows32{nullptr, K.nbr, K.n, K.width};
+    EllRows<double, WIDTH> rows64{K.val, K.nbr, K.n, K.width, K.row_len};
+    EllRows<float, WIDTH> rows32{nullptr, K.nbr, K.n, K.width, K.row_len};
     pcg1_mixed_body<kCgThreads, 1>(K, rows64, rows32, K.width);
 }
 
@@ -1236,6 +1280,34 @@ constexpr int kQrecVariant = 8;
 // blocks, one (10) or two (11) cells per thread per gather pass; falls back
 // to variant 8 when its four vectors do not fit.
 constexpr int kHaloVariant = 10;
+// Streaming q-recurrence CG with the vectors in the workspace
+// (pcg1_stream_body): 512-thread blocks, two an SM (12); 1024-thread
+// blocks (13); 256-thread blocks, four an SM (14).  FP64, one system.
+constexpr int kStreamVariant = 12;
+constexpr int kStreamVariants = 3;
+
+// ELL (octree) FP64 CG in the launch shapes of the box variants 0-4.
+template <int WIDTH, int THREADS, int U>
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_pcg1_ellv(gf_krylov_t K) {
+    EllRows<double, WIDTH> rows{K.val, K.nbr, K.n, K.width, K.row_len};
+    pcg1_body<THREADS, U>(K, rows);
+}
+
+template <int WIDTH>
+static BoxVariant ell_kernel(int variant) {
+    switch (variant) {
+        case 1:
+            return {(void*)k_pcg1_ellv<WIDTH, 256, 2>, 256, 2};
+        case 2:
+            return {(void*)k_pcg1_ellv<WIDTH, 512, 1>, 512, 1};
+        case 3:
+            return {(void*)k_pcg1_ellv<WIDTH, 1024, 1>, 1024, 1};
+        case 4:
+            return {(void*)k_pcg1_ellv<WIDTH, 1024, 2>, 1024, 2};
+        default:
+            return {(void*)k_pcg1<WIDTH>, kCgThreads, 1};
+    }
+}
 
 template <bool MIXED, bool SYM, int THREADS, int U>
 static BoxVariant box_variant() {
@@ -1839,7 +1911,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_pcg1_smem_box(gf_krylov_t K, int
 
 template <int WIDTH, int THREADS, bool KEEP_P>
 __global__ void __launch_bounds__(THREADS, 1) k_pcg1_smem_ell(gf_krylov_t K, int chunk) {
-    EllRows<double, WIDTH, int> rows{K.val, K.nbr, (int)K.n, K.width};
+    EllRows<double, WIDTH, int> rows{K.val, K.nbr, (int)K.n, K.width, K.row_len};
     pcg1_smem_body<THREADS, smem_gather_cells(THREADS), smem_update_cells(THREADS), KEEP_P>(K, rows, chunk);
 }
 
@@ -2016,8 +2088,164 @@ __global__ void __launch_bounds__(THREADS, 1) k_pcg1_qrec_box(gf_krylov_t K, int
 
 template <int WIDTH, int THREADS, int U>
 __global__ void __launch_bounds__(THREADS, 1) k_pcg1_qrec_ell(gf_krylov_t K, int chunk) {
-    EllRows<double, WIDTH, int> rows{K.val, K.nbr, (int)K.n, K.width};
+    EllRows<double, WIDTH, int> rows{K.val, K.nbr, (int)K.n, K.width, K.row_len};
     pcg1_qrec_body<THREADS, U, 2>(K, rows, chunk);
+}
+
+// ---------------------------------------------------------------------------
+// Streaming q-recurrence CG for systems too large for shared memory (octree
+// grids of millions of cells).  The recurrences are those of pcg1_qrec_body
+// (q_k = A z_k + beta q_(k-1), so the stencil gathers z alone), with every
+// vector in the workspace: an iteration reads a cell's row (up to its row
+// length), z, p, q and x in the gather pass and r, q and the Jacobi inverse
+// in the update pass, about 180 bytes a cell against 230 for pcg1_body,
+// whose gather reads z and p at every stencil point.  Each block owns one
+// contiguous chunk of cells, so the gathers of a block stay within a short
+// window of the cell order (Morton order within each refinement level).
+// x += alpha p of iteration k runs in the gather pass of iteration k + 1,
+// which reads p anyway (the same additions in the same order), and once
+// more after the last iteration.
+template <int THREADS, class Rows>
+__device__ void pcg1_stream_body(const gf_krylov_t& K, const Rows& rows, int chunk) {
+    __shared__ CgState st;
+    KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
+    barrier_init(K);
+    double* partials = K.work + kCtlDoubles;
+    double* vec = partials + kPartials;
+    const int n = (int)K.n;
+    double* z = vec;
+    double* inv = vec + n;
+    double* r = vec + 2 * (int64_t)n;
+    double* p = vec + 3 * (int64_t)n;
+    double* q = vec + 4 * (int64_t)n;
+    double* x = K.x;
+    const int c0 = blockIdx.x * chunk;
+    const int c1 = c0 + chunk < n ? c0 + chunk : n;
+    const bool jac = K.jacobi != 0, linf = K.norm_inf != 0;
+    bool ok = true;
+    {  // r = b - A x, z = M r, p = q = 0; |r| and r.z
+        double loc[2] = {0.0, 0.0};
+        auto gx = [&](int i) { return __ldcg(x + i); };
+        for (int c = c0 + threadIdx.x; c < c1; c += THREADS) {
+            const double ax = rows.apply(c, __ldg(K.diag + c), gx);
+            const double rk = __ldg(K.rhs + c) - ax;
+            const double iv = inv_diag(K.diag, c, jac);
+            const double zk = iv * rk;
+            __stcg(r + c, rk);
+            __stcg(q + c, 0.0);
+            __stcg(p + c, 0.0);
+            __stcg(inv + c, iv);
+            __stcg(z + c, zk);
+            loc[0] = norm_acc(loc[0], rk, linf);
+            loc[1] += rk * zk;
+        }
+        ok = grid_reduce<2, THREADS>(ctl, partials, loc, linf ? 1u : 0u);
+        if (threadIdx.x == 0) {
+            const double r0 = norm_fin(loc[0], linf);
+            st.r0 = r0;
+            st.final = r0;
+            st.thresh = fmax(K.atol, K.rtol * r0);
+            st.rz_old = loc[1];
+            st.beta = 0.0;
+            st.alpha = 0.0;
+            st.its = 0;
+            st.converged = 0;
+            st.status = GF_MAX_ITER;
+            st.done = 0;
+            if (r0 < st.thresh) {
+                st.done = 1;
+                st.converged = 1;
+                st.status = GF_OK;
+            } else if (!isfinite(r0)) {
+                st.done = 1;
+                st.status = GF_NONFINITE;
+            }
+        }
+        __syncthreads();
+    }
+    bool pending = false;  // x += alpha p of the last update pass not yet applied
+    for (int it = 1; ok && !st.done && it <= K.max_iter; ++it) {
+        {  // x += alpha_(k-1) p; w = A z; p = z + beta p; q = w + beta q; p . q
+            const double beta = st.beta, alpha_prev = st.alpha;
+            double loc[1] = {0.0};
+            // Plain (L1-cacheable) loads: z is written only before the grid
+            // barrier that precedes this pass (see pcg1_smem_body).
+            auto gz = [&](int j) { return z[j]; };
+            for (int c = c0 + threadIdx.x; c < c1; c += THREADS) {
+                const double zc = z[c];
+                const double w = rows.apply(c, __ldg(K.diag + c), gz);
+                const double pold = __ldcg(p + c);
+                const double qold = __ldcg(q + c);
+                if (pending) __stcg(x + c, __ldcg(x + c) + alpha_prev * pold);
+                const double pk = zc + pold * beta;
+                const double qk = w + qold * beta;
+                __stcg(p + c, pk);
+                __stcg(q + c, qk);
+                loc[0] += pk * qk;
+            }
+            ok = grid_reduce<1, THREADS>(ctl, partials, loc, 0u);
+            if (!ok) break;
+            if (threadIdx.x == 0) st.alpha = st.rz_old / loc[0];
+            __syncthreads();
+        }
+        {  // r -= alpha q; z = M r; |r|, r.z
+            const double alpha = st.alpha;
+            double loc[2] = {0.0, 0.0};
+            for (int c = c0 + threadIdx.x; c < c1; c += THREADS) {
+                const double rk = __ldcg(r + c) - alpha * __ldcg(q + c);
+                const double zk = __ldcg(inv + c) * rk;
+                __stcg(r + c, rk);
+                __stcg(z + c, zk);
+                loc[0] = norm_acc(loc[0], rk, linf);
+                loc[1] += rk * zk;
+            }
+            pending = true;
+            ok = grid_reduce<2, THREADS>(ctl, partials, loc, linf ? 1u : 0u);
+            if (!ok) break;
+            if (threadIdx.x == 0) {
+                const double fin = norm_fin(loc[0], linf);
+                st.final = fin;
+                if (fin < st.thresh) {
+                    st.done = 1;
+                    st.converged = 1;
+                    st.its = it;
+                    st.status = GF_OK;
+                } else if (!isfinite(fin)) {
+                    st.done = 1;
+                    st.its = it;
+                    st.status = GF_NONFINITE;
+                } else {
+                    st.beta = loc[1] / st.rz_old;
+                    st.rz_old = loc[1];
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (ok && pending) {  // the last iteration's x += alpha p (own cells only)
+        const double alpha = st.alpha;
+        for (int c = c0 + threadIdx.x; c < c1; c += THREADS) __stcg(x + c, __ldcg(x + c) + alpha * __ldcg(p + c));
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        double* o = K.stats;
+        o[0] = st.r0;
+        o[1] = st.final;
+        o[2] = st.done ? st.its : K.max_iter;
+        o[3] = st.converged;
+        o[4] = ok ? st.status : GF_ERR_TIMEOUT;
+    }
+}
+
+template <bool SYM, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) k_pcg1_stream_box(gf_krylov_t K, int chunk) {
+    BoxRows<double, SYM, false, int> rows{K.val, (int)K.n, (int)K.stride_y, (int)K.stride_z};
+    pcg1_stream_body<THREADS>(K, rows, chunk);
+}
+
+template <int WIDTH, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) k_pcg1_stream_ell(gf_krylov_t K, int chunk) {
+    EllRows<double, WIDTH, int> rows{K.val, K.nbr, (int)K.n, K.width, K.row_len};
+    pcg1_stream_body<THREADS>(K, rows, chunk);
 }
 
 // ---------------------------------------------------------------------------
@@ -2281,7 +2509,7 @@ __global__ void __launch_bounds__(1024, 1) k_pcg1_halo_box(gf_krylov_t K, int ch
 
 template <int WIDTH, int U>
 __global__ void __launch_bounds__(1024, 1) k_pcg1_halo_ell(gf_krylov_t K, int chunk) {
-    EllRows<double, WIDTH, int> rows{K.val, K.nbr, (int)K.n, K.width};
+    EllRows<double, WIDTH, int> rows{K.val, K.nbr, (int)K.n, K.width, K.row_len};
     pcg1_halo_body<1024, U, 2>(K, rows, chunk);
 }
 
@@ -2502,8 +2730,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_pcg1_mixed_smem_box(gf_krylov_t 
 
 template <int WIDTH, int THREADS, bool KEEP_P>
 __global__ void __launch_bounds__(THREADS, 1) k_pcg1_mixed_smem_ell(gf_krylov_t K, int chunk) {
-    EllRows<double, WIDTH, int> rows64{K.val, K.nbr, (int)K.n, K.width};
-    EllRows<float, WIDTH, int> rows32{nullptr, K.nbr, (int)K.n, K.width};
+    EllRows<double, WIDTH, int> rows64{K.val, K.nbr, (int)K.n, K.width, K.row_len};
+    EllRows<float, WIDTH, int> rows32{nullptr, K.nbr, (int)K.n, K.width, K.row_len};
     pcg1_mixed_smem_body<THREADS, smem_gather_cells(THREADS), smem_update_cells(THREADS), KEEP_P>(
         K, rows64, rows32, K.width, chunk);
 }
@@ -2706,8 +2934,8 @@ __global__ void __launch_bounds__(1024, 1) k_pcg1_mixed_qrec_box(gf_krylov_t K, 
 
 template <int WIDTH, int U>
 __global__ void __launch_bounds__(1024, 1) k_pcg1_mixed_qrec_ell(gf_krylov_t K, int chunk) {
-    EllRows<double, WIDTH, int> rows64{K.val, K.nbr, (int)K.n, K.width};
-    EllRows<float, WIDTH, int> rows32{nullptr, K.nbr, (int)K.n, K.width};
+    EllRows<double, WIDTH, int> rows64{K.val, K.nbr, (int)K.n, K.width, K.row_len};
+    EllRows<float, WIDTH, int> rows32{nullptr, K.nbr, (int)K.n, K.width, K.row_len};
     pcg1_mixed_qrec_body<1024, U, 1>(K, rows64, rows32, K.width, chunk);
 }
 
@@ -2922,8 +3150,8 @@ __global__ void __launch_bounds__(1024, 1) k_pcg1_mixed_halo_box(gf_krylov_t K, 
 
 template <int WIDTH>
 __global__ void __launch_bounds__(1024, 1) k_pcg1_mixed_halo_ell(gf_krylov_t K, int chunk) {
-    EllRows<double, WIDTH, int> rows64{K.val, K.nbr, (int)K.n, K.width};
-    EllRows<float, WIDTH, int> rows32{nullptr, K.nbr, (int)K.n, K.width};
+    EllRows<double, WIDTH, int> rows64{K.val, K.nbr, (int)K.n, K.width, K.row_len};
+    EllRows<float, WIDTH, int> rows32{nullptr, K.nbr, (int)K.n, K.width, K.row_len};
     pcg1_mixed_halo_body<1024>(K, rows64, rows32, K.width, chunk);
 }
 
@@ -3405,6 +3633,63 @@ static const void* qrec_kernel(const gf_krylov_t* k) {
 static int launch_smem_arrays(const gf_krylov_t* k, void* stream, int threads, int narr, size_t elem,
                               const void* kern);
 
+template <int THREADS, int MINB>
+static const void* stream_kernel(const gf_krylov_t* k) {
+    if (k->stride_y > 0)
+        return k->symmetric ? (const void*)k_pcg1_stream_box<true, THREADS, MINB>
+                            : (const void*)k_pcg1_stream_box<false, THREADS, MINB>;
+    return k->width == 6 ? (const void*)k_pcg1_stream_ell<6, THREADS, MINB>
+                         : (const void*)k_pcg1_stream_ell<0, THREADS, MINB>;
+}
+
+// Streaming CG (variants 12-14): every co-resident block owns one contiguous
+// chunk of cells.  GF_ERR_INVALID (no launch) where 32-bit cell indices do
+// not reach every coefficient slot.
+static int launch_stream(const gf_krylov_t* k, void* stream, int which) {
+    const char* what = "gf_pcg_solve";
+    const int64_t row_span = (int64_t)(k->stride_y > 0 ? 6 : (k->width > 6 ? k->width : 6)) * k->n;
+    if (row_span >= ((int64_t)1 << 31)) {
+        set_error("%s: system not eligible for the streaming CG", what);
+        return GF_ERR_INVALID;
+    }
+    const void* kern = which == 1 ? stream_kernel<1024, 1>(k) : which == 2 ? stream_kernel<256, 4>(k)
+                                                                           : stream_kernel<512, 2>(k);
+    const int threads = which == 1 ? 1024 : which == 2 ? 256 : 512;
+    int dev = 0, sms = 0, coop = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    int per_sm = 0;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, 0);
+    if (e != cudaSuccess || !coop || per_sm < 1) {
+        set_error("%s: streaming CG set-up failed: %s", what, cudaGetErrorString(e));
+        return GF_ERR_CUDA;
+    }
+    int64_t grid = (int64_t)per_sm * sms;
+    const int64_t want = (k->n + threads - 1) / threads;
+    if (grid > want) grid = want;
+    if (grid > kMaxBlocks) grid = kMaxBlocks;
+    if (k->block_cap > 0 && grid > k->block_cap) grid = k->block_cap;
+    if (grid < 1) grid = 1;
+    const int64_t chunk = (k->n + grid - 1) / grid;
+    grid = (k->n + chunk - 1) / chunk;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    e = cudaMemsetAsync(k->work, 0, sizeof(KCtl), st);
+    if (e != cudaSuccess) {
+        set_error("%s: %s", what, cudaGetErrorString(e));
+        return GF_ERR_CUDA;
+    }
+    gf_krylov_t arg = *k;
+    int ch = (int)chunk;
+    void* args[] = {&arg, &ch};
+    e = cudaLaunchCooperativeKernel(kern, dim3((unsigned)grid), dim3(threads), args, 0, st);
+    if (e != cudaSuccess) {
+        set_error("%s: cooperative launch failed: %s", what, cudaGetErrorString(e));
+        return GF_ERR_CUDA;
+    }
+    return GF_OK;
+}
+
 // FP64: 4 doubles a cell with p kept, else 3.  Mixed: 5 floats, else 4.
 static int launch_smem(const gf_krylov_t* k, void* stream, int threads) {
     const bool mixed = k->mixed != 0;
@@ -3647,6 +3932,10 @@ int gf_pcg_solve(const gf_krylov_t* k, void* stream) {
                 const int st = launch_halo(k, stream, k->variant == kHaloVariant ? 1 : 2);
                 if (st != GF_ERR_INVALID) return st;
             }
+            if (k->variant >= kStreamVariant && k->variant < kStreamVariant + kStreamVariants) {
+                const int st = launch_stream(k, stream, k->variant - kStreamVariant);
+                if (st != GF_ERR_INVALID) return st;
+            }
             if (box && k->variant == kStagedVariant) {
                 const int T = staged_tile(k);
                 if (T > 0) return launch_staged(k, T, stream);
@@ -3658,8 +3947,12 @@ int gf_pcg_solve(const gf_krylov_t* k, void* stream) {
                 const BoxVariant bv = k->symmetric ? box_kernel<false, true>(v) : box_kernel<false, false>(v);
                 return launch_persistent(bv.kern, k, stream, "gf_pcg_solve", bv.threads, bv.unroll);
             }
-            if (k->width == 6) return launch_persistent(k_pcg1<6>, k, stream, "gf_pcg_solve", kCgThreads);
-            return launch_persistent(k_pcg1<0>, k, stream, "gf_pcg_solve", kCgThreads);
+            {
+                // Variants beyond the five launch shapes fall back to 256 x 1.
+                const int v = (k->variant >= 0 && k->variant < kBoxVariants) ? k->variant : 0;
+                const BoxVariant ev = k->width == 6 ? ell_kernel<6>(v) : ell_kernel<0>(v);
+                return launch_persistent(ev.kern, k, stream, "gf_pcg_solve", ev.threads, ev.unroll);
+            }
         case 2:
             return launch_persistent(k_pcg<2>, k, stream, "gf_pcg_solve");
         default:

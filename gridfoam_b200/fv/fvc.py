@@ -27,16 +27,44 @@ def _eval_state(field: CellField) -> None:
 
 
 def grad(field: CellField) -> CellField:
-    """fv/fvc/grad.py:8-34 (least-squares, fv/kernels/least_squares.py:29-101)."""
+    """fv/fvc/grad.py:8-34 with the configured scheme: ``leastsquare``
+    (fv/kernels/least_squares.py:29-101) or ``linear``, Green-Gauss over the
+    hierarchy-aware linear face values (fv/schemes/grad.py:21-43)."""
     grid = field.grid
-    if schemes.grad_scheme(grid.sim_config, field.name) != GradScheme.LEASTSQUARE:
-        raise NotImplementedError("the device path implements the leastsquare gradient scheme")
     _eval_state(field)
     out = get_or_create_cellfield(grid, f"grad({field.name})", field.role, field.component_shape + (3,))
-    t = field.table
-    call("gf_lsq_grad", ctypes.byref(grid.cmesh), field.num_components, ptr(field.store), ptr(t.kind),
-         ptr(t.psib), ptr(out.store), stream_ptr())
+    configured_grad(field, out.store)
     return out
+
+
+def configured_grad(field: CellField, out: torch.Tensor, face_buf: torch.Tensor | None = None,
+                    lsq_buf: torch.Tensor | None = None) -> None:
+    """The configured gradient of ``field`` into ``out`` ``[ncomp*3, C]``
+    (boundary state must be current).  ``linear``: ``fvc.interpolate`` into
+    ``face_buf`` ``[ncomp, F + Nb]`` (its hanging-face correction takes the
+    least-squares gradient, in ``lsq_buf``), then the Green-Gauss sum
+    (fv/kernels/gauss_gradient.py:15-73).  The buffers are allocated when
+    not given."""
+    grid = field.grid
+    scheme = schemes.grad_scheme(grid.sim_config, field.name)
+    t = field.table
+    nc = field.num_components
+    s = stream_ptr()
+    if scheme == GradScheme.LEASTSQUARE:
+        call("gf_lsq_grad", ctypes.byref(grid.cmesh), nc, ptr(field.store), ptr(t.kind), ptr(t.psib), ptr(out), s)
+        return
+    if scheme != GradScheme.LINEAR:
+        raise NotImplementedError(f"gradient scheme {scheme}")
+    f64 = dict(dtype=torch.float64, device=grid.device)
+    if face_buf is None:
+        face_buf = torch.empty((nc, grid.num_internal_faces + grid.num_bnd), **f64)
+    g = None
+    if grid.num_hanging > 0:
+        g = lsq_buf if lsq_buf is not None else torch.empty((nc * 3, grid.num_cells), **f64)
+        call("gf_lsq_grad", ctypes.byref(grid.cmesh), nc, ptr(field.store), ptr(t.kind), ptr(t.psib), ptr(g), s)
+    call("gf_interpolate", ctypes.byref(grid.cmesh), nc, ptr(field.store), ptr(t.kind), ptr(t.psib), ptr(g),
+         ptr(face_buf), s)
+    call("gf_gauss_grad", ctypes.byref(grid.cmesh), nc, ptr(face_buf), ptr(out), s)
 
 
 def _hanging_grad(field: CellField) -> torch.Tensor | None:

@@ -44,13 +44,25 @@ def _base(field: CellField, mat: FvMatrix) -> GfAssembly:
 
 
 def _lsq_grad(field: CellField) -> torch.Tensor:
-    if schemes.grad_scheme(field.grid.sim_config, field.name) != GradScheme.LEASTSQUARE:
-        raise NotImplementedError("the device path implements the leastsquare gradient scheme")
+    """Least-squares gradient (the hanging-face corrections always use it)."""
     grad = torch.empty((field.num_components * 3, field.grid.num_cells), dtype=torch.float64,
                        device=field.grid.device)
     t = field.table
     call("gf_lsq_grad", ctypes.byref(field.grid.cmesh), field.num_components, ptr(field.store),
          ptr(t.kind), ptr(t.psib), ptr(grad), stream_ptr())
+    return grad
+
+
+def _cfg_grad(field: CellField, lsq: torch.Tensor | None) -> torch.Tensor:
+    """The configured gradient (the TVD limiter's, schemes/div.py:302);
+    reuses ``lsq`` when the scheme is least squares."""
+    if schemes.grad_scheme(field.grid.sim_config, field.name) == GradScheme.LEASTSQUARE:
+        return lsq if lsq is not None else _lsq_grad(field)
+    from gridfoam_b200.fv.fvc import configured_grad
+
+    grad = torch.empty((field.num_components * 3, field.grid.num_cells), dtype=torch.float64,
+                       device=field.grid.device)
+    configured_grad(field, grad, lsq_buf=lsq)
     return grad
 
 
@@ -127,23 +139,27 @@ def div(phi: FaceField, field: CellField) -> FvMatrix:
     _eval_state(field)
     scheme = schemes.div_scheme(field.grid.sim_config, phi.name, field.name)
     code = _lib.DIV_CODES[scheme.value]
-    grad = None
+    grad = lsq = None
     hanging = field.grid.num_hanging > 0
-    if code >= _lib.DIV_CODES["vanleer"] or (hanging and code == _lib.DIV_CODES["linear"]):
-        # TVD: the configured gradient; linear on hanging faces: the
-        # least-squares gradient of the offset correction (schemes/div.py).
-        grad = _lsq_grad(field)
+    if hanging and code == _lib.DIV_CODES["linear"]:
+        # linear on hanging faces: the least-squares gradient of the offset
+        # correction (schemes/div.py:134).
+        lsq = _lsq_grad(field)
+    if code >= _lib.DIV_CODES["vanleer"]:
+        # TVD: the configured gradient, also in its hanging-face offset
+        # correction (schemes/div.py:302).
+        grad = _cfg_grad(field, None)
     a = _base(field, mat)
     a.div_scheme = code
     a.div_sign = 1.0
     a.phi = ptr(phi.store)
     a.grad_psi = ptr(grad)
-    a.grad_lsq = ptr(grad) if hanging else None
+    a.grad_lsq = ptr(lsq) if hanging else None
     _run(field, a)
-    mat._keep = grad
+    mat._keep = (grad, lsq)
     if torch.is_grad_enabled() and phi.store.requires_grad:
         # Reverse with respect to the face flux: the transpose face flux.
-        keep = _frozen_state(field, a) + (grad, phi.store.detach().clone())
+        keep = _frozen_state(field, a) + (grad, lsq, phi.store.detach().clone())
         a.phi = ptr(keep[-1])
         return _attach(mat, phi.store, "gf_div_adjoint", a, keep)
     return mat

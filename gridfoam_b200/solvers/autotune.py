@@ -30,7 +30,7 @@ from gridfoam_b200.meta.config import PrecisionType, PreconditionerType, SolverC
 # Variants 0-7 differ only in launch shape and memory placement (their
 # iterates differ by the order of the dot-product partial sums); 8 and 9
 # form q = A p by recurrence.
-N_VARIANTS = 12
+N_VARIANTS = 15
 VARIANTS = {
     0: "256 threads x 1 cell/pass",
     1: "256 threads x 2 cells/pass",
@@ -44,6 +44,9 @@ VARIANTS = {
     9: "1024 threads, shared-memory vectors, q = A z + beta q recurrence, 2 cells/pass",
     10: "1024 threads, shared-memory vectors, one grid reduction and a halo sync per iteration, 1 cell/pass (FP32-inner: same form)",
     11: "1024 threads, shared-memory vectors, one grid reduction and a halo sync per iteration, 2 cells/pass",
+    12: "512 threads x 2 a SM, vectors in global memory, q = A z + beta q recurrence (any size, FP64)",
+    13: "1024 threads, vectors in global memory, q = A z + beta q recurrence (any size, FP64)",
+    14: "256 threads x 4 a SM, vectors in global memory, q = A z + beta q recurrence (any size, FP64)",
 }
 
 _LOCK = threading.Lock()

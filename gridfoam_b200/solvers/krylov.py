@@ -126,6 +126,8 @@ class DeviceKrylov(LinearSolver):
         k.atol = self.atol
         k.rtol = self.rtol
         k.nbr = ptr(grid.dev["ell_nbr"])
+        if "ell_len" in grid.dev:
+            k.row_len = ptr(grid.dev["ell_len"])
         k.diag = ptr(diag)
         k.val = ptr(val)
         k.rhs = ptr(rhs)

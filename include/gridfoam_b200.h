@@ -115,6 +115,10 @@ typedef struct gf_mesh {
      * axis-projected grid are axis-aligned: sf[k][f] = 0 for k != axis, so
      * kernels given this array read and gather one component per face. */
     const int8_t* face_axis;
+    /* One past the last internal-face slot of each row [C], or NULL: slots
+     * from ell_len[c] on hold boundary faces or nothing (zero matrix
+     * coefficients), so row products may stop there. */
+    const uint8_t* ell_len;
 } gf_mesh_t;
 
 /* Per-face boundary-condition table of one field (value-fraction form). */
@@ -219,6 +223,9 @@ typedef struct gf_krylov {
                              (grid barrier, halo flag, copy stage) gives up and
                              the solve ends with GF_ERR_TIMEOUT; 0: the
                              default, about a second of polling */
+    const uint8_t* row_len; /* [n] or NULL: row c's entries are in slots
+                             0 .. row_len[c]-1 (gf_mesh_t ell_len); the
+                             kernels skip the rest of the row */
 } gf_krylov_t;
 
 const char* gf_last_error(void);
@@ -347,6 +354,13 @@ int gf_fvc_div(const gf_mesh_t* m, int32_t ncomp, const double* phi,
 int gf_interpolate(const gf_mesh_t* m, int32_t ncomp, const double* psi,
                    const int8_t* bc_kind, const double* psib,
                    const double* grad, double* out, void* stream);
+
+/* fv/kernels/gauss_gradient.py:15-73 and fv/schemes/grad.py:21-43 (the
+ * 'linear' gradient scheme): Green-Gauss gradient of ncomp face fields
+ * psi_f ([ncomp][F + Nb], as gf_interpolate writes them); grad is
+ * [ncomp*3][C] with value(c, k, j) = grad[(k*3 + j) * C + c]. */
+int gf_gauss_grad(const gf_mesh_t* m, int32_t ncomp, const double* psi_f,
+                  double* grad, void* stream);
 
 /* fv/fvc/sn_grad.py:16-55 (internal part + boundary normal gradient,
  * boundary_ops.py:405-437).  grad ([ncomp*3][C] least-squares gradient, or

@@ -38,8 +38,19 @@ SOLVER_DEFAULTS = {
 }
 
 
+# oracle.native.enable() sets this to the multi-threaded C path (same sums,
+# same order).
+_NATIVE_SCATTER = None
+
+
 def scatter_add(n: int, index: np.ndarray, values: np.ndarray) -> np.ndarray:
     """``torch.zeros(n, *comp).index_add_(0, index, values)``."""
+    if _NATIVE_SCATTER is not None:
+        return _NATIVE_SCATTER(n, index, values, _scatter_add_numpy)
+    return _scatter_add_numpy(n, index, values)
+
+
+def _scatter_add_numpy(n: int, index: np.ndarray, values: np.ndarray) -> np.ndarray:
     values = np.asarray(values, dtype=np.float64)
     if values.ndim == 1:
         return np.bincount(index, weights=values, minlength=n)[:n]
@@ -165,6 +176,8 @@ class Case:
         hcm[self.neighbour_s[h]] = True
         self.hang_cell_mask = hcm
         self.lsq_face_idx = np.nonzero(hcm[self.owner_s] | hcm[self.neighbour_s])[0]
+        self.lsq_owner = self.owner_s[self.lsq_face_idx]
+        self.lsq_neighbour = self.neighbour_s[self.lsq_face_idx]
         self.lsq_ata_inv = self._build_lsq_ata_inv()
 
     @property
@@ -534,7 +547,18 @@ class Batch:
 
 
 def boundary_batches(field: CellField) -> list[Batch]:
-    """boundary_ops.py:121-188."""
+    """boundary_ops.py:121-188 (cached per field and set of conditions, as
+    the reference caches its batches)."""
+    key = tuple((patch, id(bc), bc.type) for patch, bc in field.bcs.items())
+    cached = getattr(field, "_batches", None)
+    if cached is not None and cached[0] == key:
+        return cached[1]
+    out = _boundary_batches(field)
+    field._batches = (key, out)
+    return out
+
+
+def _boundary_batches(field: CellField) -> list[Batch]:
     case = field.case
     out: list[Batch] = []
     for patch, bc in field.bcs.items():

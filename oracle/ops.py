@@ -200,7 +200,7 @@ def least_squares_gradient(field: CellField, *, hanging_cells_only: bool = False
     psi = field.data
     atb = np.zeros((c.num_cells,) + field.comp + (3,))
     if hanging_cells_only:
-        own, nei = c.owner_s[c.lsq_face_idx], c.neighbour_s[c.lsq_face_idx]
+        own, nei = c.lsq_owner, c.lsq_neighbour
     else:
         own, nei = c.owner_s, c.neighbour_s
     d = c.cell_centers[nei] - c.cell_centers[own]

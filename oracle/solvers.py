@@ -149,8 +149,14 @@ def bicgstab_single(A: LDU, b, x, inv_diag, cfg) -> tuple[np.ndarray, SolveStats
     return x, SolveStats("bicgstab", r0, final, it, converged)
 
 
+# oracle.native.enable() sets this to the multi-threaded C restatement.
+_NATIVE = None
+
+
 def solve(A: LDU, rhs: np.ndarray, x0: np.ndarray, cfg: dict):
     """krylov.py:34-82 plus the CG/BiCGStab dispatch of solvers/factory.py."""
+    if _NATIVE is not None:
+        return _NATIVE(A, rhs, x0, cfg)
     method = cfg["method"]
     single = {"cg": cg_single, "bicgstab": bicgstab_single}[method]
     inv_diag = jacobi_inv_diag(A, cfg["preconditioner"])

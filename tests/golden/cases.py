@@ -71,3 +71,18 @@ DIV_SCHEMES = [
     "limitedlinear",
     "koren",
 ]
+
+
+# Cases whose whole steps and gradients are also pinned with the Green-Gauss
+# ('linear') gradient scheme: SIMPLE on a box, PIMPLE with a TVD scheme (the
+# configured gradient enters the limiter), an octree with TVD (and its
+# hanging-face offset correction) and an immersed octree case.
+GRAD_LINEAR_CASES = ("cavity8", "channel", "duct_oct", "ibcyl_oct")
+
+
+def grad_linear_case(name: str) -> dict:
+    case = copy.deepcopy(ALL_CASES[name]())
+    schemes = case["simulator"].setdefault("fvSchemes", {})
+    schemes["gradSchemes"] = {"default": "linear"}
+    case["name"] = name + "_gradlinear"
+    return case

@@ -99,8 +99,8 @@ def stats_array(stats) -> np.ndarray:
     )
 
 
-def run_case(name: str, n_steps: int) -> dict:
-    case = ALL_CASES[name]()
+def run_case(name: str, n_steps: int, case: dict | None = None) -> dict:
+    case = case if case is not None else ALL_CASES[name]()
     out: dict[str, np.ndarray] = {}
     profile = case["inlet_profile"]
     original = bc_factory.create_boundary_condition
@@ -505,6 +505,20 @@ def main() -> None:
             path = HERE / f"forces_{name}.npz"
             np.savez_compressed(path, **data)
             print(f"forces {name}: {len(data)} arrays -> {path} ({path.stat().st_size} B)")
+        return
+    if args and args[0] == "--gradlinear":
+        # The Green-Gauss ('linear') gradient scheme: whole steps and the
+        # fvc.grad operator outputs of the reference with gradSchemes
+        # default linear.
+        from tests.golden.cases import GRAD_LINEAR_CASES, grad_linear_case
+
+        for name in args[1:] or GRAD_LINEAR_CASES:
+            data = run_case(name, STEPS[name], case=grad_linear_case(name))
+            keep = ("init_", "step", "op_grad", "mesh_", "residual_")
+            data = {k: v for k, v in data.items() if k.startswith(keep)}
+            path = HERE / f"gradlinear_{name}.npz"
+            np.savez_compressed(path, **data)
+            print(f"gradlinear {name}: {len(data)} arrays -> {path} ({path.stat().st_size} B)")
         return
     if args and args[0] == "--adjoint":
         for name in args[1:] or ADJOINT_CASES:

@@ -207,7 +207,9 @@ def test_krylov_wait_timeout_reports_and_recovers(method, variant):
 
     _, _, grid, algo = device_case(case_def=pipe_case(24, 48))
     A = -fvm.laplacian(1.0, algo.p)
-    A.diag = A.diag + 1e-3 * grid.cell_volumes
+    # BiCGStab gets a diagonally dominant system: on the nearly singular
+    # Laplacian it exhausts its breakdown restarts (as the reference's does).
+    A.diag = A.diag * (1.0 if method == "cg" else 1.2) + 1e-3 * grid.cell_volumes
     n = grid.num_cells
     rhs = torch.linspace(-1.0, 1.0, n, dtype=torch.float64, device="cuda").reshape(1, n)
     cls = CGSolver if method == "cg" else BiCGSTABSolver
@@ -216,7 +218,7 @@ def test_krylov_wait_timeout_reports_and_recovers(method, variant):
     ref.variant = variant
     x_ref = torch.zeros_like(rhs)
     st = ref.solve_arrays(grid, A.diag_store, A.val, rhs, x_ref, symmetric=True)
-    assert st[0].converged and st[0].iterations > 20
+    assert st[0].converged and st[0].iterations > 5
 
     s = cls(cfg)
     s.variant = variant
@@ -377,7 +379,7 @@ def test_single_reduction_cg_matches_pcg(layout):
     assert r < 1e-9 * s1.initial_residual
 
 
-@pytest.mark.parametrize("variant", [5, 6, 7, 8, 9, 10, 11])
+@pytest.mark.parametrize("variant", [5, 6, 7, 8, 9, 10, 11, 12, 13, 14])
 @pytest.mark.parametrize("shape", [(24, 20, 28), (64, 64, 40), (7, 5, 6), (130, 3, 4)])
 def test_staged_box_cg_matches_register_kernel(shape, variant):
     """The shared-memory variants against the register kernel (variant 0):
@@ -443,7 +445,7 @@ def test_smem_resident_cg_fixed_iterations_match_register_kernel(variant, box):
     assert rel(xs[1], xs[0]) < 1e-11
 
 
-@pytest.mark.parametrize("variant", [6, 7, 8, 9, 10, 11])
+@pytest.mark.parametrize("variant", [6, 7, 8, 9, 10, 11, 12, 13, 14])
 def test_smem_resident_cg_on_ell_layout(variant):
     """The shared-memory-resident CG through the general ELL rows (the
     octree path), against the register ELL kernel."""
@@ -604,7 +606,7 @@ def test_staged_assembly_matches_generic_kernel(name):
             assert torch.equal(x, y), field.name
 
 
-@pytest.mark.parametrize("variant", [8, 9, 10, 11])
+@pytest.mark.parametrize("variant", [8, 9, 10, 11, 12, 13])
 @pytest.mark.parametrize("box", [True, False])
 def test_qrec_cg_true_residual(variant, box):
     """The q-recurrence CG updates r from q = A z + beta q rather than from
@@ -624,3 +626,80 @@ def test_qrec_cg_true_residual(variant, box):
     ax = sysm.diag * x[0] + (sysm.val * x[0][nb]).sum(0)
     true = torch.linalg.vector_norm(sysm.rhs[0] - ax).item()
     assert true < 2e-10 * st.initial_residual, (true / st.initial_residual, st.iterations)
+
+
+@pytest.mark.parametrize("box", [True, False])
+@pytest.mark.parametrize("variant", [12, 13, 14])
+def test_stream_cg_fixed_iterations_match_qrec(variant, box):
+    """The streaming CG (vectors in global memory) runs the q-recurrence of
+    the shared-memory form: exactly 60 iterations of each agree up to the
+    order of the dot-product partial sums."""
+    from gridfoam_b200.solvers.autotune import BoxSystem, _solver
+
+    sysm = BoxSystem(40, 36, 44, device=torch.device("cuda"))
+    if not box:
+        sysm.box_strides = None
+    xs = []
+    for v in (8, variant):
+        s = _solver(60, False, v)
+        x = torch.zeros_like(sysm.rhs)
+        st = s.solve_arrays(sysm, sysm.diag, sysm.val, sysm.rhs, x, symmetric=True)
+        assert st[0].iterations == 60 and st[0].status == "max_iter"
+        xs.append(to_np(x))
+    assert rel(xs[1], xs[0]) < 1e-11
+
+
+@pytest.mark.parametrize("variant", [2, 12, 13])
+def test_row_lengths_skip_only_empty_slots(variant):
+    """On an octree grid (couplings first in every row) the CG with the
+    row-length early exit gives the same iterations and solution as the
+    same kernel reading every slot."""
+    from gridfoam_b200.fv import fvm
+    from gridfoam_b200.meta.config import SolverConfig
+    from gridfoam_b200.solvers.krylov import CGSolver
+
+    _, _, grid, algo = device_case("ibcyl_oct")
+    assert grid.box_strides is None
+    assert float(grid.dev["ell_len"].double().mean()) < grid.ell_width  # rows shorter than the widest
+    A = -fvm.laplacian(1.0, algo.p)
+    A.diag = A.diag + 1e-2 * grid.cell_volumes
+    rhs = torch.linspace(-1.0, 1.0, grid.num_cells, dtype=torch.float64, device="cuda").reshape(1, -1)
+    cfg = SolverConfig(method="cg", preconditioner="jacobi", tolerance=0.0, rel_tolerance=1e-10, max_iter=4000)
+    out = []
+    for use_len in (True, False):
+        saved = None if use_len else grid.dev.pop("ell_len")
+        s = CGSolver(cfg)
+        s.variant = variant
+        x = torch.zeros_like(rhs)
+        st = s.solve_arrays(grid, A.diag_store, A.val, rhs, x, symmetric=True)[0]
+        if saved is not None:
+            grid.dev["ell_len"] = saved
+        out.append((to_np(x), st.iterations, st.converged))
+    assert out[0][2] and out[1][2]
+    assert out[0][1] == out[1][1]
+    assert rel(out[0][0], out[1][0]) < 1e-13
+
+
+@pytest.mark.parametrize("name", ["cavity8", "channel", "duct_oct", "ibcyl_oct"])
+def test_grad_linear_steps_and_operator_match_reference(name):
+    """The Green-Gauss ('linear') gradient scheme (fv/schemes/grad.py:21-43):
+    whole steps with gradSchemes default linear, and fvc.grad of p and U on
+    the final state, against the reference's own run."""
+    from gridfoam_b200.fv import fvc
+    from tests.golden.cases import grad_linear_case
+
+    golden = load_golden(f"gradlinear_{name}")
+    _, _, _, algo = device_case(case_def=grad_linear_case(name))
+    tol = STEP_TOL[name]
+    for step in range(STEPS[name]):
+        algo.step()
+        torch.cuda.synchronize()
+        assert rel(to_np(algo.U.data), golden[f"step{step}_U"]) < tol, (step, "U")
+        assert rel(to_np(algo.p.data), golden[f"step{step}_p"]) < 10 * tol, (step, "p")
+        assert rel(to_np(algo.phi.pack()), golden[f"step{step}_phi"]) < tol, (step, "phi")
+        its_p = np.array([s.iterations for s in algo.last_stats["p"]])
+        slack = 1 if name in OCTREE_CASES else 0
+        assert np.all(np.abs(its_p - golden[f"step{step}_stats_p"][:, 2]) <= slack), (step, its_p)
+    _load_state(algo, golden, STEPS[name] - 1)
+    _check(fvc.grad(algo.p).data, golden["op_grad_p"], "grad_p", 1e-10)
+    _check(fvc.grad(algo.U).data, golden["op_grad_U"], "grad_U", 1e-10)

@@ -85,3 +85,60 @@ def test_oracle_operators_match_reference(name):
             continue
         scale = max(np.abs(ref).max(), 1e-300)
         assert np.abs(val - ref).max() <= 1e-11 * scale, key
+
+
+NATIVE_STEP_TOL = {"cavity8": 1e-10, "channel": 1e-9, "channel_ffp": 1e-9, "ibplane": 1e-10, "pipe10x20": 1e-4,
+                   "cavity_oct": 1e-9, "duct_oct": 1e-8, "ibcyl_oct": 1e-8}
+
+
+@pytest.fixture
+def native_krylov():
+    from oracle import native
+
+    native.enable()
+    yield
+    native.disable()
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_native_krylov_steps_match_reference(name, native_krylov):
+    """The multi-threaded C Krylov restatement (``oracle/krylov.c``, used by
+    the CPU baseline of large cases) gives the same whole steps."""
+    golden = load_golden(name)
+    _, _, _, algo = oracle_case(name)
+    # Its sums run in another order, as on the GPU: the tolerances of the
+    # GPU whole-step tests apply.
+    tol = NATIVE_STEP_TOL[name]
+    for step in range(STEPS[name]):
+        algo.step()
+        assert rel(algo.U.data, golden[f"step{step}_U"]) < tol
+        assert rel(algo.p.data, golden[f"step{step}_p"]) < 10 * tol
+        assert rel(algo.phi.pack(), golden[f"step{step}_phi"]) < tol
+        slack = 1 if name.startswith("pipe") or name.endswith("_oct") else 0
+        its_u = [s.iterations for s in algo.last_stats["U"]]
+        its_p = [s.iterations for s in algo.last_stats["p"]]
+        assert np.all(np.abs(np.array(its_u) - golden[f"step{step}_stats_U"][:, 2]) <= slack)
+        assert np.all(np.abs(np.array(its_p) - golden[f"step{step}_stats_p"][:, 2]) <= slack)
+
+
+@pytest.mark.parametrize("name", ["cavity8", "channel", "duct_oct", "ibcyl_oct"])
+def test_oracle_grad_linear_steps_match_reference(name):
+    """The oracle with the Green-Gauss ('linear') gradient scheme against
+    the reference's run of the same cases."""
+    from oracle.ops import eval_grad
+    from tests.golden.cases import grad_linear_case
+
+    golden = load_golden(f"gradlinear_{name}")
+    _, _, _, algo = oracle_case(name, case_def=grad_linear_case(name))
+    tol = NATIVE_STEP_TOL[name]
+    for step in range(STEPS[name]):
+        algo.step()
+        assert rel(algo.U.data, golden[f"step{step}_U"]) < tol
+        ptol = 10 * tol if name.endswith("_oct") else tol
+        assert rel(algo.p.data, golden[f"step{step}_p"]) < ptol
+        assert rel(algo.phi.pack(), golden[f"step{step}_phi"]) < tol
+    gp = eval_grad(algo.p)
+    scale = np.abs(golden["op_grad_p"]).max()
+    # op_grad_* were taken on the reference's final state; the oracle's final
+    # state agrees to the step tolerance above.
+    assert np.abs(gp - golden["op_grad_p"]).max() <= max(1e-10, 100 * tol) * scale
