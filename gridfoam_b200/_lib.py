@@ -196,6 +196,9 @@ _SIGNATURES = {
     "gf_pcg_solve_static": ([P, P], ctypes.c_int),
     "gf_pcg_static_scratch_doubles": ([], I64),
     "gf_bicgstab_solve": ([P, P], ctypes.c_int),
+    "gf_pcg_solve_batched": ([P, I32, P, P], ctypes.c_int),
+    "gf_bicgstab_solve_batched": ([P, I32, P, P], ctypes.c_int),
+    "gf_batch_max_blocks": ([I32], ctypes.c_int),
     "gf_rau_hbya": ([P, I32, P, P, P, P, P, P, P, P], ctypes.c_int),
     "gf_simplec_rAtU": ([P, P, P, P, P], ctypes.c_int),
     "gf_face_flux": ([P, I32, P, P, P, P, P, P, P], ctypes.c_int),
@@ -265,7 +268,8 @@ class GfError(RuntimeError):
 
 
 # Kernels launched per entry point (for launch accounting).
-_LAUNCHES_PER_CALL = {"gf_fixed_values": 3, "gf_close_fixed_flux": 2, "gf_field_residual": 2, "gf_continuity_sums": 2}
+_LAUNCHES_PER_CALL = {"gf_fixed_values": 3, "gf_close_fixed_flux": 2, "gf_field_residual": 2, "gf_continuity_sums": 2,
+                      "gf_pcg_solve_batched": 2, "gf_bicgstab_solve_batched": 2}
 LAUNCHES: collections.Counter = collections.Counter()
 
 

@@ -116,6 +116,11 @@ class _PressureVelocity:
         self._adjust_classes = self._build_adjust_classes()
         self._p_ffp = any(bc.kind == _lib.BC_FIXED_FLUX_P for bc in self.p.bcs.values())
         self.last_stats: dict = {}
+        # Not None: Krylov solves are recorded here as (solver, descriptor)
+        # instead of launched, and the step generator pauses after each one
+        # (the solve server launches the same-phase solves of many cases at
+        # once, then resumes every case).
+        self._deferred: list | None = None
         self._diagnostics = None
         self._diagnostics_step = 0
         # flux.py:132-162 correct_flux(phi, U, update_internal=True)
@@ -327,12 +332,22 @@ class _PressureVelocity:
         call("gf_gather_bnd", g.num_bnd, nc, n, ptr(faces), ptr(field.table.refv), ptr(vals), s)
         call("gf_set_cell_values", g.num_cells, nc, n, ptr(cells), ptr(vals), n, ptr(field.store), s)
 
+    def _solve(self, solver, d, v, src, x, *, symmetric: bool = False):
+        """A Krylov solve (generator): launched at once, or recorded and
+        paused on when solves are deferred."""
+        if self._deferred is None:
+            return solver.solve_arrays(self._grid, d, v, src, x, symmetric=symmetric)
+        k, _ = solver.describe(self._grid, d, v, src, x, symmetric=symmetric)
+        self._deferred.append((solver, k))
+        yield
+        return ()
+
     def _momentum_solve(self, residual_key: str | None = None):
         d, v, src = self._constrain(self.U, self.UEqn.diag_store, self.UEqn.val, self.pred_source, self.USolve,
                                     self.u_cells, self.u_faces, self.u_mask, self.u_vals, self.prescribed_U)
         if residual_key is not None:
             self._record_residual_dev(residual_key, d, v, src, self.U)
-        stats = self._solvers[self.U.name].solve_arrays(self._grid, d, v, src, self.U.store)
+        stats = yield from self._solve(self._solvers[self.U.name], d, v, src, self.U.store)
         # UEqn for H/A: constraints of the updated velocity
         if self.u_cells.numel():
             self._eval_U()
@@ -434,7 +449,7 @@ class _PressureVelocity:
             solver = self._solvers[self.p.name]
             if final_solver is not None and corr == self.n_non_orthogonal_correctors:
                 solver = final_solver
-            stats = solver.solve_arrays(g, d, v, src, self.p.store, symmetric=True)
+            stats = yield from self._solve(solver, d, v, src, self.p.store, symmetric=True)
         return stats, first_res, last_res
 
     def _correct_phi(self) -> None:
@@ -515,16 +530,22 @@ class SIMPLE(_PressureVelocity):
 
     def step(self) -> None:
         """simple.py:287-408."""
+        for _ in self.step_phases():
+            pass
+
+    def step_phases(self):
+        """One step as a generator that pauses after each deferred Krylov
+        solve (see ``_deferred``); without deferral it runs straight through."""
         g = self._grid
         self._assemble_momentum(self.alpha_U)
         key = self.U.name if self.U.name in self._residual_control else None
-        st_u = self._momentum_solve(residual_key=key)
+        st_u = yield from self._momentum_solve(residual_key=key)
         if key is not None:
             self._record(*self._pending_residual)
         self._hbya(ddt=False, consistent=self.consistent)
         self.p_old.copy_(self.p.store[0])
         record = self.p.name in self._residual_control
-        st_p, first, _ = self._pressure_solve(record=record)
+        st_p, first, _ = yield from self._pressure_solve(record=record)
         if record:
             self._record(self.p.name, first)
         self._correct_phi()
@@ -556,13 +577,18 @@ class PISO(_PressureVelocity):
 
     def step(self) -> None:
         """piso.py:227-326."""
+        for _ in self.step_phases():
+            pass
+
+    def step_phases(self):
+        """One step as a generator that pauses after each deferred solve."""
         self._assemble_momentum(0.0)
-        st_u = self._momentum_solve()
+        st_u = yield from self._momentum_solve()
         st_p = None
         for i in range(self.n_correctors):
             self._hbya(ddt=True, consistent=False)
             final = resolve_solver(self._solvers, self.p.name, is_final=(i == self.n_correctors - 1))
-            st_p, _, _ = self._pressure_solve(final_solver=final)
+            st_p, _, _ = yield from self._pressure_solve(final_solver=final)
             self._correct_phi()
             self._correct_velocity()
         self.U.update_history()
@@ -616,6 +642,11 @@ class PIMPLE(_PressureVelocity):
 
     def step(self) -> None:
         """pimple.py:290-454."""
+        for _ in self.step_phases():
+            pass
+
+    def step_phases(self):
+        """One step as a generator that pauses after each deferred solve."""
         self._outer_converged = False
         self._initial_residuals.clear()
         self._current_residuals.clear()
@@ -628,14 +659,14 @@ class PIMPLE(_PressureVelocity):
                 self._outer_converged = True
             self._assemble_momentum(0.0)
             key = self.U.name if self.U.name in self._residual_control else None
-            st_u = self._momentum_solve(residual_key=key)
+            st_u = yield from self._momentum_solve(residual_key=key)
             if key is not None:
                 self._record(*self._pending_residual)
             for inner in range(self.n_correctors):
                 self._hbya(ddt=True, consistent=self.consistent)
                 final = resolve_solver(self._solvers, self.p.name, is_final=(inner == self.n_correctors - 1))
                 record = self.p.name in self._residual_control
-                st_p, first, last = self._pressure_solve(final_solver=final, record=record)
+                st_p, first, last = yield from self._pressure_solve(final_solver=final, record=record)
                 if record:
                     if inner == 0:
                         self._record(self.p.name, first)

@@ -20,6 +20,8 @@ import copy
 import numpy as np
 
 from gridfoam_b200.mesh.builder import (
+    BLUFF_DEFAULT,
+    bluff_body_sdf,
     Body,
     BoxRegion,
     SdfRegion,
@@ -366,6 +368,8 @@ def _sdf(b: dict):
         return cylinder_sdf(tuple(b["center"]), b["radius"], b["axis"])
     if b["kind"] == "plane":
         return plane_sdf(b["point"], b["axis"])
+    if b["kind"] == "bluff":
+        return bluff_body_sdf(b.get("x0", 0.0), tuple(b.get("params", BLUFF_DEFAULT)))
     raise ValueError(b["kind"])
 
 
@@ -635,3 +639,69 @@ def pipe_analytic_uz(mesh, profile: dict) -> np.ndarray:
     c = mesh.cell_centers
     r2 = (c[:, 0] - profile["center"][0]) ** 2 + (c[:, 1] - profile["center"][1]) ** 2
     return profile["umax"] * np.clip(1.0 - r2 / profile["radius"] ** 2, 0.0, None)
+
+
+def bluff_body_case(base: tuple[int, int, int] = (128, 32, 24), levels: int = 3, params=BLUFF_DEFAULT,
+                    iterations: int = 500) -> dict:
+    """Slanted bluff body in a channel on a 4-level octree (levels 0-3):
+    domain [-2, 6] x [-1, 1] x [0, 1.2], the body (length 1, front at x = 0,
+    shape ``params``) on the floor side with its clearance; refined to level
+    1 in the box around body and near wake, 2 closer, 3 within 0.04 of the
+    surface.  Inflow 1, nu 2e-6, laminar, steady SIMPLE (SIMPLEC), upwind
+    convection; floor and body no-slip, top and sides slip."""
+    body = {"kind": "bluff", "x0": 0.0, "params": list(params), "patch": "body"}
+    sim = {
+        "control": {"deltaT": 1.0, "endTime": float(iterations), "writeInterval": 100000,
+                    "output": {"output_dir": "/tmp/gf_bluff", "base_name": "bluff"}, "precision": "float64"},
+        "fvSchemes": {"divSchemes": {"default": "upwind"}, "gradSchemes": {"default": "leastsquare"},
+                      "laplacianSchemes": {"default": "corrected"}},
+        "fvSolution": {
+            "adjustPhi": True,
+            "algorithm": {"type": "simple", "nNonOrthogonalCorrectors": 0, "consistent": True,
+                          "relaxationFactors": {"equations": {"U": 0.7, "p": 0.3}},
+                          "pRefCell": 0, "pRefValue": 0.0},
+            "solvers": {
+                "U": {"method": "bicgstab", "preconditioner": "jacobi", "tolerance": 1e-8,
+                      "rel_tolerance": 0.1, "max_iter": 2000},
+                "p": {"method": "cg", "preconditioner": "jacobi", "tolerance": 1e-7,
+                      "rel_tolerance": 0.01, "max_iter": 2000},
+            },
+        },
+        "conditions": {
+            "U": {
+                "internal": [1.0, 0.0, 0.0],
+                "boundary": {
+                    "inlet": {"type": "dirichlet", "patches": ["x_minus"], "value": [1.0, 0.0, 0.0]},
+                    "outlet": {"type": "inlet_outlet", "patches": ["x_plus"], "value": WALL0},
+                    "sides": {"type": "slip", "patches": ["y_minus", "y_plus", "z_plus"]},
+                    "floor": {"type": "dirichlet", "patches": ["z_minus"], "value": WALL0},
+                    "body": {"type": "dirichlet", "patches": ["body"], "value": WALL0},
+                },
+            },
+            "p": {
+                "internal": 0.0,
+                "boundary": {
+                    "outlet": {"type": "dirichlet", "patches": ["x_plus"], "value": 0.0},
+                    "rest": {"type": "neumann",
+                             "patches": ["x_minus", "y_minus", "y_plus", "z_minus", "z_plus", "body"],
+                             "value": 0.0},
+                },
+            },
+        },
+        "properties": _props(2e-6),
+        "device": "cpu",
+    }
+    return {
+        "name": f"bluff_body_{base[0]}x{base[1]}x{base[2]}_l{levels}",
+        "mesh": {
+            "kind": "octree", "lower": [-2.0, -1.0, 0.0], "upper": [6.0, 1.0, 1.2], "res": list(base),
+            "regions": [
+                {"kind": "box", "lo": [-0.5, -0.45, 0.0], "hi": [3.0, 0.45, 0.6], "level": 1},
+                {"kind": "box", "lo": [-0.2, -0.3, 0.0], "hi": [1.6, 0.3, 0.45], "level": 2},
+                {"kind": "sdf", "body": body, "distance": 0.04, "level": levels},
+            ],
+            "bodies": [body],
+        },
+        "simulator": sim,
+        "inlet_profile": None,
+    }

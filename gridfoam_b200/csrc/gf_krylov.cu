@@ -39,14 +39,24 @@ struct KCtl {
 // Barriers this block has passed since the kernel started, and the poll
 // limit of every bounded wait of this launch; barrier_init() must run at the
 // top of every kernel that waits on other blocks.
+// g_nblk / g_bid: the blocks taking part in this solve's reductions and
+// this block's index among them (the whole grid, or one system's share of a
+// batched launch).
 __shared__ unsigned g_epoch;
 __shared__ long long g_spin;
+__shared__ int g_nblk, g_bid;
 
-__device__ __forceinline__ void barrier_init(const gf_krylov_t& K) {
+__device__ __forceinline__ void barrier_init_v(const gf_krylov_t& K, int nblk, int bid) {
     if (threadIdx.x == 0) {
         g_epoch = 0;
         g_spin = K.spin_limit > 0 ? K.spin_limit : kSpinLimit;
+        g_nblk = nblk;
+        g_bid = bid;
     }
+}
+
+__device__ __forceinline__ void barrier_init(const gf_krylov_t& K) {
+    barrier_init_v(K, (int)gridDim.x, (int)blockIdx.x);
 }
 
 __device__ __forceinline__ int vload(const int* p) { return *(const volatile int*)p; }
@@ -138,7 +148,7 @@ __device__ bool grid_reduce_all(KCtl* ctl, double* partials, double (&v)[NV], un
                     const double y = __shfl_xor_sync(0xffffffffu, x, o);
                     x = mx ? nmax(x, y) : x + y;
                 }
-                if (lane == 0) __stcg(part + (int64_t)blockIdx.x * NV + j, x);
+                if (lane == 0) __stcg(part + (int64_t)g_bid * NV + j, x);
             }
         }
     } else if (threadIdx.x < NV) {
@@ -146,12 +156,12 @@ __device__ bool grid_reduce_all(KCtl* ctl, double* partials, double (&v)[NV], un
         const bool mx = (maxmask >> j) & 1u;
         double x = sm1[j * 32];
         for (int w = 1; w < nw; ++w) x = mx ? nmax(x, sm1[j * 32 + w]) : x + sm1[j * 32 + w];
-        __stcg(part + (int64_t)blockIdx.x * NV + j, x);
+        __stcg(part + (int64_t)g_bid * NV + j, x);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
         arrive_release(&ctl->count);
-        const unsigned long long target = (unsigned long long)(ep + 1u) * gridDim.x;
+        const unsigned long long target = (unsigned long long)(ep + 1u) * (unsigned)g_nblk;
         int err = 0;
         long long it = 0;
         while (load_acquire(&ctl->count) < target) {
@@ -187,7 +197,7 @@ __device__ bool grid_reduce_all(KCtl* ctl, double* partials, double (&v)[NV], un
 #pragma unroll
         for (int j = 0; j < NV; ++j) {
             const bool mx = (maxmask >> j) & 1u;
-            const double y = b < (int)gridDim.x ? __ldcg(part + (int64_t)b * NV + j) : 0.0;
+            const double y = b < g_nblk ? __ldcg(part + (int64_t)b * NV + j) : 0.0;
             acc[j] = mx ? nmax(acc[j], y) : acc[j] + y;
         }
     }
@@ -275,7 +285,7 @@ __device__ bool grid_reduce_w0(KCtl* ctl, double* partials, double (&v)[NV], uns
                 x[j] = comb(x[j], __shfl_xor_sync(0xffffffffu, x[j], o), (maxmask >> j) & 1u);
         if (lane == 0) {
 #pragma unroll
-            for (int j = 0; j < NV; ++j) __stcg(part + (int64_t)blockIdx.x * NV + j, x[j]);
+            for (int j = 0; j < NV; ++j) __stcg(part + (int64_t)g_bid * NV + j, x[j]);
             // The CTA barrier above orders the other warps' writes before
             // this release (cumulativity).
             arrive_release(&ctl->count);
@@ -286,7 +296,7 @@ __device__ bool grid_reduce_w0(KCtl* ctl, double* partials, double (&v)[NV], uns
             // alone with __nanosleep while the other lanes waited at a warp
             // barrier left the blocks microseconds apart on leaving (CG
             // iterations 40-60 % slower).
-            const unsigned long long target = (unsigned long long)(ep + 1u) * gridDim.x;
+            const unsigned long long target = (unsigned long long)(ep + 1u) * (unsigned)g_nblk;
             int err = 0;
             long long it = 0;
             while (true) {
@@ -317,7 +327,7 @@ __device__ bool grid_reduce_w0(KCtl* ctl, double* partials, double (&v)[NV], uns
             // shared memory (register loads would be serialised in the
             // register-capped CG kernels).  The last copy may read one
             // double past the partials, inside the same half.
-            const int nd = (int)gridDim.x * NV;
+            const int nd = g_nblk * NV;
             for (int q = lane; 2 * q < nd; q += 32) {
                 const unsigned dst = (unsigned)__cvta_generic_to_shared(g_stage + 2 * q);
                 asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(part + 2 * q) : "memory");
@@ -325,11 +335,11 @@ __device__ bool grid_reduce_w0(KCtl* ctl, double* partials, double (&v)[NV], uns
             asm volatile("cp.async.commit_group;\n\tcp.async.wait_all;" ::: "memory");
             __syncwarp();
 #pragma unroll
-            for (int j = 0; j < NV; ++j) x[j] = lane < (int)gridDim.x ? g_stage[lane * NV + j] : 0.0;
+            for (int j = 0; j < NV; ++j) x[j] = lane < g_nblk ? g_stage[lane * NV + j] : 0.0;
 #pragma unroll
             for (int k = 1; k < kW0Loads; ++k) {
                 const int b = lane + 32 * k;
-                if (b < (int)gridDim.x)
+                if (b < g_nblk)
 #pragma unroll
                     for (int j = 0; j < NV; ++j) x[j] = comb(x[j], g_stage[b * NV + j], (maxmask >> j) & 1u);
             }
@@ -607,8 +617,9 @@ __global__ void __launch_bounds__(kKThreads) k_pcg(gf_krylov_t K) {
 __device__ __forceinline__ double ld_coef(const double* p) { return __ldg(p); }
 __device__ __forceinline__ float ld_coef(const float* p) { return __ldcg(p); }
 
-// I: the cell index type (int32_t where n times the row width fits).
-template <typename T, int WIDTH, typename I = int64_t>
+// I: the cell index type (int32_t where n times the row width fits); GRP:
+// slots of a runtime-width row whose loads are issued together.
+template <typename T, int WIDTH, typename I = int64_t, int GRP = kSlotGroup>
 struct EllRows {
     const T* val;
     const int32_t* nbr;
@@ -636,20 +647,20 @@ struct EllRows {
             // waits for each slot's index before its gather).  The products
             // are added in slot order, as in the plain loop.
             const int ws = len ? (int)__ldg(len + c) : w;
-            for (int s0 = 0; s0 < ws; s0 += kSlotGroup) {
-                int nb[kSlotGroup];
-                A a[kSlotGroup];
+            for (int s0 = 0; s0 < ws; s0 += GRP) {
+                int nb[GRP];
+                A a[GRP];
 #pragma unroll
-                for (int j = 0; j < kSlotGroup; ++j) {
+                for (int j = 0; j < GRP; ++j) {
                     const int s = s0 + j;
                     nb[j] = s < ws ? __ldg(nbr + s * n + c) : (int)c;
                     a[j] = s < ws ? (A)ld_coef(val + s * n + c) : (A)0;
                 }
-                A gv[kSlotGroup];
+                A gv[GRP];
 #pragma unroll
-                for (int j = 0; j < kSlotGroup; ++j) gv[j] = s0 + j < ws ? g(nb[j]) : (A)0;
+                for (int j = 0; j < GRP; ++j) gv[j] = s0 + j < ws ? g(nb[j]) : (A)0;
 #pragma unroll
-                for (int j = 0; j < kSlotGroup; ++j)
+                for (int j = 0; j < GRP; ++j)
                     if (s0 + j < ws) acc += a[j] * gv[j];
             }
         }
@@ -718,11 +729,15 @@ struct BoxRows {
 // (bitwise identically) at the neighbours, so an iteration needs two grid
 // reductions (p.Ap, then |r| and r.z) instead of three.
 
+// vb / vn (>= 0): this block's index among the vn blocks of its system in a
+// batched launch (gf_pcg_solve_batched); by default the whole grid.
 template <int THREADS, int U, class Rows>
-__device__ void pcg1_body(const gf_krylov_t& K, const Rows& rows) {
+__device__ void pcg1_body(const gf_krylov_t& K, const Rows& rows, int vb = -1, int vn = -1) {
     __shared__ CgState st;
     KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
-    barrier_init(K);
+    const int bk = vb >= 0 ? vb : (int)blockIdx.x;
+    const int nbk = vn >= 0 ? vn : (int)gridDim.x;
+    barrier_init_v(K, nbk, bk);
     double* partials = K.work + kCtlDoubles;
     double* vec = partials + kPartials;
     const int64_t n = K.n;
@@ -733,8 +748,8 @@ __device__ void pcg1_body(const gf_krylov_t& K, const Rows& rows) {
     double* q = vec + 4 * n;
     double* x = K.x;
     const bool jac = K.jacobi != 0, linf = K.norm_inf != 0;
-    const int64_t t0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t t0 = bk * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t stride = (int64_t)nbk * blockDim.x;
     bool ok = true;
     {
         double loc[2] = {0.0, 0.0};
@@ -863,7 +878,7 @@ __device__ void pcg1_body(const gf_krylov_t& K, const Rows& rows) {
         p_old = p_new;
         p_new = tmp;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (bk == 0 && threadIdx.x == 0) {
         double* o = K.stats;
         o[0] = st.r0;
         o[1] = st.final;
@@ -1052,12 +1067,15 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_pcg1_box(gf_krylov_
 constexpr int kMaxEll = 32;
 
 template <int THREADS, int U, class Rows64, class Rows32>
-__device__ void pcg1_mixed_body(const gf_krylov_t& K, const Rows64& rows64, Rows32 rows32, int ncoef) {
+__device__ void pcg1_mixed_body(const gf_krylov_t& K, const Rows64& rows64, Rows32 rows32, int ncoef,
+                                int vb = -1, int vn = -1) {
+    const int bk = vb >= 0 ? vb : (int)blockIdx.x;
+    const int nbk = vn >= 0 ? vn : (int)gridDim.x;
     __shared__ CgState st;
     __shared__ double s_target;
     __shared__ int s_cycle_done;
     KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
-    barrier_init(K);
+    barrier_init_v(K, nbk, bk);
     double* partials = K.work + kCtlDoubles;
     double* base = partials + kPartials;
     const int64_t n = K.n;
@@ -1073,8 +1091,8 @@ __device__ void pcg1_mixed_body(const gf_krylov_t& K, const Rows64& rows64, Rows
     float* d = q + n;
     double* x = K.x;
     const bool jac = K.jacobi != 0, linf = K.norm_inf != 0;
-    const int64_t t0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t t0 = bk * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t stride = (int64_t)nbk * blockDim.x;
     const bool sym_box = K.stride_y > 0 && K.symmetric;
     bool ok = true;
     int its = 0;
@@ -1234,7 +1252,7 @@ __device__ void pcg1_mixed_body(const gf_krylov_t& K, const Rows64& rows64, Rows
         // iteration budget spent inside a cycle: keep its correction
         for (int64_t c = t0; c < n; c += stride) __stcg(x + c, __ldcg(x + c) + (double)__ldcg(d + c));
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (bk == 0 && threadIdx.x == 0) {
         double* o = K.stats;
         o[0] = st.r0;
         o[1] = st.final;
@@ -1291,6 +1309,168 @@ template <int WIDTH, int THREADS, int U>
 __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_pcg1_ellv(gf_krylov_t K) {
     EllRows<double, WIDTH> rows{K.val, K.nbr, K.n, K.width, K.row_len};
     pcg1_body<THREADS, U>(K, rows);
+}
+
+// Lean register form of pcg1_body for ELL rows: 32-bit cell indices,
+// L1-cacheable gathers of z and p (both are written only before the grid
+// barrier that precedes their next read, see pcg1_smem_body), and the
+// x += alpha p of iteration k moved into the gather pass of iteration k + 1,
+// which reads p anyway (the same additions in the same order; once more
+// after the last iteration).  About 169 bytes a cell an iteration against
+// 177 for pcg1_body.
+template <int THREADS, class Rows>
+__device__ void pcg1_ell32_body(const gf_krylov_t& K, const Rows& rows) {
+    __shared__ CgState st;
+    KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
+    barrier_init(K);
+    double* partials = K.work + kCtlDoubles;
+    double* vec = partials + kPartials;
+    const int n = (int)K.n;
+    double* r = vec;
+    double* z = vec + n;
+    double* pa = vec + 2 * (int64_t)n;
+    double* pb = vec + 3 * (int64_t)n;
+    double* q = vec + 4 * (int64_t)n;
+    double* x = K.x;
+    const bool jac = K.jacobi != 0, linf = K.norm_inf != 0;
+    const int t0 = blockIdx.x * THREADS + threadIdx.x;
+    const int stride = gridDim.x * THREADS;
+    bool ok = true;
+    {
+        double loc[2] = {0.0, 0.0};
+        auto gx = [&](int i) { return __ldcg(x + i); };
+        for (int c = t0; c < n; c += stride) {
+            const double ax = rows.apply(c, __ldg(K.diag + c), gx);
+            const double rk = __ldg(K.rhs + c) - ax;
+            const double zk = inv_diag(K.diag, c, jac) * rk;
+            __stcg(r + c, rk);
+            __stcg(z + c, zk);
+            __stcg(pa + c, 0.0);
+            loc[0] = norm_acc(loc[0], rk, linf);
+            loc[1] += rk * zk;
+        }
+        ok = grid_reduce<2, THREADS>(ctl, partials, loc, linf ? 1u : 0u);
+        if (threadIdx.x == 0) {
+            const double r0 = norm_fin(loc[0], linf);
+            st.r0 = r0;
+            st.final = r0;
+            st.thresh = fmax(K.atol, K.rtol * r0);
+            st.rz_old = loc[1];
+            st.beta = 0.0;
+            st.alpha = 0.0;
+            st.its = 0;
+            st.converged = 0;
+            st.status = GF_MAX_ITER;
+            st.done = 0;
+            if (r0 < st.thresh) {
+                st.done = 1;
+                st.converged = 1;
+                st.status = GF_OK;
+            } else if (!isfinite(r0)) {
+                st.done = 1;
+                st.status = GF_NONFINITE;
+            }
+        }
+        __syncthreads();
+    }
+    double* p_old = pa;
+    double* p_new = pb;
+    bool pending = false;
+    for (int it = 1; ok && !st.done && it <= K.max_iter; ++it) {
+        const double beta = st.beta;
+        {  // x += alpha_(k-1) p_old; p_new = z + p_old beta; q = A p_new; p_new . q
+            const double alpha_prev = st.alpha;
+            double loc[1] = {0.0};
+            auto gp = [&](int i) { return z[i] + p_old[i] * beta; };
+            for (int c = t0; c < n; c += stride) {
+                const double pold = p_old[c];
+                const double pc = z[c] + pold * beta;
+                const double ap = rows.apply(c, __ldg(K.diag + c), gp);
+                if (pending) __stcg(x + c, __ldcg(x + c) + alpha_prev * pold);
+                __stcg(p_new + c, pc);
+                __stcg(q + c, ap);
+                loc[0] += pc * ap;
+            }
+            ok = grid_reduce<1, THREADS>(ctl, partials, loc, 0u);
+            if (!ok) break;
+            if (threadIdx.x == 0) st.alpha = st.rz_old / loc[0];
+            __syncthreads();
+        }
+        {  // r -= alpha q; z = M r; |r|, r.z
+            const double alpha = st.alpha;
+            double loc[2] = {0.0, 0.0};
+            for (int c = t0; c < n; c += stride) {
+                const double rk = __ldcg(r + c) - alpha * __ldcg(q + c);
+                const double zk = inv_diag(K.diag, c, jac) * rk;
+                __stcg(r + c, rk);
+                __stcg(z + c, zk);
+                loc[0] = norm_acc(loc[0], rk, linf);
+                loc[1] += rk * zk;
+            }
+            pending = true;
+            ok = grid_reduce<2, THREADS>(ctl, partials, loc, linf ? 1u : 0u);
+            if (!ok) break;
+            if (threadIdx.x == 0) {
+                const double fin = norm_fin(loc[0], linf);
+                st.final = fin;
+                if (fin < st.thresh) {
+                    st.done = 1;
+                    st.converged = 1;
+                    st.its = it;
+                    st.status = GF_OK;
+                } else if (!isfinite(fin)) {
+                    st.done = 1;
+                    st.its = it;
+                    st.status = GF_NONFINITE;
+                } else {
+                    st.beta = loc[1] / st.rz_old;
+                    st.rz_old = loc[1];
+                }
+            }
+            __syncthreads();
+        }
+        double* tmp = p_old;
+        p_old = p_new;
+        p_new = tmp;
+    }
+    if (ok && pending) {  // the last iteration's x += alpha p (p_old after the swap)
+        const double alpha = st.alpha;
+        for (int c = t0; c < n; c += stride) __stcg(x + c, __ldcg(x + c) + alpha * __ldcg(p_old + c));
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        double* o = K.stats;
+        o[0] = st.r0;
+        o[1] = st.final;
+        o[2] = st.done ? st.its : K.max_iter;
+        o[3] = st.converged;
+        o[4] = ok ? st.status : GF_ERR_TIMEOUT;
+    }
+}
+
+template <int WIDTH, int THREADS, int MINB, int GRP>
+__global__ void __launch_bounds__(THREADS, MINB) k_pcg1_ell32(gf_krylov_t K) {
+    EllRows<double, WIDTH, int, GRP> rows{K.val, K.nbr, (int)K.n, K.width, K.row_len};
+    pcg1_ell32_body<THREADS>(K, rows);
+}
+
+// Lean ELL CG shapes (FP64, one system, 32-bit indices): 15: 256 threads, 4
+// blocks an SM, slot groups of 8; 16: 5 blocks an SM; 17: 6 blocks an SM,
+// groups of 4; 18: 512 threads, 2 blocks an SM, groups of 8.
+constexpr int kOccVariant = 15;
+constexpr int kOccVariants = 4;
+
+template <int WIDTH>
+static BoxVariant ell_occ_kernel(int which) {
+    switch (which) {
+        case 1:
+            return {(void*)k_pcg1_ell32<WIDTH, 256, 5, 8>, 256, 1};
+        case 2:
+            return {(void*)k_pcg1_ell32<WIDTH, 256, 6, 4>, 256, 1};
+        case 3:
+            return {(void*)k_pcg1_ell32<WIDTH, 512, 2, 8>, 512, 1};
+        default:
+            return {(void*)k_pcg1_ell32<WIDTH, 256, 4, 8>, 256, 1};
+    }
 }
 
 template <int WIDTH>
@@ -3205,11 +3385,13 @@ __device__ __forceinline__ void breakdown(BiState& s, int it, int max_restart) {
 // inverse of every cell is computed once per solve into the workspace (after
 // the six vectors) and gathered from there by the preconditioned SpMVs.
 template <int NC, int WIDTH>
-__global__ void __launch_bounds__(kKThreads) k_bicgstab(gf_krylov_t K) {
+__device__ void bicgstab_body(const gf_krylov_t& K, int vb, int vn) {
     __shared__ BiState st[NC];
     __shared__ int s_any;
     KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
-    barrier_init(K);
+    const int bk = vb >= 0 ? vb : (int)blockIdx.x;
+    const int nbk = vn >= 0 ? vn : (int)gridDim.x;
+    barrier_init_v(K, nbk, bk);
     double* partials = K.work + kCtlDoubles;
     double* vec = partials + kPartials;
     const int64_t n = K.n;
@@ -3222,8 +3404,8 @@ __global__ void __launch_bounds__(kKThreads) k_bicgstab(gf_krylov_t K) {
     double* inv = vec + 6 * NC * n;
     double* x = K.x;
     const bool jac = K.jacobi != 0, linf = K.norm_inf != 0;
-    const int64_t t0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t t0 = bk * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t stride = (int64_t)nbk * blockDim.x;
     bool ok = true;
 
     {  // r = b - A x; r_hat = p = r; |r|, r.r; the Jacobi inverse
@@ -3511,7 +3693,7 @@ __global__ void __launch_bounds__(kKThreads) k_bicgstab(gf_krylov_t K) {
             __syncthreads();
         }
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (bk == 0 && threadIdx.x == 0) {
         for (int k = 0; k < NC; ++k) {
             double* o = K.stats + 5 * k;
             const bool fin = st[k].mode == kDone;
@@ -3522,6 +3704,92 @@ __global__ void __launch_bounds__(kKThreads) k_bicgstab(gf_krylov_t K) {
             o[4] = ok ? (fin ? st[k].status : GF_MAX_ITER) : GF_ERR_TIMEOUT;
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// Batched solves: the systems of several independent cases (the solve
+// server's same-phase solves) in ONE cooperative launch.  System i owns the
+// blocks [blk0[i], blk0[i+1]) and runs the single-system kernel's body on
+// them with its own barrier counter and partials (its workspace), so its
+// iterates do not depend on which other systems share the launch.
+constexpr int kMaxBatch = 16;
+
+struct KBatch {
+    int count;
+    int blk0[kMaxBatch + 1];
+    gf_krylov_t sys[kMaxBatch];
+};
+
+__device__ __forceinline__ int batch_system(const KBatch& B) {
+    int s = 0;
+    while (s + 1 < B.count && (int)blockIdx.x >= B.blk0[s + 1]) ++s;
+    return s;
+}
+
+// Zeroes every system's barrier control block (one launch for the batch).
+__global__ void k_batch_reset(const KBatch B) {
+    for (int i = threadIdx.x; i < B.count; i += blockDim.x) {
+        KCtl* ctl = reinterpret_cast<KCtl*>(B.sys[i].work);
+        ctl->count = 0ull;
+        ctl->error = 0;
+        ctl->pad = 0;
+    }
+}
+
+__global__ void __launch_bounds__(kCgThreads, 4) k_pcg1_batched(const KBatch B) {
+    const int s = batch_system(B);
+    const gf_krylov_t& K = B.sys[s];
+    const int bid = (int)blockIdx.x - B.blk0[s], nb = B.blk0[s + 1] - B.blk0[s];
+    if (K.mixed) {
+        // FP32 inner iterations inside FP64 refinement (pcg1_mixed_body).
+        if (K.stride_y > 0) {
+            if (K.symmetric) {
+                BoxRows<double, true, false> rows64{K.val, K.n, K.stride_y, K.stride_z};
+                BoxRows<float, true, true> rows32{nullptr, K.n, K.stride_y, K.stride_z};
+                pcg1_mixed_body<kCgThreads, 1>(K, rows64, rows32, 3, bid, nb);
+            } else {
+                BoxRows<double, false, false> rows64{K.val, K.n, K.stride_y, K.stride_z};
+                BoxRows<float, false, false> rows32{nullptr, K.n, K.stride_y, K.stride_z};
+                pcg1_mixed_body<kCgThreads, 1>(K, rows64, rows32, 6, bid, nb);
+            }
+        } else {
+            EllRows<double, 0> rows64{K.val, K.nbr, K.n, K.width, K.row_len};
+            EllRows<float, 0> rows32{nullptr, K.nbr, K.n, K.width, K.row_len};
+            pcg1_mixed_body<kCgThreads, 1>(K, rows64, rows32, K.width, bid, nb);
+        }
+        return;
+    }
+    if (K.stride_y > 0) {
+        if (K.symmetric) {
+            BoxRows<double, true, false> rows{K.val, K.n, K.stride_y, K.stride_z};
+            pcg1_body<kCgThreads, 1>(K, rows, bid, nb);
+        } else {
+            BoxRows<double, false, false> rows{K.val, K.n, K.stride_y, K.stride_z};
+            pcg1_body<kCgThreads, 1>(K, rows, bid, nb);
+        }
+    } else if (K.width == 6) {
+        EllRows<double, 6> rows{K.val, K.nbr, K.n, K.width, K.row_len};
+        pcg1_body<kCgThreads, 1>(K, rows, bid, nb);
+    } else {
+        EllRows<double, 0> rows{K.val, K.nbr, K.n, K.width, K.row_len};
+        pcg1_body<kCgThreads, 1>(K, rows, bid, nb);
+    }
+}
+
+template <int NC>
+__global__ void __launch_bounds__(kKThreads) k_bicgstab_batched(const KBatch B) {
+    const int s = batch_system(B);
+    const gf_krylov_t& K = B.sys[s];
+    const int bid = (int)blockIdx.x - B.blk0[s], nb = B.blk0[s + 1] - B.blk0[s];
+    if (K.width == 6)
+        bicgstab_body<NC, 6>(K, bid, nb);
+    else
+        bicgstab_body<NC, 0>(K, bid, nb);
+}
+
+template <int NC, int WIDTH>
+__global__ void __launch_bounds__(kKThreads) k_bicgstab(gf_krylov_t K) {
+    bicgstab_body<NC, WIDTH>(K, -1, -1);
 }
 
 template <class Kern>
@@ -3947,6 +4215,12 @@ int gf_pcg_solve(const gf_krylov_t* k, void* stream) {
                 const BoxVariant bv = k->symmetric ? box_kernel<false, true>(v) : box_kernel<false, false>(v);
                 return launch_persistent(bv.kern, k, stream, "gf_pcg_solve", bv.threads, bv.unroll);
             }
+            if (k->variant >= kOccVariant && k->variant < kOccVariant + kOccVariants &&
+                (int64_t)(k->width > 6 ? k->width : 6) * k->n < ((int64_t)1 << 31)) {
+                const int w = k->variant - kOccVariant;
+                const BoxVariant ev = k->width == 6 ? ell_occ_kernel<6>(w) : ell_occ_kernel<0>(w);
+                return launch_persistent(ev.kern, k, stream, "gf_pcg_solve", ev.threads, 1);
+            }
             {
                 // Variants beyond the five launch shapes fall back to 256 x 1.
                 const int v = (k->variant >= 0 && k->variant < kBoxVariants) ? k->variant : 0;
@@ -3974,6 +4248,109 @@ int gf_bicgstab_solve(const gf_krylov_t* k, void* stream) {
             return w6 ? launch_persistent(k_bicgstab<3, 6>, k, stream, "gf_bicgstab_solve")
                       : launch_persistent(k_bicgstab<3, 0>, k, stream, "gf_bicgstab_solve");
     }
+}
+
+}  // extern "C"
+
+// Batched launch of count systems (gf_pcg_solve_batched /
+// gf_bicgstab_solve_batched).  blocks[i] persistent blocks for system i;
+// their sum must be co-resident.
+static int launch_batched(const gf_krylov_t* sys, int32_t count, const int32_t* blocks, void* stream, bool bicg) {
+    const char* what = bicg ? "gf_bicgstab_solve_batched" : "gf_pcg_solve_batched";
+    if (sys == nullptr || blocks == nullptr || count < 1 || count > kMaxBatch) {
+        set_error("%s: need 1..%d systems and their block counts", what, kMaxBatch);
+        return GF_ERR_INVALID;
+    }
+    KBatch B;
+    memset(&B, 0, sizeof(B));
+    B.count = count;
+    int total = 0;
+    for (int i = 0; i < count; ++i) {
+        const gf_krylov_t& k = sys[i];
+        if (k.mixed && !bicg) {
+            // FP32-inner CG: one system and the mixed workspace.
+            if (!valid_krylov(&k, 0, what) || k.ncomp != 1 || k.max_outer < 1 || k.width > kMaxEll ||
+                k.work_len < gf_krylov_workspace_size(k.n, 1, 2 + 100 * k.width)) {
+                set_error("%s: system %d: mixed precision needs one system, max_outer >= 1 and the mixed "
+                          "workspace", what, i);
+                return GF_ERR_INVALID;
+            }
+        } else {
+            const int nvec = bicg ? 6 : (k.ncomp == 1 ? 5 : 3);
+            if (!valid_krylov(&k, nvec, what, bicg ? k.n : 0)) return GF_ERR_INVALID;
+        }
+        if ((bicg && k.mixed) || k.single_reduction || (!bicg && k.ncomp != 1) ||
+            (bicg && k.ncomp != sys[0].ncomp)) {
+            set_error("%s: system %d: one system for CG, FP64 and the same component count for BiCGStab", what, i);
+            return GF_ERR_INVALID;
+        }
+        if (k.stride_y > 0 && (k.width != 6 || k.stride_z < k.stride_y || k.stride_y < 1)) {
+            set_error("%s: system %d: a box layout needs width 6 and strides 1 <= stride_y <= stride_z", what, i);
+            return GF_ERR_INVALID;
+        }
+        if (blocks[i] < 1 || blocks[i] > kMaxBlocks) {
+            set_error("%s: system %d: block count %d outside 1..%d", what, i, blocks[i], kMaxBlocks);
+            return GF_ERR_INVALID;
+        }
+        B.sys[i] = k;
+        B.blk0[i] = total;
+        total += blocks[i];
+    }
+    B.blk0[count] = total;
+    const void* kern = !bicg ? (const void*)k_pcg1_batched
+                             : (sys[0].ncomp == 1 ? (const void*)k_bicgstab_batched<1>
+                                                  : sys[0].ncomp == 2 ? (const void*)k_bicgstab_batched<2>
+                                                                      : (const void*)k_bicgstab_batched<3>);
+    const int threads = bicg ? kKThreads : kCgThreads;
+    int dev = 0, sms = 0, coop = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, 0);
+    if (e != cudaSuccess || !coop) {
+        set_error("%s: set-up failed: %s", what, cudaGetErrorString(e));
+        return GF_ERR_CUDA;
+    }
+    if (total > per_sm * sms) {
+        set_error("%s: %d blocks requested, %d co-resident at most", what, total, per_sm * sms);
+        return GF_ERR_INVALID;
+    }
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    k_batch_reset<<<1, 32, 0, st>>>(B);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error("%s: %s", what, cudaGetErrorString(e));
+        return GF_ERR_CUDA;
+    }
+    void* args[] = {&B};
+    e = cudaLaunchCooperativeKernel(kern, dim3(total), dim3(threads), args, 0, st);
+    if (e != cudaSuccess) {
+        set_error("%s: cooperative launch failed: %s", what, cudaGetErrorString(e));
+        return GF_ERR_CUDA;
+    }
+    return GF_OK;
+}
+
+extern "C" {
+
+int gf_pcg_solve_batched(const gf_krylov_t* systems, int32_t count, const int32_t* blocks, void* stream) {
+    return launch_batched(systems, count, blocks, stream, false);
+}
+
+int gf_bicgstab_solve_batched(const gf_krylov_t* systems, int32_t count, const int32_t* blocks, void* stream) {
+    return launch_batched(systems, count, blocks, stream, true);
+}
+
+int gf_batch_max_blocks(int32_t bicgstab) {
+    const void* kern = bicgstab ? (const void*)k_bicgstab_batched<3> : (const void*)k_pcg1_batched;
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
+        cudaSuccess || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, bicgstab ? kKThreads : kCgThreads,
+                                                                      0) != cudaSuccess) {
+        set_error("gf_batch_max_blocks: device query failed");
+        return -1;
+    }
+    return per_sm * sms;
 }
 
 }  // extern "C"

@@ -105,6 +105,49 @@ def plane_sdf(point: float, axis: int = 0) -> SdfFn:
     return sdf
 
 
+# Shape parameters of the slanted bluff body, in this order: length, width,
+# height, front rounding radius in plan view (vertical front edges), front
+# rounding radius in side view (horizontal front edges), rear slant angle
+# (degrees), slant length along x, ground clearance.
+BLUFF_PARAMS = ("length", "width", "height", "r_plan", "r_side", "slant_deg", "slant_len", "clearance")
+BLUFF_DEFAULT = (1.0, 0.39, 0.29, 0.1, 0.1, 25.0, 0.222, 0.05)
+
+
+def _rounded_front_rect(u: np.ndarray, v: np.ndarray, u0: float, u1: float, v0: float, v1: float,
+                        r: float) -> np.ndarray:
+    """Signed distance to the rectangle [u0, u1] x [v0, v1] whose two corners
+    at u = u0 are rounded with radius r (the rear corners stay sharp)."""
+    cu, cv = 0.5 * (u0 + u1), 0.5 * (v0 + v1)
+    bu, bv = 0.5 * (u1 - u0), 0.5 * (v1 - v0)
+    rr = np.where(u < cu, r, 0.0)
+    qu = np.abs(u - cu) - bu + rr
+    qv = np.abs(v - cv) - bv + rr
+    outside = np.sqrt(np.maximum(qu, 0.0) ** 2 + np.maximum(qv, 0.0) ** 2)
+    return outside + np.minimum(np.maximum(qu, qv), 0.0) - rr
+
+
+def bluff_body_sdf(x0: float = 0.0, params=BLUFF_DEFAULT) -> SdfFn:
+    """Level set of a slanted bluff body (an Ahmed-type car body): a box
+    from x = x0 to x0 + length, centred on y = 0, from z = clearance to
+    clearance + height, its front edges rounded in plan and side view, its
+    top rear edge cut by a plane at ``slant_deg`` to the horizontal over
+    ``slant_len``.  Negative inside.  The zero set is exact; away from it the
+    value is a bound (intersections by max)."""
+    L, Wd, H, r_plan, r_side, slant, ls, g = (float(v) for v in params)
+    th = np.deg2rad(slant)
+    nx, nz = np.sin(th), np.cos(th)
+    xs, zs = x0 + L - ls, g + H
+
+    def sdf(x: np.ndarray) -> np.ndarray:
+        px, py, pz = x[..., 0], x[..., 1], x[..., 2]
+        plan = _rounded_front_rect(px, py, x0, x0 + L, -0.5 * Wd, 0.5 * Wd, r_plan)
+        side = _rounded_front_rect(px, pz, x0, x0 + L, g, g + H, r_side)
+        cut = nx * (px - xs) + nz * (pz - zs)
+        return np.maximum(np.maximum(plan, side), cut)
+
+    return sdf
+
+
 def _segment_roots(
     sdf: SdfFn, p0: np.ndarray, p1: np.ndarray, n_bisect: int = 80
 ) -> np.ndarray:

@@ -22,13 +22,14 @@ _ALL = ["x_minus", "x_plus", "y_minus", "y_plus", "z_minus", "z_plus"]
 
 
 def cavity_simulator(nu: float, lid: float, *, p_tol: float = 1e-6, p_solver_tol: float = 1e-6,
-                     max_outer: int = 2000, inner_precision: str = "float64",
+                     p_solver_rtol: float = 0.0, max_outer: int = 2000, inner_precision: str = "float64",
                      device: str = "cuda") -> SimulatorConfig:
     """``p_tol``: residualControl on p (the RHS-normalised initial residual,
     algorithms/utils/residual.py:12-36); ``p_solver_tol``: absolute CG
     tolerance of the pressure solve.  The normalised residual cannot fall
     much below ``p_solver_tol / |b|``, so a tight ``p_tol`` needs a tight
-    solver tolerance; otherwise the run ends at ``max_outer`` (endTime).
+    solver tolerance (or a relative one, ``p_solver_rtol``); otherwise the
+    run ends at ``max_outer`` (endTime).
     ``inner_precision="float32"`` runs the pressure CG's inner iterations in
     FP32 inside FP64 iterative refinement."""
     sim = {
@@ -58,7 +59,7 @@ def cavity_simulator(nu: float, lid: float, *, p_tol: float = 1e-6, p_solver_tol
                 "U": {"method": "bicgstab", "preconditioner": "jacobi", "tolerance": 1e-8,
                       "rel_tolerance": 0.1, "max_iter": 1000},
                 "p": {"method": "cg", "preconditioner": "jacobi", "tolerance": p_solver_tol,
-                      "rel_tolerance": 0.0, "max_iter": 2000, "inner_precision": inner_precision},
+                      "rel_tolerance": p_solver_rtol, "max_iter": 2000, "inner_precision": inner_precision},
             },
         },
         "conditions": {

@@ -77,8 +77,8 @@ class _Slot:
         self.done = False
         self.draining = False
         sim = cavity_simulator(req.nu, req.lid, p_tol=engine.p_tol, p_solver_tol=engine.p_solver_tol,
-                               max_outer=engine.max_outer, inner_precision=engine.inner_precision,
-                               device=str(engine.device.type))
+                               p_solver_rtol=engine.p_solver_rtol, max_outer=engine.max_outer,
+                               inner_precision=engine.inner_precision, device=str(engine.device.type))
         self.max_outer = engine.max_outer
         self.tol = engine.p_tol
         with torch.cuda.stream(self.stream):
@@ -157,8 +157,8 @@ class ServingEngine:
 
     def __init__(self, device="cuda", *, hbm_budget: int | None = None, max_slots: int = 8,
                  use_graphs: bool = True, p_tol: float = 1e-6, p_solver_tol: float = 1e-6,
-                 max_outer: int = 2000, inner_precision: str = "float64", keep_fields: bool = False,
-                 gpu_share: float = 1.0):
+                 p_solver_rtol: float = 0.0, max_outer: int = 2000, inner_precision: str = "float64",
+                 keep_fields: bool = False, gpu_share: float = 1.0):
         self.device = torch.device(device)
         if self.device.index is None:
             self.device = torch.device("cuda", torch.cuda.current_device())
@@ -170,6 +170,7 @@ class ServingEngine:
         self.use_graphs = bool(use_graphs)
         self.p_tol = float(p_tol)
         self.p_solver_tol = float(p_solver_tol)
+        self.p_solver_rtol = float(p_solver_rtol)
         self.inner_precision = str(inner_precision)
         # Share of the GPU one case's persistent Krylov kernels may occupy
         # (< 1 leaves SMs free for the kernels of other slots).
@@ -190,8 +191,8 @@ class ServingEngine:
 
         for n in sorted(set(int(s) for s in sizes)):
             sim = cavity_simulator(1e-2, 1.0, p_tol=self.p_tol, p_solver_tol=self.p_solver_tol,
-                                   max_outer=self.max_outer, inner_precision=self.inner_precision,
-                                   device=str(self.device.type))
+                                   p_solver_rtol=self.p_solver_rtol, max_outer=self.max_outer,
+                                   inner_precision=self.inner_precision, device=str(self.device.type))
             self.topologies.grid(n, sim)
             if autotune:
                 sysm = BoxSystem(n, n, n, device=self.device)
@@ -261,7 +262,8 @@ class ServingEngine:
 
 
 def serve_sequential(requests: list[CavityRequest], device="cuda", *, p_tol: float = 1e-6,
-                     p_solver_tol: float = 1e-6, max_outer: int = 2000, keep_fields: bool = False,
+                     p_solver_tol: float = 1e-6, p_solver_rtol: float = 0.0, max_outer: int = 2000,
+                     keep_fields: bool = False,
                      topologies: TopologyCache | None = None, variants: dict | None = None,
                      clock=time.perf_counter) -> list[ServeResult]:
     """One-at-a-time FP64 baseline through the plain algorithm API: each
@@ -278,8 +280,8 @@ def serve_sequential(requests: list[CavityRequest], device="cuda", *, p_tol: flo
         if req.arrival > now:
             time.sleep(req.arrival - now)
         admitted = clock() - t0
-        sim = cavity_simulator(req.nu, req.lid, p_tol=p_tol, p_solver_tol=p_solver_tol, max_outer=max_outer,
-                               device=str(dev.type))
+        sim = cavity_simulator(req.nu, req.lid, p_tol=p_tol, p_solver_tol=p_solver_tol,
+                               p_solver_rtol=p_solver_rtol, max_outer=max_outer, device=str(dev.type))
         algo = create_algorithm(topo.grid(req.n, sim))
         if variants and req.n in variants:
             algo.solvers["p"].variant = variants[req.n]
@@ -290,10 +292,11 @@ def serve_sequential(requests: list[CavityRequest], device="cuda", *, p_tol: flo
             if algo.has_converged():
                 break
         res = float(algo.res_buf[0].item())
+        converged = res < p_tol
         U = algo.U.data.cpu().numpy() if keep_fields else None
         p = algo.p.data.cpu().numpy() if keep_fields else None
         torch.cuda.synchronize(dev)
-        results.append(ServeResult(req.id, req.n, req.arrival, admitted, clock() - t0, its, res < p_tol, res, U, p))
+        results.append(ServeResult(req.id, req.n, req.arrival, admitted, clock() - t0, its, converged, res, U, p))
         del algo
     return results
 
@@ -305,9 +308,14 @@ def summarize(results: list[ServeResult]) -> dict:
     lat = np.array([r.latency for r in results])
     first = min(r.arrival for r in results)
     last = max(r.finished for r in results)
+    statuses: dict = {}
+    for r in results:
+        st = getattr(r, "status", "converged" if r.converged else "end_time")
+        statuses[st] = statuses.get(st, 0) + 1
     return {
         "completed": len(results),
         "converged": int(sum(r.converged for r in results)),
+        "statuses": statuses,
         "solves_per_s": len(results) / max(last - first, 1e-12),
         "p50_latency_s": float(np.percentile(lat, 50)),
         "p99_latency_s": float(np.percentile(lat, 99)),

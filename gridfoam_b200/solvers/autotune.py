@@ -30,7 +30,7 @@ from gridfoam_b200.meta.config import PrecisionType, PreconditionerType, SolverC
 # Variants 0-7 differ only in launch shape and memory placement (their
 # iterates differ by the order of the dot-product partial sums); 8 and 9
 # form q = A p by recurrence.
-N_VARIANTS = 15
+N_VARIANTS = 19
 VARIANTS = {
     0: "256 threads x 1 cell/pass",
     1: "256 threads x 2 cells/pass",
@@ -47,6 +47,10 @@ VARIANTS = {
     12: "512 threads x 2 a SM, vectors in global memory, q = A z + beta q recurrence (any size, FP64)",
     13: "1024 threads, vectors in global memory, q = A z + beta q recurrence (any size, FP64)",
     14: "256 threads x 4 a SM, vectors in global memory, q = A z + beta q recurrence (any size, FP64)",
+    15: "ELL rows (box: as 2), lean 32-bit form, x update deferred: 256 threads x 4 a SM, row loads in groups of 8",
+    16: "ELL rows (box: as 2), lean 32-bit form: 256 threads x 5 a SM, groups of 8",
+    17: "ELL rows (box: as 2), lean 32-bit form: 256 threads x 6 a SM, groups of 4",
+    18: "ELL rows (box: as 2), lean 32-bit form: 512 threads x 2 a SM, groups of 8",
 }
 
 _LOCK = threading.Lock()

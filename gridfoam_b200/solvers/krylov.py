@@ -106,6 +106,28 @@ class DeviceKrylov(LinearSolver):
         ``symmetric`` declares that ``A`` is symmetric (the pressure system),
         which lets CG on a uniform box read only three coefficient arrays.
         """
+        k, stats = self.describe(grid, diag, val, rhs, x, symmetric=symmetric)
+        nc = rhs.shape[0]
+        ev = None
+        if self.profile_events is not None:
+            ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            ev[0].record()
+        call("gf_bicgstab_solve" if self.bicgstab else "gf_pcg_solve", ctypes.byref(k), stream_ptr())
+        if ev is not None:
+            ev[1].record()
+        if not self.host_stats:
+            return ()
+        buf = _StatsBuffer(stats)
+        out = tuple(SolveStats(self.solver_name, buf, i) for i in range(nc))
+        if ev is not None:
+            self.profile_events.append((ev[0], ev[1], out))
+        return out
+
+    def describe(self, grid, diag: torch.Tensor, val: torch.Tensor, rhs: torch.Tensor,
+                 x: torch.Tensor, *, symmetric: bool = False) -> tuple[GfKrylov, torch.Tensor]:
+        """The solve's descriptor (workspace and statistics buffer included)
+        without launching it: ``solve_arrays`` launches it alone, the solve
+        server batches the descriptors of many cases into one launch."""
         nc, n = rhs.shape
         key = (str(grid.device), nc)
         stats = self._stats_dev.get(key)
@@ -148,20 +170,7 @@ class DeviceKrylov(LinearSolver):
         if box is not None and not self.bicgstab and nc == 1:
             k.stride_y, k.stride_z = box
             k.symmetric = int(symmetric)
-        ev = None
-        if self.profile_events is not None:
-            ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-            ev[0].record()
-        call("gf_bicgstab_solve" if self.bicgstab else "gf_pcg_solve", ctypes.byref(k), stream_ptr())
-        if ev is not None:
-            ev[1].record()
-        if not self.host_stats:
-            return ()
-        buf = _StatsBuffer(stats)
-        out = tuple(SolveStats(self.solver_name, buf, i) for i in range(nc))
-        if ev is not None:
-            self.profile_events.append((ev[0], ev[1], out))
-        return out
+        return k, stats
 
     def _solve_matrix(self, A, rhs_store: torch.Tensor, x0_store: torch.Tensor) -> SolveResult:
         x = x0_store.contiguous().clone()

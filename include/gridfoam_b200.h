@@ -305,6 +305,25 @@ int64_t gf_pcg_static_scratch_doubles(void);
  * restarts, one persistent cooperative launch, ncomp systems at once. */
 int gf_bicgstab_solve(const gf_krylov_t* k, void* stream);
 
+/* Batched solves for the solve server (no counterpart in the reference,
+ * which solves one case at a time, solvers/krylov.py:34-82): the systems of
+ * up to 16 independent cases in ONE cooperative launch (CG: FP64 or, with
+ * mixed = 1, FP32 inner iterations in FP64 refinement; BiCGStab: FP64).  System i
+ * runs on blocks[i] persistent blocks of its own with its own workspace and
+ * statistics, exactly as gf_pcg_solve / gf_bicgstab_solve run it on a grid
+ * of blocks[i] blocks (register kernel, 256 threads a block for CG, 512 for
+ * BiCGStab), so its result does not depend on the other systems in the
+ * batch.  The block counts must fit on the device at once
+ * (gf_batch_max_blocks); CG systems have ncomp 1, BiCGStab systems share
+ * one ncomp.  Two launches: a reset of the control blocks, then the solves. */
+int gf_pcg_solve_batched(const gf_krylov_t* systems, int32_t count,
+                         const int32_t* blocks, void* stream);
+int gf_bicgstab_solve_batched(const gf_krylov_t* systems, int32_t count,
+                              const int32_t* blocks, void* stream);
+/* Co-resident blocks of the batched CG (bicgstab 0) or BiCGStab (1) kernel
+ * on the current device, or -1. */
+int gf_batch_max_blocks(int32_t bicgstab);
+
 /* core/fvmatrix.py:242-290 and algorithms/simple.py:336-337:
  * rAU = 1 / (diag / V), HbyA = rAU * H(psi); h1 (may be NULL) receives
  * H1() (fvmatrix.py:250-264). */

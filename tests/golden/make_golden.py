@@ -53,7 +53,15 @@ from gridfoam.meta.enums import DomainBoundaryPatch  # noqa: E402
 from gridfoam.solvers.bicgstab import BiCGSTABSolver  # noqa: E402
 from gridfoam.solvers.cg import CGSolver  # noqa: E402
 
-from tests.golden.cases import ALL_CASES, DIV_SCHEMES, STEPS, build_mesh  # noqa: E402
+from tests.golden.cases import (  # noqa: E402
+    ALL_CASES,
+    DIV_SCHEMES,
+    STEPS,
+    build_mesh,
+    cavity_case,
+    cylinder_wake_case,
+    pipe_case,
+)
 
 
 
@@ -97,6 +105,83 @@ def stats_array(stats) -> np.ndarray:
             for s in stats
         ]
     )
+
+
+def reference_algorithm(case: dict):
+    """The reference's grid and algorithm for a case definition, with the
+    per-face parabolic inlet where the case has one; returns
+    ``(grid, mesh, algo, captured)``, ``captured`` receiving each step's
+    solver statistics."""
+    profile = case["inlet_profile"]
+    original = bc_factory.create_boundary_condition
+
+    def patched(bc_config, dtype, device):
+        if profile is not None and [str(p) for p in bc_config.patches] == [
+            profile["patch"]
+        ] and bc_config.type == "dirichlet" and bc_config.value is not None and len(
+            np.atleast_1d(bc_config.value)
+        ) == 3:
+            return ParabolicInletBC(profile)
+        return original(bc_config, dtype, device)
+
+    ref_field.boundary_factory.create_boundary_condition = patched
+    try:
+        grid, mesh = make_grid(case)
+        algo = create_algorithm(grid)
+    finally:
+        ref_field.boundary_factory.create_boundary_condition = original
+    captured: list[dict] = []
+    orig_finalize = algo._finalize_diagnostics
+
+    def capture(phi, solve_stats):
+        captured.append(dict(solve_stats))
+        return orig_finalize(phi, solve_stats)
+
+    algo._finalize_diagnostics = capture
+    return grid, mesh, algo, captured
+
+
+# Full-size runs of the benchmark configs (fewer steps than the configs
+# name where the reference's CPU run would take hours): key -> (case
+# builder, steps, keep the full final fields).
+FULLSIZE = {
+    "cavity32_300": (lambda: cavity_case(32), 300, True),
+    "pipe64x256_20": (lambda: pipe_case(64, 256, 4.0), 20, False),
+    "wake256x160x32_10": (lambda: cylinder_wake_case((256, 160, 32)), 10, False),
+}
+
+
+def fullsize_run(key: str) -> dict:
+    """Per-step solver iterations, field norms and a fixed sample of cells of
+    the reference's own run at a benchmark config's full size; the final
+    fields in full where they are small."""
+    build, n_steps, keep_full = FULLSIZE[key]
+    case = build()
+    grid, mesh, algo, captured = reference_algorithm(case)
+    n = int(mesh.n_cells)
+    stride = max(1, n // 4096)
+    sample = np.arange(0, n, stride)
+    out: dict[str, np.ndarray] = {"sample_cells": sample, "mesh_n_cells": np.array(n)}
+    its_u, its_p, norms = [], [], []
+    for step in range(n_steps):
+        with torch.no_grad():
+            algo.step()
+        stats = captured[-1]
+        its_u.append([s.iterations for s in stats["U"]])
+        its_p.append([s.iterations for s in stats["p"]])
+        U, p = algo.U.data.numpy(), algo.p.data.numpy()
+        norms.append([np.linalg.norm(U[:, k]) for k in range(3)] + [np.linalg.norm(p)])
+        if step in (0, n_steps - 1) or (n_steps <= 20 and step % 5 == 4) or (n_steps > 20 and step % 100 == 99):
+            out[f"step{step}_U_sample"] = U[sample].copy()
+            out[f"step{step}_p_sample"] = p[sample].copy()
+        print(f"  {key} step {step}: U its {its_u[-1]}, p its {its_p[-1]}", flush=True)
+    out["its_U"] = np.array(its_u)
+    out["its_p"] = np.array(its_p)
+    out["norms"] = np.array(norms)
+    if keep_full:
+        out["final_U"] = algo.U.data.numpy().copy()
+        out["final_p"] = algo.p.data.numpy().copy()
+    return out
 
 
 def run_case(name: str, n_steps: int, case: dict | None = None) -> dict:
@@ -505,6 +590,13 @@ def main() -> None:
             path = HERE / f"forces_{name}.npz"
             np.savez_compressed(path, **data)
             print(f"forces {name}: {len(data)} arrays -> {path} ({path.stat().st_size} B)")
+        return
+    if args and args[0] == "--fullsize":
+        for key in args[1:] or list(FULLSIZE):
+            data = fullsize_run(key)
+            path = HERE / f"fullsize_{key}.npz"
+            np.savez_compressed(path, **data)
+            print(f"fullsize {key}: {len(data)} arrays -> {path} ({path.stat().st_size} B)")
         return
     if args and args[0] == "--gradlinear":
         # The Green-Gauss ('linear') gradient scheme: whole steps and the

@@ -445,7 +445,7 @@ def test_smem_resident_cg_fixed_iterations_match_register_kernel(variant, box):
     assert rel(xs[1], xs[0]) < 1e-11
 
 
-@pytest.mark.parametrize("variant", [6, 7, 8, 9, 10, 11, 12, 13, 14])
+@pytest.mark.parametrize("variant", [6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18])
 def test_smem_resident_cg_on_ell_layout(variant):
     """The shared-memory-resident CG through the general ELL rows (the
     octree path), against the register ELL kernel."""
@@ -649,7 +649,7 @@ def test_stream_cg_fixed_iterations_match_qrec(variant, box):
     assert rel(xs[1], xs[0]) < 1e-11
 
 
-@pytest.mark.parametrize("variant", [2, 12, 13])
+@pytest.mark.parametrize("variant", [2, 12, 13, 15, 17])
 def test_row_lengths_skip_only_empty_slots(variant):
     """On an octree grid (couplings first in every row) the CG with the
     row-length early exit gives the same iterations and solution as the
@@ -703,3 +703,22 @@ def test_grad_linear_steps_and_operator_match_reference(name):
     _load_state(algo, golden, STEPS[name] - 1)
     _check(fvc.grad(algo.p).data, golden["op_grad_p"], "grad_p", 1e-10)
     _check(fvc.grad(algo.U).data, golden["op_grad_U"], "grad_U", 1e-10)
+
+
+@pytest.mark.parametrize("variant", [15, 16, 17, 18])
+def test_lean_ell_cg_fixed_iterations_match_register_kernel(variant):
+    """The lean ELL CG (32-bit indices, x update moved into the next gather
+    pass) against the register kernel: exactly 60 iterations agree up to the
+    order of the dot-product partial sums."""
+    from gridfoam_b200.solvers.autotune import BoxSystem, _solver
+
+    sysm = BoxSystem(40, 36, 44, device=torch.device("cuda"))
+    sysm.box_strides = None
+    xs = []
+    for v in (0, variant):
+        s = _solver(60, False, v)
+        x = torch.zeros_like(sysm.rhs)
+        st = s.solve_arrays(sysm, sysm.diag, sysm.val, sysm.rhs, x, symmetric=True)
+        assert st[0].iterations == 60 and st[0].status == "max_iter"
+        xs.append(to_np(x))
+    assert rel(xs[1], xs[0]) < 1e-11
