@@ -261,6 +261,31 @@ def _rel(a, b) -> float:
     return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(np.asarray(b)), 1e-300))
 
 
+# Drag and lift of the cylinder (diameter 1, span 4, inflow 1): force
+# scale 0.5 rho U^2 D span.
+FORCE_PATCH, FORCE_SCALE, FORCE_COFR = "cylinder", 0.5 * 1.0 * 1.0 * 4.0, (10.0, 10.0, 2.0)
+
+
+def gpu_coefficients(grid, algo) -> dict:
+    """Cd / Cl of the cylinder from the device force integral."""
+    import numpy as np
+
+    from gridfoam_b200.post.forces import patch_force
+
+    r = patch_force(grid, algo.p, algo.U, algo.nu, FORCE_PATCH, 1.0, np.asarray(FORCE_COFR))
+    return {"Cd": float(r.force[0] / FORCE_SCALE), "Cl": float(r.force[1] / FORCE_SCALE)}
+
+
+def oracle_coefficients(oalgo, mesh) -> dict:
+    import numpy as np
+
+    from oracle.forces import patch_force
+
+    f, _, _, _ = patch_force(oalgo.p, oalgo.U, oalgo.nu, FORCE_PATCH, 1.0, np.asarray(FORCE_COFR),
+                             mesh.ap.anchor_normal)
+    return {"Cd": float(f[0] / FORCE_SCALE), "Cl": float(f[1] / FORCE_SCALE)}
+
+
 def mixed_variant(args, local: int, torch, first_fp64, oracle_first) -> dict:
     """The workload with FP32 inner iterations of the pressure CG inside FP64
     iterative refinement.  Errors: after the first step against the FP64
@@ -276,7 +301,8 @@ def mixed_variant(args, local: int, torch, first_fp64, oracle_first) -> dict:
     torch.cuda.synchronize()
     U1, p1 = algo.U.data.cpu().numpy(), algo.p.data.cpu().numpy()
     out = {"rel_l2_U_vs_fp64_gpu_step1": _rel(U1, first_fp64[0]),
-           "rel_l2_p_vs_fp64_gpu_step1": _rel(p1, first_fp64[1])}
+           "rel_l2_p_vs_fp64_gpu_step1": _rel(p1, first_fp64[1]),
+           "coefficients_step1": gpu_coefficients(grid, algo)}
     if oracle_first is not None:
         out["rel_l2_U_vs_fp64_oracle_step1"] = _rel(U1, oracle_first[0])
         out["rel_l2_p_vs_fp64_oracle_step1"] = _rel(p1, oracle_first[1])
@@ -284,6 +310,7 @@ def mixed_variant(args, local: int, torch, first_fp64, oracle_first) -> dict:
         algo.step()
     ms = _timed_steps(algo, args.steps, torch)
     its = [s.iterations for s in algo.last_stats["p"]]
+    out["coefficients_after_all_steps"] = gpu_coefficients(grid, algo)
     out.update({
         "value": grid.num_cells * args.steps / (ms * 1e-3),
         "unit": METRIC,
@@ -439,6 +466,49 @@ def cavity_variant(local: int, torch) -> dict:
             "last_p_iterations": [s.iterations for s in algo.last_stats["p"]]}
 
 
+BLUFF_BASE = (256, 64, 48)
+
+
+def bluff_variant(args, local: int, torch) -> dict:
+    """The slanted bluff body (length 1, width 0.39, height 0.29, front
+    rounding 0.1, rear slant 25 deg over 0.222) in a channel on a 4-level
+    octree (base 256x64x48, levels 0-3), inflow 1, nu 2e-6, steady SIMPLE
+    (SIMPLEC): cell-iters/s of the SIMPLE iterations after warm-up, the
+    mesh set-up time and the drag coefficient on the body."""
+    import numpy as np
+
+    from gridfoam_b200.cases import bluff_body_case, create_case
+    from gridfoam_b200.post.forces import patch_force
+
+    case = bluff_body_case(BLUFF_BASE)
+    t0 = time.perf_counter()
+    mesh, grid, algo = create_case(case, device=f"cuda:{local}")
+    torch.cuda.synchronize()
+    setup = time.perf_counter() - t0
+    for _ in range(args.warmup):
+        algo.step()
+    ms = _timed_steps(algo, args.steps, torch)
+    r = patch_force(grid, algo.p, algo.U, algo.nu, "body", 1.0, np.zeros(3))
+    area = 0.39 * 0.29
+    out = {
+        "workload": f"bluff_body_{BLUFF_BASE[0]}x{BLUFF_BASE[1]}x{BLUFF_BASE[2]}_l3_simple",
+        "cells": grid.num_cells,
+        "internal_faces": grid.num_internal_faces,
+        "hanging_faces": grid.num_hanging,
+        "immersed_faces": grid.num_immersed_faces,
+        "setup_s": setup,
+        "value": grid.num_cells * args.steps / (ms * 1e-3),
+        "unit": METRIC,
+        "ms_per_iteration": ms / args.steps,
+        "last_p_iterations": [s.iterations for s in algo.last_stats["p"]],
+        "Cd_after_all_iterations": float(r.force[0] / (0.5 * area)),
+        "note": "forward only: the shape gradient of the drag is not built",
+    }
+    del algo, grid
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_gpu(args) -> None:
     import numpy as np
     import torch
@@ -468,6 +538,7 @@ def run_gpu(args) -> None:
     algo.step()
     torch.cuda.synchronize()
     first = (algo.U.data.cpu().numpy(), algo.p.data.cpu().numpy())
+    coeff_first = gpu_coefficients(grid, algo)
     for _ in range(max(0, args.warmup - 1)):
         algo.step()
     torch.cuda.synchronize()
@@ -501,6 +572,7 @@ def run_gpu(args) -> None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     final = (algo.U.data.cpu().numpy(), algo.p.data.cpu().numpy())
+    coeff_final = gpu_coefficients(grid, algo)
 
     # Roofline of the pressure CG launches (HBM-bound at this size).
     durations, iters = [], []
@@ -563,6 +635,7 @@ def run_gpu(args) -> None:
             "setup_s": setup_s,
             "p_iterations_per_solve": (sum(iters) / len(iters)) if iters else None,
             "p_solve_share_of_step": total_time * 1e3 / ms if ms > 0 else None,
+            "cylinder_coefficients_after_warmup_and_timed_steps": coeff_final,
             "algorithmic_bytes_per_step_pcg": step_bytes,
             "algorithmic_GBps_per_step_pcg": step_bytes / (ms / args.steps * 1e-3) / 1e9,
         },
@@ -591,6 +664,8 @@ def run_gpu(args) -> None:
             "d2h_bytes_per_step": h2d,
         },
     }
+    del algo
+    torch.cuda.empty_cache()
     oracle_first = None
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         cpu, oalgo = cpu_baseline(mesh, case)
@@ -599,6 +674,8 @@ def run_gpu(args) -> None:
         line["parity_first_step_vs_fp64_oracle"] = {
             "rel_l2_U": _rel(first[0], oracle_first[0]),
             "rel_l2_p": _rel(first[1], oracle_first[1]),
+            "coefficients_gpu": coeff_first,
+            "coefficients_oracle": oracle_coefficients(oalgo, mesh),
             "note": "full mesh, first PISO step from the initial state; p solves stop at rel_tolerance 0.01 "
                     "(p) and 1e-7 absolute (pFinal), so two correct implementations differ inside that band",
         }
@@ -611,9 +688,8 @@ def run_gpu(args) -> None:
         torch.cuda.empty_cache()
         line["variants"] = {"mixed_fp32_inner": mixed,
                             "ib_pipe_64x64x256": pipe_variant(args, local, torch),
-                            "cavity_32": cavity_variant(local, torch)}
-    del algo
-    torch.cuda.empty_cache()
+                            "cavity_32": cavity_variant(local, torch),
+                            "bluff_body": bluff_variant(args, local, torch)}
     if not args.no_serving:
         line["serving"] = serving_bench(args, local, dist, rank, world)
     if rank == 0:

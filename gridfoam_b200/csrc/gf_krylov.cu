@@ -1318,7 +1318,14 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_pcg1_ellv(gf_krylov
 // which reads p anyway (the same additions in the same order; once more
 // after the last iteration).  About 169 bytes a cell an iteration against
 // 177 for pcg1_body.
-template <int THREADS, class Rows>
+// PF: before a cell is processed, the lines of the cell one grid stride on
+// (its row slots, own vector entries) are prefetched into L2, so that
+// cell's loads return at L2 rather than DRAM latency.
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
+template <int THREADS, class Rows, bool PF = false>
 __device__ void pcg1_ell32_body(const gf_krylov_t& K, const Rows& rows) {
     __shared__ CgState st;
     KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
@@ -1383,6 +1390,20 @@ __device__ void pcg1_ell32_body(const gf_krylov_t& K, const Rows& rows) {
             double loc[1] = {0.0};
             auto gp = [&](int i) { return z[i] + p_old[i] * beta; };
             for (int c = t0; c < n; c += stride) {
+                if (PF) {
+                    const int cn = c + stride;
+                    if (cn < n) {
+#pragma unroll
+                        for (int sl = 0; sl < 6; ++sl) {
+                            prefetch_l2(K.val + (int64_t)sl * n + cn);
+                            prefetch_l2(K.nbr + (int64_t)sl * n + cn);
+                        }
+                        prefetch_l2(K.diag + cn);
+                        prefetch_l2(z + cn);
+                        prefetch_l2(p_old + cn);
+                        prefetch_l2(x + cn);
+                    }
+                }
                 const double pold = p_old[c];
                 const double pc = z[c] + pold * beta;
                 const double ap = rows.apply(c, __ldg(K.diag + c), gp);
@@ -1400,6 +1421,14 @@ __device__ void pcg1_ell32_body(const gf_krylov_t& K, const Rows& rows) {
             const double alpha = st.alpha;
             double loc[2] = {0.0, 0.0};
             for (int c = t0; c < n; c += stride) {
+                if (PF) {
+                    const int cn = c + stride;
+                    if (cn < n) {
+                        prefetch_l2(r + cn);
+                        prefetch_l2(q + cn);
+                        prefetch_l2(K.diag + cn);
+                    }
+                }
                 const double rk = __ldcg(r + c) - alpha * __ldcg(q + c);
                 const double zk = inv_diag(K.diag, c, jac) * rk;
                 __stcg(r + c, rk);
@@ -1447,15 +1476,15 @@ __device__ void pcg1_ell32_body(const gf_krylov_t& K, const Rows& rows) {
     }
 }
 
-template <int WIDTH, int THREADS, int MINB, int GRP>
+template <int WIDTH, int THREADS, int MINB, int GRP, bool PF = false>
 __global__ void __launch_bounds__(THREADS, MINB) k_pcg1_ell32(gf_krylov_t K) {
     EllRows<double, WIDTH, int, GRP> rows{K.val, K.nbr, (int)K.n, K.width, K.row_len};
-    pcg1_ell32_body<THREADS>(K, rows);
+    pcg1_ell32_body<THREADS, EllRows<double, WIDTH, int, GRP>, PF>(K, rows);
 }
 
 // Lean ELL CG shapes (FP64, one system, 32-bit indices): 15: 256 threads, 4
 // blocks an SM, slot groups of 8; 16: 5 blocks an SM; 17: 6 blocks an SM,
-// groups of 4; 18: 512 threads, 2 blocks an SM, groups of 8.
+// groups of 4; 18: as 17 with the next cell's lines prefetched into L2.
 constexpr int kOccVariant = 15;
 constexpr int kOccVariants = 4;
 
@@ -1467,7 +1496,7 @@ static BoxVariant ell_occ_kernel(int which) {
         case 2:
             return {(void*)k_pcg1_ell32<WIDTH, 256, 6, 4>, 256, 1};
         case 3:
-            return {(void*)k_pcg1_ell32<WIDTH, 512, 2, 8>, 512, 1};
+            return {(void*)k_pcg1_ell32<WIDTH, 256, 6, 4, true>, 256, 1};
         default:
             return {(void*)k_pcg1_ell32<WIDTH, 256, 4, 8>, 256, 1};
     }

@@ -50,7 +50,7 @@ VARIANTS = {
     15: "ELL rows (box: as 2), lean 32-bit form, x update deferred: 256 threads x 4 a SM, row loads in groups of 8",
     16: "ELL rows (box: as 2), lean 32-bit form: 256 threads x 5 a SM, groups of 8",
     17: "ELL rows (box: as 2), lean 32-bit form: 256 threads x 6 a SM, groups of 4",
-    18: "ELL rows (box: as 2), lean 32-bit form: 512 threads x 2 a SM, groups of 8",
+    18: "ELL rows (box: as 2), lean 32-bit form: 256 threads x 6 a SM, groups of 4, next cell prefetched to L2",
 }
 
 _LOCK = threading.Lock()
