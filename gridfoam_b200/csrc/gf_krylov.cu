@@ -3736,6 +3736,285 @@ __device__ void bicgstab_body(const gf_krylov_t& K, int vb, int vn) {
 }
 
 // ---------------------------------------------------------------------------
+// Split CG for systems of millions of cells (variant 19): two ordinary
+// kernels an iteration instead of one persistent cooperative launch, so each
+// pass runs at the occupancy of a plain stream kernel (a standalone SpMV of
+// this form reads HBM at ~94 % of the copy rate on a 4M-cell octree; the
+// persistent kernel's passes reach ~60 %).  Kernel A: p = z + beta p;
+// q = A p and the block partials of p.q.  Kernel B: x += alpha p;
+// r -= alpha q; z = M r and the partials of |r| and r.z.  There is no grid
+// barrier: each kernel starts by summing the previous kernel's block
+// partials in one fixed order (every block gets the same bits), and the
+// scalars (threshold, r.z, the done flag) pass between kernels in the
+// workspace's control block, written by block 0.  All 2 max_iter + 2
+// kernels are enqueued without a host synchronisation; once the stopping
+// test has passed the remaining ones return at once.
+constexpr int kSplitVariant = 19;
+constexpr int kSplitThreads = 256;
+
+struct SplitScalars {  // in the control block, after KCtl
+    double thresh, r0, fin, rz[2];
+    int done, its, converged, status;
+};
+
+__device__ __forceinline__ SplitScalars* split_scalars(const gf_krylov_t& K) {
+    return reinterpret_cast<SplitScalars*>(K.work + 2);
+}
+
+// Sum (or max, maxmask bit j) of the NV values of nblk block partials, in
+// one fixed order; every thread gets the result.
+template <int NV>
+__device__ void split_sum(const double* part, int nblk, unsigned maxmask, double (&out)[NV]) {
+    __shared__ double sh[NV][kSplitThreads / 32];
+    double acc[NV];
+#pragma unroll
+    for (int j = 0; j < NV; ++j) acc[j] = 0.0;
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x)
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
+            const double y = __ldcg(part + (int64_t)j * nblk + b);
+            acc[j] = ((maxmask >> j) & 1u) ? nmax(acc[j], y) : acc[j] + y;
+        }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        double x = acc[j];
+        for (int o = 16; o > 0; o >>= 1) {
+            const double y = __shfl_xor_sync(0xffffffffu, x, o);
+            x = ((maxmask >> j) & 1u) ? nmax(x, y) : x + y;
+        }
+        if (lane == 0) sh[j][warp] = x;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        double x = sh[j][0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) x = ((maxmask >> j) & 1u) ? nmax(x, sh[j][w]) : x + sh[j][w];
+        out[j] = x;
+    }
+    __syncthreads();
+}
+
+// Block partials of NV values: one fixed-order block reduction, written by
+// thread 0 to part[j * nblk + blockIdx.x].
+template <int NV>
+__device__ void split_partial(double (&v)[NV], unsigned maxmask, double* part) {
+    __shared__ double sh[NV][kSplitThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        double x = v[j];
+        for (int o = 16; o > 0; o >>= 1) {
+            const double y = __shfl_xor_sync(0xffffffffu, x, o);
+            x = ((maxmask >> j) & 1u) ? nmax(x, y) : x + y;
+        }
+        if (lane == 0) sh[j][warp] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
+            double x = sh[j][0];
+            for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+                x = ((maxmask >> j) & 1u) ? nmax(x, sh[j][w]) : x + sh[j][w];
+            __stcg(part + (int64_t)j * gridDim.x + blockIdx.x, x);
+        }
+}
+
+struct SplitVec {
+    double *r, *z, *pa, *pb, *q, *p1, *p2;
+};
+
+__device__ __forceinline__ SplitVec split_vec(const gf_krylov_t& K) {
+    double* partials = K.work + kCtlDoubles;
+    double* vec = partials + kPartials;
+    const int64_t n = K.n;
+    return {vec, vec + n, vec + 2 * n, vec + 3 * n, vec + 4 * n, partials, partials + kMaxBlocks};
+}
+
+template <class Rows, int MINB>
+__global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_init(gf_krylov_t K, Rows rows) {
+    const SplitVec v = split_vec(K);
+    const int n = (int)K.n;
+    const bool jac = K.jacobi != 0, linf = K.norm_inf != 0;
+    double loc[2] = {0.0, 0.0};
+    auto gx = [&](int i) { return __ldcg(K.x + i); };
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const double ax = rows.apply(c, __ldg(K.diag + c), gx);
+        const double rk = __ldg(K.rhs + c) - ax;
+        const double zk = inv_diag(K.diag, c, jac) * rk;
+        __stcg(v.r + c, rk);
+        __stcg(v.z + c, zk);
+        __stcg(v.pa + c, 0.0);
+        loc[0] = norm_acc(loc[0], rk, linf);
+        loc[1] += rk * zk;
+    }
+    split_partial<2>(loc, linf ? 1u : 0u, v.p2);
+}
+
+// Iteration it: the stopping test on the previous update's |r| (it > 1; the
+// initial residual at it = 1), then p = z + beta p, q = A p, partials of p.q.
+// it = max_iter + 1 only finishes the statistics.
+template <class Rows, int MINB>
+__global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_a(gf_krylov_t K, Rows rows, int it, int pa_old) {
+    SplitScalars* S = split_scalars(K);
+    if (*(volatile int*)&S->done) return;
+    const SplitVec v = split_vec(K);
+    const int n = (int)K.n;
+    const bool linf = K.norm_inf != 0;
+    __shared__ double s_beta;
+    __shared__ int s_stop;
+    double red[2];
+    split_sum<2>(v.p2, gridDim.x, linf ? 1u : 0u, red);
+    if (threadIdx.x == 0) {
+        const double fin = norm_fin(red[0], linf);
+        double thresh;
+        if (it == 1) {
+            thresh = fmax(K.atol, K.rtol * fin);
+            if (blockIdx.x == 0) {
+                S->r0 = fin;
+                S->thresh = thresh;
+            }
+        } else {
+            thresh = S->thresh;
+        }
+        int status = -1;
+        if (fin < thresh) status = GF_OK;
+        else if (!isfinite(fin)) status = GF_NONFINITE;
+        else if (it > K.max_iter) status = GF_MAX_ITER;
+        s_stop = status >= 0;
+        s_beta = it == 1 ? 0.0 : red[1] / S->rz[(it - 1) & 1];
+        if (blockIdx.x == 0) {
+            S->fin = fin;
+            if (status >= 0) {
+                const int its = status == GF_MAX_ITER ? K.max_iter : it - 1;
+                double* o = K.stats;
+                o[0] = it == 1 ? fin : S->r0;
+                o[1] = fin;
+                o[2] = its;
+                o[3] = status == GF_OK;
+                o[4] = status;
+                S->its = its;
+                S->status = status;
+                S->converged = status == GF_OK;
+                __threadfence();
+                S->done = 1;
+            } else {
+                S->rz[it & 1] = red[1];
+            }
+        }
+    }
+    __syncthreads();
+    if (s_stop) return;
+    const double beta = s_beta;
+    const double* p_old = pa_old ? v.pa : v.pb;
+    double* p_new = pa_old ? v.pb : v.pa;
+    double loc[1] = {0.0};
+    auto gp = [&](int i) { return v.z[i] + p_old[i] * beta; };
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const double pc = v.z[c] + p_old[c] * beta;
+        const double ap = rows.apply(c, __ldg(K.diag + c), gp);
+        __stcg(p_new + c, pc);
+        __stcg(v.q + c, ap);
+        loc[0] += pc * ap;
+    }
+    split_partial<1>(loc, 0u, v.p1);
+}
+
+// x += alpha p; r -= alpha q; z = M r; partials of |r| and r.z.
+template <int MINB>
+__global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_b(gf_krylov_t K, int it, int p_is_b) {
+    SplitScalars* S = split_scalars(K);
+    if (*(volatile int*)&S->done) return;
+    const SplitVec v = split_vec(K);
+    const int n = (int)K.n;
+    const bool jac = K.jacobi != 0, linf = K.norm_inf != 0;
+    double red[1];
+    split_sum<1>(v.p1, gridDim.x, 0u, red);
+    const double alpha = S->rz[it & 1] / red[0];
+    const double* p = p_is_b ? v.pb : v.pa;
+    double loc[2] = {0.0, 0.0};
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        __stcg(K.x + c, __ldcg(K.x + c) + alpha * __ldcg(p + c));
+        const double rk = __ldcg(v.r + c) - alpha * __ldcg(v.q + c);
+        const double zk = inv_diag(K.diag, c, jac) * rk;
+        __stcg(v.r + c, rk);
+        __stcg(v.z + c, zk);
+        loc[0] = norm_acc(loc[0], rk, linf);
+        loc[1] += rk * zk;
+    }
+    split_partial<2>(loc, linf ? 1u : 0u, v.p2);
+}
+
+template <class Rows, int MINB>
+static int launch_split_rows(const gf_krylov_t* k, const Rows& rows, cudaStream_t st) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cgs_a<Rows, MINB>, kSplitThreads, 0);
+    if (e != cudaSuccess || per_sm < 1) {
+        set_error("gf_pcg_solve: split CG set-up failed: %s", cudaGetErrorString(e));
+        return GF_ERR_CUDA;
+    }
+    int64_t grid = (int64_t)per_sm * sms;
+    const int64_t want = (k->n + kSplitThreads - 1) / kSplitThreads;
+    if (grid > want) grid = want;
+    if (grid > kMaxBlocks) grid = kMaxBlocks;
+    if (k->block_cap > 0 && grid > k->block_cap) grid = k->block_cap;
+    if (grid < 1) grid = 1;
+    e = cudaMemsetAsync(k->work, 0, sizeof(double) * kCtlDoubles, st);
+    if (e != cudaSuccess) {
+        set_error("gf_pcg_solve: %s", cudaGetErrorString(e));
+        return GF_ERR_CUDA;
+    }
+    const gf_krylov_t K = *k;
+    const unsigned g = (unsigned)grid;
+    k_cgs_init<Rows, MINB><<<g, kSplitThreads, 0, st>>>(K, rows);
+    for (int it = 1; it <= k->max_iter; ++it) {
+        // p_old is pa at odd iterations (p_new then goes to pb), pb at even.
+        k_cgs_a<Rows, MINB><<<g, kSplitThreads, 0, st>>>(K, rows, it, it & 1);
+        k_cgs_b<MINB><<<g, kSplitThreads, 0, st>>>(K, it, it & 1);
+    }
+    k_cgs_a<Rows, MINB><<<g, kSplitThreads, 0, st>>>(K, rows, k->max_iter + 1, (k->max_iter + 1) & 1);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error("gf_pcg_solve: split CG launch failed: %s", cudaGetErrorString(e));
+        return GF_ERR_CUDA;
+    }
+    return GF_OK;
+}
+
+template <int MINB>
+static int launch_split_m(const gf_krylov_t* k, void* stream) {
+    const int64_t row_span = (int64_t)(k->stride_y > 0 ? 6 : (k->width > 6 ? k->width : 6)) * k->n;
+    if (row_span >= ((int64_t)1 << 31)) {
+        set_error("gf_pcg_solve: system not eligible for the split CG");
+        return GF_ERR_INVALID;
+    }
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (k->stride_y > 0) {
+        if (k->symmetric)
+            return launch_split_rows<BoxRows<double, true, false, int>, MINB>(
+                k, BoxRows<double, true, false, int>{k->val, (int)k->n, (int)k->stride_y, (int)k->stride_z}, st);
+        return launch_split_rows<BoxRows<double, false, false, int>, MINB>(
+            k, BoxRows<double, false, false, int>{k->val, (int)k->n, (int)k->stride_y, (int)k->stride_z}, st);
+    }
+    // One slot at a time (the loop of a plain SpMV): the occupancy, not the
+    // loads of one thread, keeps the memory system busy.
+    if (k->width == 6)
+        return launch_split_rows<EllRows<double, 6, int, 1>, MINB>(
+            k, EllRows<double, 6, int, 1>{k->val, k->nbr, (int)k->n, k->width, k->row_len}, st);
+    return launch_split_rows<EllRows<double, 0, int, 1>, MINB>(
+        k, EllRows<double, 0, int, 1>{k->val, k->nbr, (int)k->n, k->width, k->row_len}, st);
+}
+
+// Variant 19: 8 blocks of 256 threads an SM; 20: 6 (more registers).
+static int launch_split(const gf_krylov_t* k, void* stream, int which) {
+    return which == 1 ? launch_split_m<6>(k, stream) : launch_split_m<8>(k, stream);
+}
+
+// ---------------------------------------------------------------------------
 // Batched solves: the systems of several independent cases (the solve
 // server's same-phase solves) in ONE cooperative launch.  System i owns the
 // blocks [blk0[i], blk0[i+1]) and runs the single-system kernel's body on
@@ -4231,6 +4510,10 @@ int gf_pcg_solve(const gf_krylov_t* k, void* stream) {
             }
             if (k->variant >= kStreamVariant && k->variant < kStreamVariant + kStreamVariants) {
                 const int st = launch_stream(k, stream, k->variant - kStreamVariant);
+                if (st != GF_ERR_INVALID) return st;
+            }
+            if (k->variant == kSplitVariant || k->variant == kSplitVariant + 1) {
+                const int st = launch_split(k, stream, k->variant - kSplitVariant);
                 if (st != GF_ERR_INVALID) return st;
             }
             if (box && k->variant == kStagedVariant) {

@@ -30,7 +30,7 @@ from gridfoam_b200.meta.config import PrecisionType, PreconditionerType, SolverC
 # Variants 0-7 differ only in launch shape and memory placement (their
 # iterates differ by the order of the dot-product partial sums); 8 and 9
 # form q = A p by recurrence.
-N_VARIANTS = 19
+N_VARIANTS = 21
 VARIANTS = {
     0: "256 threads x 1 cell/pass",
     1: "256 threads x 2 cells/pass",
@@ -51,6 +51,8 @@ VARIANTS = {
     16: "ELL rows (box: as 2), lean 32-bit form: 256 threads x 5 a SM, groups of 8",
     17: "ELL rows (box: as 2), lean 32-bit form: 256 threads x 6 a SM, groups of 4",
     18: "ELL rows (box: as 2), lean 32-bit form: 256 threads x 6 a SM, groups of 4, next cell prefetched to L2",
+    19: "split: two plain kernels an iteration (no grid barrier), 256 threads x 8 a SM (FP64, large systems)",
+    20: "split: two plain kernels an iteration (no grid barrier), 256 threads x 6 a SM (FP64, large systems)",
 }
 
 _LOCK = threading.Lock()

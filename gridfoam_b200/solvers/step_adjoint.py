@@ -172,6 +172,11 @@ class DifferentiablePisoStep:
 
 @dataclass
 class StepGradient:
+    """Result of ``piso_gradient``: the objective, its derivative with
+    respect to nu, and the checkpoint accounting (states held at most:
+    ``peak_states`` states of ``3 C + F + Nb + C`` doubles each, plus one
+    step's autograd graph)."""
+
     objective: float
     grad_nu: float
     steps: int
@@ -235,4 +240,4 @@ def piso_gradient(algo, n_steps: int, objective, *, checkpoint_every: int | None
             grads = torch.autograd.grad(outs, (U_in, phi_in, p_in, nu_t), grad_outputs=adj, allow_unused=True)
             adj = tuple(torch.zeros_like(x) if g_ is None else g_ for g_, x in zip(grads[:3], (U_in, phi_in, p_in)))
             nu_bar += 0.0 if grads[3] is None else float(grads[3])
-    return StepGradient(float(J), nu_bar, n_steps, len(checkpoints), recomputed, peak)
+    return StepGradient(float(J.detach()), nu_bar, n_steps, len(checkpoints), recomputed, peak)

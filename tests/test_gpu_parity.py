@@ -379,7 +379,7 @@ def test_single_reduction_cg_matches_pcg(layout):
     assert r < 1e-9 * s1.initial_residual
 
 
-@pytest.mark.parametrize("variant", [5, 6, 7, 8, 9, 10, 11, 12, 13, 14])
+@pytest.mark.parametrize("variant", [5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 19, 20])
 @pytest.mark.parametrize("shape", [(24, 20, 28), (64, 64, 40), (7, 5, 6), (130, 3, 4)])
 def test_staged_box_cg_matches_register_kernel(shape, variant):
     """The shared-memory variants against the register kernel (variant 0):
@@ -445,7 +445,7 @@ def test_smem_resident_cg_fixed_iterations_match_register_kernel(variant, box):
     assert rel(xs[1], xs[0]) < 1e-11
 
 
-@pytest.mark.parametrize("variant", [6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18])
+@pytest.mark.parametrize("variant", [6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18, 19, 20])
 def test_smem_resident_cg_on_ell_layout(variant):
     """The shared-memory-resident CG through the general ELL rows (the
     octree path), against the register ELL kernel."""
@@ -606,7 +606,7 @@ def test_staged_assembly_matches_generic_kernel(name):
             assert torch.equal(x, y), field.name
 
 
-@pytest.mark.parametrize("variant", [8, 9, 10, 11, 12, 13])
+@pytest.mark.parametrize("variant", [8, 9, 10, 11, 12, 13, 19])
 @pytest.mark.parametrize("box", [True, False])
 def test_qrec_cg_true_residual(variant, box):
     """The q-recurrence CG updates r from q = A z + beta q rather than from
@@ -649,7 +649,7 @@ def test_stream_cg_fixed_iterations_match_qrec(variant, box):
     assert rel(xs[1], xs[0]) < 1e-11
 
 
-@pytest.mark.parametrize("variant", [2, 12, 13, 15, 17])
+@pytest.mark.parametrize("variant", [2, 12, 13, 15, 17, 19])
 def test_row_lengths_skip_only_empty_slots(variant):
     """On an octree grid (couplings first in every row) the CG with the
     row-length early exit gives the same iterations and solution as the
@@ -705,7 +705,7 @@ def test_grad_linear_steps_and_operator_match_reference(name):
     _check(fvc.grad(algo.U).data, golden["op_grad_U"], "grad_U", 1e-10)
 
 
-@pytest.mark.parametrize("variant", [15, 16, 17, 18])
+@pytest.mark.parametrize("variant", [15, 16, 17, 18, 19, 20])
 def test_lean_ell_cg_fixed_iterations_match_register_kernel(variant):
     """The lean ELL CG (32-bit indices, x update moved into the next gather
     pass) against the register kernel: exactly 60 iterations agree up to the
@@ -722,3 +722,30 @@ def test_lean_ell_cg_fixed_iterations_match_register_kernel(variant):
         assert st[0].iterations == 60 and st[0].status == "max_iter"
         xs.append(to_np(x))
     assert rel(xs[1], xs[0]) < 1e-11
+
+
+def test_split_cg_limits_and_statuses():
+    """The split CG (variant 19) reports iteration 0 on a zero right-hand
+    side, max_iter and non-finite input like the persistent kernels."""
+    from gridfoam_b200.fv import fvm
+    from gridfoam_b200.meta.config import SolverConfig
+    from gridfoam_b200.solvers.krylov import CGSolver
+
+    _, _, grid, algo = device_case("cavity8")
+    A = -fvm.laplacian(1.0, algo.p)
+    A.diag = A.diag + grid.cell_volumes
+    n = grid.num_cells
+    zero = torch.zeros((1, n), dtype=torch.float64, device="cuda")
+    s = CGSolver(SolverConfig(method="cg", preconditioner="jacobi", tolerance=1e-12, rel_tolerance=0.0))
+    s.variant = 19
+    st = s.solve_arrays(grid, A.diag_store, A.val, zero, torch.zeros_like(zero))
+    assert st[0].iterations == 0 and st[0].converged
+    s2 = CGSolver(SolverConfig(method="cg", preconditioner="jacobi", tolerance=1e-30, rel_tolerance=0.0, max_iter=3))
+    s2.variant = 19
+    rhs = torch.ones((1, n), dtype=torch.float64, device="cuda")
+    st = s2.solve_arrays(grid, A.diag_store, A.val, rhs, torch.zeros_like(zero))
+    assert st[0].iterations == 3 and not st[0].converged and st[0].status == "max_iter"
+    bad = rhs.clone()
+    bad[0, 5] = float("nan")
+    st = s2.solve_arrays(grid, A.diag_store, A.val, bad, torch.zeros_like(zero))
+    assert not st[0].converged and st[0].status == "nonfinite"
