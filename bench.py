@@ -640,7 +640,10 @@ def run_gpu(args) -> None:
             "algorithmic_GBps_per_step_pcg": step_bytes / (ms / args.steps * 1e-3) / 1e9,
         },
         "roofline": {
-            "kernel": f"pressure CG, variant {variant} (persistent Jacobi-PCG on the octree ELL rows, fp64)",
+            "kernel": (f"pressure CG, variant {variant}: " + (
+                "split Jacobi-PCG (k_cgs_a: p update + SpMV + p.q partials; k_cgs_b: x/r/z update + partials), "
+                "octree ELL rows, fp64" if variant in (19, 20) else
+                "persistent Jacobi-PCG on the octree ELL rows, fp64")),
             "bound": "hbm",
             "achieved": achieved,
             "peak": peak,

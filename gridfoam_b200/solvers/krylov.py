@@ -14,7 +14,7 @@ import ctypes
 
 import torch
 
-from gridfoam_b200._lib import GfKrylov, call, load, ptr, stream_ptr
+from gridfoam_b200._lib import LAUNCHES, GfKrylov, call, load, ptr, stream_ptr
 from gridfoam_b200.meta.config import NormType, PrecisionType, PreconditionerType, SolverConfig
 from gridfoam_b200.solvers.adjoint import attach_implicit_adjoint
 from gridfoam_b200.solvers.base import LinearSolver, SolveResult, SolveStats, _StatsBuffer
@@ -44,8 +44,8 @@ def default_variant(n: int, mixed: bool, symmetric: bool, box: bool = True) -> i
     for 256-thread register blocks at 48^3, 8.0 against 8.2 for the
     q-recurrence form at 64^3); then, up to ~1.3M cells, the q-recurrence
     form (q = A z + beta q, z alone gathered; 14.7 us at 1M cells); above
-    that the shared-memory tiled kernel for symmetric boxes, else
-    512-thread blocks.  FP32-inner (mixed) solves: 256-thread register
+    that the shared-memory tiled kernel for symmetric boxes, else the split
+    CG (two plain kernels an iteration).  FP32-inner (mixed) solves: 256-thread register
     blocks below ~32K cells (6.5 us an inner iteration at 24^3, as for the
     shared-memory forms); then, up to ~1.3M cells, the single-reduction
     form with the halo sync (6.7 against 7.0 us for the q-recurrence form
@@ -60,7 +60,11 @@ def default_variant(n: int, mixed: bool, symmetric: bool, box: bool = True) -> i
         return 10
     if n <= 1300000:
         return 8
-    return 5 if symmetric and box else 2
+    # Above ~1.3M cells (beyond L2): the staged tiles on symmetric boxes;
+    # on other rows the split CG, two plain kernels an iteration (160.7
+    # against 170.4 us for the 256-thread register kernel on the 4.08M-cell
+    # cylinder-wake octree).
+    return 5 if symmetric and box else 19
 
 
 class DeviceKrylov(LinearSolver):
@@ -113,6 +117,10 @@ class DeviceKrylov(LinearSolver):
             ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
             ev[0].record()
         call("gf_bicgstab_solve" if self.bicgstab else "gf_pcg_solve", ctypes.byref(k), stream_ptr())
+        if k.variant in (19, 20) and not self.bicgstab and not k.mixed and nc == 1 and not k.single_reduction:
+            # the split CG enqueues an initial kernel, two a permitted
+            # iteration and a final one (those after convergence return at once)
+            LAUNCHES["gf_pcg_solve"] += 2 * k.max_iter + 1
         if ev is not None:
             ev[1].record()
         if not self.host_stats:
