@@ -271,6 +271,21 @@ class GfError(RuntimeError):
 _LAUNCHES_PER_CALL = {"gf_fixed_values": 3, "gf_close_fixed_flux": 2, "gf_field_residual": 2, "gf_continuity_sums": 2,
                       "gf_pcg_solve_batched": 2, "gf_bicgstab_solve_batched": 2}
 LAUNCHES: collections.Counter = collections.Counter()
+# Launches known only after the device ran (the split CG's graph loop runs
+# two kernels an iteration): callables giving their counts, kept while
+# TRACK_DEFERRED is set (see ``launch_total``).
+TRACK_DEFERRED = False
+DEFERRED_LAUNCHES: list = []
+
+
+def clear_launches() -> None:
+    LAUNCHES.clear()
+    DEFERRED_LAUNCHES.clear()
+
+
+def launch_total() -> int:
+    """Kernels launched since ``clear_launches`` (read after a synchronize)."""
+    return sum(LAUNCHES.values()) + sum(int(f()) for f in DEFERRED_LAUNCHES)
 
 
 def call(name: str, *args) -> int:

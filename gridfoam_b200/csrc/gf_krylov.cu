@@ -11,6 +11,8 @@
 // co-resident and the barrier is always reachable.
 #include "gf_common.cuh"
 
+#include <cstdlib>
+#include <cstring>
 #include <mutex>
 
 namespace gf {
@@ -3755,6 +3757,10 @@ constexpr int kSplitThreads = 256;
 struct SplitScalars {  // in the control block, after KCtl
     double thresh, r0, fin, rz[2];
     int done, its, converged, status;
+    // Iteration numbers of the graph loop: it_a is read by k_cgs_a and
+    // written by k_cgs_b, it_b the other way round, so no kernel reads a
+    // counter that one of its own blocks writes.
+    int it_a, it_b;
 };
 
 __device__ __forceinline__ SplitScalars* split_scalars(const gf_krylov_t& K) {
@@ -3849,16 +3855,27 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_init(gf_krylov_t K,
         loc[0] = norm_acc(loc[0], rk, linf);
         loc[1] += rk * zk;
     }
+    if (blockIdx.x == 0 && threadIdx.x == 0) split_scalars(K)->it_a = 1;
     split_partial<2>(loc, linf ? 1u : 0u, v.p2);
 }
 
 // Iteration it: the stopping test on the previous update's |r| (it > 1; the
 // initial residual at it = 1), then p = z + beta p, q = A p, partials of p.q.
-// it = max_iter + 1 only finishes the statistics.
-template <class Rows, int MINB>
-__global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_a(gf_krylov_t K, Rows rows, int it, int pa_old) {
+// it = max_iter + 1 only finishes the statistics.  LOOP: the body of a
+// CUDA graph while-loop; it comes from the control block and the kernel that
+// ends the solve sets the loop's condition to 0.
+template <class Rows, int MINB, bool LOOP>
+__global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_a(gf_krylov_t K, Rows rows, int it, int pa_old,
+                                                              cudaGraphConditionalHandle loop) {
     SplitScalars* S = split_scalars(K);
-    if (*(volatile int*)&S->done) return;
+    if (*(volatile int*)&S->done) {
+        if (LOOP && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(loop, 0);
+        return;
+    }
+    if (LOOP) {
+        it = *(volatile int*)&S->it_a;
+        pa_old = it & 1;
+    }
     const SplitVec v = split_vec(K);
     const int n = (int)K.n;
     const bool linf = K.norm_inf != 0;
@@ -3881,7 +3898,7 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_a(gf_krylov_t K, Ro
         int status = -1;
         if (fin < thresh) status = GF_OK;
         else if (!isfinite(fin)) status = GF_NONFINITE;
-        else if (it > K.max_iter) status = GF_MAX_ITER;
+        else if (it > K.max_iter || it < 1) status = GF_MAX_ITER;
         s_stop = status >= 0;
         s_beta = it == 1 ? 0.0 : red[1] / S->rz[(it - 1) & 1];
         if (blockIdx.x == 0) {
@@ -3899,8 +3916,10 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_a(gf_krylov_t K, Ro
                 S->converged = status == GF_OK;
                 __threadfence();
                 S->done = 1;
+                if (LOOP) cudaGraphSetConditional(loop, 0);
             } else {
                 S->rz[it & 1] = red[1];
+                if (LOOP) S->it_b = it;
             }
         }
     }
@@ -3922,10 +3941,15 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_a(gf_krylov_t K, Ro
 }
 
 // x += alpha p; r -= alpha q; z = M r; partials of |r| and r.z.
-template <int MINB>
+template <int MINB, bool LOOP>
 __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_b(gf_krylov_t K, int it, int p_is_b) {
     SplitScalars* S = split_scalars(K);
     if (*(volatile int*)&S->done) return;
+    if (LOOP) {
+        it = *(volatile int*)&S->it_b;
+        p_is_b = it & 1;
+        if (blockIdx.x == 0 && threadIdx.x == 0) S->it_a = it + 1;
+    }
     const SplitVec v = split_vec(K);
     const int n = (int)K.n;
     const bool jac = K.jacobi != 0, linf = K.norm_inf != 0;
@@ -3946,13 +3970,129 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_b(gf_krylov_t K, in
     split_partial<2>(loc, linf ? 1u : 0u, v.p2);
 }
 
+// Graph while-loops of the split CG, cached by everything their kernel
+// nodes hold (the descriptor, the row operator, the grid size and the
+// device), so the repeated solves of an algorithm reuse one instantiated
+// graph; the least recently used of kSplitLoops entries is replaced.
+constexpr int kSplitLoops = 64;
+
+struct SplitLoop {
+    int dev = -1;
+    const void* fa = nullptr;
+    const void* fb = nullptr;
+    unsigned grid = 0;
+    unsigned char kbytes[sizeof(gf_krylov_t)] = {};
+    unsigned char rbytes[64] = {};
+    size_t rlen = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t used = 0;
+};
+
+static std::mutex g_split_mu;
+static SplitLoop g_split_loops[kSplitLoops];
+static uint64_t g_split_clock = 0;
+
+static bool split_graph_enabled() {
+    static const bool on = [] {
+        const char* v = getenv("GF_SPLIT_GRAPH");
+        return v == nullptr || v[0] != '0';
+    }();
+    return on;
+}
+
+static int split_loop_exec(const void* fa, const void* fb, const gf_krylov_t& K, const void* rows, size_t rlen,
+                           unsigned grid, cudaGraphExec_t* out) {
+    if (rlen > sizeof(SplitLoop::rbytes)) {
+        set_error("gf_pcg_solve: split CG row operator too large for the graph cache");
+        return GF_ERR_INVALID;
+    }
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        set_error("gf_pcg_solve: %s", cudaGetErrorString(e));
+        return GF_ERR_CUDA;
+    }
+    std::lock_guard<std::mutex> lock(g_split_mu);
+    SplitLoop* victim = &g_split_loops[0];
+    for (SplitLoop& L : g_split_loops) {
+        if (L.exec != nullptr && L.dev == dev && L.fa == fa && L.fb == fb && L.grid == grid && L.rlen == rlen &&
+            memcmp(L.kbytes, &K, sizeof(gf_krylov_t)) == 0 && memcmp(L.rbytes, rows, rlen) == 0) {
+            L.used = ++g_split_clock;
+            *out = L.exec;
+            return GF_OK;
+        }
+        if (L.used < victim->used) victim = &L;
+    }
+    // Build: graph { while (cond) { k_cgs_a -> k_cgs_b } }, cond = 1 at launch.
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaGraphConditionalHandle handle = 0;
+    e = cudaGraphCreate(&graph, 0);
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault);
+    cudaGraphNodeParams cp = {};
+    cudaGraphNode_t cond = nullptr, na = nullptr, nb = nullptr;
+    if (e == cudaSuccess) {
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = handle;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        e = cudaGraphAddNode(&cond, graph, nullptr, 0, &cp);
+    }
+    gf_krylov_t kcopy = K;
+    alignas(16) unsigned char rcopy[sizeof(SplitLoop::rbytes)];
+    memcpy(rcopy, rows, rlen);
+    int it0 = 0, par0 = 0;
+    if (e == cudaSuccess) {
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        void* a_args[] = {&kcopy, rcopy, &it0, &par0, &handle};
+        cudaKernelNodeParams ka = {};
+        ka.func = const_cast<void*>(fa);
+        ka.gridDim = dim3(grid);
+        ka.blockDim = dim3(kSplitThreads);
+        ka.kernelParams = a_args;
+        e = cudaGraphAddKernelNode(&na, body, nullptr, 0, &ka);
+        if (e == cudaSuccess) {
+            void* b_args[] = {&kcopy, &it0, &par0};
+            cudaKernelNodeParams kb = {};
+            kb.func = const_cast<void*>(fb);
+            kb.gridDim = dim3(grid);
+            kb.blockDim = dim3(kSplitThreads);
+            kb.kernelParams = b_args;
+            e = cudaGraphAddKernelNode(&nb, body, &na, 1, &kb);
+        }
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e != cudaSuccess) {
+        if (graph != nullptr) cudaGraphDestroy(graph);
+        set_error("gf_pcg_solve: split CG graph set-up failed: %s", cudaGetErrorString(e));
+        return GF_ERR_CUDA;
+    }
+    // An in-flight executable graph is released when its launch completes.
+    if (victim->exec != nullptr) cudaGraphExecDestroy(victim->exec);
+    if (victim->graph != nullptr) cudaGraphDestroy(victim->graph);
+    victim->dev = dev;
+    victim->fa = fa;
+    victim->fb = fb;
+    victim->grid = grid;
+    memcpy(victim->kbytes, &K, sizeof(gf_krylov_t));
+    memset(victim->rbytes, 0, sizeof(victim->rbytes));
+    memcpy(victim->rbytes, rows, rlen);
+    victim->rlen = rlen;
+    victim->graph = graph;
+    victim->exec = exec;
+    victim->used = ++g_split_clock;
+    *out = exec;
+    return GF_OK;
+}
+
 template <class Rows, int MINB>
 static int launch_split_rows(const gf_krylov_t* k, const Rows& rows, cudaStream_t st) {
     int dev = 0, sms = 0, per_sm = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cgs_a<Rows, MINB>, kSplitThreads, 0);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cgs_a<Rows, MINB, false>, kSplitThreads, 0);
     if (e != cudaSuccess || per_sm < 1) {
         set_error("gf_pcg_solve: split CG set-up failed: %s", cudaGetErrorString(e));
         return GF_ERR_CUDA;
@@ -3971,12 +4111,35 @@ static int launch_split_rows(const gf_krylov_t* k, const Rows& rows, cudaStream_
     const gf_krylov_t K = *k;
     const unsigned g = (unsigned)grid;
     k_cgs_init<Rows, MINB><<<g, kSplitThreads, 0, st>>>(K, rows);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error("gf_pcg_solve: split CG launch failed: %s", cudaGetErrorString(e));
+        return GF_ERR_CUDA;
+    }
+    // Outside stream capture the iterations run as a CUDA graph while-loop
+    // (one graph launch, the loop ends on the device when the solve stops);
+    // inside a capture every permitted iteration is enqueued and those
+    // after the stop return at once.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (split_graph_enabled() && cudaStreamIsCapturing(st, &cap) == cudaSuccess &&
+        cap == cudaStreamCaptureStatusNone) {
+        cudaGraphExec_t exec = nullptr;
+        const int rc = split_loop_exec((const void*)k_cgs_a<Rows, MINB, true>, (const void*)k_cgs_b<MINB, true>, K,
+                                       &rows, sizeof(Rows), g, &exec);
+        if (rc != GF_OK) return rc;
+        e = cudaGraphLaunch(exec, st);
+        if (e != cudaSuccess) {
+            set_error("gf_pcg_solve: split CG graph launch failed: %s", cudaGetErrorString(e));
+            return GF_ERR_CUDA;
+        }
+        return GF_OK;
+    }
     for (int it = 1; it <= k->max_iter; ++it) {
         // p_old is pa at odd iterations (p_new then goes to pb), pb at even.
-        k_cgs_a<Rows, MINB><<<g, kSplitThreads, 0, st>>>(K, rows, it, it & 1);
-        k_cgs_b<MINB><<<g, kSplitThreads, 0, st>>>(K, it, it & 1);
+        k_cgs_a<Rows, MINB, false><<<g, kSplitThreads, 0, st>>>(K, rows, it, it & 1, 0);
+        k_cgs_b<MINB, false><<<g, kSplitThreads, 0, st>>>(K, it, it & 1);
     }
-    k_cgs_a<Rows, MINB><<<g, kSplitThreads, 0, st>>>(K, rows, k->max_iter + 1, (k->max_iter + 1) & 1);
+    k_cgs_a<Rows, MINB, false><<<g, kSplitThreads, 0, st>>>(K, rows, k->max_iter + 1, (k->max_iter + 1) & 1, 0);
     e = cudaGetLastError();
     if (e != cudaSuccess) {
         set_error("gf_pcg_solve: split CG launch failed: %s", cudaGetErrorString(e));

@@ -11,9 +11,11 @@ restarts follow ``solvers/bicgstab.py:123-272``.
 from __future__ import annotations
 
 import ctypes
+import os
 
 import torch
 
+from gridfoam_b200 import _lib
 from gridfoam_b200._lib import LAUNCHES, GfKrylov, call, load, ptr, stream_ptr
 from gridfoam_b200.meta.config import NormType, PrecisionType, PreconditionerType, SolverConfig
 from gridfoam_b200.solvers.adjoint import attach_implicit_adjoint
@@ -34,6 +36,12 @@ def workspace(cache: dict, device: torch.device, n: int, ncomp: int, kind: int) 
         ws = torch.empty(size, dtype=torch.float64, device=device)
         cache[key] = ws
     return ws
+
+
+def _split_graph_loop() -> bool:
+    """Whether the library runs the split CG's iterations as a CUDA graph
+    while-loop (outside stream capture, unless GF_SPLIT_GRAPH=0)."""
+    return os.environ.get("GF_SPLIT_GRAPH", "1")[:1] != "0" and not torch.cuda.is_current_stream_capturing()
 
 
 def default_variant(n: int, mixed: bool, symmetric: bool, box: bool = True) -> int:
@@ -117,9 +125,12 @@ class DeviceKrylov(LinearSolver):
             ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
             ev[0].record()
         call("gf_bicgstab_solve" if self.bicgstab else "gf_pcg_solve", ctypes.byref(k), stream_ptr())
-        if k.variant in (19, 20) and not self.bicgstab and not k.mixed and nc == 1 and not k.single_reduction:
-            # the split CG enqueues an initial kernel, two a permitted
-            # iteration and a final one (those after convergence return at once)
+        split = k.variant in (19, 20) and not self.bicgstab and not k.mixed and nc == 1 and not k.single_reduction
+        graph_loop = split and _split_graph_loop()
+        if split and not graph_loop:
+            # inside a stream capture the split CG enqueues an initial
+            # kernel, two a permitted iteration and a final one (those after
+            # the stop return at once)
             LAUNCHES["gf_pcg_solve"] += 2 * k.max_iter + 1
         if ev is not None:
             ev[1].record()
@@ -127,6 +138,9 @@ class DeviceKrylov(LinearSolver):
             return ()
         buf = _StatsBuffer(stats)
         out = tuple(SolveStats(self.solver_name, buf, i) for i in range(nc))
+        if graph_loop and _lib.TRACK_DEFERRED:
+            # the graph loop runs its two kernels iterations + 1 times
+            _lib.DEFERRED_LAUNCHES.append(lambda st=out[0]: 2 * (st.iterations + 1))
         if ev is not None:
             self.profile_events.append((ev[0], ev[1], out))
         return out

@@ -12,6 +12,7 @@ import copy
 from gridfoam_b200.cases import (  # noqa: F401
     TRANSIENT,
     WALL0,
+    bluff_body_case,
     build_mesh,
     cavity_case,
     cavity_oct_case,

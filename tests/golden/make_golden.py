@@ -8,6 +8,8 @@ naming its ``src`` directory (required; there is no default)::
     GRIDFOAM_REF=<reference>/src python tests/golden/make_golden.py --forces
     GRIDFOAM_REF=<reference>/src python tests/golden/make_golden.py --potential
     GRIDFOAM_REF=<reference>/src python tests/golden/make_golden.py --diagnostics
+    GRIDFOAM_REF=<reference>/src python tests/golden/make_golden.py --fullsize
+    GRIDFOAM_REF=<reference>/src python tests/golden/make_golden.py --downscaled
 
 It imports the unmodified reference package (with the import stubs in
 ``tests/golden/refshim`` for its absent optional dependencies), builds each
@@ -57,6 +59,7 @@ from tests.golden.cases import (  # noqa: E402
     ALL_CASES,
     DIV_SCHEMES,
     STEPS,
+    bluff_body_case,
     build_mesh,
     cavity_case,
     cylinder_wake_case,
@@ -150,12 +153,18 @@ FULLSIZE = {
     "wake256x160x32_10": (lambda: cylinder_wake_case((256, 160, 32)), 10, False),
 }
 
+# Downscaled runs of benchmark configs whose full size the reference's CPU
+# run cannot reach in reasonable time (same layout as FULLSIZE).
+DOWNSCALED = {
+    "bluff64x16x12_20": (lambda: bluff_body_case((64, 16, 12)), 20, False),
+}
+
 
 def fullsize_run(key: str) -> dict:
     """Per-step solver iterations, field norms and a fixed sample of cells of
     the reference's own run at a benchmark config's full size; the final
     fields in full where they are small."""
-    build, n_steps, keep_full = FULLSIZE[key]
+    build, n_steps, keep_full = FULLSIZE[key] if key in FULLSIZE else DOWNSCALED[key]
     case = build()
     grid, mesh, algo, captured = reference_algorithm(case)
     n = int(mesh.n_cells)
@@ -599,6 +608,13 @@ def main() -> None:
             path = HERE / f"fullsize_{key}.npz"
             np.savez_compressed(path, **data)
             print(f"fullsize {key}: {len(data)} arrays -> {path} ({path.stat().st_size} B)")
+        return
+    if args and args[0] == "--downscaled":
+        for key in args[1:] or list(DOWNSCALED):
+            data = fullsize_run(key)
+            path = HERE / f"downscaled_{key}.npz"
+            np.savez_compressed(path, **data)
+            print(f"downscaled {key}: {len(data)} arrays -> {path} ({path.stat().st_size} B)")
         return
     if args and args[0] == "--gradlinear":
         # The Green-Gauss ('linear') gradient scheme: whole steps and the

@@ -5,7 +5,10 @@ CPU run of the same mesh and case (``make_golden.py --fullsize``).
 * cavity 32^3, 300 SIMPLE iterations (the CPU-runnable config in full);
 * immersed pipe 64x64x256, the first 20 PISO steps;
 * cylinder wake on the 3-level octree (base 256x160x32, 4.08M cells), the
-  first 10 PISO steps.
+  first 10 PISO steps;
+* the slanted bluff body on its 4-level octree, downscaled to base
+  64x16x12 (96,344 cells, hanging and immersed faces), the first 20 steady
+  SIMPLE(C) iterations (``make_golden.py --downscaled``).
 
 The fixtures hold per-step Krylov iteration counts and field norms, a fixed
 sample of cells at some steps and (cavity) the final fields in full.  The
@@ -40,8 +43,8 @@ def rel(a, b) -> float:
     return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(np.asarray(b)), 1e-300))
 
 
-def _fixture(key: str) -> dict:
-    path = GOLDEN / f"fullsize_{key}.npz"
+def _fixture(key: str, prefix: str = "fullsize") -> dict:
+    path = GOLDEN / f"{prefix}_{key}.npz"
     if not path.exists():
         pytest.skip(f"fixture {path.name} not generated")
     with np.load(path) as d:
@@ -105,3 +108,10 @@ def test_cylinder_wake_full_first_10_steps_match_reference():
 
     ref = _fixture("wake256x160x32_10")
     _run(cylinder_wake_case((256, 160, 32)), ref, 10, field_tol=1e-4, its_slack=12)
+
+
+def test_bluff_body_downscaled_first_20_iterations_match_reference():
+    from gridfoam_b200.cases import bluff_body_case
+
+    ref = _fixture("bluff64x16x12_20", prefix="downscaled")
+    _run(bluff_body_case((64, 16, 12)), ref, 20, field_tol=1e-4, its_slack=12)

@@ -749,3 +749,48 @@ def test_split_cg_limits_and_statuses():
     bad[0, 5] = float("nan")
     st = s2.solve_arrays(grid, A.diag_store, A.val, bad, torch.zeros_like(zero))
     assert not st[0].converged and st[0].status == "nonfinite"
+
+
+def test_split_cg_graph_loop_matches_captured_form():
+    """Outside stream capture the split CG runs its iterations as a CUDA
+    graph while-loop that ends on the device; inside a capture it enqueues
+    every permitted iteration.  Both run the same kernels in the same order:
+    the same iterations and the same bits, solve after solve."""
+    from gridfoam_b200.fv import fvm
+    from gridfoam_b200.meta.config import SolverConfig
+    from gridfoam_b200.solvers.krylov import CGSolver
+
+    _, _, grid, algo = device_case("ibcyl_oct")
+    A = -fvm.laplacian(1.0, algo.p)
+    A.diag = A.diag + 1e-2 * grid.cell_volumes
+    rhs = torch.linspace(-1.0, 1.0, grid.num_cells, dtype=torch.float64, device="cuda").reshape(1, -1)
+    cfg = SolverConfig(method="cg", preconditioner="jacobi", tolerance=0.0, rel_tolerance=1e-8, max_iter=500)
+    s = CGSolver(cfg)
+    s.variant = 19
+    x_loop = torch.zeros_like(rhs)
+    loops = []
+    for _ in range(3):
+        x_loop.zero_()
+        loops.append(s.solve_arrays(grid, A.diag_store, A.val, rhs, x_loop, symmetric=True)[0].iterations)
+    s_cap = CGSolver(cfg)
+    s_cap.variant = 19
+    s_cap.host_stats = False
+    x_cap = torch.zeros_like(rhs)
+    stream = torch.cuda.Stream()
+    stream.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(stream):
+        s_cap.solve_arrays(grid, A.diag_store, A.val, rhs, x_cap, symmetric=True)  # workspace allocation
+    torch.cuda.synchronize()
+    x_cap.zero_()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=stream):
+        s_cap.solve_arrays(grid, A.diag_store, A.val, rhs, x_cap, symmetric=True)
+    for _ in range(3):
+        x_cap.zero_()
+        torch.cuda.synchronize()
+        g.replay()
+        torch.cuda.synchronize()
+    stats = next(iter(s_cap._stats_dev.values())).cpu().numpy()
+    assert 0 < loops[0] < 500 and loops[0] == loops[1] == loops[2]
+    assert int(stats[0, 2]) == loops[2]
+    assert torch.equal(x_loop, x_cap)
