@@ -332,7 +332,8 @@ def serving_bench(args, local: int, dist=None, rank: int = 0, world: int = 1) ->
     import numpy as np
     import torch
 
-    from gridfoam_b200.serving import SIZES, BatchedEngine, poisson_stream, serve_sequential, summarize
+    from gridfoam_b200.serving import (SIZES, BatchedEngine, ServingEngine, poisson_stream, serve_sequential,
+                                       summarize)
     from gridfoam_b200.serving.shard import merge_summaries, shard_stream
 
     stream = poisson_stream(args.serve_requests, rate=50.0, sizes=SIZES, seed=0)
@@ -369,13 +370,27 @@ def serving_bench(args, local: int, dist=None, rank: int = 0, world: int = 1) ->
                      "batched_launches": eng.launches, "graph_captures": eng.captures}
         del eng
         torch.cuda.empty_cache()
+    # Per-case graphs on concurrent streams (no lockstep): each slot's
+    # iteration is one graph replay, the slots' kernels overlap on the GPU.
+    for name, prec in (("slots_fp64", "float64"), ("slots_mixed", "float32")):
+        eng = ServingEngine(device=f"cuda:{local}", max_slots=args.serve_slots, inner_precision=prec, **common)
+        t0 = time.perf_counter()
+        eng.prepare(SIZES)
+        prep = time.perf_counter() - t0
+        res = eng.run(reqs)
+        runs[name] = {r.id: r for r in res}
+        out[name] = {**whole(res), "prepare_s": prep, "slots": args.serve_slots}
+        del eng
+        torch.cuda.empty_cache()
     seq = serve_sequential(reqs, device=f"cuda:{local}", **common)
     runs["sequential_fp64"] = {r.id: r for r in seq}
     out["sequential_fp64"] = whole(seq)
 
     def max_err(a: str, b: str) -> float:
+        # at equal residual: requests that converged in both runs
         errs = [float(np.linalg.norm(runs[a][i].U - runs[b][i].U) / max(np.linalg.norm(runs[b][i].U), 1e-300))
-                for i in runs[a] if runs[a][i].U is not None and i in runs[b] and runs[b][i].U is not None]
+                for i in runs[a] if runs[a][i].U is not None and i in runs[b] and runs[b][i].U is not None
+                and runs[a][i].converged and runs[b][i].converged]
         m = max(errs, default=0.0)
         if dist is not None:
             both = [None] * world
@@ -387,7 +402,10 @@ def serving_bench(args, local: int, dist=None, rank: int = 0, world: int = 1) ->
     out["batched_fp64"]["max_rel_l2_U_vs_sequential_fp64"] = max_err("batched_fp64", "sequential_fp64")
     out["batched_mixed"]["max_rel_l2_U_vs_batched_fp64"] = max_err("batched_mixed", "batched_fp64")
     out["batched_mixed"]["max_rel_l2_U_vs_sequential_fp64"] = max_err("batched_mixed", "sequential_fp64")
-    for k in ("batched_fp64", "batched_mixed"):
+    out["slots_fp64"]["max_rel_l2_U_vs_sequential_fp64"] = max_err("slots_fp64", "sequential_fp64")
+    out["slots_mixed"]["max_rel_l2_U_vs_slots_fp64"] = max_err("slots_mixed", "slots_fp64")
+    out["slots_mixed"]["max_rel_l2_U_vs_sequential_fp64"] = max_err("slots_mixed", "sequential_fp64")
+    for k in ("batched_fp64", "batched_mixed", "slots_fp64", "slots_mixed"):
         out[k]["speedup_solves_per_s_vs_sequential"] = (
             out[k]["solves_per_s"] / out["sequential_fp64"]["solves_per_s"])
     return out

@@ -642,7 +642,8 @@ def pipe_analytic_uz(mesh, profile: dict) -> np.ndarray:
 
 
 def bluff_body_case(base: tuple[int, int, int] = (128, 32, 24), levels: int = 3, params=BLUFF_DEFAULT,
-                    iterations: int = 500, nu: float = 0.0024) -> dict:
+                    iterations: int = 500, nu: float = 0.0024, uniform: bool = False,
+                    lower=(-2.0, -1.0, 0.0), upper=(6.0, 1.0, 1.2)) -> dict:
     """Slanted bluff body in a channel on a 4-level octree (levels 0-3):
     domain [-2, 6] x [-1, 1] x [0, 1.2], the body (length 1, front at x = 0,
     shape ``params``) on the floor side with its clearance; refined to level
@@ -656,7 +657,10 @@ def bluff_body_case(base: tuple[int, int, int] = (128, 32, 24), levels: int = 3,
     these grids: the cells enclosed by the body carry almost no flux, so
     their momentum diagonal (outflow plus nu terms, no time derivative)
     nearly vanishes and 1/A blows up in the first iterations, in the
-    reference's own run of this case as here."""
+    reference's own run of this case as here.
+
+    ``uniform``: one level of ``base`` cells over [``lower``, ``upper``]
+    (no refinement, no hanging faces)."""
     body = {"kind": "bluff", "x0": 0.0, "params": list(params), "patch": "body"}
     sim = {
         "control": {"deltaT": 1.0, "endTime": float(iterations), "writeInterval": 100000,
@@ -699,10 +703,18 @@ def bluff_body_case(base: tuple[int, int, int] = (128, 32, 24), levels: int = 3,
         "properties": _props(nu),
         "device": "cpu",
     }
+    if uniform:
+        return {
+            "name": f"bluff_body_{base[0]}x{base[1]}x{base[2]}_uniform",
+            "mesh": {"kind": "uniform", "lower": list(lower), "upper": list(upper), "res": list(base),
+                     "bodies": [body]},
+            "simulator": sim,
+            "inlet_profile": None,
+        }
     return {
         "name": f"bluff_body_{base[0]}x{base[1]}x{base[2]}_l{levels}",
         "mesh": {
-            "kind": "octree", "lower": [-2.0, -1.0, 0.0], "upper": [6.0, 1.0, 1.2], "res": list(base),
+            "kind": "octree", "lower": list(lower), "upper": list(upper), "res": list(base),
             "regions": [
                 {"kind": "box", "lo": [-0.5, -0.45, 0.0], "hi": [3.0, 0.45, 0.6], "level": 1},
                 {"kind": "box", "lo": [-0.2, -0.3, 0.0], "hi": [1.6, 0.3, 0.45], "level": 2},

@@ -1,5 +1,6 @@
 """Lockstep solve server: the same-phase Krylov solves of every resident case
-in ONE launch, each batched iteration captured in a CUDA graph.
+in ONE launch, each batched iteration captured in a CUDA graph; cases above
+``solo_cells`` cells run beside that lane as solo slots.
 
 Life of a request:
 
@@ -25,6 +26,15 @@ Life of a request:
 4. *Draining*: U and p are copied to pinned host memory; the slot is freed
    when the copy has landed (the request's finish time).
 
+Large cases (more than ``solo_cells`` cells, default 200,000: the 64^3 and
+96^3 cavities) are bandwidth-bound and already fill the GPU alone; in the
+batched launch their fixed block share makes them slower than alone and
+holds the lockstep back.  They run as *solo slots* instead
+(``serving.engine``'s slot: the case's own stream, its single-system Krylov
+kernels, one captured graph an iteration, at most ``max_solo`` at once),
+asynchronously beside the lockstep lane of the small cases; the host loop
+polls the lane and every solo slot and relaunches whichever has finished.
+
 Failure handling: a request whose footprint can never fit the budget, or
 whose first iteration raises (an allocation failure, a NaN input), is
 rejected with ``status`` set and does not stop the others; a non-finite
@@ -48,11 +58,14 @@ from gridfoam_b200.serving.requests import CavityRequest
 
 def blocks_for(n_cells: int, bicgstab: bool) -> int:
     """Persistent blocks of one case's solves in a batched launch: about
-    4096 cells a 256-thread CG block (at most 148) and 65536 cells a
-    512-thread BiCGStab block (at most 24)."""
+    1024 cells a 256-thread CG block (at most 296, two an SM) and 8192 cells
+    a 512-thread BiCGStab block (at most 74).  A fixed count per grid size
+    keeps a case's iterates independent of what else shares the launch;
+    fewer, fuller blocks (4096 and 65536 cells) made the small cases'
+    solves latency-bound at about twice the time an iteration."""
     if bicgstab:
-        return int(min(24, max(1, -(-n_cells // 65536))))
-    return int(min(148, max(1, -(-n_cells // 4096))))
+        return int(min(74, max(1, -(-n_cells // 8192))))
+    return int(min(296, max(1, -(-n_cells // 1024))))
 
 
 class _Case:
@@ -96,7 +109,7 @@ class BatchedEngine:
     def __init__(self, device="cuda", *, hbm_budget: int | None = None, max_slots: int = 8,
                  use_graphs: bool = True, p_tol: float = 1e-6, p_solver_tol: float = 1e-12,
                  p_solver_rtol: float = 0.01, max_outer: int = 2000, inner_precision: str = "float64",
-                 keep_fields: bool = False):
+                 keep_fields: bool = False, solo_cells: int | None = 200_000, max_solo: int = 2):
         self.device = torch.device(device)
         if self.device.index is None:
             self.device = torch.device("cuda", torch.cuda.current_device())
@@ -114,6 +127,12 @@ class BatchedEngine:
         self.keep_fields = bool(keep_fields)
         self.topologies = TopologyCache(self.device)
         self.footprint: dict[int, int] = {}
+        # Solo slots (see the module doc); None: every case in the lane.
+        self.solo_cells = None if solo_cells is None else int(solo_cells)
+        self.max_solo = int(max_solo)
+        self.variants: dict[int, int] = {}
+        self.gpu_share = 1.0
+        self.sms = torch.cuda.get_device_properties(self.device).multi_processor_count
         self.stream = torch.cuda.Stream(self.device)
         with torch.cuda.device(self.device):
             lib = load()
@@ -135,15 +154,28 @@ class BatchedEngine:
     def prepare(self, sizes) -> None:
         """Start-up per grid size: build the topology and measure one case's
         device footprint (fields, matrices, workspaces)."""
+        from gridfoam_b200.serving.engine import _Slot
+
         for n in sorted(set(int(s) for s in sizes)):
             torch.cuda.synchronize(self.device)
             before = torch.cuda.memory_allocated(self.device)
-            case = _Case(self, CavityRequest(-1, n, 100.0, 1.0, 0.0), 0.0)
-            self._iteration([case], capture=False)
-            torch.cuda.synchronize(self.device)
-            used = torch.cuda.memory_allocated(self.device) - before
-            del case
+            req = CavityRequest(-1, n, 100.0, 1.0, 0.0)
+            if self.is_solo(n):
+                slot = _Slot(self, req, 0.0)
+                torch.cuda.synchronize(self.device)
+                used = torch.cuda.memory_allocated(self.device) - before
+                slot.release()
+                del slot
+            else:
+                case = _Case(self, req, 0.0)
+                self._iteration([case], capture=False)
+                torch.cuda.synchronize(self.device)
+                used = torch.cuda.memory_allocated(self.device) - before
+                del case
             self.footprint[n] = int(1.1 * used) + (1 << 20)
+
+    def is_solo(self, n: int) -> bool:
+        return self.solo_cells is not None and n**3 > self.solo_cells
 
     def estimate(self, n: int) -> int:
         if n in self.footprint:
@@ -230,78 +262,28 @@ class BatchedEngine:
         """Serve ``requests`` (arrival times relative to the call); returns
         results in completion order (rejected requests included, with
         ``status`` set)."""
+        from gridfoam_b200.serving.engine import _Slot
+
         pending = deque(sorted(requests, key=lambda r: r.arrival))
         queue: deque = deque()
-        active: list[_Case] = []
+        lane: list[_Case] = []
+        solos: list = []
         results: list[ServeResult] = []
         used = 0
         graph = None
         graph_set: tuple = ()
-        done_ev = torch.cuda.Event()
+        # lane state: "idle" | "eager" (an uncaptured iteration in flight) |
+        # "replay" (a graph replay in flight)
+        state = "idle"
+        lane_ev = torch.cuda.Event()
         t0 = clock()
-        while pending or queue or active:
-            now = clock() - t0
-            while pending and pending[0].arrival <= now:
-                queue.append(pending.popleft())
-            # Admission by slots, HBM budget and persistent blocks.
-            while queue and len(active) < self.max_slots:
-                req = queue[0]
-                need = self.estimate(req.n)
-                if need > self.hbm_budget:
-                    queue.popleft()
-                    results.append(self._reject(req, clock() - t0, "rejected_memory"))
-                    continue
-                cg = sum(c.cg_blocks for c in active) + blocks_for(req.n**3, False)
-                bi = sum(c.bicg_blocks for c in active) + blocks_for(req.n**3, True)
-                if active and (used + need > self.hbm_budget or cg > self.cg_capacity or bi > self.bicg_capacity):
-                    break
-                queue.popleft()
-                try:
-                    if self.admission_hook is not None:
-                        self.admission_hook(req)
-                    case = _Case(self, req, clock() - t0)
-                    if self.case_hook is not None:
-                        self.case_hook(case)
-                except (RuntimeError, ValueError, torch.cuda.OutOfMemoryError) as exc:
-                    results.append(self._reject(req, clock() - t0, f"rejected: {type(exc).__name__}"))
-                    continue
-                case.need = need
-                used += need
-                active.append(case)
-            if not active:
-                if pending:
-                    time.sleep(max(0.0, min(1e-3, pending[0].arrival - (clock() - t0))))
-                continue
-            key = tuple(id(c) for c in active)
-            if self.use_graphs:
-                if graph is None or key != graph_set:
-                    # A new set of resident cases: one eager iteration (new
-                    # cases allocate their workspaces), then capture.
-                    self._iteration(active, capture=False)
-                    done_ev.record(self.stream)
-                    done_ev.synchronize()
-                    self._finish(active, clock() - t0)
-                    graph = None
-                    if not any(c.status != "running" for c in active):
-                        torch.cuda.synchronize(self.device)
-                        graph = torch.cuda.CUDAGraph()
-                        with torch.cuda.graph(graph, stream=self.stream):
-                            self._iteration(active, capture=True)
-                        self.captures += 1
-                        graph_set = key
-                else:
-                    with torch.cuda.stream(self.stream):
-                        graph.replay()
-                    done_ev.record(self.stream)
-                    done_ev.synchronize()
-                    self._finish(active, clock() - t0)
-            else:
-                self._iteration(active, capture=False)
-                done_ev.record(self.stream)
-                done_ev.synchronize()
-                self._finish(active, clock() - t0)
-            # Retire finished cases.
-            for c in [c for c in active if c.status != "running"]:
+
+        def now() -> float:
+            return clock() - t0
+
+        def retire_lane() -> None:
+            nonlocal used
+            for c in [c for c in lane if c.status != "running"]:
                 with torch.cuda.stream(c.stream):
                     c.stream.wait_stream(self.stream)
                     c.U_host = torch.empty(c.algo.U.data.shape, dtype=torch.float64, pin_memory=True)
@@ -309,12 +291,105 @@ class BatchedEngine:
                     c.U_host.copy_(c.algo.U.data, non_blocking=True)
                     c.p_host.copy_(c.algo.p.data, non_blocking=True)
                 c.stream.synchronize()
-                results.append(self._result(c, clock() - t0))
-                active.remove(c)
+                results.append(self._result(c, now()))
+                lane.remove(c)
                 used -= c.need
                 c.algo = None
-            if graph is not None and tuple(id(c) for c in active) != graph_set:
-                graph = None
+
+        while pending or queue or lane or solos:
+            while pending and pending[0].arrival <= now():
+                queue.append(pending.popleft())
+            # Admission (first admissible request in arrival order) by slots,
+            # HBM budget, persistent blocks and, for the lane, an idle lane.
+            admitted = True
+            while admitted and queue and len(lane) + len(solos) < self.max_slots:
+                admitted = False
+                for req in list(queue):
+                    need = self.estimate(req.n)
+                    if need > self.hbm_budget:
+                        queue.remove(req)
+                        results.append(self._reject(req, now(), "rejected_memory"))
+                        admitted = True
+                        break
+                    if (lane or solos) and used + need > self.hbm_budget:
+                        continue
+                    solo = self.is_solo(req.n)
+                    if solo and len(solos) >= self.max_solo:
+                        continue
+                    if not solo:
+                        cg = sum(c.cg_blocks for c in lane) + blocks_for(req.n**3, False)
+                        bi = sum(c.bicg_blocks for c in lane) + blocks_for(req.n**3, True)
+                        if state != "idle" or (lane and (cg > self.cg_capacity or bi > self.bicg_capacity)):
+                            continue
+                    queue.remove(req)
+                    admitted = True
+                    try:
+                        if self.admission_hook is not None:
+                            self.admission_hook(req)
+                        case = _Slot(self, req, now()) if solo else _Case(self, req, now())
+                        if self.case_hook is not None:
+                            self.case_hook(case)
+                    except (RuntimeError, ValueError, torch.cuda.OutOfMemoryError) as exc:
+                        results.append(self._reject(req, now(), f"rejected: {type(exc).__name__}"))
+                        break
+                    case.need = need
+                    used += need
+                    (solos if solo else lane).append(case)
+                    break
+            progressed = False
+            # Solo slots: one captured iteration in flight each.
+            for slot in list(solos):
+                if not slot.ready():
+                    continue
+                progressed = True
+                if slot.draining:
+                    res = slot.result(now(), self.keep_fields)
+                    res.status = "converged" if res.converged else (
+                        "nonfinite" if not np.isfinite(res.residual) else "end_time")
+                    results.append(res)
+                    slot.release()
+                    used -= slot.need
+                    solos.remove(slot)
+                    continue
+                slot.finish_iteration()
+                if slot.done:
+                    slot.start_drain()
+                else:
+                    slot.launch()
+            # The lockstep lane.
+            if state != "idle" and lane_ev.query():
+                progressed = True
+                self._finish(lane, now())
+                running = not any(c.status != "running" for c in lane)
+                if state == "eager" and running and self.use_graphs:
+                    g = torch.cuda.CUDAGraph()
+                    with torch.cuda.graph(g, stream=self.stream):
+                        self._iteration(lane, capture=True)
+                    self.captures += 1
+                    graph, graph_set = g, tuple(id(c) for c in lane)
+                state = "idle"
+                retire_lane()
+                if tuple(id(c) for c in lane) != graph_set:
+                    graph = None
+            if state == "idle" and lane:
+                progressed = True
+                key = tuple(id(c) for c in lane)
+                if graph is not None and key == graph_set:
+                    with torch.cuda.stream(self.stream):
+                        graph.replay()
+                    state = "replay"
+                else:
+                    # a new set of resident cases: one eager iteration (new
+                    # cases allocate their workspaces), captured after it
+                    graph = None
+                    self._iteration(lane, capture=False)
+                    state = "eager"
+                lane_ev.record(self.stream)
+            if not progressed:
+                if pending and not (lane or solos or queue):
+                    time.sleep(max(0.0, min(1e-3, pending[0].arrival - now())))
+                else:
+                    time.sleep(2e-5)
         return results
 
     def _finish(self, cases: list[_Case], now: float) -> None:

@@ -187,7 +187,7 @@ class ServingEngine:
         """Start-up for each grid size: build the topology, pick the
         pressure-CG launch shape with the autotuner and measure one case's
         device footprint (fields, matrices, workspaces, graph pool)."""
-        from gridfoam_b200.solvers.autotune import BoxSystem, best_variant
+        from gridfoam_b200.solvers.autotune import PERSISTENT_VARIANTS, BoxSystem, best_variant
 
         for n in sorted(set(int(s) for s in sizes)):
             sim = cavity_simulator(1e-2, 1.0, p_tol=self.p_tol, p_solver_tol=self.p_solver_tol,
@@ -196,8 +196,10 @@ class ServingEngine:
             self.topologies.grid(n, sim)
             if autotune:
                 sysm = BoxSystem(n, n, n, device=self.device)
+                # each iteration is one captured graph: single-launch variants only
                 self.variants[n] = best_variant(sysm, sysm.diag, sysm.val, sysm.rhs, symmetric=True,
-                                                mixed=self.inner_precision == "float32")
+                                                mixed=self.inner_precision == "float32",
+                                                variants=PERSISTENT_VARIANTS)
                 del sysm
             torch.cuda.synchronize(self.device)
             before = torch.cuda.memory_allocated(self.device)

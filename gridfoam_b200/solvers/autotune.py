@@ -10,10 +10,12 @@ iterations of every variant on the caller's own matrix and caches the
 winner per (device, cells, strides, symmetric, precision).  That cache is
 the package's only global state and a lock guards it.
 
-Run as a module it times one synthetic box system, for profiling a single
-fixed-length kernel launch::
+Run as a module it times one synthetic box system, or the pressure system
+of the cylinder wake's octree after one PISO step (``--wake``), for
+profiling a single fixed-length kernel launch::
 
     python -m gridfoam_b200.solvers.autotune --box 64 64 256 --iters 200
+    python -m gridfoam_b200.solvers.autotune --wake 192 120 24 --iters 40 --variant 19
 """
 
 from __future__ import annotations
@@ -143,17 +145,26 @@ def time_variant(grid, diag, val, rhs, *, symmetric: bool, mixed: bool, variant:
     return best, its
 
 
-def best_variant(grid, diag, val, rhs, *, symmetric: bool, mixed: bool, iters: int = 60) -> int:
-    """Fastest box CG variant for this system shape (timed once, then cached)."""
+# The persistent single-launch variants: the ones a captured CUDA graph
+# holds as one kernel node (the split CG, 19 and 20, enqueues every
+# permitted iteration when it is captured).
+PERSISTENT_VARIANTS = tuple(v for v in range(N_VARIANTS) if v not in (19, 20))
+
+
+def best_variant(grid, diag, val, rhs, *, symmetric: bool, mixed: bool, iters: int = 60,
+                 variants=None) -> int:
+    """Fastest box CG variant for this system shape among ``variants``
+    (default all; timed once, then cached)."""
+    cands = tuple(range(N_VARIANTS) if variants is None else variants)
     key = (str(grid.device), torch.cuda.get_device_name(grid.device), grid.num_cells,
-           tuple(grid.box_strides), bool(symmetric), bool(mixed))
+           tuple(grid.box_strides), bool(symmetric), bool(mixed), cands)
     with _LOCK:
         hit = _CACHE.get(key)
         if hit is not None:
             return hit
-        times = [time_variant(grid, diag, val, rhs, symmetric=symmetric, mixed=mixed, variant=v,
-                              iters=iters, repeats=2)[0] for v in range(N_VARIANTS)]
-        best = min(range(N_VARIANTS), key=lambda v: times[v])
+        times = {v: time_variant(grid, diag, val, rhs, symmetric=symmetric, mixed=mixed, variant=v,
+                                 iters=iters, repeats=2)[0] for v in cands}
+        best = min(cands, key=lambda v: times[v])
         _CACHE[key] = best
         return best
 
@@ -168,22 +179,36 @@ def main() -> None:
                     help="float32: FP32 inner CG inside FP64 refinement")
     ap.add_argument("--single-reduction", action="store_true",
                     help="FP64 Chronopoulos-Gear CG (one grid reduction per iteration)")
+    ap.add_argument("--wake", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
+                    help="the cylinder wake's pressure system on this base grid (2 refinement levels)")
     args = ap.parse_args()
     dev = torch.device("cuda")
-    sysm = BoxSystem(*args.box, device=dev)
     mixed = args.precision == "float32"
     variants = range(N_VARIANTS) if args.variant < 0 else [args.variant]
-    n = sysm.num_cells
-    for v in variants:
-        us, its = time_variant(sysm, sysm.diag, sysm.val, sysm.rhs, symmetric=True, mixed=mixed, variant=v,
-                               iters=args.iters, repeats=args.repeats, single_reduction=args.single_reduction)
-        # Algorithmic bytes of one fused symmetric PCG-Jacobi iteration:
-        # 14 C s + F (s + 8), F the internal faces of the box.
-        s = 4 if mixed else 8
+    if args.wake is not None:
+        from gridfoam_b200.cases import create_case, cylinder_wake_case
+
+        _, grid, algo = create_case(cylinder_wake_case(tuple(args.wake)), device=dev)
+        algo.step()
+        torch.cuda.synchronize()
+        diag, val, rhs = algo.pEqn.diag_store, algo.pEqn.val, algo.pEqn.source_store
+        n, f, label = grid.num_cells, grid.num_internal_faces, {"wake": args.wake}
+        sysm = grid
+    else:
+        sysm = BoxSystem(*args.box, device=dev)
+        diag, val, rhs = sysm.diag, sysm.val, sysm.rhs
+        n = sysm.num_cells
         nx, ny, nz = args.box
         f = (nx - 1) * ny * nz + nx * (ny - 1) * nz + nx * ny * (nz - 1)
+        label = {"box": args.box}
+    for v in variants:
+        us, its = time_variant(sysm, diag, val, rhs, symmetric=True, mixed=mixed, variant=v,
+                               iters=args.iters, repeats=args.repeats, single_reduction=args.single_reduction)
+        # Algorithmic bytes of one fused symmetric PCG-Jacobi iteration:
+        # 14 C s + F (s + 8), F the internal faces.
+        s = 4 if mixed else 8
         gbs = (14 * n * s + f * (s + 8)) / (us * 1e-6) / 1e9
-        print(json.dumps({"box": args.box, "cells": n, "precision": args.precision,
+        print(json.dumps({**label, "cells": n, "faces": f, "precision": args.precision,
                           "single_reduction": args.single_reduction, "variant": v,
                           "shape": VARIANTS[v], "iterations": its, "us_per_iter": round(us, 3),
                           "algorithmic_GBps": round(gbs, 1)}))

@@ -100,11 +100,22 @@ def test_small_cavity_converges_to_residual_control():
 def test_batched_block_shares():
     from gridfoam_b200.serving import blocks_for
 
-    assert blocks_for(16**3, False) == 1 and blocks_for(96**3, False) == 148
-    assert blocks_for(64**3, False) == 64 and blocks_for(32**3, False) == 8
-    assert blocks_for(16**3, True) == 1 and blocks_for(96**3, True) == 14
-    # a full mix of the largest size fits the batched CG's co-resident blocks
-    assert 4 * blocks_for(96**3, False) <= 4 * 148
+    assert blocks_for(16**3, False) == 4 and blocks_for(96**3, False) == 296
+    assert blocks_for(48**3, False) == 108 and blocks_for(32**3, False) == 32
+    assert blocks_for(16**3, True) == 1 and blocks_for(48**3, True) == 14 and blocks_for(96**3, True) == 74
+    # the lane's sizes (up to 48^3) fit the batched CG's co-resident blocks
+    # (4 a SM of 148) several at a time
+    assert 5 * blocks_for(48**3, False) <= 4 * 148
+
+
+def test_solo_threshold():
+    from gridfoam_b200.serving.batched import BatchedEngine
+
+    eng = BatchedEngine.__new__(BatchedEngine)
+    eng.solo_cells = 200_000
+    assert not eng.is_solo(48) and eng.is_solo(64) and eng.is_solo(96)
+    eng.solo_cells = None
+    assert not eng.is_solo(96)
 
 
 def test_batched_stopping_rule_statuses():
