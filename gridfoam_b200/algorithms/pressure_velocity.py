@@ -209,9 +209,23 @@ class _PressureVelocity:
         self.u_cells, self.u_faces, self.u_mask = self.U.table.constraints()
         self.p_cells, self.p_faces, self.p_mask = self.p.table.constraints()
         self.p_fixed_faces, self.p_fixed_frac = self.p.table.fixed_faces()
-        self.u_vals = torch.zeros((3, max(1, self.u_cells.numel())), **f64)
-        self.p_vals = torch.zeros((1, max(1, self.p_cells.numel())), **f64)
-        self.fix_scratch = torch.zeros(max(1, self.p_fixed_faces.numel()), **f64)
+        # inletOutlet on near immersed faces: selections follow the flux
+        self._u_dynamic = self.U.table.dynamic
+        self._p_dynamic = self.p.table.dynamic or self.p.table._dynamic_fixed is not None
+        self.u_vals = torch.zeros((3, max(1, self.U.table.num_constraint_candidates)), **f64)
+        self.p_vals = torch.zeros((1, max(1, self.p.table.num_constraint_candidates)), **f64)
+        n_fix = g.num_bnd if self._p_dynamic else self.p_fixed_faces.numel()
+        self.fix_scratch = torch.zeros(max(1, n_fix), **f64)
+
+    def _refresh_constraints(self, *, u: bool = False, p: bool = False) -> None:
+        """Re-select the flux-dependent immersed constraints (inletOutlet on
+        near immersed faces fixes the faces carrying inflow) from the
+        current face flux, as the reference evaluates them at each use."""
+        if u and self._u_dynamic:
+            self.u_cells, self.u_faces, self.u_mask = self.U.table.constraints()
+        if p and self._p_dynamic:
+            self.p_cells, self.p_faces, self.p_mask = self.p.table.constraints()
+            self.p_fixed_faces, self.p_fixed_frac = self.p.table.fixed_faces()
 
     def _build_adjust_classes(self) -> torch.Tensor:
         """adjust_phi.py:21-41 classes per domain face: 0 skip, 1 fixed, 2 adjustable."""
@@ -259,6 +273,7 @@ class _PressureVelocity:
     # ------------------------------------------------------------------
     def _assemble_momentum(self, relax: float) -> None:
         g = self._grid
+        self._refresh_constraints(u=True)
         self._eval_U()
         tvd = self._div_code >= _lib.DIV_CODES["vanleer"]
         if tvd:
@@ -413,6 +428,7 @@ class _PressureVelocity:
         s = stream_ptr()
         stats = None
         first_res = last_res = None
+        self._refresh_constraints(p=True)
         for corr in range(self.n_non_orthogonal_correctors + 1):
             self._eval_p()
             t = self.p.table
@@ -456,6 +472,7 @@ class _PressureVelocity:
         """pressure_correction.py:270-335."""
         g = self._grid
         s = stream_ptr()
+        self._refresh_constraints(p=True)
         self._eval_p()
         t = self.p.table
         call("gf_correct_phi", byref(g.cmesh), ptr(self.phi_hbya.store), ptr(self.rAtU.store), ptr(self.p.store),
@@ -469,6 +486,7 @@ class _PressureVelocity:
     def _correct_velocity(self) -> None:
         """pressure_correction.py:338-363."""
         g = self._grid
+        self._refresh_constraints(u=True, p=True)
         self._eval_p()
         self._grad_cfg(self.p, self.grad_p, self.grad_p_lsq)
         call("gf_correct_velocity", byref(g.cmesh), ptr(self.HbyA.store), ptr(self.rAtU.store), ptr(self.grad_p),
@@ -550,6 +568,7 @@ class SIMPLE(_PressureVelocity):
             self._record(self.p.name, first)
         self._correct_phi()
         call("gf_relax_field", g.num_cells, self.alpha_p, ptr(self.p_old), ptr(self.p.store), stream_ptr())
+        self._refresh_constraints(p=True)
         if self.p_cells.numel():
             self._eval_p()
             self._apply_fixed(self.p, self.p_cells, self.p_faces, self.p_vals)

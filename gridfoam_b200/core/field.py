@@ -69,21 +69,65 @@ class BoundaryTable:
         self.cstate = GfBcState(ptr(self.frac), ptr(self.refv), ptr(self.refg), ptr(self.psib))
         self._constraints = None
         self._fixed_faces = None
+        # Flux-dependent candidates (inletOutlet on near immersed faces):
+        # (cells, distances, faces, dynamic mask, phi name) on the device.
+        self._dynamic = None
+        self._dynamic_fixed = None
+        self.num_constraint_candidates = 0
         self._field = field
 
-    # fv/boundary_ops.py:440-535 (selection is geometric for fixed-value
-    # and slip conditions, so it is computed once here).
+    # fv/boundary_ops.py:440-535.  Fixed-value and slip conditions select
+    # their faces by geometry alone, so that selection is computed once; an
+    # inletOutlet condition on near immersed faces fixes the faces that
+    # currently carry inflow (fraction 1, phi < 0), so with one the
+    # selection is redone from the current face flux on every call.
+    @property
+    def dynamic(self) -> bool:
+        self.constraints()
+        return self._dynamic is not None
+
     def constraints(self):
         """``(cells[K] int32, faces[K] int32, mask[C] uint8)`` on the device."""
         if self._constraints is None:
             self._constraints = self._build_constraints()
+        if self._dynamic is not None:
+            return self._select_dynamic()
         return self._constraints
+
+    def _phi_boundary(self, name: str) -> torch.Tensor:
+        phi = self._field.grid.get_facefield(name)
+        if phi is None:
+            raise ValueError(f"Field {name} is not found.")
+        return phi.boundary_store[0]
+
+    def _select_dynamic(self):
+        """The closest constraining face per cell among the geometric
+        candidates and the inflow faces of the flux-dependent ones (ties:
+        candidate order, which is the reference's batch order)."""
+        cell, dist, face, dyn, phi_name = self._dynamic
+        grid = self._field.grid
+        C = grid.num_cells
+        n = int(cell.numel())
+        active = ~dyn | (self._phi_boundary(phi_name)[face] < 0.0)
+        inf = torch.full_like(dist, float("inf"))
+        d = torch.where(active, dist, inf)
+        closest = torch.full((C,), float("inf"), dtype=torch.float64, device=grid.device)
+        closest = closest.scatter_reduce(0, cell, d, reduce="amin")
+        idx = torch.arange(n, device=grid.device)
+        cand = torch.where(active & (d == closest[cell]), idx, torch.full_like(idx, n))
+        selected = torch.full((C,), n, dtype=torch.int64, device=grid.device)
+        selected = selected.scatter_reduce(0, cell, cand, reduce="amin")
+        unique = torch.nonzero(selected < n).reshape(-1)
+        mask = torch.zeros(C, dtype=torch.uint8, device=grid.device)
+        mask[unique] = 1
+        return unique.to(torch.int32), face[selected[unique]].to(torch.int32), mask
 
     def _build_constraints(self):
         field = self._field
         grid = field.grid
         h = grid.host
-        cand_cell, cand_dist, cand_face = [], [], []
+        cand_cell, cand_dist, cand_face, cand_dyn = [], [], [], []
+        phi_name = None
         for patch, bc in field.bcs.items():
             faces = grid.patch_faces(patch)
             if faces.size == 0 or isinstance(bc, (EmptyBC, NeumannBC)):
@@ -92,15 +136,29 @@ class BoundaryTable:
             if imm.size == 0:
                 continue
             near = h.bnd_near[imm] != 0
+            dyn = False
             if isinstance(bc, DirichletBC) or (isinstance(bc, SlipBC) and field.num_components == 3):
                 sel = imm[near]
             elif isinstance(bc, InletOutletBC) and near.any():
-                raise NotImplementedError("inletOutlet on near immersed faces needs a flux-dependent selection")
+                sel = imm[near]
+                dyn = True
+                phi_name = bc.phi_name
             else:
                 sel = imm[:0]
             cand_cell.append(h.bnd_cell[sel])
             cand_dist.append(h.bnd_mag_d[sel])
             cand_face.append(sel)
+            cand_dyn.append(np.full(sel.size, dyn))
+        if any(d.any() for d in cand_dyn):
+            dev = grid.device
+            self._dynamic = (
+                torch.as_tensor(np.concatenate(cand_cell).astype(np.int64), device=dev),
+                torch.as_tensor(np.concatenate(cand_dist), dtype=torch.float64, device=dev),
+                torch.as_tensor(np.concatenate(cand_face).astype(np.int64), device=dev),
+                torch.as_tensor(np.concatenate(cand_dyn), device=dev),
+                phi_name,
+            )
+        self.num_constraint_candidates = int(sum(c.size for c in cand_cell))
         C = grid.num_cells
         dev = grid.device
         if cand_cell:
@@ -132,12 +190,13 @@ class BoundaryTable:
 
     def fixed_faces(self):
         """Faces flagged ``near & fraction == 1`` and their area share per cell
-        (pressure_correction.py:308-335), as device tensors."""
+        (pressure_correction.py:308-335), as device tensors (recomputed from
+        the current flux when an inletOutlet condition has near faces)."""
         if self._fixed_faces is None:
             field = self._field
             grid = field.grid
             h = grid.host
-            faces = []
+            faces, dyn_faces = [], []
             for patch, bc in field.bcs.items():
                 fb = grid.patch_faces(patch)
                 if fb.size == 0 or isinstance(bc, EmptyBC):
@@ -145,10 +204,25 @@ class BoundaryTable:
                 always_one = isinstance(bc, DirichletBC) or (
                     isinstance(bc, SlipBC) and field.num_components == 3
                 )
+                near = fb[h.bnd_near[fb] != 0]
+                if isinstance(bc, InletOutletBC) and near.size:
+                    dyn_faces.append((near, bc.phi_name))
                 if not always_one:
                     continue
-                faces.append(fb[h.bnd_near[fb] != 0])
+                faces.append(near)
             faces = np.concatenate(faces) if faces else np.zeros(0, dtype=np.int64)
+            if dyn_faces:
+                dev = grid.device
+                allf = np.concatenate([faces] + [f for f, _ in dyn_faces])
+                dyn = np.concatenate([np.zeros(faces.size, dtype=bool)] + [np.ones(f.size, dtype=bool)
+                                                                          for f, _ in dyn_faces])
+                self._dynamic_fixed = (
+                    torch.as_tensor(allf.astype(np.int64), device=dev),
+                    torch.as_tensor(dyn, device=dev),
+                    torch.as_tensor(h.bnd_mag_sf[allf], dtype=torch.float64, device=dev),
+                    torch.as_tensor(h.bnd_cell[allf].astype(np.int64), device=dev),
+                    dyn_faces[0][1],
+                )
             area = h.bnd_mag_sf[faces]
             cells = h.bnd_cell[faces]
             area_sum = np.bincount(cells, weights=area, minlength=grid.num_cells)
@@ -159,6 +233,16 @@ class BoundaryTable:
                 torch.as_tensor(faces.astype(np.int32), device=dev),
                 torch.as_tensor(frac, device=dev),
             )
+        if self._dynamic_fixed is not None:
+            faces, dyn, area, cells, phi_name = self._dynamic_fixed
+            grid = self._field.grid
+            active = ~dyn | (self._phi_boundary(phi_name)[faces] < 0.0)
+            sel = torch.nonzero(active).reshape(-1)
+            area, cells = area[sel], cells[sel]
+            total = torch.zeros(grid.num_cells, dtype=torch.float64, device=grid.device).index_add(0, cells, area)
+            t = total[cells]
+            frac = area / torch.where(t > 0, t, torch.ones_like(t))
+            return faces[sel].to(torch.int32), frac
         return self._fixed_faces
 
 

@@ -57,8 +57,23 @@ __global__ void k_ldu_grad_faces(gf_mesh_t m, int nc, const double* __restrict__
     }
 }
 
-// Reverse of the Laplacian assembly with respect to gamma (linear face
-// interpolation gamma_f = w gamma_O + (1 - w) gamma_N).  The cotangent of a
+// d gamma_f / d gamma of the owner (side 0) or neighbour (side 1) cell.
+// Linear: w, 1 - w.  Harmonic (fv/fvm/laplacian.py:38-73): the forward's
+// min(go, gn) / (w go / s + (1 - w) gn / s), s = max(go, gn), equals
+// go gn / D with D = w go + (1 - w) gn, so the derivatives are
+// (1 - w) gn^2 / D^2 and w go^2 / D^2 (also at go = gn, where torch's
+// min/max split the cotangent evenly and give the same values); with both
+// zero the forward is min(go, gn) and each side gets half.
+__device__ __forceinline__ double gamma_face_weight(const gf_assembly_t& a, double w, int o, int n, int side) {
+    if (!a.lap_harmonic || a.gamma == nullptr) return side ? (1.0 - w) : w;
+    const double go = a.gamma[o], gn = a.gamma[n];
+    const double D = w * go + (1.0 - w) * gn;
+    if (!(D > 0.0)) return 0.5;
+    return side ? (w * go * go) / (D * D) : ((1.0 - w) * gn * gn) / (D * D);
+}
+
+// Reverse of the Laplacian assembly with respect to gamma (face
+// interpolation gamma_f linear or harmonic, gamma_face_weight).  The cotangent of a
 // face conductance is |Sf| delta (gu + gl - gd_O - gd_N) plus, on hanging
 // faces, |Sf| sum_k corr_k (gs_kN - gs_kO); each cell gathers w (owner) or
 // 1 - w (neighbour) of it, and its boundary conductances add
@@ -89,7 +104,7 @@ __global__ void k_laplacian_adjoint(gf_mesh_t m, gf_assembly_t a, const double* 
                         gf += msf * corr * (gs[k * C + n] - gs[k * C + o]);
                     }
                 }
-                acc += (sl.side ? (1.0 - w) : w) * gf;
+                acc += gamma_face_weight(a, w, o, n, sl.side) * gf;
             } else if (sl.kind == kBoundary) {
                 const int b = sl.bnd;
                 if (a.bc_kind[b] == GF_BC_NONE) continue;

@@ -197,8 +197,6 @@ def laplacian(gamma, field: CellField) -> FvMatrix:
     _run(field, a)
     mat._keep = (g_t, grad)
     if torch.is_grad_enabled() and isinstance(gamma, torch.Tensor) and gamma.requires_grad:
-        if a.lap_harmonic:
-            raise NotImplementedError("the diffusivity adjoint covers linear interpolation only")
         keep = _frozen_state(field, a) + (g_t, grad)
         return _attach(mat, gamma, "gf_laplacian_adjoint", a, keep)
     return mat

@@ -89,6 +89,8 @@ def _check_supported(algo) -> None:
         raise NotImplementedError("pressure conditions other than dirichlet/neumann")
     if algo.p_cells.numel() or algo.p_fixed_faces.numel():
         raise NotImplementedError("pressure constraints at immersed faces")
+    if algo.U.table.dynamic:
+        raise NotImplementedError("flux-dependent velocity constraints (inletOutlet on near immersed faces)")
     if algo._u_harmonic or algo._p_harmonic:
         raise NotImplementedError("harmonic diffusivity interpolation")
 

@@ -43,12 +43,26 @@ def potential_case(name: str) -> dict:
 
 
 
+def ibplane_io_case() -> dict:
+    """The immersed plate with an inletOutlet velocity condition on the
+    plate: its near faces (zero ray distance) constrain their cells only
+    while they carry inflow, so the Gibou constraints and the fixed-cell
+    flux closure follow the flux (boundary_ops.py:440-535)."""
+    case = copy.deepcopy(ibplane_case())
+    bnd = case["simulator"]["conditions"]["U"]["boundary"]
+    bnd["wall"]["patches"] = [p for p in bnd["wall"]["patches"] if p != "plate"]
+    bnd["plate"] = {"type": "inlet_outlet", "patches": ["plate"], "value": [0.0, 0.0, 0.0]}
+    case["name"] = "ibplane_io"
+    return case
+
+
 ALL_CASES = {
     "cavity8": lambda: cavity_case(8),
     "pipe10x20": lambda: pipe_case(10, 20),
     "channel": channel_case,
     "channel_ffp": ffp_case,
     "ibplane": ibplane_case,
+    "ibplane_io": ibplane_io_case,
     "cavity_oct": cavity_oct_case,
     "duct_oct": duct_oct_case,
     "ibcyl_oct": ibcyl_oct_case,
@@ -60,7 +74,7 @@ POTENTIAL_CASES = ("duct_oct", "ibcyl_oct")
 
 
 # Steps stored per golden case and the convection schemes dumped per case.
-STEPS = {"cavity8": 4, "pipe10x20": 3, "channel": 3, "channel_ffp": 3, "ibplane": 3,
+STEPS = {"cavity8": 4, "pipe10x20": 3, "channel": 3, "channel_ffp": 3, "ibplane": 3, "ibplane_io": 3,
          "cavity_oct": 4, "duct_oct": 3, "ibcyl_oct": 3}
 DIV_SCHEMES = [
     "upwind",

@@ -21,7 +21,7 @@ from tests.golden.oracle_ops_check import oracle_operator_outputs
 
 CASES = list(STEPS)
 # Relative L2 tolerance of whole-step fields against the reference.
-STEP_TOL = {"cavity8": 1e-12, "channel": 1e-11, "channel_ffp": 1e-11, "ibplane": 1e-12, "pipe10x20": 1e-4,
+STEP_TOL = {"cavity8": 1e-12, "channel": 1e-11, "channel_ffp": 1e-11, "ibplane": 1e-12, "ibplane_io": 1e-12, "pipe10x20": 1e-4,
             "cavity_oct": 1e-11, "duct_oct": 1e-9, "ibcyl_oct": 1e-9}
 
 
@@ -87,7 +87,7 @@ def test_oracle_operators_match_reference(name):
         assert np.abs(val - ref).max() <= 1e-11 * scale, key
 
 
-NATIVE_STEP_TOL = {"cavity8": 1e-10, "channel": 1e-9, "channel_ffp": 1e-9, "ibplane": 1e-10, "pipe10x20": 1e-4,
+NATIVE_STEP_TOL = {"cavity8": 1e-10, "channel": 1e-9, "channel_ffp": 1e-9, "ibplane": 1e-10, "ibplane_io": 1e-10, "pipe10x20": 1e-4,
                    "cavity_oct": 1e-9, "duct_oct": 1e-8, "ibcyl_oct": 1e-8}
 
 
