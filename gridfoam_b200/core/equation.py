@@ -40,8 +40,8 @@ class Equation:
         self.target = target
         cells, values = immersed_dirichlet_constraints(target)
         _, _, mask = target.table.constraints()
-        if cells.numel() and fv_matrix.requires_grad:
-            raise NotImplementedError("gradients through immersed-boundary cell constraints are not implemented")
+        # differentiable coefficients: the elimination carries their graph
+        # (FvMatrix.with_fixed_values)
         self.fv_matrix = fv_matrix.with_fixed_values(cells, values, mask=mask) if cells.numel() else fv_matrix
 
 

@@ -19,6 +19,30 @@ from gridfoam_b200._lib import call, ptr, stream_ptr
 from gridfoam_b200.core.field import CellField, ctypes_ref
 
 
+def fixed_values_ldu(grid, diag: torch.Tensor, upper: torch.Tensor, lower: torch.Tensor, source: torch.Tensor,
+                     cells: torch.Tensor, values: torch.Tensor):
+    """core/fvmatrix.py:325-394 on LDU tensors (``source`` and ``values``
+    ``[*, ncomp]``): the prescribed cells' couplings move to the right-hand
+    side, their rows and columns are removed, each fixed row keeps its
+    nonzero diagonal (a zero one becomes -1 if the diagonal sums to a
+    negative value, else +1) and its right-hand side is that diagonal times
+    the value.  Device tensor algebra, differentiable in every input."""
+    own, nei = grid.owner.to(diag.device), grid.neighbour.to(diag.device)
+    fixed = torch.zeros(grid.num_cells, dtype=torch.bool, device=diag.device)
+    fixed[cells] = True
+    prescribed = torch.zeros_like(source).index_copy(0, cells, values.to(source.dtype))
+    unit = torch.where(diag.sum() < 0, -torch.ones_like(diag), torch.ones_like(diag))
+    cdiag = torch.where(diag != 0, diag, unit)
+    d2 = torch.where(fixed, cdiag, diag)
+    conn = fixed[own] | fixed[nei]
+    up2 = torch.where(conn, torch.zeros_like(upper), upper)
+    lo2 = torch.where(conn, torch.zeros_like(lower), lower)
+    pn, po = prescribed[nei], prescribed[own]
+    src = source.index_add(0, own, -upper[:, None] * pn).index_add(0, nei, -lower[:, None] * po)
+    src = src.index_copy(0, cells, cdiag[cells][:, None] * values.to(source.dtype))
+    return d2, up2, lo2, src
+
+
 class FvMatrix:
     def __init__(self, field: CellField, *, _alloc: bool = True):
         self._field = field
@@ -257,7 +281,10 @@ class FvMatrix:
 
     def with_fixed_values(self, cells: torch.Tensor, values: torch.Tensor, *, mask: torch.Tensor | None = None,
                           out: "FvMatrix | None" = None) -> "FvMatrix":
-        """core/fvmatrix.py:325-394 (symmetric elimination)."""
+        """core/fvmatrix.py:325-394 (symmetric elimination).  With
+        differentiable coefficients or values the eliminated matrix also
+        carries the elimination as device tensor algebra, so gradients reach
+        the coefficients and the prescribed values."""
         n = int(cells.numel())
         if n == 0:
             return self
@@ -279,6 +306,13 @@ class FvMatrix:
             ptr(scratch), s,
         )
         res._ffc = self._ffc
+        values_grad = isinstance(values, torch.Tensor) and values.requires_grad
+        if torch.is_grad_enabled() and (self.requires_grad or values_grad):
+            diag, upper, lower, source = self.autograd_tensors()
+            src = source.reshape(g.num_cells, nc)
+            vals_t = torch.as_tensor(values, dtype=torch.float64, device=g.device).reshape(n, nc)
+            d2, up2, lo2, src2 = fixed_values_ldu(g, diag, upper, lower, src, cells.to(g.device).long(), vals_t)
+            res._ad = {"diag": d2, "upper": up2, "lower": lo2, "source": src2.reshape(source.shape)}
         return res
 
     def as_transpose(self) -> "FvMatrix":

@@ -221,19 +221,9 @@ class DifferentiableSimpleIteration:
         """fvmatrix.py:325-394 (symmetric elimination) on LDU tensors."""
         if cells.numel() == 0:
             return diag, upper, lower, source
-        fixed = torch.zeros(self.C, dtype=torch.bool, device=diag.device)
-        fixed[cells] = True
-        prescribed = torch.zeros_like(source).index_copy(0, cells, values)
-        unit = torch.where(diag.sum() < 0, -torch.ones_like(diag), torch.ones_like(diag))
-        cdiag = torch.where(diag != 0, diag, unit)
-        d2 = torch.where(fixed, cdiag, diag)
-        conn = fixed[self.own] | fixed[self.nei]
-        up2 = torch.where(conn, torch.zeros_like(upper), upper)
-        lo2 = torch.where(conn, torch.zeros_like(lower), lower)
-        pn, po = prescribed[self.nei], prescribed[self.own]
-        src = source.index_add(0, self.own, -upper[:, None] * pn).index_add(0, self.nei, -lower[:, None] * po)
-        src = src.index_copy(0, cells, cdiag[cells][:, None] * values)
-        return d2, up2, lo2, src
+        from gridfoam_b200.core.fvmatrix import fixed_values_ldu
+
+        return fixed_values_ldu(self.grid, diag, upper, lower, source, cells, values)
 
     def _solve(self, solver, field, diag, upper, lower, source, x0, symmetric):
         from gridfoam_b200.core.fvmatrix import FvMatrix

@@ -341,7 +341,7 @@ def operator_dumps(grid: AxisProjectedGrid, algo) -> dict:
 
 
 
-ADJOINT_CASES = ("cavity8", "cavity_oct", "cavity_oct_harmonic")
+ADJOINT_CASES = ("cavity8", "cavity_oct", "cavity_oct_harmonic", "ibplane")
 
 
 def adjoint_case(name: str) -> dict:

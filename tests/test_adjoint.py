@@ -96,7 +96,7 @@ def test_krylov_adjoint_gradcheck(kind, symmetric, seed):
     assert torch.autograd.gradcheck(solve_fn, inputs, eps=1e-6, atol=1e-4, rtol=1e-3, fast_mode=True)
 
 
-@pytest.mark.parametrize("name", ["cavity8", "cavity_oct", "cavity_oct_harmonic"])
+@pytest.mark.parametrize("name", ["cavity8", "cavity_oct", "cavity_oct_harmonic", "ibplane"])
 def test_gradients_match_reference_autograd(name):
     from gridfoam_b200.core.equation import equation
     from gridfoam_b200.fv import fvm

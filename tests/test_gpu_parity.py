@@ -794,3 +794,30 @@ def test_split_cg_graph_loop_matches_captured_form():
     assert 0 < loops[0] < 500 and loops[0] == loops[1] == loops[2]
     assert int(stats[0, 2]) == loops[2]
     assert torch.equal(x_loop, x_cap)
+
+
+def test_inlet_outlet_constraints_track_flow_reversal():
+    """inletOutlet on near immersed faces constrains their cells only while
+    the faces carry inflow (boundary_ops.py:440-535; the reference's
+    tests/integration/fv/test_immersed_dirichlet.py flow-reversal case):
+    no cells with outflow everywhere, the oracle's selection with inflow,
+    none again after the reversal."""
+    import oracle.case as oc
+    from tests.golden.oracle_harness import oracle_case
+
+    _, _, grid, algo = device_case("ibplane_io")
+    _, _, ocase, oalgo = oracle_case("ibplane_io")
+    F, Fb = grid.num_internal_faces, grid.num_domain_bnd_faces
+    phi = grid.get_facefield("phi")
+    counts = []
+    for flux in (1.0, -1.0, 1.0):
+        with torch.no_grad():
+            phi.store[0, F + Fb:] = flux
+        cells, faces, mask = algo.U.table.constraints()
+        counts.append(int(cells.numel()))
+        assert int(mask.sum()) == counts[-1]
+        oalgo.phi.immersed_upper[:] = flux
+        oalgo.phi.immersed_lower[:] = flux
+        ocells, _ = oc.immersed_dirichlet_constraints(oalgo.U)
+        assert np.array_equal(np.sort(to_np(cells).astype(np.int64)), np.sort(ocells))
+    assert counts[0] == 0 and counts[1] > 0 and counts[2] == 0
