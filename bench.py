@@ -604,7 +604,8 @@ def bluff_variant(args, local: int, torch) -> dict:
         "ms_per_iteration": ms / args.steps,
         "last_p_iterations": [s.iterations for s in algo.last_stats["p"]],
         "Cd_after_all_iterations": float(r.force[0] / (0.5 * area)),
-        "note": "forward only: the shape gradient of the drag is not built",
+        "note": "forward; the drag's shape gradient runs on the uniform channel (bluff_body_shape_gradient), "
+                "the octree's is not built",
     }
     del algo, grid
     torch.cuda.empty_cache()

@@ -248,10 +248,6 @@ int gf_laplacian_adjoint(const gf_mesh_t* m, const gf_assembly_t* a, const doubl
         set_error("gf_laplacian_adjoint: invalid arguments");
         return GF_ERR_INVALID;
     }
-    if (a->lap_harmonic) {
-        set_error("gf_laplacian_adjoint: harmonic interpolation has no adjoint here");
-        return GF_ERR_INVALID;
-    }
     k_laplacian_adjoint<<<grid_for(m->n_cells), kThreads, 0, GF_STREAM(stream)>>>(*m, *a, g_diag, g_upper, g_lower,
                                                                                   g_source, g_gamma);
     return check_launch("gf_laplacian_adjoint");
