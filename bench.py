@@ -139,10 +139,11 @@ def pcg_bytes_setup(C: int, F: int, s: int = 8) -> float:
 
 
 # Measured DRAM bytes (read + write) per cell per iteration of the pressure
-# CG on the cylinder-wake octree, from ncu captures of fixed-length launches
-# on the 192x120x24 base (1,729,632 cells; the working set exceeds L2, so
-# the traffic grows in proportion to the cells).
-PCG_DRAM_BYTES_PER_CELL_ITER = None
+# CG on the cylinder-wake octree: one k_cgs_a (189.9 MB) plus one k_cgs_b
+# (75.1 MB) launch of the split CG in an ncu capture on the 192x120x24 base
+# (1,729,632 cells; the working set exceeds L2, so the traffic grows in
+# proportion to the cells), against 159.8 B of the byte model.
+PCG_DRAM_BYTES_PER_CELL_ITER = 153.2
 
 
 def _oracle_threads() -> int:
@@ -661,10 +662,12 @@ def run_gpu(args) -> None:
     gl.clear_launches()
     gl.TRACK_DEFERRED = True
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("timed_steps")  # for profilers' range filters
     start.record()
     for _ in range(args.steps):
         algo.step()
     stop.record()
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     launches = gl.launch_total()
     gl.TRACK_DEFERRED = False
