@@ -3752,6 +3752,7 @@ __device__ void bicgstab_body(const gf_krylov_t& K, int vb, int vn) {
 // kernels are enqueued without a host synchronisation; once the stopping
 // test has passed the remaining ones return at once.
 constexpr int kSplitVariant = 19;
+constexpr int kSplitVariants = 4;
 constexpr int kSplitThreads = 256;
 
 struct SplitScalars {  // in the control block, after KCtl
@@ -3941,7 +3942,7 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_a(gf_krylov_t K, Ro
 }
 
 // x += alpha p; r -= alpha q; z = M r; partials of |r| and r.z.
-template <int MINB, bool LOOP>
+template <int MINB, bool LOOP, bool PAIRS>
 __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_b(gf_krylov_t K, int it, int p_is_b) {
     SplitScalars* S = split_scalars(K);
     if (*(volatile int*)&S->done) return;
@@ -3958,14 +3959,45 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_b(gf_krylov_t K, in
     const double alpha = S->rz[it & 1] / red[0];
     const double* p = p_is_b ? v.pb : v.pa;
     double loc[2] = {0.0, 0.0};
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-        __stcg(K.x + c, __ldcg(K.x + c) + alpha * __ldcg(p + c));
-        const double rk = __ldcg(v.r + c) - alpha * __ldcg(v.q + c);
-        const double zk = inv_diag(K.diag, c, jac) * rk;
-        __stcg(v.r + c, rk);
-        __stcg(v.z + c, zk);
-        loc[0] = norm_acc(loc[0], rk, linf);
-        loc[1] += rk * zk;
+    // Pairs of cells with 16-byte loads and stores where every vector is
+    // 16-byte aligned (the workspace vectors are when n is even): half the
+    // memory instructions of the streaming update.
+    const bool pairs = PAIRS && (n & 1) == 0 &&
+                       ((reinterpret_cast<uintptr_t>(K.x) | reinterpret_cast<uintptr_t>(K.diag)) & 15u) == 0;
+    if (pairs) {
+        const int n2 = n >> 1;
+        double2* x2 = reinterpret_cast<double2*>(K.x);
+        const double2* p2 = reinterpret_cast<const double2*>(p);
+        double2* r2 = reinterpret_cast<double2*>(v.r);
+        const double2* q2 = reinterpret_cast<const double2*>(v.q);
+        double2* z2 = reinterpret_cast<double2*>(v.z);
+        const double2* d2 = reinterpret_cast<const double2*>(K.diag);
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += gridDim.x * blockDim.x) {
+            const double2 xv = __ldcg(x2 + i), pv = __ldcg(p2 + i), rv = __ldcg(r2 + i), qv = __ldcg(q2 + i);
+            const double2 dv = __ldg(d2 + i);
+            const double r0 = rv.x - alpha * qv.x, r1 = rv.y - alpha * qv.y;
+            double i0 = 1.0, i1 = 1.0;
+            if (jac) {
+                i0 = fabs(dv.x) < 2.220446049250313e-16 ? 1.0 : 1.0 / dv.x;
+                i1 = fabs(dv.y) < 2.220446049250313e-16 ? 1.0 : 1.0 / dv.y;
+            }
+            const double z0 = i0 * r0, z1 = i1 * r1;
+            __stcg(x2 + i, make_double2(xv.x + alpha * pv.x, xv.y + alpha * pv.y));
+            __stcg(r2 + i, make_double2(r0, r1));
+            __stcg(z2 + i, make_double2(z0, z1));
+            loc[0] = norm_acc(norm_acc(loc[0], r0, linf), r1, linf);
+            loc[1] += r0 * z0 + r1 * z1;
+        }
+    } else {
+        for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+            __stcg(K.x + c, __ldcg(K.x + c) + alpha * __ldcg(p + c));
+            const double rk = __ldcg(v.r + c) - alpha * __ldcg(v.q + c);
+            const double zk = inv_diag(K.diag, c, jac) * rk;
+            __stcg(v.r + c, rk);
+            __stcg(v.z + c, zk);
+            loc[0] = norm_acc(loc[0], rk, linf);
+            loc[1] += rk * zk;
+        }
     }
     split_partial<2>(loc, linf ? 1u : 0u, v.p2);
 }
@@ -4086,7 +4118,7 @@ static int split_loop_exec(const void* fa, const void* fb, const gf_krylov_t& K,
     return GF_OK;
 }
 
-template <class Rows, int MINB>
+template <class Rows, int MINB, bool PAIRS>
 static int launch_split_rows(const gf_krylov_t* k, const Rows& rows, cudaStream_t st) {
     int dev = 0, sms = 0, per_sm = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -4124,7 +4156,7 @@ static int launch_split_rows(const gf_krylov_t* k, const Rows& rows, cudaStream_
     if (split_graph_enabled() && cudaStreamIsCapturing(st, &cap) == cudaSuccess &&
         cap == cudaStreamCaptureStatusNone) {
         cudaGraphExec_t exec = nullptr;
-        const int rc = split_loop_exec((const void*)k_cgs_a<Rows, MINB, true>, (const void*)k_cgs_b<MINB, true>, K,
+        const int rc = split_loop_exec((const void*)k_cgs_a<Rows, MINB, true>, (const void*)k_cgs_b<MINB, true, PAIRS>, K,
                                        &rows, sizeof(Rows), g, &exec);
         if (rc != GF_OK) return rc;
         e = cudaGraphLaunch(exec, st);
@@ -4137,7 +4169,7 @@ static int launch_split_rows(const gf_krylov_t* k, const Rows& rows, cudaStream_
     for (int it = 1; it <= k->max_iter; ++it) {
         // p_old is pa at odd iterations (p_new then goes to pb), pb at even.
         k_cgs_a<Rows, MINB, false><<<g, kSplitThreads, 0, st>>>(K, rows, it, it & 1, 0);
-        k_cgs_b<MINB, false><<<g, kSplitThreads, 0, st>>>(K, it, it & 1);
+        k_cgs_b<MINB, false, PAIRS><<<g, kSplitThreads, 0, st>>>(K, it, it & 1);
     }
     k_cgs_a<Rows, MINB, false><<<g, kSplitThreads, 0, st>>>(K, rows, k->max_iter + 1, (k->max_iter + 1) & 1, 0);
     e = cudaGetLastError();
@@ -4148,7 +4180,7 @@ static int launch_split_rows(const gf_krylov_t* k, const Rows& rows, cudaStream_
     return GF_OK;
 }
 
-template <int MINB>
+template <int MINB, bool PAIRS>
 static int launch_split_m(const gf_krylov_t* k, void* stream) {
     const int64_t row_span = (int64_t)(k->stride_y > 0 ? 6 : (k->width > 6 ? k->width : 6)) * k->n;
     if (row_span >= ((int64_t)1 << 31)) {
@@ -4158,23 +4190,29 @@ static int launch_split_m(const gf_krylov_t* k, void* stream) {
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     if (k->stride_y > 0) {
         if (k->symmetric)
-            return launch_split_rows<BoxRows<double, true, false, int>, MINB>(
+            return launch_split_rows<BoxRows<double, true, false, int>, MINB, PAIRS>(
                 k, BoxRows<double, true, false, int>{k->val, (int)k->n, (int)k->stride_y, (int)k->stride_z}, st);
-        return launch_split_rows<BoxRows<double, false, false, int>, MINB>(
+        return launch_split_rows<BoxRows<double, false, false, int>, MINB, PAIRS>(
             k, BoxRows<double, false, false, int>{k->val, (int)k->n, (int)k->stride_y, (int)k->stride_z}, st);
     }
     // One slot at a time (the loop of a plain SpMV): the occupancy, not the
     // loads of one thread, keeps the memory system busy.
     if (k->width == 6)
-        return launch_split_rows<EllRows<double, 6, int, 1>, MINB>(
+        return launch_split_rows<EllRows<double, 6, int, 1>, MINB, PAIRS>(
             k, EllRows<double, 6, int, 1>{k->val, k->nbr, (int)k->n, k->width, k->row_len}, st);
-    return launch_split_rows<EllRows<double, 0, int, 1>, MINB>(
+    return launch_split_rows<EllRows<double, 0, int, 1>, MINB, PAIRS>(
         k, EllRows<double, 0, int, 1>{k->val, k->nbr, (int)k->n, k->width, k->row_len}, st);
 }
 
-// Variant 19: 8 blocks of 256 threads an SM; 20: 6 (more registers).
+// Variant 19: 8 blocks of 256 threads an SM; 20: 6 (more registers);
+// 21: 8 with the update kernel on pairs of cells; 22: 7, pairs.
 static int launch_split(const gf_krylov_t* k, void* stream, int which) {
-    return which == 1 ? launch_split_m<6>(k, stream) : launch_split_m<8>(k, stream);
+    switch (which) {
+        case 1: return launch_split_m<6, false>(k, stream);
+        case 2: return launch_split_m<8, true>(k, stream);
+        case 3: return launch_split_m<7, true>(k, stream);
+        default: return launch_split_m<8, false>(k, stream);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -4675,7 +4713,7 @@ int gf_pcg_solve(const gf_krylov_t* k, void* stream) {
                 const int st = launch_stream(k, stream, k->variant - kStreamVariant);
                 if (st != GF_ERR_INVALID) return st;
             }
-            if (k->variant == kSplitVariant || k->variant == kSplitVariant + 1) {
+            if (k->variant >= kSplitVariant && k->variant < kSplitVariant + kSplitVariants) {
                 const int st = launch_split(k, stream, k->variant - kSplitVariant);
                 if (st != GF_ERR_INVALID) return st;
             }

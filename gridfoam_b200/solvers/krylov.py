@@ -53,7 +53,7 @@ def default_variant(n: int, mixed: bool, symmetric: bool, box: bool = True) -> i
     q-recurrence form at 64^3); then, up to ~1.3M cells, the q-recurrence
     form (q = A z + beta q, z alone gathered; 14.7 us at 1M cells); above
     that the shared-memory tiled kernel for symmetric boxes, else the split
-    CG (two plain kernels an iteration).  FP32-inner (mixed) solves: 256-thread register
+    CG (two plain kernels an iteration, variant 21).  FP32-inner (mixed) solves: 256-thread register
     blocks below ~32K cells (6.5 us an inner iteration at 24^3, as for the
     shared-memory forms); then, up to ~1.3M cells, the single-reduction
     form with the halo sync (6.7 against 7.0 us for the q-recurrence form
@@ -69,10 +69,12 @@ def default_variant(n: int, mixed: bool, symmetric: bool, box: bool = True) -> i
     if n <= 1300000:
         return 8
     # Above ~1.3M cells (beyond L2): the staged tiles on symmetric boxes;
-    # on other rows the split CG, two plain kernels an iteration (160.7
-    # against 170.4 us for the 256-thread register kernel on the 4.08M-cell
-    # cylinder-wake octree).
-    return 5 if symmetric and box else 19
+    # on other rows the split CG, two plain kernels an iteration, its update
+    # kernel on pairs of cells (fixed 100 iterations on the 4.08M-cell
+    # cylinder-wake octree: 161.3 us an iteration, against 163.0 with the
+    # update one cell at a time and 164.5 for the 512-thread persistent
+    # kernel).
+    return 5 if symmetric and box else 21
 
 
 class DeviceKrylov(LinearSolver):
@@ -125,7 +127,7 @@ class DeviceKrylov(LinearSolver):
             ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
             ev[0].record()
         call("gf_bicgstab_solve" if self.bicgstab else "gf_pcg_solve", ctypes.byref(k), stream_ptr())
-        split = k.variant in (19, 20) and not self.bicgstab and not k.mixed and nc == 1 and not k.single_reduction
+        split = k.variant in (19, 20, 21, 22) and not self.bicgstab and not k.mixed and nc == 1 and not k.single_reduction
         graph_loop = split and _split_graph_loop()
         if split and not graph_loop:
             # inside a stream capture the split CG enqueues an initial

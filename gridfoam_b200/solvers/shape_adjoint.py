@@ -35,8 +35,8 @@ algorithms/utils/pressure_correction.py:68-363) term by term, and
 ``DifferentiableSimpleIteration.check`` compares one forward evaluation with
 the library's own SIMPLE step.
 
-Scope: uniform grids (no hanging faces) with immersed bodies, steady SIMPLE
-or SIMPLEC, upwind convection, least-squares gradients, velocity conditions
+Scope: uniform and octree grids (hanging-face offset and skewness terms)
+with immersed bodies, steady SIMPLE or SIMPLEC, upwind convection, least-squares gradients, velocity conditions
 dirichlet / neumann / slip / inlet_outlet, pressure conditions dirichlet /
 neumann, a pressure outlet (no adjustPhi, no reference cell) and no
 pressure constraints at immersed faces.
@@ -69,8 +69,6 @@ def _check_supported(algo) -> None:
     g = algo.grid
     if not isinstance(algo, SIMPLE):
         raise NotImplementedError("the shape adjoint differentiates steady SIMPLE solutions")
-    if g.num_hanging:
-        raise NotImplementedError("the shape adjoint covers grids without hanging faces")
     sim = g.sim_config
     if schemes.div_scheme(sim, algo.phi.name, algo.U.name).value != "upwind":
         raise NotImplementedError("the shape adjoint covers upwind convection")
@@ -163,6 +161,20 @@ class DifferentiableSimpleIteration:
         self.u_uncovered = torch.as_tensor(uncov, device=dev)
         self.u_cells = algo.u_cells.long()
         self.u_faces = algo.u_faces.long()
+        # Hanging (coarse-fine) faces, as positions among the single faces:
+        # offset of the face centre from the linear-weight point and the
+        # tangential moves from each cell centre (face_geometry.py:141-162).
+        hf = np.asarray(h.extra["hang_faces"], dtype=np.int64)
+        self.H = int(hf.size)
+        if self.H:
+            pos = np.full(self.F, -1, dtype=np.int64)
+            pos[s] = np.arange(s.size)
+            self.hpos = torch.as_tensor(pos[hf], device=dev)
+            self.hoff = torch.as_tensor(np.asarray(h.extra["hang_offset"]), **f64)
+            self.hmo = torch.as_tensor(np.asarray(h.extra["hang_move_o"]), **f64)
+            self.hmn = torch.as_tensor(np.asarray(h.extra["hang_move_n"]), **f64)
+            self.u_corrected = bool(algo._u_corrected)
+            self.p_corrected = bool(algo._p_corrected)
         self.u_solver = BiCGSTABSolver(_tight("bicgstab"))
         self.p_solver = CGSolver(_tight("cg"))
 
@@ -202,6 +214,22 @@ class DifferentiableSimpleIteration:
         vgc = torch.where(active, frac / safe, torch.zeros_like(frac))
         covered = kind != codes["none"]
         return frac, refv, refg, psib, vgc, covered
+
+    def _hang_sn(self, grad):
+        """face_interpolation.py:99-145 on the hanging faces:
+        delta (grad_N . move_N - grad_O . move_O), ``grad [C, nc, 3]``."""
+        hp = self.hpos
+        o, n = self.own_s[hp], self.nei_s[hp]
+        gn = torch.einsum("hkj,hj->hk", grad[n], self.hmn)
+        go = torch.einsum("hkj,hj->hk", grad[o], self.hmo)
+        return self.delta_s[hp][:, None] * (gn - go)
+
+    def _hang_value(self, grad):
+        """face_interpolation.py:45-96: offset . (w grad_O + (1 - w) grad_N)."""
+        hp = self.hpos
+        w = self.w_s[hp][:, None, None]
+        gf = w * grad[self.own_s[hp]] + (1.0 - w) * grad[self.nei_s[hp]]
+        return torch.einsum("hkj,hj->hk", gf, self.hoff)
 
     def lsq_grad(self, psi, psib, covered, dist_b):
         """least_squares.py:29-101: single faces plus every conditioned
@@ -278,6 +306,13 @@ class DifferentiableSimpleIteration:
         cg = torch.where(cov, cond * (1.0 - f), torch.zeros_like(f))
         diag = diag + self._scatter(self.bcell, cv)
         source = source + self._scatter(self.bcell, cv[:, None] * refv + cg[:, None] * refg)
+        if self.H and self.u_corrected:
+            # laplacian.py:162-176: the explicit skewness source on hanging
+            # faces from the velocity's least-squares gradient
+            gU = self.lsq_grad(U, psib, cov, dist_b)
+            hp = self.hpos
+            hsrc = (self.nu * self.magSf_s[hp])[:, None] * self._hang_sn(gU)
+            source = source + self._scatter(self.own_s[hp], hsrc) - self._scatter(self.nei_s[hp], hsrc)
         # relaxation (fvmatrix relax): A/alpha, b + (1 - alpha)/alpha A U
         a = self.alpha_U
         source = source + ((1.0 - a) / a * diag)[:, None] * U
@@ -300,6 +335,12 @@ class DifferentiableSimpleIteration:
         # phiHbyA (flux.py:32-129): linear interpolation on single faces; the
         # boundary carries HbyA's cell value, U's value on non-assignable faces
         Hf = self.w_s[:, None] * HbyA[self.own_s] + (1.0 - self.w_s)[:, None] * HbyA[self.nei_s]
+        if self.H:
+            # fvc.interpolate(HbyA): HbyA carries no boundary conditions, so
+            # its least-squares gradient has internal equations only
+            none = torch.zeros(self.Nb, dtype=torch.bool, device=U.device)
+            gH = self.lsq_grad(HbyA, torch.zeros_like(HbyA[self.bcell]), none, dist_b)
+            Hf = Hf.index_add(0, self.hpos, self._hang_value(gH))
         phiH_s = (Hf * self.Sf_s).sum(1)
         _, _, _, Ub, _, _ = self.bc_state(self.ukind, self.uval, Us[self.bcell], phi_b, dist_b)
         flux_h = (HbyA[self.bcell] * self.bsf).sum(1)
@@ -313,6 +354,9 @@ class DifferentiableSimpleIteration:
             d_r = rAtU - rAU
             drf = self.w_s * d_r[self.own_s] + (1.0 - self.w_s) * d_r[self.nei_s]
             sn = self.delta_s * (p[self.nei_s] - p[self.own_s])
+            if self.H:
+                gp3 = self.lsq_grad(p2, ppsib, pcov, dist_b)
+                sn = sn.index_add(0, self.hpos, self._hang_sn(gp3)[:, 0])
             phiH_s = phiH_s + drf * self.magSf_s * sn
             ng = pvgc * (prefv[:, 0] - p[self.bcell]) + (1.0 - pf) * prefg[:, 0]
             ng = torch.where(pcov, ng, torch.zeros_like(ng))
@@ -333,11 +377,21 @@ class DifferentiableSimpleIteration:
         pcg = torch.where(pcov, pcond * (1.0 - pf), torch.zeros_like(pf))
         p_diag = p_diag + self._scatter(self.bcell, pcv)
         p_src = self._scatter(self.bcell, pcv * prefv[:, 0] + pcg * prefg[:, 0])
+        ffc = None
+        if self.H and self.p_corrected:
+            # the Laplacian's hanging skewness source from the pressure's
+            # least-squares gradient, also the matrix's face-flux correction
+            hp = self.hpos
+            gpl = self.lsq_grad(p2, ppsib, pcov, dist_b)
+            ffc = gam_f[hp] * self.magSf_s[hp] * self._hang_sn(gpl)[:, 0]
+            p_src = p_src + self._scatter(self.own_s[hp], ffc) - self._scatter(self.nei_s[hp], ffc)
         div = self._scatter(self.own_s, phiH_s) - self._scatter(self.nei_s, phiH_s) + self._scatter(self.bcell, phiH_b)
         p_src = p_src - div
         p_new = self._solve(self.p_solver, algo.p, p_diag, -p_up, -p_up, p_src[:, None], p2, symmetric=True)[:, 0]
         # flux correction (pressure_correction.py:270-305)
         phi_s_new = phiH_s - pc * (p_new[self.nei_s] - p_new[self.own_s])
+        if ffc is not None:
+            phi_s_new = phi_s_new.index_add(0, self.hpos, -ffc)
         pf2, prefv2, prefg2, _, pvgc2, pcov2 = self.bc_state(self.pkind, self.pval, p_new[:, None][self.bcell], phi_b,
                                                              dist_b)
         ng2 = pvgc2 * (prefv2[:, 0] - p_new[self.bcell]) + (1.0 - pf2) * prefg2[:, 0]
