@@ -557,15 +557,19 @@ class ShapeGradient:
 
 
 class exact_solves:
-    """Context: ``algo``'s Krylov solves converge to ``rtol`` (absolute
-    tolerance 0) instead of their configured tolerances.  A SIMPLE fixed
-    point reached with the configured ones satisfies the discrete steady
-    equations only to those tolerances (a solve whose initial residual is
-    below its absolute tolerance returns at once), which is not sharp enough
-    to difference; with exact solves the fixed point is the discrete
-    solution."""
+    """Context: ``algo``'s Krylov solves reduce their residual by ``rtol``
+    with no absolute tolerance, instead of their configured tolerances.  A
+    SIMPLE fixed point reached with the configured ones satisfies the
+    discrete steady equations only to those tolerances (a solve whose
+    initial residual is below its absolute tolerance returns at once), which
+    is not sharp enough to difference; without an absolute tolerance every
+    solve keeps reducing the residual, so the fixed point is the discrete
+    solution (a relative reduction per solve is enough, and cheaper than
+    solving each system to round-off; round-off-level tolerances also let
+    the pressure CG wander in the body's enclosed cells, whose block of the
+    system is singular)."""
 
-    def __init__(self, algo, rtol: float = 1e-13):
+    def __init__(self, algo, rtol: float = 1e-6):
         self.solvers = list(algo.solvers.values())
         self.rtol = rtol
 

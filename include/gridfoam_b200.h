@@ -213,7 +213,12 @@ typedef struct gf_krylov {
     int64_t stride_z;
     int32_t symmetric;    /* 1 (box only): A is symmetric, only + slots read */
     int32_t block_cap;    /* > 0: at most this many persistent blocks (tuning) */
-    int32_t variant;      /* CG launch shape (0..11, see gf_krylov.cu) */
+    int32_t variant;      /* CG launch shape (0..22, see gf_krylov.cu and
+                             solvers/autotune.py); 19..22: the split CG, two
+                             plain kernels an iteration, run as a CUDA graph
+                             while-loop on the stream (every permitted
+                             iteration enqueued inside a stream capture, or
+                             with the environment variable GF_SPLIT_GRAPH=0) */
     int32_t single_reduction; /* 1 (FP64 CG, one system): Chronopoulos-Gear
                              CG, one grid reduction per iteration; needs the
                              kind-0 workspace (7 vectors) */
