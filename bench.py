@@ -490,11 +490,10 @@ BLUFF_BASE = (256, 64, 48)
 
 def bluff_adjoint_variant(args, local: int, torch) -> dict:
     """The drag's shape gradient with respect to the body's 8 parameters on
-    the bluff body's channel as one uniform level (256x64x48 cells over
-    [-2, 6] x [-1, 1] x [0, 1.2], no hanging faces: the shape adjoint does
-    not cover octree hanging faces): the steady state converged with exact
-    solves, the fixed-point adjoint, and central differences (h = 1e-3) of
-    two parameters as a spot check."""
+    the bluff body's 4-level octree channel at base 128x32x24 (731,062
+    cells; the full base 256x64x48 is the forward variant): the steady state
+    converged with exact solves, the fixed-point adjoint, and central
+    differences at h = 1e-4 of two parameters as a spot check."""
     import numpy as np
 
     from gridfoam_b200.cases import bluff_body_case, create_case
@@ -502,11 +501,11 @@ def bluff_adjoint_variant(args, local: int, torch) -> dict:
     from gridfoam_b200.post.forces import patch_force
     from gridfoam_b200.solvers import shape_adjoint as sa
 
-    base = (256, 64, 48)
+    base = (128, 32, 24)
     theta = np.array(BLUFF_DEFAULT)
 
     def make(params):
-        return create_case(bluff_body_case(base, params=params, uniform=True), device=f"cuda:{local}")
+        return create_case(bluff_body_case(base, levels=3, params=params), device=f"cuda:{local}")
 
     def drag(grid, algo) -> float:
         return float(patch_force(grid, algo.p, algo.U, algo.nu, "body", 1.0, np.zeros(3)).force[0])
@@ -525,18 +524,17 @@ def bluff_adjoint_variant(args, local: int, torch) -> dict:
     state = (algo.U.data.detach().clone(), algo.p.data.detach().clone(), algo.phi.store[0].detach().clone())
     imm0, near0 = np.asarray(grid.host.imm_faces), np.asarray(grid.host.bnd_near)
     spot = {}
-    # (on this grid a 1e-3 change of length, height, the side-view rounding,
-    # slant length or clearance moves some segment crossing past a cell
-    # centre -- another discrete structure; width and the plan-view
-    # rounding do not)
+    # (on this mesh a 1e-4 change of the side-view rounding or the clearance
+    # moves some segment crossing past a cell centre -- another discrete
+    # structure; width and the plan-view rounding do not)
     for j in (1, 3):
         J, same = [], True
         for sign in (1.0, -1.0):
             th = theta.copy()
-            th[j] += sign * 1e-3
+            th[j] += sign * 1e-4
             _, gj, aj = make(th)
-            same &= np.array_equal(np.asarray(gj.host.imm_faces), imm0) and np.array_equal(
-                np.asarray(gj.host.bnd_near), near0)
+            same &= gj.num_cells == grid.num_cells and np.array_equal(np.asarray(gj.host.imm_faces), imm0) \
+                and np.array_equal(np.asarray(gj.host.bnd_near), near0)
             if not same:
                 break
             with torch.no_grad():
@@ -549,13 +547,14 @@ def bluff_adjoint_variant(args, local: int, torch) -> dict:
         if not same:
             spot[BLUFF_PARAMS[j]] = {"adjoint": float(g.grad[j]), "discrete_structure_unchanged": False}
             continue
-        fd = (J[0] - J[1]) / 2e-3
-        spot[BLUFF_PARAMS[j]] = {"fd_h1e-3": fd, "adjoint": float(g.grad[j]),
+        fd = (J[0] - J[1]) / 2e-4
+        spot[BLUFF_PARAMS[j]] = {"fd_h1e-4": fd, "adjoint": float(g.grad[j]),
                                  "rel": abs(fd - g.grad[j]) / abs(fd), "discrete_structure_unchanged": True}
     area = 0.39 * 0.29
     out = {
-        "workload": "bluff_body_256x64x48_uniform_simple_shape_gradient",
+        "workload": "bluff_body_128x32x24_l3_simple_shape_gradient",
         "cells": grid.num_cells,
+        "hanging_faces": grid.num_hanging,
         "immersed_faces": grid.num_immersed_faces,
         "drag": g.objective,
         "Cd": g.objective / (0.5 * area),
@@ -565,7 +564,6 @@ def bluff_adjoint_variant(args, local: int, torch) -> dict:
         "adjoint_sweeps": g.adjoint_sweeps,
         "adjoint_s": adjoint_s,
         "spot_check": spot,
-        "note": "uniform grid; the octree (hanging-face) shape adjoint is not built",
     }
     del algo, grid
     torch.cuda.empty_cache()
@@ -605,8 +603,7 @@ def bluff_variant(args, local: int, torch) -> dict:
         "ms_per_iteration": ms / args.steps,
         "last_p_iterations": [s.iterations for s in algo.last_stats["p"]],
         "Cd_after_all_iterations": float(r.force[0] / (0.5 * area)),
-        "note": "forward; the drag's shape gradient runs on the uniform channel (bluff_body_shape_gradient), "
-                "the octree's is not built",
+        "note": "forward; the drag's shape gradient: bluff_body_shape_gradient (same channel, base 128x32x24)",
     }
     del algo, grid
     torch.cuda.empty_cache()

@@ -263,7 +263,10 @@ class DifferentiableSimpleIteration:
         src = source[:, 0] if source.shape[1] == 1 else source
         M.source = src
         with torch.no_grad():
-            x = x0.detach().t().contiguous() if x0.shape[1] > 1 else x0.detach().reshape(1, -1).contiguous()
+            # a copy: the solve writes its solution into x, and the guess
+            # must stay the caller's (the scalar case would be a view)
+            x = (x0.detach().t() if x0.shape[1] > 1 else x0.detach().reshape(1, -1)).clone(
+                memory_format=torch.contiguous_format)
             solver.solve_arrays(self.grid, M.diag_store, M.val, M.source_store, x, symmetric=symmetric)
         sol = x[0] if source.shape[1] == 1 else x.t()
         if not torch.is_grad_enabled():
