@@ -3752,7 +3752,7 @@ __device__ void bicgstab_body(const gf_krylov_t& K, int vb, int vn) {
 // kernels are enqueued without a host synchronisation; once the stopping
 // test has passed the remaining ones return at once.
 constexpr int kSplitVariant = 19;
-constexpr int kSplitVariants = 4;
+constexpr int kSplitVariants = 6;
 constexpr int kSplitThreads = 256;
 
 struct SplitScalars {  // in the control block, after KCtl
@@ -4180,7 +4180,7 @@ static int launch_split_rows(const gf_krylov_t* k, const Rows& rows, cudaStream_
     return GF_OK;
 }
 
-template <int MINB, bool PAIRS>
+template <int MINB, bool PAIRS, int GRP = 1>
 static int launch_split_m(const gf_krylov_t* k, void* stream) {
     const int64_t row_span = (int64_t)(k->stride_y > 0 ? 6 : (k->width > 6 ? k->width : 6)) * k->n;
     if (row_span >= ((int64_t)1 << 31)) {
@@ -4200,17 +4200,20 @@ static int launch_split_m(const gf_krylov_t* k, void* stream) {
     if (k->width == 6)
         return launch_split_rows<EllRows<double, 6, int, 1>, MINB, PAIRS>(
             k, EllRows<double, 6, int, 1>{k->val, k->nbr, (int)k->n, k->width, k->row_len}, st);
-    return launch_split_rows<EllRows<double, 0, int, 1>, MINB, PAIRS>(
-        k, EllRows<double, 0, int, 1>{k->val, k->nbr, (int)k->n, k->width, k->row_len}, st);
+    return launch_split_rows<EllRows<double, 0, int, GRP>, MINB, PAIRS>(
+        k, EllRows<double, 0, int, GRP>{k->val, k->nbr, (int)k->n, k->width, k->row_len}, st);
 }
 
 // Variant 19: 8 blocks of 256 threads an SM; 20: 6 (more registers);
-// 21: 8 with the update kernel on pairs of cells; 22: 7, pairs.
+// 21: 8 with the update kernel on pairs of cells; 22: 7, pairs; 23: 7,
+// pairs, ELL slots loaded two at a time; 24: 6, pairs, four at a time.
 static int launch_split(const gf_krylov_t* k, void* stream, int which) {
     switch (which) {
         case 1: return launch_split_m<6, false>(k, stream);
         case 2: return launch_split_m<8, true>(k, stream);
         case 3: return launch_split_m<7, true>(k, stream);
+        case 4: return launch_split_m<7, true, 2>(k, stream);
+        case 5: return launch_split_m<6, true, 4>(k, stream);
         default: return launch_split_m<8, false>(k, stream);
     }
 }

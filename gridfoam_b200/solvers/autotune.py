@@ -32,7 +32,7 @@ from gridfoam_b200.meta.config import PrecisionType, PreconditionerType, SolverC
 # Variants 0-7 differ only in launch shape and memory placement (their
 # iterates differ by the order of the dot-product partial sums); 8 and 9
 # form q = A p by recurrence.
-N_VARIANTS = 23
+N_VARIANTS = 25
 VARIANTS = {
     0: "256 threads x 1 cell/pass",
     1: "256 threads x 2 cells/pass",
@@ -57,6 +57,8 @@ VARIANTS = {
     20: "split: two plain kernels an iteration (no grid barrier), 256 threads x 6 a SM (FP64, large systems)",
     21: "split, update kernel on pairs of cells (16-byte accesses), 256 threads x 8 a SM (FP64, large systems)",
     22: "split, update kernel on pairs of cells (16-byte accesses), 256 threads x 7 a SM (FP64, large systems)",
+    23: "split, pairs, ELL slots loaded two at a time, 256 threads x 7 a SM (FP64, large systems)",
+    24: "split, pairs, ELL slots loaded four at a time, 256 threads x 6 a SM (FP64, large systems)",
 }
 
 _LOCK = threading.Lock()
@@ -147,7 +149,7 @@ def time_variant(grid, diag, val, rhs, *, symmetric: bool, mixed: bool, variant:
     return best, its
 
 
-SPLIT_VARIANTS = (19, 20, 21, 22)
+SPLIT_VARIANTS = (19, 20, 21, 22, 23, 24)
 # The persistent single-launch variants: the ones a captured CUDA graph
 # holds as one kernel node (the split CG, 19 and 20, enqueues every
 # permitted iteration when it is captured).

@@ -19,6 +19,7 @@ from gridfoam_b200 import _lib
 from gridfoam_b200._lib import LAUNCHES, GfKrylov, call, load, ptr, stream_ptr
 from gridfoam_b200.meta.config import NormType, PrecisionType, PreconditionerType, SolverConfig
 from gridfoam_b200.solvers.adjoint import attach_implicit_adjoint
+from gridfoam_b200.solvers.autotune import SPLIT_VARIANTS
 from gridfoam_b200.solvers.base import LinearSolver, SolveResult, SolveStats, _StatsBuffer
 
 def workspace(cache: dict, device: torch.device, n: int, ncomp: int, kind: int) -> torch.Tensor:
@@ -127,7 +128,7 @@ class DeviceKrylov(LinearSolver):
             ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
             ev[0].record()
         call("gf_bicgstab_solve" if self.bicgstab else "gf_pcg_solve", ctypes.byref(k), stream_ptr())
-        split = k.variant in (19, 20, 21, 22) and not self.bicgstab and not k.mixed and nc == 1 and not k.single_reduction
+        split = k.variant in SPLIT_VARIANTS and not self.bicgstab and not k.mixed and nc == 1 and not k.single_reduction
         graph_loop = split and _split_graph_loop()
         if split and not graph_loop:
             # inside a stream capture the split CG enqueues an initial

@@ -705,7 +705,7 @@ def test_grad_linear_steps_and_operator_match_reference(name):
     _check(fvc.grad(algo.U).data, golden["op_grad_U"], "grad_U", 1e-10)
 
 
-@pytest.mark.parametrize("variant", [15, 16, 17, 18, 19, 20, 21, 22])
+@pytest.mark.parametrize("variant", [15, 16, 17, 18, 19, 20, 21, 22, 23, 24])
 def test_lean_ell_cg_fixed_iterations_match_register_kernel(variant):
     """The lean ELL CG (32-bit indices, x update moved into the next gather
     pass) against the register kernel: exactly 60 iterations agree up to the
