@@ -206,11 +206,17 @@ class DeviceKrylov(LinearSolver):
     def solve(self, eq) -> SolveResult:
         """solvers/base.py:96-122: with ``grad_mode="adjoint"`` (default) and
         differentiable coefficients, the solve is detached and the implicit
-        adjoint attached; the device path has no unrolled mode."""
+        adjoint attached; with ``"unrolled"`` the iterations run as
+        differentiable device tensor algebra (``solvers/unrolled.py``)."""
         A = eq.fv_matrix
         if torch.is_grad_enabled() and A.requires_grad:
+            if self.grad_mode == "unrolled":
+                from gridfoam_b200.solvers.unrolled import solve_unrolled
+
+                sol, stats = solve_unrolled(self, A, A.source, eq.target.data.detach())
+                return SolveResult(solution=sol, stats=stats)
             if self.grad_mode != "adjoint":
-                raise NotImplementedError("the device solvers differentiate by the implicit adjoint only")
+                raise ValueError(f"unknown grad_mode {self.grad_mode!r}")
             with torch.no_grad():
                 res = self._solve_primal(eq)
             sol = attach_implicit_adjoint(A, res.solution, solve_transpose=self.solve_transpose)

@@ -341,7 +341,7 @@ def operator_dumps(grid: AxisProjectedGrid, algo) -> dict:
 
 
 
-ADJOINT_CASES = ("cavity8", "cavity_oct", "cavity_oct_harmonic", "ibplane")
+ADJOINT_CASES = ("cavity8", "cavity_oct", "cavity_oct_harmonic", "ibplane", "cavity8_unrolled")
 
 
 def adjoint_case(name: str) -> dict:
@@ -354,7 +354,8 @@ def adjoint_case(name: str) -> dict:
       ``div(phi, U) - laplacian(nu_eff, U) + V/dt``, gradient in ``nu_eff``.
     """
     harmonic = name.endswith("_harmonic")
-    base = name[: -len("_harmonic")] if harmonic else name
+    unrolled = name.endswith("_unrolled")
+    base = name[: -len("_harmonic")] if harmonic else name[: -len("_unrolled")] if unrolled else name
     case = ALL_CASES[base]()
     if harmonic:
         case["simulator"]["fvSchemes"]["laplacianSchemes"] = {"default": "Gauss harmonic corrected"}
@@ -404,6 +405,37 @@ def adjoint_case(name: str) -> dict:
     out.update(adj_nu=nu.detach().numpy().copy(), adj_usrc=usrc.numpy().copy(), adj_r3=r3.numpy().copy(),
                adj_u=u.detach().numpy().copy(), adj_grad_nu=nu.grad.numpy().copy(),
                adj_phi=packed(phi))
+    if unrolled:
+        # grad_mode="unrolled" (solvers/base.py:111-115): gradients through
+        # the iterations that ran, loose tolerances so the difference from
+        # the implicit adjoint shows
+        g2 = torch.from_numpy(out["adj_gamma"]).requires_grad_(True)
+        pm = -fvm.laplacian(g2, p)
+        pm.source = pm.source - src * grid.cell_volumes
+        if needs_reference_value(p):
+            set_reference_value(pm, 0, 0.0)
+        with torch.no_grad():
+            p.data.zero_()
+        cgu = CGSolver(SolverConfig.model_validate(
+            {"method": "cg", "preconditioner": "jacobi", "tolerance": 0.0, "rel_tolerance": 1e-3,
+             "max_iter": 5000}))
+        cgu.grad_mode = "unrolled"
+        xu = cgu.solve(equation(p, pm)).solution
+        (r * xu).sum().backward()
+        n2 = torch.from_numpy(out["adj_nu"]).requires_grad_(True)
+        um = fvm.div(phi, U) - fvm.laplacian(n2, U)
+        um.diag = um.diag + grid.cell_volumes / 0.01
+        um.source = um.source + usrc * grid.cell_volumes[:, None]
+        with torch.no_grad():
+            U.data.zero_()
+        biu = BiCGSTABSolver(SolverConfig.model_validate(
+            {"method": "bicgstab", "preconditioner": "jacobi", "tolerance": 0.0, "rel_tolerance": 1e-3,
+             "max_iter": 5000}))
+        biu.grad_mode = "unrolled"
+        uu = biu.solve(equation(U, um)).solution
+        (r3 * uu).sum().backward()
+        out.update(unr_x=xu.detach().numpy().copy(), unr_grad_gamma=g2.grad.numpy().copy(),
+                   unr_u=uu.detach().numpy().copy(), unr_grad_nu=n2.grad.numpy().copy())
     return out
 
 

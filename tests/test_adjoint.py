@@ -29,6 +29,10 @@ pytestmark = pytest.mark.gpu
 HERE = pathlib.Path(__file__).resolve().parent / "golden"
 
 
+def rel(a, b) -> float:
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(np.asarray(b)), 1e-300))
+
+
 @pytest.fixture(autouse=True)
 def _cuda():
     if not torch.cuda.is_available():
@@ -262,3 +266,47 @@ def test_piso_gradient_through_steps_matches_central_differences(checkpoint_ever
     fd = (J(nu0 + h) - J(nu0 - h)) / (2 * h)
     assert abs(res.objective - J(nu0)) <= 1e-12 * abs(res.objective)
     assert abs(res.grad_nu - fd) <= 1e-4 * abs(fd), (res.grad_nu, fd)
+
+
+def test_unrolled_gradients_match_reference_autograd():
+    """grad_mode="unrolled" (solvers/base.py:111-115): gradients through the
+    CG and BiCGStab iterations that ran (relative tolerance 1e-3, so they
+    differ from the implicit adjoint's by 6 % and 0.1 %), against the
+    reference's own unrolled run on the same inputs."""
+    from gridfoam_b200.core.equation import equation
+    from gridfoam_b200.fv import fvm
+    from gridfoam_b200.meta.config import SolverConfig
+    from gridfoam_b200.solvers.krylov import BiCGSTABSolver, CGSolver
+
+    ref = np.load(HERE / "adjoint_cavity8_unrolled.npz")
+    grid, algo = _state("cavity8")
+    U, p, phi = algo.U, algo.p, algo.phi
+    dev = dict(dtype=torch.float64, device="cuda")
+    loose = dict(preconditioner="jacobi", tolerance=0.0, rel_tolerance=1e-3, max_iter=5000)
+
+    gamma = torch.as_tensor(ref["adj_gamma"], **dev).requires_grad_(True)
+    pmat = -fvm.laplacian(gamma, p)
+    pmat.source = pmat.source - torch.as_tensor(ref["adj_src"], **dev) * grid.cell_volumes
+    if algo.p_needs_ref:
+        d = pmat.diag
+        pmat.diag = d + torch.nn.functional.one_hot(torch.tensor(0), grid.num_cells).cuda() * d[0]
+    p.data = torch.zeros(grid.num_cells, **dev)
+    cg = CGSolver(SolverConfig(method="cg", **loose))
+    cg.grad_mode = "unrolled"
+    res = cg.solve(equation(p, pmat))
+    (torch.as_tensor(ref["adj_r"], **dev) * res.solution).sum().backward()
+    assert rel(to_np(res.solution), ref["unr_x"]) < 1e-10
+    assert rel(to_np(gamma.grad), ref["unr_grad_gamma"]) < 1e-8
+    assert rel(to_np(gamma.grad), ref["adj_grad_gamma"]) > 1e-3  # not the implicit adjoint's
+
+    nu = torch.as_tensor(ref["adj_nu"], **dev).requires_grad_(True)
+    umat = fvm.div(phi, U) - fvm.laplacian(nu, U)
+    umat.diag = umat.diag + grid.cell_volumes / 0.01
+    umat.source = umat.source + torch.as_tensor(ref["adj_usrc"], **dev) * grid.cell_volumes[:, None]
+    U.data = torch.zeros((grid.num_cells, 3), **dev)
+    bi = BiCGSTABSolver(SolverConfig(method="bicgstab", **loose))
+    bi.grad_mode = "unrolled"
+    res = bi.solve(equation(U, umat))
+    (torch.as_tensor(ref["adj_r3"], **dev) * res.solution).sum().backward()
+    assert rel(to_np(res.solution), ref["unr_u"]) < 1e-10
+    assert rel(to_np(nu.grad), ref["unr_grad_nu"]) < 1e-8
