@@ -56,7 +56,7 @@ def _jacobi(diag: torch.Tensor, kind) -> torch.Tensor | None:
 
 
 def _norm(r: torch.Tensor, linf: bool) -> torch.Tensor:
-    return torch.linalg.vector_norm(r, ord=float("inf") if linf else 2)
+    return torch.linalg.vector_norm(r.detach(), ord=float("inf") if linf else 2)
 
 
 def _cg(A, b, x, inv, s) -> tuple[torch.Tensor, list[float]]:
@@ -93,8 +93,8 @@ def _bicgstab(A, b, x, inv, s) -> tuple[torch.Tensor, list[float]]:
         return v if inv is None else inv * v
 
     def tol(u=None, v=None):
-        un = 1.0 if u is None else float(torch.linalg.vector_norm(u))
-        vn = 1.0 if v is None else float(torch.linalg.vector_norm(v))
+        un = 1.0 if u is None else float(torch.linalg.vector_norm(u.detach()))
+        vn = 1.0 if v is None else float(torch.linalg.vector_norm(v.detach()))
         return 1e-6 * un * vn
 
     def restart(r):
@@ -112,7 +112,7 @@ def _bicgstab(A, b, x, inv, s) -> tuple[torch.Tensor, list[float]]:
         y = prec(p)
         v = A(y)
         den = torch.sum(r_hat * v)
-        if abs(float(den)) <= tol(r_hat, v):
+        if abs(float(den.detach())) <= tol(r_hat, v):
             if restarts >= s.max_restart:
                 status = GF_BREAKDOWN
                 break
@@ -127,7 +127,7 @@ def _bicgstab(A, b, x, inv, s) -> tuple[torch.Tensor, list[float]]:
         z = prec(s_vec)
         t = A(z)
         den_w = torch.sum(t * t)
-        if abs(float(den_w)) <= tol(t, t):
+        if abs(float(den_w.detach())) <= tol(t, t):
             if restarts >= s.max_restart:
                 status = GF_BREAKDOWN
                 break
@@ -135,7 +135,7 @@ def _bicgstab(A, b, x, inv, s) -> tuple[torch.Tensor, list[float]]:
             r_hat, p, rho_old = restart(r)
             continue
         omega = torch.sum(t * s_vec) / den_w
-        if abs(float(omega)) <= tol():
+        if abs(float(omega.detach())) <= tol():
             if restarts >= s.max_restart:
                 status = GF_BREAKDOWN
                 break
@@ -148,7 +148,7 @@ def _bicgstab(A, b, x, inv, s) -> tuple[torch.Tensor, list[float]]:
         if final < thresh:
             return x, [r0, final, it, 1, GF_OK]
         rho_new = torch.sum(r_hat * r)
-        if abs(float(rho_new)) <= tol(r_hat, r):
+        if abs(float(rho_new.detach())) <= tol(r_hat, r):
             if restarts >= s.max_restart:
                 status = GF_BREAKDOWN
                 break
