@@ -3738,6 +3738,387 @@ __device__ void bicgstab_body(const gf_krylov_t& K, int vb, int vn) {
 }
 
 // ---------------------------------------------------------------------------
+// Mixed precision BiCGStab: FP32 inner BiCGStab cycles inside FP64
+// iterative refinement, for all NC components in one launch.  Each cycle
+// starts from the true FP64 residual r = b - A x of every component (also
+// its stopping test, |r| < max(atol, rtol |r0|) as in FP64), runs the
+// reference's right-preconditioned BiCGStab (bicgstab_body, restarts
+// included) in FP32 on A e = r with FP64-accumulated dot products until its
+// recurrence residual falls below max(eta |r|, margin thresh), and folds
+// x += e in FP64.  The FP32 copies of the coefficients (every ELL slot and
+// the diagonal) and of the Jacobi inverse are made once per solve.
+// Workspace (after the header): (width + 2) n floats of coefficients and 7 NC
+// n floats of vectors (r, r_hat, p, v, s, t, e).
+template <int NC, int WIDTH, class G>
+__device__ __forceinline__ void row_apply32(const gf_krylov_t& K, const float* __restrict__ val32,
+                                            const float* __restrict__ diag32, int64_t c, const G& g,
+                                            float (&out)[NC]) {
+    const int64_t n = K.n;
+    const float d = __ldcg(diag32 + c);
+#pragma unroll
+    for (int k = 0; k < NC; ++k) out[k] = d * g(k, c);
+    const int W = WIDTH > 0 ? WIDTH : (K.row_len ? (int)__ldg(K.row_len + c) : K.width);
+    for (int s0 = 0; s0 < W; s0 += kSlotGroup) {
+        int nb[kSlotGroup];
+        float a[kSlotGroup];
+#pragma unroll
+        for (int j = 0; j < kSlotGroup; ++j) {
+            const int s = s0 + j;
+            nb[j] = s < W ? __ldg(K.nbr + s * n + c) : (int)c;
+            a[j] = s < W ? __ldcg(val32 + s * n + c) : 0.0f;
+        }
+#pragma unroll
+        for (int j = 0; j < kSlotGroup; ++j)
+            if (s0 + j < W)
+#pragma unroll
+                for (int k = 0; k < NC; ++k) out[k] += a[j] * g(k, nb[j]);
+    }
+}
+
+struct MixBiState {
+    double thresh, r0, true_final, target, rho_old, alpha, omega, beta;
+    int mode, restarts, its, converged, status, done, ran;
+};
+
+template <int NC, int WIDTH>
+__global__ void __launch_bounds__(kKThreads) k_bicgstab_mixed(gf_krylov_t K) {
+    __shared__ MixBiState st[NC];
+    __shared__ int s_any;
+    KCtl* ctl = reinterpret_cast<KCtl*>(K.work);
+    barrier_init_v(K, (int)gridDim.x, (int)blockIdx.x);
+    double* partials = K.work + kCtlDoubles;
+    float* f = reinterpret_cast<float*>(partials + kPartials);
+    const int64_t n = K.n;
+    const int W = K.width;
+    float* val32 = f;
+    float* diag32 = val32 + (int64_t)W * n;
+    float* inv32 = diag32 + n;
+    float* r = inv32 + n;
+    float* rh = r + NC * n;
+    float* p = r + 2 * NC * n;
+    float* v = r + 3 * NC * n;
+    float* s = r + 4 * NC * n;
+    float* t = r + 5 * NC * n;
+    float* e = r + 6 * NC * n;
+    double* x = K.x;
+    const bool jac = K.jacobi != 0, linf = K.norm_inf != 0;
+    const int64_t t0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const double margin = K.inner_margin > 0.0 && K.inner_margin <= 1.0 ? K.inner_margin : 0.5;
+    bool ok = true;
+
+    for (int64_t c = t0; c < n; c += stride) {
+        for (int sl = 0; sl < W; ++sl) __stcg(val32 + sl * n + c, (float)__ldg(K.val + sl * n + c));
+        __stcg(diag32 + c, (float)__ldg(K.diag + c));
+        __stcg(inv32 + c, (float)inv_diag(K.diag, c, jac));
+    }
+    if (threadIdx.x == 0)
+        for (int k = 0; k < NC; ++k) {
+            st[k].its = 0;
+            st[k].converged = 0;
+            st[k].status = GF_MAX_ITER;
+            st[k].done = 0;
+            st[k].ran = 0;
+            st[k].r0 = st[k].true_final = 0.0;
+        }
+    __syncthreads();
+    int its_total = 0;
+    for (int cycle = 0; ok && cycle <= K.max_outer; ++cycle) {
+        {  // fold the corrections, then the true residual in FP64
+            for (int64_t c = t0; c < n; c += stride)
+#pragma unroll
+                for (int k = 0; k < NC; ++k)
+                    if (st[k].ran) __stcg(x + k * n + c, __ldcg(x + k * n + c) + (double)__ldcg(e + k * n + c));
+            // The barrier also publishes the FP32 coefficients (cycle 0).
+            double dummy[1] = {0.0};
+            ok = grid_reduce<1>(ctl, partials, dummy, 0u);
+            if (!ok) break;
+            double loc[2 * NC];
+#pragma unroll
+            for (int j = 0; j < 2 * NC; ++j) loc[j] = 0.0;
+            auto gx = [&](int k, int64_t i) { return __ldcg(x + k * n + i); };
+            for (int64_t c = t0; c < n; c += stride) {
+                double ax[NC];
+                row_apply<NC, WIDTH>(K, c, gx, ax);
+#pragma unroll
+                for (int k = 0; k < NC; ++k) {
+                    const double rk = __ldg(K.rhs + k * n + c) - ax[k];
+                    const float r32 = (float)rk;
+                    __stcg(r + k * n + c, r32);
+                    __stcg(rh + k * n + c, r32);
+                    __stcg(p + k * n + c, r32);
+                    __stcg(e + k * n + c, 0.0f);
+                    loc[k] = norm_acc(loc[k], rk, linf);
+                    loc[NC + k] += (double)r32 * (double)r32;
+                }
+            }
+            ok = grid_reduce<2 * NC>(ctl, partials, loc, linf ? ((1u << NC) - 1u) : 0u);
+            if (!ok) break;
+            if (threadIdx.x == 0) {
+                int any = 0;
+                for (int k = 0; k < NC; ++k) {
+                    MixBiState& b = st[k];
+                    b.ran = 0;
+                    const double fin = norm_fin(loc[k], linf);
+                    if (cycle == 0) {
+                        b.r0 = fin;
+                        b.thresh = fmax(K.atol, K.rtol * fin);
+                    }
+                    if (b.done) continue;
+                    b.true_final = fin;
+                    if (fin < b.thresh) {
+                        b.done = 1;
+                        b.converged = 1;
+                        b.status = GF_OK;
+                    } else if (!isfinite(fin)) {
+                        b.done = 1;
+                        b.status = GF_NONFINITE;
+                    } else if (cycle == K.max_outer || its_total >= K.max_iter) {
+                        b.done = 1;
+                        b.status = GF_MAX_ITER;
+                    } else {
+                        b.mode = kRun;
+                        b.ran = 1;
+                        b.restarts = 0;
+                        b.target = fmax(K.inner_eta * fin, margin * b.thresh);
+                        b.rho_old = loc[NC + k];
+                        any = 1;
+                    }
+                }
+                s_any = any;
+            }
+            __syncthreads();
+            if (!s_any) break;
+        }
+        // Inner FP32 BiCGStab on A e = r (e = 0 to start).
+        for (int it = 1; ok && its_total < K.max_iter; ++it) {
+            if (threadIdx.x == 0) {
+                int any = 0;
+                for (int k = 0; k < NC; ++k) {
+                    if (st[k].mode == kIdle) st[k].mode = kRun;
+                    any |= st[k].ran && (st[k].mode == kRun);
+                }
+                s_any = any;
+            }
+            __syncthreads();
+            if (!s_any) break;
+            ++its_total;
+            {  // P1: y = M p, v = A y; r_hat.v, |r_hat|^2, |v|^2
+                double loc[3 * NC];
+#pragma unroll
+                for (int j = 0; j < 3 * NC; ++j) loc[j] = 0.0;
+                auto gy = [&](int k, int64_t i) { return __ldcg(inv32 + i) * __ldcg(p + k * n + i); };
+                for (int64_t c = t0; c < n; c += stride) {
+                    float av[NC];
+                    row_apply32<NC, WIDTH>(K, val32, diag32, c, gy, av);
+#pragma unroll
+                    for (int k = 0; k < NC; ++k) {
+                        if (!st[k].ran || st[k].mode != kRun) continue;
+                        __stcg(v + k * n + c, av[k]);
+                        const double h = __ldcg(rh + k * n + c);
+                        loc[k] += h * (double)av[k];
+                        loc[NC + k] += h * h;
+                        loc[2 * NC + k] += (double)av[k] * (double)av[k];
+                    }
+                }
+                ok = grid_reduce<3 * NC>(ctl, partials, loc, 0u);
+                if (!ok) break;
+                if (threadIdx.x == 0)
+                    for (int k = 0; k < NC; ++k) {
+                        MixBiState& b = st[k];
+                        if (!b.ran || b.mode != kRun) continue;
+                        b.its += 1;
+                        const double da = loc[k];
+                        if (fabs(da) <= 1e-6 * sqrt(loc[NC + k]) * sqrt(loc[2 * NC + k])) {
+                            if (b.restarts >= K.max_restart) b.mode = kDone;
+                            else { b.restarts += 1; b.mode = kRestart; }
+                        } else {
+                            b.alpha = b.rho_old / da;
+                        }
+                    }
+                __syncthreads();
+            }
+            {  // P2: s = r - alpha v, |s|; restarting systems copy r
+                double loc[2 * NC];
+#pragma unroll
+                for (int j = 0; j < 2 * NC; ++j) loc[j] = 0.0;
+                for (int64_t c = t0; c < n; c += stride)
+#pragma unroll
+                    for (int k = 0; k < NC; ++k) {
+                        if (!st[k].ran) continue;
+                        const int md = st[k].mode;
+                        if (md == kRun) {
+                            const float sk = __ldcg(r + k * n + c) - (float)st[k].alpha * __ldcg(v + k * n + c);
+                            __stcg(s + k * n + c, sk);
+                            loc[k] = norm_acc(loc[k], (double)sk, linf);
+                        } else if (md == kRestart) {
+                            const float rk = __ldcg(r + k * n + c);
+                            __stcg(rh + k * n + c, rk);
+                            __stcg(p + k * n + c, rk);
+                            loc[NC + k] += (double)rk * (double)rk;
+                        }
+                    }
+                ok = grid_reduce<2 * NC>(ctl, partials, loc, linf ? ((1u << NC) - 1u) : 0u);
+                if (!ok) break;
+                if (threadIdx.x == 0)
+                    for (int k = 0; k < NC; ++k) {
+                        MixBiState& b = st[k];
+                        if (!b.ran) continue;
+                        if (b.mode == kRestart) {
+                            b.rho_old = loc[NC + k];
+                            b.mode = kIdle;
+                        } else if (b.mode == kRun) {
+                            const double fin = norm_fin(loc[k], linf);
+                            if (fin < b.target) b.mode = kConvS;
+                            else if (!isfinite(fin)) b.mode = kDone;
+                        }
+                    }
+                __syncthreads();
+            }
+            {  // P3: converged-on-s systems take e += alpha y; others z = M s, t = A z
+                double loc[2 * NC];
+#pragma unroll
+                for (int j = 0; j < 2 * NC; ++j) loc[j] = 0.0;
+                auto gz = [&](int k, int64_t i) { return __ldcg(inv32 + i) * __ldcg(s + k * n + i); };
+                for (int64_t c = t0; c < n; c += stride) {
+                    float at[NC];
+                    row_apply32<NC, WIDTH>(K, val32, diag32, c, gz, at);
+                    const float ic = __ldcg(inv32 + c);
+#pragma unroll
+                    for (int k = 0; k < NC; ++k) {
+                        if (!st[k].ran) continue;
+                        const int md = st[k].mode;
+                        if (md == kConvS) {
+                            __stcg(e + k * n + c, __ldcg(e + k * n + c) + (float)st[k].alpha * ic * __ldcg(p + k * n + c));
+                        } else if (md == kRun) {
+                            __stcg(t + k * n + c, at[k]);
+                            loc[k] += (double)at[k] * (double)at[k];
+                            loc[NC + k] += (double)at[k] * (double)__ldcg(s + k * n + c);
+                        }
+                    }
+                }
+                ok = grid_reduce<2 * NC>(ctl, partials, loc, 0u);
+                if (!ok) break;
+                if (threadIdx.x == 0)
+                    for (int k = 0; k < NC; ++k) {
+                        MixBiState& b = st[k];
+                        if (!b.ran) continue;
+                        if (b.mode == kConvS) {
+                            b.mode = kDone;
+                            continue;
+                        }
+                        if (b.mode != kRun) continue;
+                        const double dd = loc[k];
+                        if (fabs(dd) <= 1e-6 * dd || (b.omega = loc[NC + k] / dd, fabs(b.omega) <= 1e-6)) {
+                            if (b.restarts >= K.max_restart) b.mode = kDone;
+                            else { b.restarts += 1; b.mode = kRestart; }
+                        }
+                    }
+                __syncthreads();
+            }
+            {  // P4: e += alpha y + omega z, r = s - omega t; |r|, r_hat.r, |r_hat|^2, |r|^2
+                double loc[4 * NC];
+#pragma unroll
+                for (int j = 0; j < 4 * NC; ++j) loc[j] = 0.0;
+                for (int64_t c = t0; c < n; c += stride) {
+                    const float ic = __ldcg(inv32 + c);
+#pragma unroll
+                    for (int k = 0; k < NC; ++k) {
+                        if (!st[k].ran) continue;
+                        const int md = st[k].mode;
+                        if (md == kRun) {
+                            const float sk = __ldcg(s + k * n + c);
+                            const float y = ic * __ldcg(p + k * n + c);
+                            const float z = ic * sk;
+                            __stcg(e + k * n + c,
+                                   __ldcg(e + k * n + c) + (float)st[k].alpha * y + (float)st[k].omega * z);
+                            const float rk = sk - (float)st[k].omega * __ldcg(t + k * n + c);
+                            __stcg(r + k * n + c, rk);
+                            const double h = __ldcg(rh + k * n + c);
+                            loc[k] = norm_acc(loc[k], (double)rk, linf);
+                            loc[NC + k] += h * rk;
+                            loc[2 * NC + k] += h * h;
+                            loc[3 * NC + k] += (double)rk * (double)rk;
+                        } else if (md == kRestart) {
+                            const float rk = __ldcg(r + k * n + c);
+                            __stcg(rh + k * n + c, rk);
+                            __stcg(p + k * n + c, rk);
+                            loc[3 * NC + k] += (double)rk * (double)rk;
+                        }
+                    }
+                }
+                ok = grid_reduce<4 * NC>(ctl, partials, loc, linf ? ((1u << NC) - 1u) : 0u);
+                if (!ok) break;
+                if (threadIdx.x == 0)
+                    for (int k = 0; k < NC; ++k) {
+                        MixBiState& b = st[k];
+                        if (!b.ran) continue;
+                        if (b.mode == kRestart) {
+                            b.rho_old = loc[3 * NC + k];
+                            b.mode = kIdle;
+                            continue;
+                        }
+                        if (b.mode != kRun) continue;
+                        const double fin = norm_fin(loc[k], linf);
+                        if (fin < b.target || !isfinite(fin)) {
+                            b.mode = kDone;
+                            continue;
+                        }
+                        const double rho_new = loc[NC + k];
+                        if (fabs(rho_new) <= 1e-6 * sqrt(loc[2 * NC + k]) * sqrt(loc[3 * NC + k])) {
+                            if (b.restarts >= K.max_restart) b.mode = kDone;
+                            else { b.restarts += 1; b.mode = kRestart; }
+                            continue;
+                        }
+                        b.beta = (rho_new / b.rho_old) * (b.alpha / b.omega);
+                        b.rho_old = rho_new;
+                    }
+                __syncthreads();
+            }
+            {  // P5: p = r + beta (p - omega v); restarting systems copy r
+                double loc[NC];
+#pragma unroll
+                for (int k = 0; k < NC; ++k) loc[k] = 0.0;
+                for (int64_t c = t0; c < n; c += stride)
+#pragma unroll
+                    for (int k = 0; k < NC; ++k) {
+                        if (!st[k].ran) continue;
+                        const int md = st[k].mode;
+                        if (md == kRun) {
+                            const float pk = __ldcg(p + k * n + c);
+                            __stcg(p + k * n + c, __ldcg(r + k * n + c) +
+                                                      (float)st[k].beta * (pk - (float)st[k].omega * __ldcg(v + k * n + c)));
+                        } else if (md == kRestart) {
+                            const float rk = __ldcg(r + k * n + c);
+                            __stcg(rh + k * n + c, rk);
+                            __stcg(p + k * n + c, rk);
+                            loc[k] += (double)rk * (double)rk;
+                        }
+                    }
+                ok = grid_reduce<NC>(ctl, partials, loc, 0u);
+                if (!ok) break;
+                if (threadIdx.x == 0)
+                    for (int k = 0; k < NC; ++k)
+                        if (st[k].ran && st[k].mode == kRestart) {
+                            st[k].rho_old = loc[k];
+                            st[k].mode = kIdle;
+                        }
+                __syncthreads();
+            }
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        for (int k = 0; k < NC; ++k) {
+            double* o = K.stats + 5 * k;
+            o[0] = st[k].r0;
+            o[1] = st[k].true_final;
+            o[2] = st[k].its;
+            o[3] = st[k].converged;
+            o[4] = ok ? st[k].status : GF_ERR_TIMEOUT;
+        }
+}
+
+// ---------------------------------------------------------------------------
 // Split CG for systems of millions of cells (variant 19): two ordinary
 // kernels an iteration instead of one persistent cooperative launch, so each
 // pass runs at the occupancy of a plain stream kernel (a standalone SpMV of
@@ -4634,6 +5015,13 @@ using namespace gf;
 extern "C" {
 
 int64_t gf_krylov_workspace_size(int64_t n, int32_t ncomp, int32_t kind) {
+    // kind 3 + 100 * width: mixed-precision BiCGStab (ncomp components):
+    // (width + 2) n coefficient floats and 7 ncomp n vector floats.
+    if (kind >= 3 && kind % 100 == 3) {
+        const int64_t width = (kind - 3) / 100 > 0 ? (kind - 3) / 100 : kMaxEll;
+        const int64_t floats = (width + 2 + 7 * (int64_t)ncomp) * n;
+        return kHeader + (floats + 1) / 2 + 1;
+    }
     // kind 2 + 100 * width: mixed-precision CG for an ELL of that width.
     if (kind >= 2) {
         const int64_t width = (kind - 2) / 100 > 0 ? (kind - 2) / 100 : kMaxEll;
@@ -4751,6 +5139,27 @@ int gf_pcg_solve(const gf_krylov_t* k, void* stream) {
 }
 
 int gf_bicgstab_solve(const gf_krylov_t* k, void* stream) {
+    if (k != nullptr && k->mixed) {
+        // FP32 inner cycles in FP64 refinement (k_bicgstab_mixed).
+        if (!valid_krylov(k, 0, "gf_bicgstab_solve") || k->max_outer < 1 || k->width > kMaxEll ||
+            k->work_len < gf_krylov_workspace_size(k->n, k->ncomp, 3 + 100 * k->width)) {
+            set_error("gf_bicgstab_solve: mixed precision needs max_outer >= 1, width <= %d and the mixed "
+                      "BiCGStab workspace", kMaxEll);
+            return GF_ERR_INVALID;
+        }
+        const bool m6 = k->width == 6;
+        switch (k->ncomp) {
+            case 1:
+                return m6 ? launch_persistent(k_bicgstab_mixed<1, 6>, k, stream, "gf_bicgstab_solve")
+                          : launch_persistent(k_bicgstab_mixed<1, 0>, k, stream, "gf_bicgstab_solve");
+            case 2:
+                return m6 ? launch_persistent(k_bicgstab_mixed<2, 6>, k, stream, "gf_bicgstab_solve")
+                          : launch_persistent(k_bicgstab_mixed<2, 0>, k, stream, "gf_bicgstab_solve");
+            default:
+                return m6 ? launch_persistent(k_bicgstab_mixed<3, 6>, k, stream, "gf_bicgstab_solve")
+                          : launch_persistent(k_bicgstab_mixed<3, 0>, k, stream, "gf_bicgstab_solve");
+        }
+    }
     if (!valid_krylov(k, 6, "gf_bicgstab_solve", k ? k->n : 0)) return GF_ERR_INVALID;
     const bool w6 = k->width == 6;
     switch (k->ncomp) {
@@ -4783,6 +5192,10 @@ static int launch_batched(const gf_krylov_t* sys, int32_t count, const int32_t* 
     int total = 0;
     for (int i = 0; i < count; ++i) {
         const gf_krylov_t& k = sys[i];
+        if (k.mixed && bicg) {
+            set_error("%s: system %d: the batched BiCGStab has no FP32-inner form", what, i);
+            return GF_ERR_INVALID;
+        }
         if (k.mixed && !bicg) {
             // FP32-inner CG: one system and the mixed workspace.
             if (!valid_krylov(&k, 0, what) || k.ncomp != 1 || k.max_outer < 1 || k.width > kMaxEll ||

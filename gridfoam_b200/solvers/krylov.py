@@ -28,7 +28,8 @@ def workspace(cache: dict, device: torch.device, n: int, ncomp: int, kind: int) 
 
     Each solver owns its cache: solves on different streams (concurrent
     cases) must never share scratch.  ``kind``: 0 CG, 1 BiCGStab,
-    ``2 + 100 * width`` mixed-precision CG.
+    ``2 + 100 * width`` mixed-precision CG, ``3 + 100 * width``
+    mixed-precision BiCGStab.
     """
     key = (str(device), n, ncomp, kind)
     ws = cache.get(key)
@@ -159,8 +160,12 @@ class DeviceKrylov(LinearSolver):
         if stats is None:
             stats = torch.zeros((nc, 5), dtype=torch.float64, device=grid.device)
             self._stats_dev[key] = stats
-        mixed = self.mixed and nc == 1 and not self.bicgstab
-        kind = (2 + 100 * grid.ell_width) if mixed else int(self.bicgstab)
+        # FP32 inner cycles: CG for one system, BiCGStab for every component
+        mixed = self.mixed and (nc == 1 or self.bicgstab)
+        if mixed:
+            kind = (3 if self.bicgstab else 2) + 100 * grid.ell_width
+        else:
+            kind = int(self.bicgstab)
         ws = workspace(self._workspaces, grid.device, n, nc, kind)
         k = GfKrylov()
         k.n = n

@@ -204,7 +204,8 @@ typedef struct gf_krylov {
     double* stats;        /* out [ncomp][5]: initial residual, final residual,
                              iterations, converged (0/1), status (GF_*) */
     int32_t mixed;        /* 1: FP32 inner iterations inside FP64 iterative
-                             refinement (CG, one system); 0: FP64 throughout */
+                             refinement (CG: one system; BiCGStab: every
+                             component); 0: FP64 throughout */
     int32_t max_outer;    /* refinement cycles allowed when mixed (>= 1) */
     double inner_eta;     /* inner FP32 cycle stops at eta * |r_true| */
     int64_t stride_y;     /* > 0: the ELL is a uniform lexicographic box with
@@ -237,7 +238,8 @@ const char* gf_last_error(void);
 int gf_version(void);
 
 /* Number of doubles a workspace for gf_pcg_solve / gf_bicgstab_solve needs
- * (kind 0: CG, 1: BiCGStab, 2: mixed-precision CG; width = ELL width). */
+ * (kind 0: CG, 1: BiCGStab, 2 + 100 width: mixed-precision CG, 3 + 100 width:
+ * mixed-precision BiCGStab; width = ELL width). */
 int64_t gf_krylov_workspace_size(int64_t n, int32_t ncomp, int32_t kind);
 
 /* fv/boundary_ops.py:311-326 and the evaluate() methods of boundaries/**:
