@@ -414,7 +414,8 @@ def serving_bench(args, local: int, dist=None, rank: int = 0, world: int = 1) ->
 
 def pipe_variant(args, local: int, torch) -> dict:
     """The immersed Hagen-Poiseuille pipe (64x64x256 cells, PISO dt 1e-3),
-    FP64 and FP32-inner: cell-iters/s over the timed steps, the pressure CG
+    FP64 and FP32-inner (pressure CG and momentum BiCGStab, each in FP64
+    refinement): cell-iters/s over the timed steps, the pressure CG
     per iteration (its working set is L2-resident: against the measured
     floor of its two grid reductions, not HBM), and after ``pipe_steps``
     steps the relative L2 error of u_z against the analytic profile
@@ -427,8 +428,9 @@ def pipe_variant(args, local: int, torch) -> dict:
     finals = {}
     for name, prec in (("fp64", "float64"), ("fp32_inner", "float32")):
         case = pipe_case(64, 256, 4.0)
-        for key in ("p", "pFinal"):
-            case["simulator"]["fvSolution"]["solvers"][key]["inner_precision"] = prec
+        for key in ("p", "pFinal", "U"):
+            if key in case["simulator"]["fvSolution"]["solvers"]:
+                case["simulator"]["fvSolution"]["solvers"][key]["inner_precision"] = prec
         mesh, grid, algo = create_case(case, device=f"cuda:{local}")
         psolvers = [s for n, s in algo.solvers.items() if n.startswith("p")]
         for _ in range(args.warmup):
