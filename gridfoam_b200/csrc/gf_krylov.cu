@@ -4133,7 +4133,7 @@ __global__ void __launch_bounds__(kKThreads) k_bicgstab_mixed(gf_krylov_t K) {
 // kernels are enqueued without a host synchronisation; once the stopping
 // test has passed the remaining ones return at once.
 constexpr int kSplitVariant = 19;
-constexpr int kSplitVariants = 6;
+constexpr int kSplitVariants = 7;
 constexpr int kSplitThreads = 256;
 
 struct SplitScalars {  // in the control block, after KCtl
@@ -4246,7 +4246,7 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_init(gf_krylov_t K,
 // it = max_iter + 1 only finishes the statistics.  LOOP: the body of a
 // CUDA graph while-loop; it comes from the control block and the kernel that
 // ends the solve sets the loop's condition to 0.
-template <class Rows, int MINB, bool LOOP>
+template <class Rows, int MINB, bool LOOP, bool QREC = false>
 __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_a(gf_krylov_t K, Rows rows, int it, int pa_old,
                                                               cudaGraphConditionalHandle loop) {
     SplitScalars* S = split_scalars(K);
@@ -4311,13 +4311,29 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_a(gf_krylov_t K, Ro
     const double* p_old = pa_old ? v.pa : v.pb;
     double* p_new = pa_old ? v.pb : v.pa;
     double loc[1] = {0.0};
-    auto gp = [&](int i) { return v.z[i] + p_old[i] * beta; };
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-        const double pc = v.z[c] + p_old[c] * beta;
-        const double ap = rows.apply(c, __ldg(K.diag + c), gp);
-        __stcg(p_new + c, pc);
-        __stcg(v.q + c, ap);
-        loc[0] += pc * ap;
+    if (QREC) {
+        // q = A p by recurrence, q = A z + beta q: the rows gather z alone
+        // (one vector instead of two), q of the own cell is read back.
+        const bool first = it == 1;
+        auto gz = [&](int i) { return v.z[i]; };
+        for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+            const double zc = v.z[c];
+            const double pc = first ? zc : zc + p_old[c] * beta;
+            const double az = rows.apply(c, __ldg(K.diag + c), gz);
+            const double qc = first ? az : az + __ldcg(v.q + c) * beta;
+            __stcg(p_new + c, pc);
+            __stcg(v.q + c, qc);
+            loc[0] += pc * qc;
+        }
+    } else {
+        auto gp = [&](int i) { return v.z[i] + p_old[i] * beta; };
+        for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+            const double pc = v.z[c] + p_old[c] * beta;
+            const double ap = rows.apply(c, __ldg(K.diag + c), gp);
+            __stcg(p_new + c, pc);
+            __stcg(v.q + c, ap);
+            loc[0] += pc * ap;
+        }
     }
     split_partial<1>(loc, 0u, v.p1);
 }
@@ -4499,13 +4515,13 @@ static int split_loop_exec(const void* fa, const void* fb, const gf_krylov_t& K,
     return GF_OK;
 }
 
-template <class Rows, int MINB, bool PAIRS>
+template <class Rows, int MINB, bool PAIRS, bool QREC = false>
 static int launch_split_rows(const gf_krylov_t* k, const Rows& rows, cudaStream_t st) {
     int dev = 0, sms = 0, per_sm = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cgs_a<Rows, MINB, false>, kSplitThreads, 0);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cgs_a<Rows, MINB, false, QREC>, kSplitThreads, 0);
     if (e != cudaSuccess || per_sm < 1) {
         set_error("gf_pcg_solve: split CG set-up failed: %s", cudaGetErrorString(e));
         return GF_ERR_CUDA;
@@ -4537,7 +4553,7 @@ static int launch_split_rows(const gf_krylov_t* k, const Rows& rows, cudaStream_
     if (split_graph_enabled() && cudaStreamIsCapturing(st, &cap) == cudaSuccess &&
         cap == cudaStreamCaptureStatusNone) {
         cudaGraphExec_t exec = nullptr;
-        const int rc = split_loop_exec((const void*)k_cgs_a<Rows, MINB, true>, (const void*)k_cgs_b<MINB, true, PAIRS>, K,
+        const int rc = split_loop_exec((const void*)k_cgs_a<Rows, MINB, true, QREC>, (const void*)k_cgs_b<MINB, true, PAIRS>, K,
                                        &rows, sizeof(Rows), g, &exec);
         if (rc != GF_OK) return rc;
         e = cudaGraphLaunch(exec, st);
@@ -4549,10 +4565,10 @@ static int launch_split_rows(const gf_krylov_t* k, const Rows& rows, cudaStream_
     }
     for (int it = 1; it <= k->max_iter; ++it) {
         // p_old is pa at odd iterations (p_new then goes to pb), pb at even.
-        k_cgs_a<Rows, MINB, false><<<g, kSplitThreads, 0, st>>>(K, rows, it, it & 1, 0);
+        k_cgs_a<Rows, MINB, false, QREC><<<g, kSplitThreads, 0, st>>>(K, rows, it, it & 1, 0);
         k_cgs_b<MINB, false, PAIRS><<<g, kSplitThreads, 0, st>>>(K, it, it & 1);
     }
-    k_cgs_a<Rows, MINB, false><<<g, kSplitThreads, 0, st>>>(K, rows, k->max_iter + 1, (k->max_iter + 1) & 1, 0);
+    k_cgs_a<Rows, MINB, false, QREC><<<g, kSplitThreads, 0, st>>>(K, rows, k->max_iter + 1, (k->max_iter + 1) & 1, 0);
     e = cudaGetLastError();
     if (e != cudaSuccess) {
         set_error("gf_pcg_solve: split CG launch failed: %s", cudaGetErrorString(e));
@@ -4561,7 +4577,7 @@ static int launch_split_rows(const gf_krylov_t* k, const Rows& rows, cudaStream_
     return GF_OK;
 }
 
-template <int MINB, bool PAIRS, int GRP = 1>
+template <int MINB, bool PAIRS, int GRP = 1, bool QREC = false>
 static int launch_split_m(const gf_krylov_t* k, void* stream) {
     const int64_t row_span = (int64_t)(k->stride_y > 0 ? 6 : (k->width > 6 ? k->width : 6)) * k->n;
     if (row_span >= ((int64_t)1 << 31)) {
@@ -4571,23 +4587,24 @@ static int launch_split_m(const gf_krylov_t* k, void* stream) {
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     if (k->stride_y > 0) {
         if (k->symmetric)
-            return launch_split_rows<BoxRows<double, true, false, int>, MINB, PAIRS>(
+            return launch_split_rows<BoxRows<double, true, false, int>, MINB, PAIRS, QREC>(
                 k, BoxRows<double, true, false, int>{k->val, (int)k->n, (int)k->stride_y, (int)k->stride_z}, st);
-        return launch_split_rows<BoxRows<double, false, false, int>, MINB, PAIRS>(
+        return launch_split_rows<BoxRows<double, false, false, int>, MINB, PAIRS, QREC>(
             k, BoxRows<double, false, false, int>{k->val, (int)k->n, (int)k->stride_y, (int)k->stride_z}, st);
     }
     // One slot at a time (the loop of a plain SpMV): the occupancy, not the
     // loads of one thread, keeps the memory system busy.
     if (k->width == 6)
-        return launch_split_rows<EllRows<double, 6, int, 1>, MINB, PAIRS>(
+        return launch_split_rows<EllRows<double, 6, int, 1>, MINB, PAIRS, QREC>(
             k, EllRows<double, 6, int, 1>{k->val, k->nbr, (int)k->n, k->width, k->row_len}, st);
-    return launch_split_rows<EllRows<double, 0, int, GRP>, MINB, PAIRS>(
+    return launch_split_rows<EllRows<double, 0, int, GRP>, MINB, PAIRS, QREC>(
         k, EllRows<double, 0, int, GRP>{k->val, k->nbr, (int)k->n, k->width, k->row_len}, st);
 }
 
 // Variant 19: 8 blocks of 256 threads an SM; 20: 6 (more registers);
 // 21: 8 with the update kernel on pairs of cells; 22: 7, pairs; 23: 7,
-// pairs, ELL slots loaded two at a time; 24: 6, pairs, four at a time.
+// pairs, ELL slots loaded two at a time; 24: 6, pairs, four at a time;
+// 25: 8, pairs, q = A p by recurrence (the rows gather z alone).
 static int launch_split(const gf_krylov_t* k, void* stream, int which) {
     switch (which) {
         case 1: return launch_split_m<6, false>(k, stream);
@@ -4595,6 +4612,7 @@ static int launch_split(const gf_krylov_t* k, void* stream, int which) {
         case 3: return launch_split_m<7, true>(k, stream);
         case 4: return launch_split_m<7, true, 2>(k, stream);
         case 5: return launch_split_m<6, true, 4>(k, stream);
+        case 6: return launch_split_m<8, true, 1, true>(k, stream);
         default: return launch_split_m<8, false>(k, stream);
     }
 }
