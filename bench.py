@@ -139,11 +139,12 @@ def pcg_bytes_setup(C: int, F: int, s: int = 8) -> float:
 
 
 # Measured DRAM bytes (read + write) per cell per iteration of the pressure
-# CG on the cylinder-wake octree: one k_cgs_a (189.9 MB) plus one k_cgs_b
-# (75.1 MB) launch of the split CG in an ncu capture on the 192x120x24 base
-# (1,729,632 cells; the working set exceeds L2, so the traffic grows in
-# proportion to the cells), against 159.8 B of the byte model.
-PCG_DRAM_BYTES_PER_CELL_ITER = 153.2
+# CG on the cylinder-wake octree: one k_cgs_a (204.6 MB) plus one k_cgs_b
+# (83.5 MB) launch of the default split CG (variant 25, q by recurrence) in
+# an ncu capture on the 192x120x24 base (1,729,632 cells; the working set
+# exceeds L2, so the traffic grows in proportion to the cells), against
+# 159.8 B of the byte model (the recurrence reads q of the own cell).
+PCG_DRAM_BYTES_PER_CELL_ITER = 166.6
 
 
 def _oracle_threads() -> int:
