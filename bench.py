@@ -751,8 +751,8 @@ def run_gpu(args) -> None:
         "roofline": {
             "kernel": (f"pressure CG, variant {variant}: " + (
                 ("split Jacobi-PCG (k_cgs_a: p update + q = A z + beta q + p.q partials; "
-                 if variant == 25 else "split Jacobi-PCG (k_cgs_a: p update + SpMV + p.q partials; ") +
-                "k_cgs_b: x/r/z update + partials), octree ELL rows, fp64" if variant in (19, 20, 21, 22, 23, 24, 25) else
+                 if variant in (25, 26) else "split Jacobi-PCG (k_cgs_a: p update + SpMV + p.q partials; ") +
+                "k_cgs_b: x/r/z update + partials), octree ELL rows, fp64" if variant in (19, 20, 21, 22, 23, 24, 25, 26) else
                 "persistent Jacobi-PCG on the octree ELL rows, fp64")),
             "bound": "hbm",
             "achieved": achieved,

@@ -4133,7 +4133,7 @@ __global__ void __launch_bounds__(kKThreads) k_bicgstab_mixed(gf_krylov_t K) {
 // kernels are enqueued without a host synchronisation; once the stopping
 // test has passed the remaining ones return at once.
 constexpr int kSplitVariant = 19;
-constexpr int kSplitVariants = 7;
+constexpr int kSplitVariants = 8;
 constexpr int kSplitThreads = 256;
 
 struct SplitScalars {  // in the control block, after KCtl
@@ -4604,7 +4604,8 @@ static int launch_split_m(const gf_krylov_t* k, void* stream) {
 // Variant 19: 8 blocks of 256 threads an SM; 20: 6 (more registers);
 // 21: 8 with the update kernel on pairs of cells; 22: 7, pairs; 23: 7,
 // pairs, ELL slots loaded two at a time; 24: 6, pairs, four at a time;
-// 25: 8, pairs, q = A p by recurrence (the rows gather z alone).
+// 25: 8, pairs, q = A p by recurrence (the rows gather z alone); 26: 8,
+// q by recurrence, update one cell at a time.
 static int launch_split(const gf_krylov_t* k, void* stream, int which) {
     switch (which) {
         case 1: return launch_split_m<6, false>(k, stream);
@@ -4613,6 +4614,7 @@ static int launch_split(const gf_krylov_t* k, void* stream, int which) {
         case 4: return launch_split_m<7, true, 2>(k, stream);
         case 5: return launch_split_m<6, true, 4>(k, stream);
         case 6: return launch_split_m<8, true, 1, true>(k, stream);
+        case 7: return launch_split_m<8, false, 1, true>(k, stream);
         default: return launch_split_m<8, false>(k, stream);
     }
 }
