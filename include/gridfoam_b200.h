@@ -214,8 +214,8 @@ typedef struct gf_krylov {
     int64_t stride_z;
     int32_t symmetric;    /* 1 (box only): A is symmetric, only + slots read */
     int32_t block_cap;    /* > 0: at most this many persistent blocks (tuning) */
-    int32_t variant;      /* CG launch shape (0..22, see gf_krylov.cu and
-                             solvers/autotune.py); 19..22: the split CG, two
+    int32_t variant;      /* CG launch shape (0..26, see gf_krylov.cu and
+                             solvers/autotune.py); 19..26: the split CG, two
                              plain kernels an iteration, run as a CUDA graph
                              while-loop on the stream (every permitted
                              iteration enqueued inside a stream capture, or
