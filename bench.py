@@ -139,12 +139,12 @@ def pcg_bytes_setup(C: int, F: int, s: int = 8) -> float:
 
 
 # Measured DRAM bytes (read + write) per cell per iteration of the pressure
-# CG on the cylinder-wake octree: one k_cgs_a (204.6 MB) plus one k_cgs_b
-# (83.5 MB) launch of the default split CG (variant 25, q by recurrence) in
-# an ncu capture on the 192x120x24 base (1,729,632 cells; the working set
-# exceeds L2, so the traffic grows in proportion to the cells), against
-# 159.8 B of the byte model (the recurrence reads q of the own cell).
-PCG_DRAM_BYTES_PER_CELL_ITER = 166.6
+# CG on the cylinder-wake octree, by split-CG variant: one k_cgs_a plus one
+# k_cgs_b launch in an ncu capture on the 192x120x24 base (1,729,632 cells;
+# the working set exceeds L2, so the traffic grows in proportion to the
+# cells), against 159.8 B of the byte model.  Variant 25 (q by recurrence):
+# 204.6 + 83.5 MB (the recurrence reads q of the own cell).
+PCG_DRAM_BYTES_PER_CELL_ITER = {25: 166.6}
 
 
 def _oracle_threads() -> int:
@@ -721,8 +721,8 @@ def run_gpu(args) -> None:
     torch.cuda.empty_cache()
 
     per_launch_traffic = None
-    if PCG_DRAM_BYTES_PER_CELL_ITER is not None and iters:
-        per_launch_traffic = PCG_DRAM_BYTES_PER_CELL_ITER * C * sum(iters) / len(iters)
+    if variant in PCG_DRAM_BYTES_PER_CELL_ITER and iters:
+        per_launch_traffic = PCG_DRAM_BYTES_PER_CELL_ITER[variant] * C * sum(iters) / len(iters)
     value = C * world * args.steps / (ms * 1e-3)
     line = {
         "metric": METRIC,
@@ -750,9 +750,11 @@ def run_gpu(args) -> None:
         },
         "roofline": {
             "kernel": (f"pressure CG, variant {variant}: " + (
-                ("split Jacobi-PCG (k_cgs_a: p update + q = A z + beta q + p.q partials; "
-                 if variant in (25, 26) else "split Jacobi-PCG (k_cgs_a: p update + SpMV + p.q partials; ") +
-                "k_cgs_b: x/r/z update + partials), octree ELL rows, fp64" if variant in (19, 20, 21, 22, 23, 24, 25, 26) else
+                "split Jacobi-PCG (k_cgs_a: " + ("x += alpha p, " if variant in (27, 28) else "") +
+                ("p update + q = A z + beta q + p.q partials; " if variant in (25, 26, 27)
+                 else "p update + SpMV + p.q partials; ") +
+                ("k_cgs_b: r/z update + partials" if variant in (27, 28) else "k_cgs_b: x/r/z update + partials") +
+                "), octree ELL rows, fp64" if 19 <= variant <= 28 else
                 "persistent Jacobi-PCG on the octree ELL rows, fp64")),
             "bound": "hbm",
             "achieved": achieved,

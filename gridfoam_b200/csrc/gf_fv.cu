@@ -264,6 +264,119 @@ __global__ void __launch_bounds__(256, 2) k_lsq_grad6(gf_mesh_t m, const double*
     }
 }
 
+// G ELL slots [s0, s0 + G) of row c for the least-squares gradient, staged
+// as in k_lsq_grad6 (slot codes and neighbours, then immersed ordinals and
+// the neighbours' centres and values, all before any is used; slots at or
+// past W count as empty and load nothing), then accumulated into atb in slot
+// order with the arithmetic of k_lsq_grad.
+template <int NC, int G>
+__device__ __forceinline__ void lsq_slots(const gf_mesh_t& m, int64_t c, int s0, int W,
+                                           const double* __restrict__ psi, const int8_t* __restrict__ kind,
+                                           const double* __restrict__ psib, const double (&cc)[3],
+                                           const double (&pc)[NC], double (&atb)[NC][3]) {
+    const int64_t C = m.n_cells;
+    const int64_t nb = m.n_bnd;
+    const int F = (int)m.n_faces;
+    int code[G], nbr[G], imm[G];
+#pragma unroll
+    for (int s = 0; s < G; ++s) {
+        const bool in = s0 + s < W;
+        code[s] = in ? __ldg(m.ell_code + (s0 + s) * C + c) : -1;
+        nbr[s] = in ? __ldg(m.ell_nbr + (s0 + s) * C + c) : (int)c;
+    }
+    double cn[G][3], pn[G][NC];
+#pragma unroll
+    for (int s = 0; s < G; ++s) {
+        const int f = code[s] >> 1;
+        const int fc = (code[s] >= 0 && f < F) ? f : 0;
+        imm[s] = m.imm_index ? __ldg(m.imm_index + fc) : -1;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) cn[s][j] = __ldg(m.center + j * C + nbr[s]);
+#pragma unroll
+        for (int k = 0; k < NC; ++k) pn[s][k] = psi[k * C + nbr[s]];
+    }
+#pragma unroll
+    for (int s = 0; s < G; ++s) {
+        const int f = code[s] >> 1;
+        const int side = code[s] & 1;
+        if (code[s] < 0) continue;
+        if (f < F && imm[s] < 0) {
+            double d0 = cn[s][0] - cc[0], d1 = cn[s][1] - cc[1], d2 = cn[s][2] - cc[2];
+            if (side == 1) {
+                d0 = -d0;
+                d1 = -d1;
+                d2 = -d2;
+            }
+            const double dd = d0 * d0 + d1 * d1 + d2 * d2;
+            const double w2 = 1.0 / (dd > 0.0 ? dd : 1.0);
+            const double wd0 = w2 * d0, wd1 = w2 * d1, wd2 = w2 * d2;
+#pragma unroll
+            for (int k = 0; k < NC; ++k) {
+                double dpsi = pn[s][k] - pc[k];
+                if (side == 1) dpsi = -dpsi;
+                atb[k][0] += dpsi * wd0;
+                atb[k][1] += dpsi * wd1;
+                atb[k][2] += dpsi * wd2;
+            }
+        } else {
+            const int b = f >= F ? f - F : (int)m.n_domain + (side ? (int)m.n_imm : 0) + imm[s];
+            if (kind[b] == GF_BC_NONE) continue;
+            const double d0 = __ldg(m.bnd_d + b), d1 = __ldg(m.bnd_d + nb + b), d2 = __ldg(m.bnd_d + 2 * nb + b);
+            const double dd = d0 * d0 + d1 * d1 + d2 * d2;
+            const double w2 = 1.0 / (dd > 0.0 ? dd : 1.0);
+            const double wd0 = w2 * d0, wd1 = w2 * d1, wd2 = w2 * d2;
+#pragma unroll
+            for (int k = 0; k < NC; ++k) {
+                const double dpsi = psib[k * nb + b] - pc[k];
+                atb[k][0] += dpsi * wd0;
+                atb[k][1] += dpsi * wd1;
+                atb[k][2] += dpsi * wd2;
+            }
+        }
+    }
+}
+
+// k_lsq_grad for octree rows (6 < W <= 12): a row's slots in staged groups
+// (six for one component, three for three: the neighbours' values of six
+// slots spill there), the groups from slot 6 on only where their first slot
+// is used (cells with hanging faces; a row's used slots come first, and a
+// row of the axis-projected grid holds at least six, one or more faces in
+// each direction).  Same sums in the same order as k_lsq_grad (same bits); a
+// row reads only its own slots instead of all W.
+template <int NC>
+__global__ void __launch_bounds__(256, 2) k_lsq_grad12(gf_mesh_t m, const double* __restrict__ psi,
+                                                       const int8_t* __restrict__ kind,
+                                                       const double* __restrict__ psib, double* __restrict__ grad) {
+    const int64_t C = m.n_cells;
+    const int W = m.ell_width;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < C;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        double atb[NC][3];
+#pragma unroll
+        for (int k = 0; k < NC; ++k) atb[k][0] = atb[k][1] = atb[k][2] = 0.0;
+        const double cc[3] = {__ldg(m.center + c), __ldg(m.center + C + c), __ldg(m.center + 2 * C + c)};
+        double pc[NC];
+#pragma unroll
+        for (int k = 0; k < NC; ++k) pc[k] = psi[k * C + c];
+        constexpr int G = NC == 1 ? 6 : 3;
+        for (int s0 = 0; s0 < W; s0 += G) {
+            if (s0 >= 6 && __ldg(m.ell_code + s0 * C + c) < 0) break;
+            lsq_slots<NC, G>(m, c, s0, W, psi, kind, psib, cc, pc, atb);
+        }
+        double inv[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) inv[i] = __ldg(m.lsq_ata_inv + i * C + c);
+#pragma unroll
+        for (int k = 0; k < NC; ++k) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                grad[(k * 3 + i) * C + c] =
+                    inv[i * 3 + 0] * atb[k][0] + inv[i * 3 + 1] * atb[k][1] + inv[i * 3 + 2] * atb[k][2];
+            }
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Matrix assembly: ddt + div_sign div(phi, psi) + lap_sign laplacian(gamma, psi)
 // (fv/fvm/ddt.py:7-40, fv/fvm/div.py:15-73, fv/schemes/div.py:36-351,
@@ -609,6 +722,196 @@ __global__ void __launch_bounds__(256, 2) k_assemble6(gf_mesh_t m, gf_assembly_t
         }
 #pragma unroll
         for (int s = 0; s < W; ++s) a.val[s * C + c] = vals[s];
+        a.diag[c] = diag;
+#pragma unroll
+        for (int k = 0; k < NC; ++k) a.source[k * C + c] = src[k];
+    }
+}
+
+// G ELL slots [s0, s0 + G) of row c for the assembly (no TVD scheme): the
+// slot codes and neighbours, then the immersed and hanging ordinals, then
+// the face data (at clamped indices) are loaded for all G before any is
+// used; the contributions are then added to diag / src in slot order with
+// the arithmetic of k_assemble, and the slots' coefficients (and face flux
+// corrections) written.  Slots at or past W are skipped.
+template <int NC, bool CONV, bool LAP, int G>
+__device__ __forceinline__ void assemble_slots(const gf_mesh_t& m, const gf_assembly_t& a, int64_t c, int s0,
+                                               int W, double& diag, double (&src)[NC]) {
+    const int64_t C = m.n_cells;
+    const int F = (int)m.n_faces;
+    const int64_t nb = m.n_bnd;
+    const bool linear = a.div_scheme == GF_DIV_LINEAR;
+    int code[G], nbr[G], fc[G], imm[G], hg[G];
+#pragma unroll
+    for (int s = 0; s < G; ++s) {
+        const bool in = s0 + s < W;
+        code[s] = in ? __ldg(m.ell_code + (s0 + s) * C + c) : -1;
+        nbr[s] = in ? __ldg(m.ell_nbr + (s0 + s) * C + c) : (int)c;
+    }
+#pragma unroll
+    for (int s = 0; s < G; ++s) {
+        const int f = code[s] >> 1;
+        fc[s] = (code[s] >= 0 && f < F) ? f : 0;
+        imm[s] = m.imm_index ? __ldg(m.imm_index + fc[s]) : -1;
+        hg[s] = hang_of(m, fc[s]);
+    }
+    double w[G], phi[G], msf[G], dl[G], go[G], gn[G];
+#pragma unroll
+    for (int s = 0; s < G; ++s) {
+        const int side = code[s] & 1;
+        const int o = side ? nbr[s] : (int)c;
+        const int n = side ? (int)c : nbr[s];
+        w[s] = __ldg(m.weight + fc[s]);
+        if (CONV) phi[s] = __ldg(a.phi + fc[s]);
+        if (LAP) {
+            msf[s] = __ldg(m.mag_sf + fc[s]);
+            dl[s] = __ldg(m.delta + fc[s]);
+            go[s] = a.gamma ? __ldg(a.gamma + o) : 0.0;
+            gn[s] = a.gamma ? __ldg(a.gamma + n) : 0.0;
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < G; ++s) {
+        if (s0 + s >= W) break;
+        double val = 0.0;
+        const int f = code[s] >> 1;
+        const int side = code[s] & 1;
+        const bool empty = code[s] < 0;
+        if (!empty && f < F && imm[s] < 0) {
+            const int o = side ? nbr[s] : (int)c;
+            const int n = side ? (int)c : nbr[s];
+            const int h = hg[s];
+            if (CONV) {
+                const double flux = phi[s], ww = w[s];
+                double upper, lower, dO, dN;
+                if (linear) {
+                    upper = flux * (1.0 - ww);
+                    lower = -flux * ww;
+                    dO = flux * ww;
+                    dN = -flux * (1.0 - ww);
+                } else {
+                    const double pos = fmax(flux, 0.0), neg = fmin(flux, 0.0);
+                    upper = neg;
+                    lower = -pos;
+                    dO = pos;
+                    dN = -neg;
+                }
+                if (side == 0) {
+                    val += a.div_sign * upper;
+                    diag += a.div_sign * dO;
+                } else {
+                    val += a.div_sign * lower;
+                    diag += a.div_sign * dN;
+                }
+                if (linear && h >= 0 && a.grad_lsq != nullptr) {
+#pragma unroll
+                    for (int k = 0; k < NC; ++k) {
+                        const double base = ww * a.psi[k * C + o] + (1.0 - ww) * a.psi[k * C + n];
+                        const double corrected = base + hang_value_corr(m, a.grad_lsq, k, o, n, ww, h);
+                        const double sf = -flux * (corrected - base);
+                        src[k] += (side == 0 ? a.div_sign : -a.div_sign) * sf;
+                    }
+                }
+            }
+            double ffc_k[NC];
+#pragma unroll
+            for (int k = 0; k < NC; ++k) ffc_k[k] = 0.0;
+            if (LAP) {
+                double gf;
+                if (a.gamma == nullptr) {
+                    gf = a.gamma_scalar;
+                } else if (!a.lap_harmonic) {
+                    gf = w[s] * go[s] + (1.0 - w[s]) * gn[s];
+                } else {
+                    const double scale = fmax(go[s], gn[s]);
+                    const double safe = scale > 0.0 ? scale : 1.0;
+                    const double den = w[s] * (go[s] / safe) + (1.0 - w[s]) * (gn[s] / safe);
+                    gf = fmin(go[s], gn[s]) / (den > 0.0 ? den : 1.0);
+                }
+                const double coeff = gf * msf[s] * dl[s];
+                val += a.lap_sign * coeff;
+                diag += a.lap_sign * (-coeff);
+                if (h >= 0 && a.lap_corrected && a.grad_lsq != nullptr) {
+#pragma unroll
+                    for (int k = 0; k < NC; ++k) {
+                        const double corr = hang_sn_corr(m, a.grad_lsq, k, o, n, dl[s], h);
+                        const double cs = (gf * msf[s]) * corr;
+                        src[k] += a.lap_sign * (side == 0 ? -cs : cs);
+                        ffc_k[k] = cs;
+                    }
+                }
+            }
+            if (a.ffc != nullptr && side == 0) {
+#pragma unroll
+                for (int k = 0; k < NC; ++k) a.ffc[k * (int64_t)F + f] = ffc_k[k];
+            }
+        } else if (!empty) {
+            const int b = f >= F ? f - F : (int)m.n_domain + (side ? (int)m.n_imm : 0) + imm[s];
+            if (a.bc_kind[b] != GF_BC_NONE) {
+                const double fr = a.frac[b];
+                const double mag_d = __ldg(m.bnd_mag_d + b);
+                if (CONV) {
+                    const double flux = a.phi[F + b];
+                    diag += a.div_sign * (flux * (1.0 - fr));
+#pragma unroll
+                    for (int k = 0; k < NC; ++k) {
+                        const double bsrc = fr * a.refv[k * nb + b] + (1.0 - fr) * mag_d * a.refg[k * nb + b];
+                        src[k] += -a.div_sign * (flux * bsrc);
+                    }
+                }
+                if (LAP) {
+                    const double g = a.gamma ? a.gamma[c] : a.gamma_scalar;
+                    const double cond = g * __ldg(m.bnd_mag_sf + b);
+                    const double cv = cond * value_grad_coeff(m, b, fr);
+                    const double cg = cond * (1.0 - fr);
+                    diag += a.lap_sign * (-cv);
+#pragma unroll
+                    for (int k = 0; k < NC; ++k) {
+                        const double ls = cv * a.refv[k * nb + b] + cg * a.refg[k * nb + b];
+                        src[k] += a.lap_sign * (-ls);
+                    }
+                }
+            }
+        }
+        a.val[(s0 + s) * C + c] = val;
+    }
+}
+
+// k_assemble for octree rows (6 < W <= 12) and schemes without a TVD
+// correction: a row's slots in staged groups of three (three slots' face
+// data in registers at once; six spill), the groups from slot 6 on only
+// where their first slot is used (cells with hanging faces; a row's used
+// slots come first, and every row of the axis-projected grid has at least
+// six), zeros written to the unused slots without reading them.  Same
+// contributions in the same order as k_assemble (same bits).
+template <int NC, bool CONV, bool LAP>
+__global__ void __launch_bounds__(256, 2) k_assemble12(gf_mesh_t m, gf_assembly_t a) {
+    const int64_t C = m.n_cells;
+    const int W = m.ell_width;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < C;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        double diag = 0.0;
+        double src[NC];
+#pragma unroll
+        for (int k = 0; k < NC; ++k) src[k] = 0.0;
+        if (a.use_ddt) {
+            const double vdt = __ldg(m.volume + c) / a.dt;
+            diag += a.ddt_a * vdt;
+#pragma unroll
+            for (int k = 0; k < NC; ++k) {
+                double hist = a.ddt_b * a.psi_old[k * C + c];
+                if (a.ddt_c != 0.0) hist = hist - a.ddt_c * a.psi_older[k * C + c];
+                src[k] += vdt * hist;
+            }
+        }
+        constexpr int G = 3;
+        for (int s0 = 0; s0 < W; s0 += G) {
+            if (s0 >= 6 && __ldg(m.ell_code + s0 * C + c) < 0) {
+                for (int s = s0; s < W; ++s) a.val[s * C + c] = 0.0;
+                break;
+            }
+            assemble_slots<NC, CONV, LAP, G>(m, a, c, s0, W, diag, src);
+        }
         a.diag[c] = diag;
 #pragma unroll
         for (int k = 0; k < NC; ++k) a.source[k * C + c] = src[k];
@@ -1422,6 +1725,14 @@ int gf_lsq_grad(const gf_mesh_t* m, int32_t ncomp, const double* psi, const int8
     const unsigned g = grid_for(m->n_cells);
     cudaStream_t st = GF_STREAM(stream);
     const bool six = m->ell_width == 6 && m->n_faces < (int64_t)INT32_MAX;
+    // Octree rows (6 < W <= 12, every row at least six slots): staged slots,
+    // each row read to its last used slot.
+    const bool twelve = m->ell_width > 6 && m->ell_width <= 12 && m->n_faces > 0 && m->n_faces < (int64_t)INT32_MAX;
+    if (twelve) {
+        if (ncomp == 1) k_lsq_grad12<1><<<g, kThreads, 0, st>>>(*m, psi, bc_kind, psib, grad);
+        else k_lsq_grad12<3><<<g, kThreads, 0, st>>>(*m, psi, bc_kind, psib, grad);
+        return check_launch("gf_lsq_grad");
+    }
     // One component: the per-slot kernel is as fast (fewer registers).
     if (ncomp == 1) {
         k_lsq_grad<1><<<g, kThreads, 0, st>>>(*m, psi, bc_kind, psib, grad);
@@ -1454,6 +1765,10 @@ int gf_assemble(const gf_mesh_t* m, const gf_assembly_t* a, void* stream) {
     }
     const bool fast = m->ell_width == 6 && m->n_hang == 0 && a->ffc == nullptr &&
                       a->div_scheme <= GF_DIV_LINEAR && m->n_faces < (int64_t)INT32_MAX;
+    // Octree rows without a TVD correction: staged slots, each row read to
+    // its last used slot.
+    const bool twelve = m->ell_width > 6 && m->ell_width <= 12 && a->div_scheme <= GF_DIV_LINEAR &&
+                        m->n_faces > 0 && m->n_faces < (int64_t)INT32_MAX;
     const bool conv = a->div_scheme != GF_DIV_NONE, lap = a->lap_sign != 0.0;
     cudaStream_t st = GF_STREAM(stream);
     const unsigned g = grid_for(m->n_cells);
@@ -1466,6 +1781,16 @@ int gf_assemble(const gf_mesh_t* m, const gf_assembly_t* a, void* stream) {
             if (conv && lap) k_assemble6<3, true, true><<<g, kThreads, 0, st>>>(*m, *a);
             else if (conv) k_assemble6<3, true, false><<<g, kThreads, 0, st>>>(*m, *a);
             else k_assemble6<3, false, true><<<g, kThreads, 0, st>>>(*m, *a);
+        }
+    } else if (twelve) {
+        if (a->ncomp == 1) {
+            if (conv && lap) k_assemble12<1, true, true><<<g, kThreads, 0, st>>>(*m, *a);
+            else if (conv) k_assemble12<1, true, false><<<g, kThreads, 0, st>>>(*m, *a);
+            else k_assemble12<1, false, true><<<g, kThreads, 0, st>>>(*m, *a);
+        } else {
+            if (conv && lap) k_assemble12<3, true, true><<<g, kThreads, 0, st>>>(*m, *a);
+            else if (conv) k_assemble12<3, true, false><<<g, kThreads, 0, st>>>(*m, *a);
+            else k_assemble12<3, false, true><<<g, kThreads, 0, st>>>(*m, *a);
         }
     } else if (a->ncomp == 1) {
         k_assemble<1><<<g, kThreads, 0, st>>>(*m, *a);

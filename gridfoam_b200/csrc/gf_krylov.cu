@@ -4133,17 +4133,26 @@ __global__ void __launch_bounds__(kKThreads) k_bicgstab_mixed(gf_krylov_t K) {
 // kernels are enqueued without a host synchronisation; once the stopping
 // test has passed the remaining ones return at once.
 constexpr int kSplitVariant = 19;
-constexpr int kSplitVariants = 8;
+constexpr int kSplitVariants = 10;
 constexpr int kSplitThreads = 256;
 
 struct SplitScalars {  // in the control block, after KCtl
     double thresh, r0, fin, rz[2];
+    // alpha of the last update (XA forms: written by k_cgs_b, read by the
+    // next k_cgs_a, which applies x += alpha p).
+    double alpha;
     int done, its, converged, status;
     // Iteration numbers of the graph loop: it_a is read by k_cgs_a and
     // written by k_cgs_b, it_b the other way round, so no kernel reads a
     // counter that one of its own blocks writes.
     int it_a, it_b;
+    // XA forms: set by the k_cgs_a that stops the solve; the next k_cgs_b
+    // turns it into done (the stopping k_cgs_a still has work to finish in
+    // all its blocks, so it must not set the flag its own blocks test).
+    int stop;
 };
+static_assert(2 * sizeof(double) + sizeof(SplitScalars) <= kCtlDoubles * sizeof(double),
+              "split CG scalars exceed the control block");
 
 __device__ __forceinline__ SplitScalars* split_scalars(const gf_krylov_t& K) {
     return reinterpret_cast<SplitScalars*>(K.work + 2);
@@ -4245,8 +4254,11 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_init(gf_krylov_t K,
 // initial residual at it = 1), then p = z + beta p, q = A p, partials of p.q.
 // it = max_iter + 1 only finishes the statistics.  LOOP: the body of a
 // CUDA graph while-loop; it comes from the control block and the kernel that
-// ends the solve sets the loop's condition to 0.
-template <class Rows, int MINB, bool LOOP, bool QREC = false>
+// ends the solve sets the loop's condition to 0.  XA: this kernel also
+// applies the previous iteration's x += alpha p (it reads p_old anyway), so
+// the update kernel reads neither x nor p; x gets the same values in the
+// same order as in the other forms.
+template <class Rows, int MINB, bool LOOP, bool QREC = false, bool XA = false>
 __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_a(gf_krylov_t K, Rows rows, int it, int pa_old,
                                                               cudaGraphConditionalHandle loop) {
     SplitScalars* S = split_scalars(K);
@@ -4297,7 +4309,8 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_a(gf_krylov_t K, Ro
                 S->status = status;
                 S->converged = status == GF_OK;
                 __threadfence();
-                S->done = 1;
+                if (XA) S->stop = 1;
+                else S->done = 1;
                 if (LOOP) cudaGraphSetConditional(loop, 0);
             } else {
                 S->rz[it & 1] = red[1];
@@ -4306,9 +4319,17 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_a(gf_krylov_t K, Ro
         }
     }
     __syncthreads();
-    if (s_stop) return;
-    const double beta = s_beta;
     const double* p_old = pa_old ? v.pa : v.pb;
+    // XA: x += alpha p of the previous iteration (none before the first).
+    const bool upd = XA && it > 1;
+    const double alpha = upd ? S->alpha : 0.0;
+    if (s_stop) {
+        if (upd)
+            for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+                __stcg(K.x + c, __ldcg(K.x + c) + alpha * __ldcg(p_old + c));
+        return;
+    }
+    const double beta = s_beta;
     double* p_new = pa_old ? v.pb : v.pa;
     double loc[1] = {0.0};
     if (QREC) {
@@ -4318,7 +4339,9 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_a(gf_krylov_t K, Ro
         auto gz = [&](int i) { return v.z[i]; };
         for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
             const double zc = v.z[c];
-            const double pc = first ? zc : zc + p_old[c] * beta;
+            const double po = first ? 0.0 : p_old[c];
+            if (upd) __stcg(K.x + c, __ldcg(K.x + c) + alpha * po);
+            const double pc = first ? zc : zc + po * beta;
             const double az = rows.apply(c, __ldg(K.diag + c), gz);
             const double qc = first ? az : az + __ldcg(v.q + c) * beta;
             __stcg(p_new + c, pc);
@@ -4328,7 +4351,9 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_a(gf_krylov_t K, Ro
     } else {
         auto gp = [&](int i) { return v.z[i] + p_old[i] * beta; };
         for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-            const double pc = v.z[c] + p_old[c] * beta;
+            const double po = p_old[c];
+            if (upd) __stcg(K.x + c, __ldcg(K.x + c) + alpha * po);
+            const double pc = v.z[c] + po * beta;
             const double ap = rows.apply(c, __ldg(K.diag + c), gp);
             __stcg(p_new + c, pc);
             __stcg(v.q + c, ap);
@@ -4338,11 +4363,16 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_a(gf_krylov_t K, Ro
     split_partial<1>(loc, 0u, v.p1);
 }
 
-// x += alpha p; r -= alpha q; z = M r; partials of |r| and r.z.
-template <int MINB, bool LOOP, bool PAIRS>
+// x += alpha p (not in the XA forms, whose k_cgs_a applies it); r -= alpha q;
+// z = M r; partials of |r| and r.z.
+template <int MINB, bool LOOP, bool PAIRS, bool XA = false>
 __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_b(gf_krylov_t K, int it, int p_is_b) {
     SplitScalars* S = split_scalars(K);
     if (*(volatile int*)&S->done) return;
+    if (XA && *(volatile int*)&S->stop) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) S->done = 1;
+        return;
+    }
     if (LOOP) {
         it = *(volatile int*)&S->it_b;
         p_is_b = it & 1;
@@ -4354,6 +4384,7 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_b(gf_krylov_t K, in
     double red[1];
     split_sum<1>(v.p1, gridDim.x, 0u, red);
     const double alpha = S->rz[it & 1] / red[0];
+    if (XA && blockIdx.x == 0 && threadIdx.x == 0) S->alpha = alpha;
     const double* p = p_is_b ? v.pb : v.pa;
     double loc[2] = {0.0, 0.0};
     // Pairs of cells with 16-byte loads and stores where every vector is
@@ -4370,7 +4401,12 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_b(gf_krylov_t K, in
         double2* z2 = reinterpret_cast<double2*>(v.z);
         const double2* d2 = reinterpret_cast<const double2*>(K.diag);
         for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += gridDim.x * blockDim.x) {
-            const double2 xv = __ldcg(x2 + i), pv = __ldcg(p2 + i), rv = __ldcg(r2 + i), qv = __ldcg(q2 + i);
+            double2 xv = make_double2(0.0, 0.0), pv = xv;
+            if (!XA) {
+                xv = __ldcg(x2 + i);
+                pv = __ldcg(p2 + i);
+            }
+            const double2 rv = __ldcg(r2 + i), qv = __ldcg(q2 + i);
             const double2 dv = __ldg(d2 + i);
             const double r0 = rv.x - alpha * qv.x, r1 = rv.y - alpha * qv.y;
             double i0 = 1.0, i1 = 1.0;
@@ -4379,7 +4415,7 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_b(gf_krylov_t K, in
                 i1 = fabs(dv.y) < 2.220446049250313e-16 ? 1.0 : 1.0 / dv.y;
             }
             const double z0 = i0 * r0, z1 = i1 * r1;
-            __stcg(x2 + i, make_double2(xv.x + alpha * pv.x, xv.y + alpha * pv.y));
+            if (!XA) __stcg(x2 + i, make_double2(xv.x + alpha * pv.x, xv.y + alpha * pv.y));
             __stcg(r2 + i, make_double2(r0, r1));
             __stcg(z2 + i, make_double2(z0, z1));
             loc[0] = norm_acc(norm_acc(loc[0], r0, linf), r1, linf);
@@ -4387,7 +4423,7 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_b(gf_krylov_t K, in
         }
     } else {
         for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-            __stcg(K.x + c, __ldcg(K.x + c) + alpha * __ldcg(p + c));
+            if (!XA) __stcg(K.x + c, __ldcg(K.x + c) + alpha * __ldcg(p + c));
             const double rk = __ldcg(v.r + c) - alpha * __ldcg(v.q + c);
             const double zk = inv_diag(K.diag, c, jac) * rk;
             __stcg(v.r + c, rk);
@@ -4515,13 +4551,13 @@ static int split_loop_exec(const void* fa, const void* fb, const gf_krylov_t& K,
     return GF_OK;
 }
 
-template <class Rows, int MINB, bool PAIRS, bool QREC = false>
+template <class Rows, int MINB, bool PAIRS, bool QREC = false, bool XA = false>
 static int launch_split_rows(const gf_krylov_t* k, const Rows& rows, cudaStream_t st) {
     int dev = 0, sms = 0, per_sm = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cgs_a<Rows, MINB, false, QREC>, kSplitThreads, 0);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cgs_a<Rows, MINB, false, QREC, XA>, kSplitThreads, 0);
     if (e != cudaSuccess || per_sm < 1) {
         set_error("gf_pcg_solve: split CG set-up failed: %s", cudaGetErrorString(e));
         return GF_ERR_CUDA;
@@ -4553,7 +4589,8 @@ static int launch_split_rows(const gf_krylov_t* k, const Rows& rows, cudaStream_
     if (split_graph_enabled() && cudaStreamIsCapturing(st, &cap) == cudaSuccess &&
         cap == cudaStreamCaptureStatusNone) {
         cudaGraphExec_t exec = nullptr;
-        const int rc = split_loop_exec((const void*)k_cgs_a<Rows, MINB, true, QREC>, (const void*)k_cgs_b<MINB, true, PAIRS>, K,
+        const int rc = split_loop_exec((const void*)k_cgs_a<Rows, MINB, true, QREC, XA>,
+                                       (const void*)k_cgs_b<MINB, true, PAIRS, XA>, K,
                                        &rows, sizeof(Rows), g, &exec);
         if (rc != GF_OK) return rc;
         e = cudaGraphLaunch(exec, st);
@@ -4565,10 +4602,10 @@ static int launch_split_rows(const gf_krylov_t* k, const Rows& rows, cudaStream_
     }
     for (int it = 1; it <= k->max_iter; ++it) {
         // p_old is pa at odd iterations (p_new then goes to pb), pb at even.
-        k_cgs_a<Rows, MINB, false, QREC><<<g, kSplitThreads, 0, st>>>(K, rows, it, it & 1, 0);
-        k_cgs_b<MINB, false, PAIRS><<<g, kSplitThreads, 0, st>>>(K, it, it & 1);
+        k_cgs_a<Rows, MINB, false, QREC, XA><<<g, kSplitThreads, 0, st>>>(K, rows, it, it & 1, 0);
+        k_cgs_b<MINB, false, PAIRS, XA><<<g, kSplitThreads, 0, st>>>(K, it, it & 1);
     }
-    k_cgs_a<Rows, MINB, false, QREC><<<g, kSplitThreads, 0, st>>>(K, rows, k->max_iter + 1, (k->max_iter + 1) & 1, 0);
+    k_cgs_a<Rows, MINB, false, QREC, XA><<<g, kSplitThreads, 0, st>>>(K, rows, k->max_iter + 1, (k->max_iter + 1) & 1, 0);
     e = cudaGetLastError();
     if (e != cudaSuccess) {
         set_error("gf_pcg_solve: split CG launch failed: %s", cudaGetErrorString(e));
@@ -4577,7 +4614,7 @@ static int launch_split_rows(const gf_krylov_t* k, const Rows& rows, cudaStream_
     return GF_OK;
 }
 
-template <int MINB, bool PAIRS, int GRP = 1, bool QREC = false>
+template <int MINB, bool PAIRS, int GRP = 1, bool QREC = false, bool XA = false>
 static int launch_split_m(const gf_krylov_t* k, void* stream) {
     const int64_t row_span = (int64_t)(k->stride_y > 0 ? 6 : (k->width > 6 ? k->width : 6)) * k->n;
     if (row_span >= ((int64_t)1 << 31)) {
@@ -4587,17 +4624,17 @@ static int launch_split_m(const gf_krylov_t* k, void* stream) {
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     if (k->stride_y > 0) {
         if (k->symmetric)
-            return launch_split_rows<BoxRows<double, true, false, int>, MINB, PAIRS, QREC>(
+            return launch_split_rows<BoxRows<double, true, false, int>, MINB, PAIRS, QREC, XA>(
                 k, BoxRows<double, true, false, int>{k->val, (int)k->n, (int)k->stride_y, (int)k->stride_z}, st);
-        return launch_split_rows<BoxRows<double, false, false, int>, MINB, PAIRS, QREC>(
+        return launch_split_rows<BoxRows<double, false, false, int>, MINB, PAIRS, QREC, XA>(
             k, BoxRows<double, false, false, int>{k->val, (int)k->n, (int)k->stride_y, (int)k->stride_z}, st);
     }
     // One slot at a time (the loop of a plain SpMV): the occupancy, not the
     // loads of one thread, keeps the memory system busy.
     if (k->width == 6)
-        return launch_split_rows<EllRows<double, 6, int, 1>, MINB, PAIRS, QREC>(
+        return launch_split_rows<EllRows<double, 6, int, 1>, MINB, PAIRS, QREC, XA>(
             k, EllRows<double, 6, int, 1>{k->val, k->nbr, (int)k->n, k->width, k->row_len}, st);
-    return launch_split_rows<EllRows<double, 0, int, GRP>, MINB, PAIRS, QREC>(
+    return launch_split_rows<EllRows<double, 0, int, GRP>, MINB, PAIRS, QREC, XA>(
         k, EllRows<double, 0, int, GRP>{k->val, k->nbr, (int)k->n, k->width, k->row_len}, st);
 }
 
@@ -4605,7 +4642,9 @@ static int launch_split_m(const gf_krylov_t* k, void* stream) {
 // 21: 8 with the update kernel on pairs of cells; 22: 7, pairs; 23: 7,
 // pairs, ELL slots loaded two at a time; 24: 6, pairs, four at a time;
 // 25: 8, pairs, q = A p by recurrence (the rows gather z alone); 26: 8,
-// q by recurrence, update one cell at a time.
+// q by recurrence, update one cell at a time; 27: 25 with x += alpha p in
+// the row kernel (the update kernel reads neither x nor p); 28: 21 with the
+// same.
 static int launch_split(const gf_krylov_t* k, void* stream, int which) {
     switch (which) {
         case 1: return launch_split_m<6, false>(k, stream);
@@ -4615,6 +4654,8 @@ static int launch_split(const gf_krylov_t* k, void* stream, int which) {
         case 5: return launch_split_m<6, true, 4>(k, stream);
         case 6: return launch_split_m<8, true, 1, true>(k, stream);
         case 7: return launch_split_m<8, false, 1, true>(k, stream);
+        case 8: return launch_split_m<8, true, 1, true, true>(k, stream);
+        case 9: return launch_split_m<8, true, 1, false, true>(k, stream);
         default: return launch_split_m<8, false>(k, stream);
     }
 }

@@ -90,7 +90,9 @@ typedef struct gf_mesh {
     /* ELL adjacency [W][C]: slot code s = (face << 1) | side, face < F an
      * internal face (side 0: cell is owner), face >= F the domain face
      * face - F; -1 marks an empty slot.  nbr is the coupled cell (the cell
-     * itself for boundary or empty slots). */
+     * itself for boundary or empty slots).  A row's used slots come first
+     * (no used slot after an empty one): the octree kernels (6 < W <= 12)
+     * stop a row at its first empty slot from slot 6 on. */
     const int32_t* ell_code;
     const int32_t* ell_nbr;
     /* boundary faces [Nb] */
@@ -214,8 +216,8 @@ typedef struct gf_krylov {
     int64_t stride_z;
     int32_t symmetric;    /* 1 (box only): A is symmetric, only + slots read */
     int32_t block_cap;    /* > 0: at most this many persistent blocks (tuning) */
-    int32_t variant;      /* CG launch shape (0..26, see gf_krylov.cu and
-                             solvers/autotune.py); 19..26: the split CG, two
+    int32_t variant;      /* CG launch shape (0..28, see gf_krylov.cu and
+                             solvers/autotune.py); 19..28: the split CG, two
                              plain kernels an iteration, run as a CUDA graph
                              while-loop on the stream (every permitted
                              iteration enqueued inside a stream capture, or

@@ -705,7 +705,7 @@ def test_grad_linear_steps_and_operator_match_reference(name):
     _check(fvc.grad(algo.U).data, golden["op_grad_U"], "grad_U", 1e-10)
 
 
-@pytest.mark.parametrize("variant", [15, 16, 17, 18, 19, 20, 21, 22, 23, 24, 25, 26])
+@pytest.mark.parametrize("variant", [15, 16, 17, 18, 19, 20, 21, 22, 23, 24, 25, 26, 27, 28])
 def test_lean_ell_cg_fixed_iterations_match_register_kernel(variant):
     """The lean ELL CG (32-bit indices, x update moved into the next gather
     pass) and the split CG forms against the register kernel: exactly 60
@@ -722,7 +722,62 @@ def test_lean_ell_cg_fixed_iterations_match_register_kernel(variant):
         st = s.solve_arrays(sysm, sysm.diag, sysm.val, sysm.rhs, x, symmetric=True)
         assert st[0].iterations == 60 and st[0].status == "max_iter"
         xs.append(to_np(x))
-    assert rel(xs[1], xs[0]) < (1e-9 if variant in (25, 26) else 1e-11)
+    assert rel(xs[1], xs[0]) < (1e-9 if variant in (25, 26, 27) else 1e-11)
+
+
+@pytest.mark.parametrize("xa,base", [(27, 25), (28, 21)])
+@pytest.mark.parametrize("max_iter,rtol", [(60, 0.0), (500, 1e-8)])
+def test_split_cg_x_update_in_row_kernel_is_bitwise(xa, base, max_iter, rtol):
+    """Variants 27/28 apply x += alpha p in the next row kernel (and, at the
+    stop, in the kernel that ends the solve) instead of the update kernel:
+    the same values in the same order, so x is bitwise that of 25/21, on a
+    fixed-length solve and on one that converges, through the graph loop
+    and enqueued inside a stream capture."""
+    from gridfoam_b200.fv import fvm
+    from gridfoam_b200.meta.config import SolverConfig
+    from gridfoam_b200.solvers.krylov import CGSolver
+
+    _, _, grid, algo = device_case("ibcyl_oct")
+    A = -fvm.laplacian(1.0, algo.p)
+    A.diag = A.diag + 1e-2 * grid.cell_volumes
+    rhs = torch.linspace(-1.0, 1.0, grid.num_cells, dtype=torch.float64, device="cuda").reshape(1, -1)
+    cfg = SolverConfig(method="cg", preconditioner="jacobi", tolerance=0.0, rel_tolerance=rtol, max_iter=max_iter)
+    xs, its = [], []
+    for v in (base, xa):
+        s = CGSolver(cfg)
+        s.variant = v
+        x = torch.zeros_like(rhs)
+        st = s.solve_arrays(grid, A.diag_store, A.val, rhs, x, symmetric=True)[0]
+        its.append((st.iterations, st.status))
+        xs.append(x)
+    assert its[0] == its[1]
+    assert (its[0][0] == max_iter) if rtol == 0.0 else (0 < its[0][0] < max_iter)
+    assert torch.equal(xs[0], xs[1])
+    caps = []
+    for v in (base, xa):
+        s = CGSolver(cfg)
+        s.variant = v
+        s.host_stats = False
+        x = torch.zeros_like(rhs)
+        stream = torch.cuda.Stream()
+        stream.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(stream):
+            s.solve_arrays(grid, A.diag_store, A.val, rhs, x, symmetric=True)  # workspace allocation
+        torch.cuda.synchronize()
+        x.zero_()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=stream):
+            s.solve_arrays(grid, A.diag_store, A.val, rhs, x, symmetric=True)
+        x.zero_()
+        torch.cuda.synchronize()
+        g.replay()
+        torch.cuda.synchronize()
+        stats = next(iter(s._stats_dev.values())).cpu().numpy()
+        assert int(stats[0, 2]) == its[0][0]
+        caps.append(x.clone())
+        del g
+    assert torch.equal(caps[0], caps[1])
+    assert torch.equal(caps[1], xs[1])
 
 
 def test_split_cg_limits_and_statuses():
