@@ -143,8 +143,9 @@ def pcg_bytes_setup(C: int, F: int, s: int = 8) -> float:
 # k_cgs_b launch in an ncu capture on the 192x120x24 base (1,729,632 cells;
 # the working set exceeds L2, so the traffic grows in proportion to the
 # cells), against 159.8 B of the byte model.  Variant 25 (q by recurrence):
-# 204.6 + 83.5 MB (the recurrence reads q of the own cell).
-PCG_DRAM_BYTES_PER_CELL_ITER = {25: 166.6}
+# 204.6 + 83.5 MB (the recurrence reads q of the own cell); variant 27 (the
+# same with x += alpha p in the row kernel): 231.0 + 43.4 MB.
+PCG_DRAM_BYTES_PER_CELL_ITER = {25: 166.6, 27: 158.6}
 
 
 def _oracle_threads() -> int:
