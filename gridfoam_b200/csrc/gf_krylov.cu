@@ -4133,7 +4133,7 @@ __global__ void __launch_bounds__(kKThreads) k_bicgstab_mixed(gf_krylov_t K) {
 // kernels are enqueued without a host synchronisation; once the stopping
 // test has passed the remaining ones return at once.
 constexpr int kSplitVariant = 19;
-constexpr int kSplitVariants = 10;
+constexpr int kSplitVariants = 12;
 constexpr int kSplitThreads = 256;
 
 struct SplitScalars {  // in the control block, after KCtl
@@ -4229,6 +4229,23 @@ __device__ __forceinline__ SplitVec split_vec(const gf_krylov_t& K) {
     return {vec, vec + n, vec + 2 * n, vec + 3 * n, vec + 4 * n, partials, partials + kMaxBlocks};
 }
 
+// L2 prefetch of one address (a hint: no register result, no fault; every
+// address given is inside its array).
+__device__ __forceinline__ void pf_l2(const void* p) { asm volatile("prefetch.L2 [%0];" ::"l"(p)); }
+
+// The first slots (up to six) of row c of an ELL operator: what the row
+// kernel's first pass reads of the matrix.  Box operators: nothing.
+template <class Rows>
+__device__ __forceinline__ void split_prefetch_rows(const Rows&, int) {}
+template <typename T, int WIDTH, typename I, int GRP>
+__device__ __forceinline__ void split_prefetch_rows(const EllRows<T, WIDTH, I, GRP>& r, int c) {
+    const int ws = WIDTH > 0 ? WIDTH : (r.w < 6 ? r.w : 6);
+    for (int s = 0; s < ws; ++s) {
+        pf_l2(r.val + (int64_t)s * r.n + c);
+        pf_l2(r.nbr + (int64_t)s * r.n + c);
+    }
+}
+
 template <class Rows, int MINB>
 __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_init(gf_krylov_t K, Rows rows) {
     const SplitVec v = split_vec(K);
@@ -4258,7 +4275,10 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_init(gf_krylov_t K,
 // applies the previous iteration's x += alpha p (it reads p_old anyway), so
 // the update kernel reads neither x nor p; x gets the same values in the
 // same order as in the other forms.
-template <class Rows, int MINB, bool LOOP, bool QREC = false, bool XA = false>
+// PF: before summing the previous kernel's partials (a chain of dependent
+// L2 reads during which HBM would idle), each thread prefetches into L2 what
+// its first PF cells will read, so the streaming starts with the kernel.
+template <class Rows, int MINB, bool LOOP, bool QREC = false, bool XA = false, int PF = 0>
 __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_a(gf_krylov_t K, Rows rows, int it, int pa_old,
                                                               cudaGraphConditionalHandle loop) {
     SplitScalars* S = split_scalars(K);
@@ -4273,6 +4293,18 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_a(gf_krylov_t K, Ro
     const SplitVec v = split_vec(K);
     const int n = (int)K.n;
     const bool linf = K.norm_inf != 0;
+    if (PF > 0) {
+        const int step = gridDim.x * blockDim.x;
+        int c = blockIdx.x * blockDim.x + threadIdx.x;
+        for (int k = 0; k < PF && c < n; ++k, c += step) {
+            pf_l2(v.z + c);
+            if (it > 1) pf_l2((pa_old ? v.pa : v.pb) + c);
+            if (QREC && it > 1) pf_l2(v.q + c);
+            if (XA && it > 1) pf_l2(K.x + c);
+            pf_l2(K.diag + c);
+            split_prefetch_rows(rows, c);
+        }
+    }
     __shared__ double s_beta;
     __shared__ int s_stop;
     double red[2];
@@ -4365,7 +4397,7 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_a(gf_krylov_t K, Ro
 
 // x += alpha p (not in the XA forms, whose k_cgs_a applies it); r -= alpha q;
 // z = M r; partials of |r| and r.z.
-template <int MINB, bool LOOP, bool PAIRS, bool XA = false>
+template <int MINB, bool LOOP, bool PAIRS, bool XA = false, int PF = 0>
 __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_b(gf_krylov_t K, int it, int p_is_b) {
     SplitScalars* S = split_scalars(K);
     if (*(volatile int*)&S->done) return;
@@ -4381,6 +4413,20 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_b(gf_krylov_t K, in
     const SplitVec v = split_vec(K);
     const int n = (int)K.n;
     const bool jac = K.jacobi != 0, linf = K.norm_inf != 0;
+    if (PF > 0) {
+        // the first 2 PF cells (pairs) of this thread's grid-stride loop
+        const int64_t step = (int64_t)gridDim.x * blockDim.x * (PAIRS ? 2 : 1);
+        for (int64_t c = (int64_t)(blockIdx.x * blockDim.x + threadIdx.x) * (PAIRS ? 2 : 1), k = 0; k < 2 * PF && c < n;
+             ++k, c += step) {
+            pf_l2(v.r + c);
+            pf_l2(v.q + c);
+            pf_l2(K.diag + c);
+            if (!XA) {
+                pf_l2(K.x + c);
+                pf_l2((p_is_b ? v.pb : v.pa) + c);
+            }
+        }
+    }
     double red[1];
     split_sum<1>(v.p1, gridDim.x, 0u, red);
     const double alpha = S->rz[it & 1] / red[0];
@@ -4551,13 +4597,13 @@ static int split_loop_exec(const void* fa, const void* fb, const gf_krylov_t& K,
     return GF_OK;
 }
 
-template <class Rows, int MINB, bool PAIRS, bool QREC = false, bool XA = false>
+template <class Rows, int MINB, bool PAIRS, bool QREC = false, bool XA = false, int PF = 0>
 static int launch_split_rows(const gf_krylov_t* k, const Rows& rows, cudaStream_t st) {
     int dev = 0, sms = 0, per_sm = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cgs_a<Rows, MINB, false, QREC, XA>, kSplitThreads, 0);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cgs_a<Rows, MINB, false, QREC, XA, PF>, kSplitThreads, 0);
     if (e != cudaSuccess || per_sm < 1) {
         set_error("gf_pcg_solve: split CG set-up failed: %s", cudaGetErrorString(e));
         return GF_ERR_CUDA;
@@ -4589,8 +4635,8 @@ static int launch_split_rows(const gf_krylov_t* k, const Rows& rows, cudaStream_
     if (split_graph_enabled() && cudaStreamIsCapturing(st, &cap) == cudaSuccess &&
         cap == cudaStreamCaptureStatusNone) {
         cudaGraphExec_t exec = nullptr;
-        const int rc = split_loop_exec((const void*)k_cgs_a<Rows, MINB, true, QREC, XA>,
-                                       (const void*)k_cgs_b<MINB, true, PAIRS, XA>, K,
+        const int rc = split_loop_exec((const void*)k_cgs_a<Rows, MINB, true, QREC, XA, PF>,
+                                       (const void*)k_cgs_b<MINB, true, PAIRS, XA, PF>, K,
                                        &rows, sizeof(Rows), g, &exec);
         if (rc != GF_OK) return rc;
         e = cudaGraphLaunch(exec, st);
@@ -4602,10 +4648,10 @@ static int launch_split_rows(const gf_krylov_t* k, const Rows& rows, cudaStream_
     }
     for (int it = 1; it <= k->max_iter; ++it) {
         // p_old is pa at odd iterations (p_new then goes to pb), pb at even.
-        k_cgs_a<Rows, MINB, false, QREC, XA><<<g, kSplitThreads, 0, st>>>(K, rows, it, it & 1, 0);
-        k_cgs_b<MINB, false, PAIRS, XA><<<g, kSplitThreads, 0, st>>>(K, it, it & 1);
+        k_cgs_a<Rows, MINB, false, QREC, XA, PF><<<g, kSplitThreads, 0, st>>>(K, rows, it, it & 1, 0);
+        k_cgs_b<MINB, false, PAIRS, XA, PF><<<g, kSplitThreads, 0, st>>>(K, it, it & 1);
     }
-    k_cgs_a<Rows, MINB, false, QREC, XA><<<g, kSplitThreads, 0, st>>>(K, rows, k->max_iter + 1, (k->max_iter + 1) & 1, 0);
+    k_cgs_a<Rows, MINB, false, QREC, XA, PF><<<g, kSplitThreads, 0, st>>>(K, rows, k->max_iter + 1, (k->max_iter + 1) & 1, 0);
     e = cudaGetLastError();
     if (e != cudaSuccess) {
         set_error("gf_pcg_solve: split CG launch failed: %s", cudaGetErrorString(e));
@@ -4614,7 +4660,7 @@ static int launch_split_rows(const gf_krylov_t* k, const Rows& rows, cudaStream_
     return GF_OK;
 }
 
-template <int MINB, bool PAIRS, int GRP = 1, bool QREC = false, bool XA = false>
+template <int MINB, bool PAIRS, int GRP = 1, bool QREC = false, bool XA = false, int PF = 0>
 static int launch_split_m(const gf_krylov_t* k, void* stream) {
     const int64_t row_span = (int64_t)(k->stride_y > 0 ? 6 : (k->width > 6 ? k->width : 6)) * k->n;
     if (row_span >= ((int64_t)1 << 31)) {
@@ -4624,17 +4670,17 @@ static int launch_split_m(const gf_krylov_t* k, void* stream) {
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     if (k->stride_y > 0) {
         if (k->symmetric)
-            return launch_split_rows<BoxRows<double, true, false, int>, MINB, PAIRS, QREC, XA>(
+            return launch_split_rows<BoxRows<double, true, false, int>, MINB, PAIRS, QREC, XA, PF>(
                 k, BoxRows<double, true, false, int>{k->val, (int)k->n, (int)k->stride_y, (int)k->stride_z}, st);
-        return launch_split_rows<BoxRows<double, false, false, int>, MINB, PAIRS, QREC, XA>(
+        return launch_split_rows<BoxRows<double, false, false, int>, MINB, PAIRS, QREC, XA, PF>(
             k, BoxRows<double, false, false, int>{k->val, (int)k->n, (int)k->stride_y, (int)k->stride_z}, st);
     }
     // One slot at a time (the loop of a plain SpMV): the occupancy, not the
     // loads of one thread, keeps the memory system busy.
     if (k->width == 6)
-        return launch_split_rows<EllRows<double, 6, int, 1>, MINB, PAIRS, QREC, XA>(
+        return launch_split_rows<EllRows<double, 6, int, 1>, MINB, PAIRS, QREC, XA, PF>(
             k, EllRows<double, 6, int, 1>{k->val, k->nbr, (int)k->n, k->width, k->row_len}, st);
-    return launch_split_rows<EllRows<double, 0, int, GRP>, MINB, PAIRS, QREC, XA>(
+    return launch_split_rows<EllRows<double, 0, int, GRP>, MINB, PAIRS, QREC, XA, PF>(
         k, EllRows<double, 0, int, GRP>{k->val, k->nbr, (int)k->n, k->width, k->row_len}, st);
 }
 
@@ -4644,7 +4690,9 @@ static int launch_split_m(const gf_krylov_t* k, void* stream) {
 // 25: 8, pairs, q = A p by recurrence (the rows gather z alone); 26: 8,
 // q by recurrence, update one cell at a time; 27: 25 with x += alpha p in
 // the row kernel (the update kernel reads neither x nor p); 28: 21 with the
-// same.
+// same; 29: 27 with the first cell's data prefetched into L2 while each
+// kernel sums the previous kernel's partials; 30: the same for the first two
+// cells (four of the update kernel).
 static int launch_split(const gf_krylov_t* k, void* stream, int which) {
     switch (which) {
         case 1: return launch_split_m<6, false>(k, stream);
@@ -4656,6 +4704,8 @@ static int launch_split(const gf_krylov_t* k, void* stream, int which) {
         case 7: return launch_split_m<8, false, 1, true>(k, stream);
         case 8: return launch_split_m<8, true, 1, true, true>(k, stream);
         case 9: return launch_split_m<8, true, 1, false, true>(k, stream);
+        case 10: return launch_split_m<8, true, 1, true, true, 1>(k, stream);
+        case 11: return launch_split_m<8, true, 1, true, true, 2>(k, stream);
         default: return launch_split_m<8, false>(k, stream);
     }
 }

@@ -55,7 +55,7 @@ def default_variant(n: int, mixed: bool, symmetric: bool, box: bool = True) -> i
     q-recurrence form at 64^3); then, up to ~1.3M cells, the q-recurrence
     form (q = A z + beta q, z alone gathered; 14.7 us at 1M cells); above
     that the shared-memory tiled kernel for symmetric boxes, else the split
-    CG (two plain kernels an iteration, variant 27).  FP32-inner (mixed) solves: 256-thread register
+    CG (two plain kernels an iteration, variant 29).  FP32-inner (mixed) solves: 256-thread register
     blocks below ~32K cells (6.5 us an inner iteration at 24^3, as for the
     shared-memory forms); then, up to ~1.3M cells, the single-reduction
     form with the halo sync (6.7 against 7.0 us for the q-recurrence form
@@ -73,12 +73,15 @@ def default_variant(n: int, mixed: bool, symmetric: bool, box: bool = True) -> i
     # Above ~1.3M cells (beyond L2): the staged tiles on symmetric boxes;
     # on other rows the split CG, two plain kernels an iteration, with
     # q = A p by recurrence (the rows gather z alone), x += alpha p in the
-    # row kernel and the update kernel on pairs of cells (fixed 100
-    # iterations on the 4.08M-cell cylinder-wake octree: 157.4-157.7 us an
-    # iteration, against 158.5-159.6 with x updated in the update kernel,
-    # 163.0 with q gathered from p, 163.0 with the update one cell at a time
-    # and 164.5 for the 512-thread persistent kernel).
-    return 5 if symmetric and box else 27
+    # row kernel, the update kernel on pairs of cells, and each thread's
+    # first cell prefetched into L2 while the kernel sums the previous
+    # kernel's partials (fixed 100 iterations on the 4.08M-cell
+    # cylinder-wake octree: 152.4-152.7 us an iteration against 155.7-156.2
+    # without the prefetch (159.6 prefetching two cells), 158.5-159.6 with x
+    # updated in the update kernel, 163.0 with q gathered from p, 163.0 with
+    # the update one cell at a time and 164.5 for the 512-thread persistent
+    # kernel).
+    return 5 if symmetric and box else 29
 
 
 class DeviceKrylov(LinearSolver):
