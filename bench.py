@@ -144,8 +144,9 @@ def pcg_bytes_setup(C: int, F: int, s: int = 8) -> float:
 # the working set exceeds L2, so the traffic grows in proportion to the
 # cells), against 159.8 B of the byte model.  Variant 25 (q by recurrence):
 # 204.6 + 83.5 MB (the recurrence reads q of the own cell); variant 27 (the
-# same with x += alpha p in the row kernel): 231.0 + 43.4 MB.
-PCG_DRAM_BYTES_PER_CELL_ITER = {25: 166.6, 27: 158.6}
+# same with x += alpha p in the row kernel): 231.0 + 43.4 MB; variant 29
+# (27 with L2 prefetches of each thread's first cell): 229.1 + 42.4 MB.
+PCG_DRAM_BYTES_PER_CELL_ITER = {25: 166.6, 27: 158.6, 29: 157.0}
 
 
 def _oracle_threads() -> int:
