@@ -752,12 +752,12 @@ def run_gpu(args) -> None:
         },
         "roofline": {
             "kernel": (f"pressure CG, variant {variant}: " + (
-                "split Jacobi-PCG (k_cgs_a: " + ("x += alpha p, " if variant in (27, 28, 29, 30) else "") +
-                ("p update + q = A z + beta q + p.q partials; " if variant in (25, 26, 27, 29, 30)
+                "split Jacobi-PCG (k_cgs_a: " + ("x += alpha p, " if variant in (27, 28, 29, 30, 31) else "") +
+                ("p update + q = A z + beta q + p.q partials; " if variant in (25, 26, 27, 29, 30, 31)
                  else "p update + SpMV + p.q partials; ") +
-                ("k_cgs_b: r/z update + partials" if variant in (27, 28, 29, 30) else "k_cgs_b: x/r/z update + partials") +
-                ("; first cell prefetched into L2" if variant == 29 else "") +
-                "), octree ELL rows, fp64" if 19 <= variant <= 30 else
+                ("k_cgs_b: r/z update + partials" if variant in (27, 28, 29, 30, 31) else "k_cgs_b: x/r/z update + partials") +
+                ("; first cell prefetched into L2" if variant in (29, 31) else "") +
+                "), octree ELL rows, fp64" if 19 <= variant <= 31 else
                 "persistent Jacobi-PCG on the octree ELL rows, fp64")),
             "bound": "hbm",
             "achieved": achieved,

@@ -4133,7 +4133,7 @@ __global__ void __launch_bounds__(kKThreads) k_bicgstab_mixed(gf_krylov_t K) {
 // kernels are enqueued without a host synchronisation; once the stopping
 // test has passed the remaining ones return at once.
 constexpr int kSplitVariant = 19;
-constexpr int kSplitVariants = 12;
+constexpr int kSplitVariants = 13;
 constexpr int kSplitThreads = 256;
 
 struct SplitScalars {  // in the control block, after KCtl
@@ -4278,10 +4278,29 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_init(gf_krylov_t K,
 // PF: before summing the previous kernel's partials (a chain of dependent
 // L2 reads during which HBM would idle), each thread prefetches into L2 what
 // its first PF cells will read, so the streaming starts with the kernel.
-template <class Rows, int MINB, bool LOOP, bool QREC = false, bool XA = false, int PF = 0>
+// EARLY: in the graph loop, the prefetches that do not depend on the
+// iteration number go out before the loop's control reads, and the scalars
+// of the previous kernels (threshold, r.z, alpha) are read before the
+// partial sums instead of after them (the same values).
+template <class Rows, int MINB, bool LOOP, bool QREC = false, bool XA = false, int PF = 0, bool EARLY = false>
 __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_a(gf_krylov_t K, Rows rows, int it, int pa_old,
                                                               cudaGraphConditionalHandle loop) {
     SplitScalars* S = split_scalars(K);
+    const SplitVec v = split_vec(K);
+    const int n = (int)K.n;
+    // early prefetch: what does not depend on the iteration number (in the
+    // graph loop this kernel never runs after the solve has stopped)
+    constexpr bool early_pf = EARLY && LOOP && PF > 0;
+    if (early_pf) {
+        const int c = blockIdx.x * blockDim.x + threadIdx.x;
+        if (c < n) {
+            pf_l2(v.z + c);
+            if (QREC) pf_l2(v.q + c);
+            if (XA) pf_l2(K.x + c);
+            pf_l2(K.diag + c);
+            split_prefetch_rows(rows, c);
+        }
+    }
     if (*(volatile int*)&S->done) {
         if (LOOP && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(loop, 0);
         return;
@@ -4290,10 +4309,11 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_a(gf_krylov_t K, Ro
         it = *(volatile int*)&S->it_a;
         pa_old = it & 1;
     }
-    const SplitVec v = split_vec(K);
-    const int n = (int)K.n;
     const bool linf = K.norm_inf != 0;
-    if (PF > 0) {
+    if (early_pf) {
+        const int c = blockIdx.x * blockDim.x + threadIdx.x;
+        if (c < n && it > 1) pf_l2((pa_old ? v.pa : v.pb) + c);
+    } else if (PF > 0) {
         const int step = gridDim.x * blockDim.x;
         int c = blockIdx.x * blockDim.x + threadIdx.x;
         for (int k = 0; k < PF && c < n; ++k, c += step) {
@@ -4303,6 +4323,14 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_a(gf_krylov_t K, Ro
             if (XA && it > 1) pf_l2(K.x + c);
             pf_l2(K.diag + c);
             split_prefetch_rows(rows, c);
+        }
+    }
+    double e_thresh = 0.0, e_rz = 0.0, e_alpha = 0.0;
+    if (EARLY && it > 1) {
+        e_alpha = S->alpha;
+        if (threadIdx.x == 0) {
+            e_thresh = S->thresh;
+            e_rz = S->rz[(it - 1) & 1];
         }
     }
     __shared__ double s_beta;
@@ -4319,14 +4347,14 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_a(gf_krylov_t K, Ro
                 S->thresh = thresh;
             }
         } else {
-            thresh = S->thresh;
+            thresh = EARLY ? e_thresh : S->thresh;
         }
         int status = -1;
         if (fin < thresh) status = GF_OK;
         else if (!isfinite(fin)) status = GF_NONFINITE;
         else if (it > K.max_iter || it < 1) status = GF_MAX_ITER;
         s_stop = status >= 0;
-        s_beta = it == 1 ? 0.0 : red[1] / S->rz[(it - 1) & 1];
+        s_beta = it == 1 ? 0.0 : red[1] / (EARLY ? e_rz : S->rz[(it - 1) & 1]);
         if (blockIdx.x == 0) {
             S->fin = fin;
             if (status >= 0) {
@@ -4354,7 +4382,7 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_a(gf_krylov_t K, Ro
     const double* p_old = pa_old ? v.pa : v.pb;
     // XA: x += alpha p of the previous iteration (none before the first).
     const bool upd = XA && it > 1;
-    const double alpha = upd ? S->alpha : 0.0;
+    const double alpha = upd ? (EARLY ? e_alpha : S->alpha) : 0.0;
     if (s_stop) {
         if (upd)
             for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
@@ -4397,9 +4425,29 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_a(gf_krylov_t K, Ro
 
 // x += alpha p (not in the XA forms, whose k_cgs_a applies it); r -= alpha q;
 // z = M r; partials of |r| and r.z.
-template <int MINB, bool LOOP, bool PAIRS, bool XA = false, int PF = 0>
+template <int MINB, bool LOOP, bool PAIRS, bool XA = false, int PF = 0, bool EARLY = false>
 __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_b(gf_krylov_t K, int it, int p_is_b) {
     SplitScalars* S = split_scalars(K);
+    const SplitVec v = split_vec(K);
+    const int n = (int)K.n;
+    // the first 2 PF cells (pairs) of this thread's grid-stride loop; with
+    // EARLY in the graph loop (XA: nothing here depends on the iteration
+    // number) before the loop's control reads
+    auto prefetch = [&](int pb) {
+        const int64_t step = (int64_t)gridDim.x * blockDim.x * (PAIRS ? 2 : 1);
+        for (int64_t c = (int64_t)(blockIdx.x * blockDim.x + threadIdx.x) * (PAIRS ? 2 : 1), k = 0; k < 2 * PF && c < n;
+             ++k, c += step) {
+            pf_l2(v.r + c);
+            pf_l2(v.q + c);
+            pf_l2(K.diag + c);
+            if (!XA) {
+                pf_l2(K.x + c);
+                pf_l2((pb ? v.pb : v.pa) + c);
+            }
+        }
+    };
+    constexpr bool early_pf = EARLY && LOOP && XA && PF > 0;
+    if (early_pf) prefetch(0);
     if (*(volatile int*)&S->done) return;
     if (XA && *(volatile int*)&S->stop) {
         if (blockIdx.x == 0 && threadIdx.x == 0) S->done = 1;
@@ -4410,26 +4458,12 @@ __global__ void __launch_bounds__(kSplitThreads, MINB) k_cgs_b(gf_krylov_t K, in
         p_is_b = it & 1;
         if (blockIdx.x == 0 && threadIdx.x == 0) S->it_a = it + 1;
     }
-    const SplitVec v = split_vec(K);
-    const int n = (int)K.n;
     const bool jac = K.jacobi != 0, linf = K.norm_inf != 0;
-    if (PF > 0) {
-        // the first 2 PF cells (pairs) of this thread's grid-stride loop
-        const int64_t step = (int64_t)gridDim.x * blockDim.x * (PAIRS ? 2 : 1);
-        for (int64_t c = (int64_t)(blockIdx.x * blockDim.x + threadIdx.x) * (PAIRS ? 2 : 1), k = 0; k < 2 * PF && c < n;
-             ++k, c += step) {
-            pf_l2(v.r + c);
-            pf_l2(v.q + c);
-            pf_l2(K.diag + c);
-            if (!XA) {
-                pf_l2(K.x + c);
-                pf_l2((p_is_b ? v.pb : v.pa) + c);
-            }
-        }
-    }
+    if (PF > 0 && !early_pf) prefetch(p_is_b);
+    const double rz = EARLY ? S->rz[it & 1] : 0.0;
     double red[1];
     split_sum<1>(v.p1, gridDim.x, 0u, red);
-    const double alpha = S->rz[it & 1] / red[0];
+    const double alpha = (EARLY ? rz : S->rz[it & 1]) / red[0];
     if (XA && blockIdx.x == 0 && threadIdx.x == 0) S->alpha = alpha;
     const double* p = p_is_b ? v.pb : v.pa;
     double loc[2] = {0.0, 0.0};
@@ -4597,13 +4631,13 @@ static int split_loop_exec(const void* fa, const void* fb, const gf_krylov_t& K,
     return GF_OK;
 }
 
-template <class Rows, int MINB, bool PAIRS, bool QREC = false, bool XA = false, int PF = 0>
+template <class Rows, int MINB, bool PAIRS, bool QREC = false, bool XA = false, int PF = 0, bool EARLY = false>
 static int launch_split_rows(const gf_krylov_t* k, const Rows& rows, cudaStream_t st) {
     int dev = 0, sms = 0, per_sm = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cgs_a<Rows, MINB, false, QREC, XA, PF>, kSplitThreads, 0);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cgs_a<Rows, MINB, false, QREC, XA, PF, EARLY>, kSplitThreads, 0);
     if (e != cudaSuccess || per_sm < 1) {
         set_error("gf_pcg_solve: split CG set-up failed: %s", cudaGetErrorString(e));
         return GF_ERR_CUDA;
@@ -4635,8 +4669,8 @@ static int launch_split_rows(const gf_krylov_t* k, const Rows& rows, cudaStream_
     if (split_graph_enabled() && cudaStreamIsCapturing(st, &cap) == cudaSuccess &&
         cap == cudaStreamCaptureStatusNone) {
         cudaGraphExec_t exec = nullptr;
-        const int rc = split_loop_exec((const void*)k_cgs_a<Rows, MINB, true, QREC, XA, PF>,
-                                       (const void*)k_cgs_b<MINB, true, PAIRS, XA, PF>, K,
+        const int rc = split_loop_exec((const void*)k_cgs_a<Rows, MINB, true, QREC, XA, PF, EARLY>,
+                                       (const void*)k_cgs_b<MINB, true, PAIRS, XA, PF, EARLY>, K,
                                        &rows, sizeof(Rows), g, &exec);
         if (rc != GF_OK) return rc;
         e = cudaGraphLaunch(exec, st);
@@ -4648,10 +4682,10 @@ static int launch_split_rows(const gf_krylov_t* k, const Rows& rows, cudaStream_
     }
     for (int it = 1; it <= k->max_iter; ++it) {
         // p_old is pa at odd iterations (p_new then goes to pb), pb at even.
-        k_cgs_a<Rows, MINB, false, QREC, XA, PF><<<g, kSplitThreads, 0, st>>>(K, rows, it, it & 1, 0);
-        k_cgs_b<MINB, false, PAIRS, XA, PF><<<g, kSplitThreads, 0, st>>>(K, it, it & 1);
+        k_cgs_a<Rows, MINB, false, QREC, XA, PF, EARLY><<<g, kSplitThreads, 0, st>>>(K, rows, it, it & 1, 0);
+        k_cgs_b<MINB, false, PAIRS, XA, PF, EARLY><<<g, kSplitThreads, 0, st>>>(K, it, it & 1);
     }
-    k_cgs_a<Rows, MINB, false, QREC, XA, PF><<<g, kSplitThreads, 0, st>>>(K, rows, k->max_iter + 1, (k->max_iter + 1) & 1, 0);
+    k_cgs_a<Rows, MINB, false, QREC, XA, PF, EARLY><<<g, kSplitThreads, 0, st>>>(K, rows, k->max_iter + 1, (k->max_iter + 1) & 1, 0);
     e = cudaGetLastError();
     if (e != cudaSuccess) {
         set_error("gf_pcg_solve: split CG launch failed: %s", cudaGetErrorString(e));
@@ -4660,7 +4694,7 @@ static int launch_split_rows(const gf_krylov_t* k, const Rows& rows, cudaStream_
     return GF_OK;
 }
 
-template <int MINB, bool PAIRS, int GRP = 1, bool QREC = false, bool XA = false, int PF = 0>
+template <int MINB, bool PAIRS, int GRP = 1, bool QREC = false, bool XA = false, int PF = 0, bool EARLY = false>
 static int launch_split_m(const gf_krylov_t* k, void* stream) {
     const int64_t row_span = (int64_t)(k->stride_y > 0 ? 6 : (k->width > 6 ? k->width : 6)) * k->n;
     if (row_span >= ((int64_t)1 << 31)) {
@@ -4670,17 +4704,17 @@ static int launch_split_m(const gf_krylov_t* k, void* stream) {
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     if (k->stride_y > 0) {
         if (k->symmetric)
-            return launch_split_rows<BoxRows<double, true, false, int>, MINB, PAIRS, QREC, XA, PF>(
+            return launch_split_rows<BoxRows<double, true, false, int>, MINB, PAIRS, QREC, XA, PF, EARLY>(
                 k, BoxRows<double, true, false, int>{k->val, (int)k->n, (int)k->stride_y, (int)k->stride_z}, st);
-        return launch_split_rows<BoxRows<double, false, false, int>, MINB, PAIRS, QREC, XA, PF>(
+        return launch_split_rows<BoxRows<double, false, false, int>, MINB, PAIRS, QREC, XA, PF, EARLY>(
             k, BoxRows<double, false, false, int>{k->val, (int)k->n, (int)k->stride_y, (int)k->stride_z}, st);
     }
     // One slot at a time (the loop of a plain SpMV): the occupancy, not the
     // loads of one thread, keeps the memory system busy.
     if (k->width == 6)
-        return launch_split_rows<EllRows<double, 6, int, 1>, MINB, PAIRS, QREC, XA, PF>(
+        return launch_split_rows<EllRows<double, 6, int, 1>, MINB, PAIRS, QREC, XA, PF, EARLY>(
             k, EllRows<double, 6, int, 1>{k->val, k->nbr, (int)k->n, k->width, k->row_len}, st);
-    return launch_split_rows<EllRows<double, 0, int, GRP>, MINB, PAIRS, QREC, XA, PF>(
+    return launch_split_rows<EllRows<double, 0, int, GRP>, MINB, PAIRS, QREC, XA, PF, EARLY>(
         k, EllRows<double, 0, int, GRP>{k->val, k->nbr, (int)k->n, k->width, k->row_len}, st);
 }
 
@@ -4692,7 +4726,8 @@ static int launch_split_m(const gf_krylov_t* k, void* stream) {
 // the row kernel (the update kernel reads neither x nor p); 28: 21 with the
 // same; 29: 27 with the first cell's data prefetched into L2 while each
 // kernel sums the previous kernel's partials; 30: the same for the first two
-// cells (four of the update kernel).
+// cells (four of the update kernel); 31: 29 with the prefetches and the
+// scalar reads moved ahead of the loop's control reads and partial sums.
 static int launch_split(const gf_krylov_t* k, void* stream, int which) {
     switch (which) {
         case 1: return launch_split_m<6, false>(k, stream);
@@ -4706,6 +4741,7 @@ static int launch_split(const gf_krylov_t* k, void* stream, int which) {
         case 9: return launch_split_m<8, true, 1, false, true>(k, stream);
         case 10: return launch_split_m<8, true, 1, true, true, 1>(k, stream);
         case 11: return launch_split_m<8, true, 1, true, true, 2>(k, stream);
+        case 12: return launch_split_m<8, true, 1, true, true, 1, true>(k, stream);
         default: return launch_split_m<8, false>(k, stream);
     }
 }

@@ -32,7 +32,7 @@ from gridfoam_b200.meta.config import PrecisionType, PreconditionerType, SolverC
 # Variants 0-7 differ only in launch shape and memory placement (their
 # iterates differ by the order of the dot-product partial sums); 8 and 9
 # form q = A p by recurrence.
-N_VARIANTS = 31
+N_VARIANTS = 32
 VARIANTS = {
     0: "256 threads x 1 cell/pass",
     1: "256 threads x 2 cells/pass",
@@ -65,6 +65,7 @@ VARIANTS = {
     28: "split as 21, x += alpha p in the row kernel (update kernel reads neither x nor p) (FP64, large systems)",
     29: "split as 27, first cell's data prefetched into L2 while the partials are summed (FP64, large systems)",
     30: "split as 27, first two cells' data prefetched into L2 while the partials are summed (FP64, large systems)",
+    31: "split as 29, prefetches and scalar reads ahead of the loop control reads and partial sums (FP64, large systems)",
 }
 
 _LOCK = threading.Lock()
@@ -155,7 +156,7 @@ def time_variant(grid, diag, val, rhs, *, symmetric: bool, mixed: bool, variant:
     return best, its
 
 
-SPLIT_VARIANTS = (19, 20, 21, 22, 23, 24, 25, 26, 27, 28, 29, 30)
+SPLIT_VARIANTS = (19, 20, 21, 22, 23, 24, 25, 26, 27, 28, 29, 30, 31)
 # The persistent single-launch variants: the ones a captured CUDA graph
 # holds as one kernel node (the split CG, 19 and 20, enqueues every
 # permitted iteration when it is captured).

@@ -216,8 +216,8 @@ typedef struct gf_krylov {
     int64_t stride_z;
     int32_t symmetric;    /* 1 (box only): A is symmetric, only + slots read */
     int32_t block_cap;    /* > 0: at most this many persistent blocks (tuning) */
-    int32_t variant;      /* CG launch shape (0..30, see gf_krylov.cu and
-                             solvers/autotune.py); 19..30: the split CG, two
+    int32_t variant;      /* CG launch shape (0..31, see gf_krylov.cu and
+                             solvers/autotune.py); 19..31: the split CG, two
                              plain kernels an iteration, run as a CUDA graph
                              while-loop on the stream (every permitted
                              iteration enqueued inside a stream capture, or

@@ -33,4 +33,4 @@ def test_default_variant_bands(n, mixed, symmetric, box, want):
 
 def test_variant_table_covers_every_launch_shape():
     assert sorted(VARIANTS) == list(range(N_VARIANTS))
-    assert N_VARIANTS == 31
+    assert N_VARIANTS == 32
