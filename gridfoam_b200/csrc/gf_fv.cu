@@ -337,14 +337,15 @@ __device__ __forceinline__ void lsq_slots(const gf_mesh_t& m, int64_t c, int s0,
 }
 
 // k_lsq_grad for octree rows (6 < W <= 12): a row's slots in staged groups
-// (six for one component, three for three: the neighbours' values of six
-// slots spill there), the groups from slot 6 on only where their first slot
+// of three (80 registers for one component, three blocks an SM; three
+// components take 110, two blocks: six slots of them spill), the groups from
+// slot 6 on only where their first slot
 // is used (cells with hanging faces; a row's used slots come first, and a
 // row of the axis-projected grid holds at least six, one or more faces in
 // each direction).  Same sums in the same order as k_lsq_grad (same bits); a
 // row reads only its own slots instead of all W.
 template <int NC>
-__global__ void __launch_bounds__(256, 2) k_lsq_grad12(gf_mesh_t m, const double* __restrict__ psi,
+__global__ void __launch_bounds__(256, NC == 1 ? 3 : 2) k_lsq_grad12(gf_mesh_t m, const double* __restrict__ psi,
                                                        const int8_t* __restrict__ kind,
                                                        const double* __restrict__ psib, double* __restrict__ grad) {
     const int64_t C = m.n_cells;
@@ -358,7 +359,7 @@ __global__ void __launch_bounds__(256, 2) k_lsq_grad12(gf_mesh_t m, const double
         double pc[NC];
 #pragma unroll
         for (int k = 0; k < NC; ++k) pc[k] = psi[k * C + c];
-        constexpr int G = NC == 1 ? 6 : 3;
+        constexpr int G = 3;
         for (int s0 = 0; s0 < W; s0 += G) {
             if (s0 >= 6 && __ldg(m.ell_code + s0 * C + c) < 0) break;
             lsq_slots<NC, G>(m, c, s0, W, psi, kind, psib, cc, pc, atb);
