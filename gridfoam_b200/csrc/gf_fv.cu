@@ -337,13 +337,13 @@ __device__ __forceinline__ void lsq_slots(const gf_mesh_t& m, int64_t c, int s0,
 }
 
 // k_lsq_grad for octree rows (6 < W <= 12): a row's slots in staged groups
-// of three (80 registers for one component, three blocks an SM; three
-// components take 110, two blocks: six slots of them spill), the groups from
-// slot 6 on only where their first slot
-// is used (cells with hanging faces; a row's used slots come first, and a
-// row of the axis-projected grid holds at least six, one or more faces in
-// each direction).  Same sums in the same order as k_lsq_grad (same bits); a
-// row reads only its own slots instead of all W.
+// of three (one component: 80 registers, three blocks an SM; three
+// components: 110 registers, two blocks, and groups of six would spill), the
+// groups from slot 6 on only where their first slot is used (cells with
+// hanging faces; a row's used slots come first, and a row of the
+// axis-projected grid holds at least six, one or more faces in each
+// direction).  Same sums in the same order as k_lsq_grad (same bits); a row
+// reads only its own slots instead of all W.
 template <int NC>
 __global__ void __launch_bounds__(256, NC == 1 ? 3 : 2) k_lsq_grad12(gf_mesh_t m, const double* __restrict__ psi,
                                                        const int8_t* __restrict__ kind,
