@@ -34,3 +34,23 @@ def test_default_variant_bands(n, mixed, symmetric, box, want):
 def test_variant_table_covers_every_launch_shape():
     assert sorted(VARIANTS) == list(range(N_VARIANTS))
     assert N_VARIANTS == 32
+
+
+def test_split_and_persistent_variant_sets():
+    """Every launch shape is either a split CG (graph-loop) form or a
+    single-launch form; the headline octree's pressure CG takes a split one."""
+    from gridfoam_b200.solvers.autotune import PERSISTENT_VARIANTS, SPLIT_VARIANTS
+
+    assert not set(SPLIT_VARIANTS) & set(PERSISTENT_VARIANTS)
+    assert set(SPLIT_VARIANTS) | set(PERSISTENT_VARIANTS) == set(range(N_VARIANTS))
+    assert default_variant(4_079_808, False, True, False) in SPLIT_VARIANTS
+
+
+def test_bench_traffic_table_holds_the_default_variant():
+    """The bench's measured DRAM bytes per cell-iteration (its roofline's
+    ``traffic``) exist for the variant the 4.08M-cell wake runs by default."""
+    import bench
+
+    v = default_variant(4_079_808, False, True, False)
+    assert v in bench.PCG_DRAM_BYTES_PER_CELL_ITER
+    assert 0.9 < bench.PCG_DRAM_BYTES_PER_CELL_ITER[v] / (14 * 8 + 3 * 16) < 1.2
