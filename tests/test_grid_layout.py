@@ -69,3 +69,28 @@ def test_permuted_mesh_is_not_a_box():
     mesh.domain_bnd_faces_owner = inv[mesh.domain_bnd_faces_owner]
     g = AxisProjectedGrid(SimulatorConfig.model_validate(case["simulator"]), mesh, device="cpu")
     assert g.box_strides is None
+
+
+@pytest.mark.parametrize("name", ["cavity_oct", "duct_oct", "ibcyl_oct", "ibplane"])
+def test_ell_rows_are_packed_with_at_least_six_slots(name):
+    """The octree gradient and assembly kernels (6 < W <= 12) stage a row's
+    first six slots unconditionally and read slot 6 on to the row's first
+    empty slot: every row holds one or more faces in each of its six
+    directions, its used slots come first, and its internal-face slots (the
+    matrix couplings, up to ell_len) lead it."""
+    _, g = _grid(name)
+    h = g.host
+    C, F, W = g.num_cells, g.num_internal_faces, g.ell_width
+    code = h.extra["ell_code"].reshape(W, C)
+    used = code >= 0
+    count = used.sum(0)
+    assert count.min() >= 6
+    # packed: slot s used exactly when s < count
+    assert np.array_equal(used, np.arange(W)[:, None] < count[None, :])
+    # couplings first: internal-face slots exactly below ell_len
+    internal = used & (code < 2 * F)
+    ell_len = np.asarray(h.extra["ell_len"])
+    if g.box_strides is None:
+        assert np.array_equal(internal, np.arange(W)[:, None] < ell_len[None, :])
+    if name != "ibplane":
+        assert 6 < W <= 12
