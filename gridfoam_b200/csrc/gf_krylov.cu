@@ -1558,7 +1558,8 @@ static BoxVariant box_kernel(int variant) {
 // Per cell the arithmetic and its order are those of BoxRows, so matrix
 // products are bitwise those of k_pcg1_box.  Requires a symmetric box, even
 // n and 16-byte aligned arrays (the host checks; other systems use
-// k_pcg1_box).  No copy uses cluster multicast.
+// k_pcg1_box).  Every copy reads this GPU's own memory into the issuing
+// block's own shared memory.
 constexpr int kStThreads = 512;
 constexpr int kStMaxSmem = 220 * 1024;
 
